@@ -1,0 +1,91 @@
+"""Seeded synthetic batches with the shapes and value distributions of the
+reference's workloads.
+
+The reference has no public dataset; its benchmarks solve the tridiagonal
+systems of a 3-D heat ADI step and of a channel-flow Poisson/momentum solve.
+These generators stand in for them:
+
+* ``heat_sweep``      constant-coefficient heat sweep, A = C = -r, B = 1+2r with
+                      one r for the whole batch (r = 1 gives rho = 1/3, as in the
+                      reference's 64^3 heat case; apps/heat_cpu/solve_theta.cpp:
+                      142-327 builds the same stencil).
+* ``diag_dominant``   per-system r drawn log-uniform in [r_lo, r_hi]
+                      (A = C = -r, B = 1+2r), D uniform in [-1, 1].
+* ``weak_dominance``  per-system rho uniform in [rho_lo, rho_hi], r = rho/(1-2rho).
+
+All arrays are [n_row, n_sys] row-interleaved (row j of system i at
+j*n_sys + i), as the reference lays them out.  numpy generation (``device=None``)
+is bit-reproducible across machines; torch generation on a CUDA device is
+reproducible for a given seed on that device type and is used for the large
+benchmark batches.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+try:
+    import torch
+except ImportError:  # numpy-only use
+    torch = None
+
+
+def _np_batch(r_sys: np.ndarray, n_row: int, D: np.ndarray, dtype):
+    n_sys = r_sys.shape[0]
+    r = np.broadcast_to(r_sys[None, :], (n_row, n_sys))
+    A = np.ascontiguousarray(-r, dtype=dtype)
+    C = np.ascontiguousarray(-r, dtype=dtype)
+    B = np.ascontiguousarray(1.0 + 2.0 * r, dtype=dtype)
+    return A, B, C, np.ascontiguousarray(D, dtype=dtype)
+
+
+def heat_sweep(n_sys: int, n_row: int, r: float = 1.0, seed: int = 1, dtype=np.float64,
+               device=None):
+    if device is not None:
+        return _torch_batch(np.full(1, r), n_sys, n_row, seed, dtype, device, const_r=r)
+    rng = np.random.default_rng(seed)
+    D = rng.uniform(-1.0, 1.0, size=(n_row, n_sys))
+    return _np_batch(np.full(n_sys, r), n_row, D, dtype)
+
+
+def diag_dominant(n_sys: int, n_row: int, r_lo: float = 0.1, r_hi: float = 10.0, seed: int = 2,
+                  dtype=np.float64, device=None):
+    if device is not None:
+        return _torch_batch(None, n_sys, n_row, seed, dtype, device,
+                            log_r=(np.log10(r_lo), np.log10(r_hi)))
+    rng = np.random.default_rng(seed)
+    r = 10.0 ** rng.uniform(np.log10(r_lo), np.log10(r_hi), size=n_sys)
+    D = rng.uniform(-1.0, 1.0, size=(n_row, n_sys))
+    return _np_batch(r, n_row, D, dtype)
+
+
+def weak_dominance(n_sys: int, n_row: int, rho_lo: float = 0.45, rho_hi: float = 0.499,
+                   seed: int = 3, dtype=np.float64, device=None):
+    if device is not None:
+        return _torch_batch(None, n_sys, n_row, seed, dtype, device, rho=(rho_lo, rho_hi))
+    rng = np.random.default_rng(seed)
+    rho = rng.uniform(rho_lo, rho_hi, size=n_sys)
+    r = rho / (1.0 - 2.0 * rho)
+    D = rng.uniform(-1.0, 1.0, size=(n_row, n_sys))
+    return _np_batch(r, n_row, D, dtype)
+
+
+def _torch_batch(_unused, n_sys, n_row, seed, dtype, device, const_r=None, log_r=None, rho=None):
+    if torch is None:
+        raise RuntimeError("torch is required for device-side generation")
+    tdt = {np.float64: torch.float64, np.float32: torch.float32}.get(dtype, dtype)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    if const_r is not None:
+        r = torch.full((n_sys,), float(const_r), dtype=torch.float64, device=device)
+    elif log_r is not None:
+        u = torch.rand(n_sys, generator=g, dtype=torch.float64, device=device)
+        r = 10.0 ** (log_r[0] + (log_r[1] - log_r[0]) * u)
+    else:
+        u = torch.rand(n_sys, generator=g, dtype=torch.float64, device=device)
+        rh = rho[0] + (rho[1] - rho[0]) * u
+        r = rh / (1.0 - 2.0 * rh)
+    D = torch.rand((n_row, n_sys), generator=g, dtype=torch.float64, device=device) * 2.0 - 1.0
+    A = (-r).expand(n_row, n_sys).contiguous().to(tdt)
+    C = A.clone()
+    B = (1.0 + 2.0 * r).expand(n_row, n_sys).contiguous().to(tdt)
+    return A, B, C, D.to(tdt)
