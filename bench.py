@@ -1,0 +1,339 @@
+"""Benchmark of the batched tridiagonal solve on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one step = one solve of one batch, inputs resident in HBM):
+  262144 systems x 512 rows, FP64, A = C = -r, B = 1 + 2r with per-system r
+  log-uniform in [0.1, 10], D uniform in [-1, 1] (the reference's Filtered-vs-
+  PaScaL comparison shape), solved by PaScaL with P = 8 segments per system.
+  A, B, C, D are 4.3 GB, far above the 126 MB L2, so no flush is needed between
+  steps.  Under torchrun every rank solves its own batch (systems are
+  independent: weak scaling, no collective on the data path).
+
+Printed by rank 0: one JSON line with value = rows/s over all ranks (device
+time, max over ranks), the roofline of the dominant kernel, the CPU baseline
+(the reference's own CPU library on this host's cores), an end-to-end figure
+through the public API with host buffers, the SM clocks seen during the timed
+region and the other solve variants on the same batch.
+
+``--impl reference`` times the reference's CPU implementation (PaScaLTDMA with
+one thread rank per host core, built from its sources into oracle/_ref) on a
+bounded sample of the same workload; under torchrun only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "rows/s & HBM GB/s: FP32+refine vs plain FP64 at ≤1e-12 rel err, 1 B200"
+N_SYS, N_ROW, P = 262144, 512, 8
+BYTES_PER_ROW_F64 = 40  # read A, B, C, D + write x, FP64
+WORKLOAD = ("262144 systems x 512 rows FP64, per-system r log-uniform [0.1,10] "
+            "(A=C=-r, B=1+2r), D uniform [-1,1]; PaScaL, 8 segments per system")
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return 6650.0, "fallback (no MEASURED_PEAKS.json)"
+
+
+def ncu_traffic(kernel_tag):
+    """DRAM bytes per launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", f"{kernel_tag}.txt")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch_full_size:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self._t.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference_rate(sample_sys, reps, warm=1):
+    """rows/s of the reference's CPU PaScaL on this host (thread ranks = cores),
+    or of the oracle's single-thread restatement when the reference build is absent."""
+    import numpy as np
+    from filtered_tdma_b200 import workloads as W
+    from oracle import oracle as O
+    A, B, C, D = W.diag_dominant(sample_sys, N_ROW, seed=2)
+    rows = sample_sys * N_ROW
+    cores = len(os.sched_getaffinity(0))
+    if O.ref_available():
+        nprocs = max(1, min(cores, N_ROW // 3))
+        t = O.ref_time_solve(A, B, C, D, nprocs, "pascal", reps=warm + reps)[warm:]
+        kind, used = "reference", nprocs
+        desc = (f"reference PaScaLTDMA::solve (libs/pascal_tdma/cpu/pascal_tdma.cpp) with "
+                f"{nprocs} thread ranks, {sample_sys} systems x {N_ROW} rows, median of {reps}")
+    else:
+        ts = []
+        for _ in range(warm + reps):
+            t0 = time.perf_counter()
+            O.pascal(A, B, C, D, P)
+            ts.append(time.perf_counter() - t0)
+        t = ts[warm:]
+        kind, used = "port", 1
+        desc = f"oracle PaScaL restatement, 1 thread, {sample_sys} x {N_ROW}, median of {reps}"
+    med = float(np.median(t))
+    return rows / med, kind, used, desc, t
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    steps_rate = []
+    rate0 = None
+    kind = used = desc = None
+    sample = 16384
+    for i in range(args.warmup + args.steps):
+        rate, kind, used, desc, _ = cpu_reference_rate(sample, reps=1, warm=0)
+        if i >= args.warmup:
+            steps_rate.append(rate)
+        rate0 = rate
+    value = statistics.median(steps_rate) if steps_rate else rate0
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "rows/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sample * N_ROW / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_sys": N_SYS, "n_row": N_ROW, "P": P,
+                   "method": "pascal", "sample_systems": sample},
+        "cpu_baseline": {"value": value, "unit": "rows/s", "cores": used, "kind": kind,
+                         "sample": desc},
+        "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def time_variant(torch, solver, A, B, C, D, X, steps, warmup, launches_per_step):
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        solver.solve_out(A, B, C, D, X)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for e0, e1 in ev:
+        e0.record(stream)
+        solver.solve_out(A, B, C, D, X)
+        e1.record(stream)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    per = [e0.elapsed_time(e1) for e0, e1 in ev]
+    return t0.elapsed_time(t1), per, steps * launches_per_step
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    from filtered_tdma_b200 import Solver
+    from filtered_tdma_b200 import workloads as W
+
+    A, B, C, D = W.diag_dominant(N_SYS, N_ROW, seed=2 + rank, device=dev)
+    X = torch.empty_like(D)
+    rows = N_SYS * N_ROW
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---------------------------------------------------------- headline
+    pas = Solver("pascal", N_SYS, N_ROW, P)
+    barrier()
+    with ClockSampler(local) as clk:
+        total_ms, per, launches = time_variant(torch, pas, A, B, C, D, X, args.steps,
+                                               args.warmup, 1)
+    barrier()
+    t = torch.tensor([total_ms], device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ms_step = total_ms / args.steps
+    value = world * rows / (ms_step * 1e-3)
+
+    peak, peak_src = measured_peak()
+    k_ms = sum(per) / len(per)  # one kernel launch per PaScaL step
+    achieved = BYTES_PER_ROW_F64 * rows / (k_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": ncu_traffic("seg_pascal_f64_262144x512"),
+                "kernel": "btdma::seg_f64_kernel<PASCAL>", "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": BYTES_PER_ROW_F64 * rows}
+
+    # ---------------------------------------------------------- variants (rank 0 reports)
+    variants = {}
+    if rank == 0:
+        def gbps(ms, bpr):
+            return bpr * rows / (ms * 1e-3) / 1e9
+
+        for name, method, Pv, lps in (("filtered_v2_P8", "filtered_v2", 8, 3),
+                                      ("thomas_P1", "pascal", 1, 1)):
+            s = Solver(method, N_SYS, N_ROW, Pv)
+            if method != "pascal":
+                s.set_eps_constant(1e-3)
+                s.set_rho(A, B, C, all_systems=True)
+            tot, pv, _ = time_variant(torch, s, A, B, C, D, X, max(3, args.steps // 2), 3, lps)
+            ms = tot / max(3, args.steps // 2)
+            variants[name] = {"rows_per_s": rows / (ms * 1e-3), "ms_per_step": ms,
+                              "hbm_gbs_algorithmic": gbps(ms, BYTES_PER_ROW_F64),
+                              "frac_of_peak": gbps(ms, BYTES_PER_ROW_F64) / peak}
+            if method != "pascal":
+                variants[name]["J"] = s.last_J()
+            s.close()
+
+    # ---------------------------------------------------------- end to end
+    e2e = None
+    if not args.no_e2e:
+        hA, hB, hC, hD = [x.cpu().pin_memory() for x in (A, B, C, D)]
+        hX = torch.empty_like(hD).pin_memory()
+        e2e_steps = max(2, min(args.steps, 5))
+        barrier()
+
+        def e2e_step():
+            for h, d in ((hA, A), (hB, B), (hC, C), (hD, D)):
+                d.copy_(h, non_blocking=True)
+            pas.solve_out(A, B, C, D, X)
+            hX.copy_(X, non_blocking=True)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        e0.record()
+        for _ in range(e2e_steps):
+            e2e_step()
+        e1.record()
+        torch.cuda.synchronize()
+        t = torch.tensor([e0.elapsed_time(e1) / e2e_steps], device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        e2e = {"value": world * rows / (ms * 1e-3), "unit": "rows/s",
+               "h2d_bytes_per_step": 4 * 8 * rows, "d2h_bytes_per_step": 8 * rows,
+               "ms_per_step": ms, "path": "Solver.solve_out (C ABI btdma_solve_out) with "
+                                         "pinned host buffers copied in and out every step"}
+        del hA, hB, hC, hD, hX
+
+    # ---------------------------------------------------------- CPU baseline
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, kind, used, desc, _ = cpu_reference_rate(16384, reps=3)
+        cpu = {"value": rate, "unit": "rows/s", "cores": used, "kind": kind, "sample": desc}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_sys": N_SYS, "n_row": N_ROW, "P": P,
+                       "method": "pascal", "per_rank_batch": True,
+                       "l2": "inputs 4.3 GB per rank > 126 MB L2; no flush needed"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clk.summary(), "variants": variants,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

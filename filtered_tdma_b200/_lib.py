@@ -1,0 +1,70 @@
+"""ctypes binding of the C ABI in include/btdma.h (libbtdma.so, built in-tree).
+
+Importing this module loads the CUDA library; it raises if the library is
+missing, because there is no other implementation of the solve.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libbtdma.so")
+
+# enums of include/btdma.h
+PASCAL, FILTERED_V1, FILTERED_V2 = 0, 1, 2
+FP64, FP32_REFINE = 0, 1
+FLAG_J_HOST = 1
+OK, ERR_ARG, ERR_SEGMENT, ERR_CUDA, ERR_SIZE, ERR_UNSUPPORTED, ERR_DEVICE = 0, -1, -2, -3, -4, -5, -6
+STATUS_TIMEOUT, STATUS_NONFINITE = 1, 2
+
+# every exported symbol of include/btdma.h
+EXPORTS = (
+    "btdma_create", "btdma_destroy", "btdma_solve", "btdma_solve_cyclic", "btdma_solve_out",
+    "btdma_set_eps_constant", "btdma_set_rho", "btdma_set_rho_all", "btdma_last_J",
+    "btdma_status", "btdma_set_method", "btdma_segments", "btdma_last_error",
+)
+
+
+class BtdmaError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"btdma error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """The loaded CUDA library (raises FileNotFoundError when it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(
+                f"{LIB_PATH} is missing: build it with `python -m filtered_tdma_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        L.btdma_create.argtypes = [i, i, i, i, i, i, ctypes.POINTER(vp)]
+        L.btdma_destroy.argtypes = [vp]
+        L.btdma_solve.argtypes = [vp, vp, vp, vp, vp, i, i, vp]
+        L.btdma_solve_cyclic.argtypes = [vp, vp, vp, vp, vp, i, i, vp]
+        L.btdma_solve_out.argtypes = [vp, vp, vp, vp, vp, vp, i, i, i, vp]
+        L.btdma_set_eps_constant.argtypes = [vp, d]
+        L.btdma_set_rho.argtypes = [vp, vp, vp, vp, i, i, vp]
+        L.btdma_set_rho_all.argtypes = [vp, vp, vp, vp, i, i, vp]
+        L.btdma_last_J.argtypes = [vp, ctypes.POINTER(i), i, ctypes.POINTER(i)]
+        L.btdma_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint)]
+        L.btdma_set_method.argtypes = [vp, i]
+        L.btdma_segments.argtypes = [vp, ctypes.POINTER(i)]
+        L.btdma_last_error.restype = ctypes.c_char_p
+        for name in EXPORTS:
+            if name != "btdma_last_error":
+                getattr(L, name).restype = i
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != OK:
+        msg = lib().btdma_last_error()
+        raise BtdmaError(rc, msg.decode() if msg else "")

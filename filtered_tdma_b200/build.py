@@ -1,0 +1,51 @@
+"""Build the CUDA library in-tree: filtered_tdma_b200/libbtdma.so (sm_100a only).
+
+    python -m filtered_tdma_b200.build
+
+nvcc cross-compiles for sm_100a without a GPU.  The CUDA runtime is linked
+statically, so the library does not depend on which libcudart the host process
+(e.g. PyTorch) has loaded; the driver entry point for tensor-map encoding is
+resolved at run time through cudaGetDriverEntryPoint.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+LIB = os.path.join(PKG, "libbtdma.so")
+SOURCES = [os.path.join(PKG, "csrc", "btdma_api.cu")]
+DEPS = SOURCES + [os.path.join(PKG, "csrc", f) for f in os.listdir(os.path.join(PKG, "csrc"))] + [
+    os.path.join(ROOT, "include", "btdma.h")]
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-lineinfo", "-O3", "-std=c++17",
+    "-Xcompiler", "-fPIC,-Wall",
+    "-shared", "-cudart", "static",
+    "-I" + os.path.join(ROOT, "include"),
+]
+
+
+def stale() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    return any(os.path.getmtime(f) > t for f in DEPS if os.path.exists(f))
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if force or stale():
+        cmd = ["nvcc", *NVCC_FLAGS, "-o", LIB, *SOURCES]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    print(LIB)

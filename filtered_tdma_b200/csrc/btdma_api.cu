@@ -1,0 +1,398 @@
+// C ABI of the batched tridiagonal library (declared in include/btdma.h).
+//
+// One translation unit: the kernels are header-only (k_*.cuh) and instantiated
+// here.  The handle owns every device buffer a solve needs (allocated once in
+// btdma_create), so solves allocate nothing and can be captured in CUDA graphs.
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "btdma_common.cuh"
+#include "k_filtered_j.cuh"
+#include "k_segment.cuh"
+#include "k_thomas.cuh"
+
+using namespace btdma;
+
+struct btdma_handle {
+    int method, P, precision, flags;
+    int n_sys_cap, n_row_cap;
+    double eps_constant;
+    double* rho_row = nullptr;               // [n_row_cap] per-row spectral bound
+    int* J = nullptr;                        // [P]
+    unsigned long long* work = nullptr;      // [2P] J accumulators (kept zero between solves)
+    unsigned* status = nullptr;              // device status word
+    double* scratch = nullptr;               // P == 1: c' and e' [2][n_row_cap * n_sys_cap]
+    cudaStream_t last_stream = nullptr;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(BTDMA_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                              \
+    } while (0)
+
+// ------------------------------------------------------------ tensor maps
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// [n_row x n_sys] FP64 array, boxes of SEG_BOXR rows x SEG_S systems.
+bool make_map(CUtensorMap* map, const void* ptr, int n_sys, int n_row) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)n_sys, (cuuint64_t)n_row};
+    cuuint64_t strides[1] = {(cuuint64_t)n_sys * sizeof(double)};
+    cuuint32_t box[2] = {(cuuint32_t)SEG_S, (cuuint32_t)SEG_BOXR};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void*>(ptr), dims, strides,
+                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+bool tma_ok(const void* p, int n_sys) {
+    return ((reinterpret_cast<uintptr_t>(p) & 15) == 0) && (n_sys % 2 == 0);
+}
+
+int auto_segments(int n_row) {
+    // ~64 rows per segment, at least 3, at most the cluster limit.
+    if (n_row < 6) return 1;
+    int P = (n_row + 63) / 64;
+    P = std::max(2, std::min(P, SEG_MAX_P));
+    while (P > 1 && n_row / P < 3) --P;
+    return P;
+}
+
+int seg_mcap(int n_row, int P) {
+    int mmax = (n_row + P - 1) / P;
+    return (mmax + SEG_BOXR - 1) / SEG_BOXR * SEG_BOXR;
+}
+
+int max_smem_optin() {
+    static int v = -1;
+    if (v < 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+            v = 48 * 1024;
+    }
+    return v;
+}
+
+template <int METHOD, bool CYCLIC>
+int launch_seg(const CUtensorMap* maps, const SegArgs& a, int groups, cudaStream_t st) {
+    auto kern = seg_f64_kernel<METHOD, CYCLIC>;
+    static bool attr_done = false;
+    if (!attr_done) {
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                max_smem_optin()));
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        attr_done = true;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(a.P, groups, 1);
+    cfg.blockDim = dim3(SEG_S, 1, 1);
+    cfg.dynamicSmemBytes = seg_smem_bytes(a.mcap, a.P, CYCLIC);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = a.P;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, kern, maps[0], maps[1], maps[2], maps[3], maps[4], a));
+    return BTDMA_OK;
+}
+
+template <bool CYCLIC>
+int launch_seg_method(int method, const CUtensorMap* maps, const SegArgs& a, int groups,
+                      cudaStream_t st) {
+    switch (method) {
+        case BTDMA_PASCAL: return launch_seg<SEG_PASCAL, CYCLIC>(maps, a, groups, st);
+        case BTDMA_FILTERED_V1: return launch_seg<SEG_FILT_V1, CYCLIC>(maps, a, groups, st);
+        default: return launch_seg<SEG_FILT_V2, CYCLIC>(maps, a, groups, st);
+    }
+}
+
+int jmax_launch(btdma_t h, const double* D, int n_sys, int n_row, cudaStream_t st) {
+    int blocks = std::max(1, std::min((n_sys + JRED_BLOCK - 1) / JRED_BLOCK, 1184 / h->P + 1));
+    jmax_kernel<<<dim3(blocks, h->P), JRED_BLOCK, 0, st>>>(
+        D, n_sys, n_row, h->P, (h->flags & BTDMA_FLAG_J_HOST) ? 1 : 0, h->work);
+    CK(cudaGetLastError());
+    return BTDMA_OK;
+}
+
+int jfinal_launch(btdma_t h, int n_row, int version, cudaStream_t st) {
+    jfinal_kernel<<<1, 32, 0, st>>>(h->work, h->J, h->rho_row, n_row, h->P, h->eps_constant,
+                                    version, (h->flags & BTDMA_FLAG_J_HOST) ? 1 : 0);
+    CK(cudaGetLastError());
+    return BTDMA_OK;
+}
+
+int check_sizes(btdma_t h, int n_sys, int n_row) {
+    if (!h) return fail(BTDMA_ERR_ARG, "null handle");
+    if (n_sys <= 0 || n_row <= 0) return fail(BTDMA_ERR_ARG, "n_sys and n_row must be positive");
+    if (n_sys > h->n_sys_cap || n_row > h->n_row_cap)
+        return fail(BTDMA_ERR_SIZE, "batch %d x %d exceeds the handle's %d x %d", n_row, n_sys,
+                    h->n_row_cap, h->n_sys_cap);
+    if (h->P > 1 && n_row / h->P < 3)
+        return fail(BTDMA_ERR_SEGMENT, "n_row %d gives segments shorter than 3 rows at P=%d", n_row,
+                    h->P);
+    return BTDMA_OK;
+}
+
+int solve_impl(btdma_t h, const double* A, const double* B, const double* C, const double* D,
+               double* X, int n_sys, int n_row, bool cyclic, cudaStream_t st) {
+    int rc = check_sizes(h, n_sys, n_row);
+    if (rc) return rc;
+    if (!A || !B || !C || !D || !X) return fail(BTDMA_ERR_ARG, "null array");
+    if (h->precision != BTDMA_FP64)
+        return fail(BTDMA_ERR_UNSUPPORTED, "FP64 arrays passed to an FP32-refine handle");
+    h->last_stream = st;
+
+    if (h->P == 1) {
+        if (cyclic && n_row < 3) return fail(BTDMA_ERR_ARG, "periodic systems need n_row >= 3");
+        const int grid = (n_sys + THOMAS_BLOCK - 1) / THOMAS_BLOCK;
+        double* Cs = h->scratch;
+        double* Es = h->scratch + (size_t)h->n_row_cap * h->n_sys_cap;
+        if (cyclic)
+            thomas_cyclic_f64_kernel<<<grid, THOMAS_BLOCK, 0, st>>>(A, B, C, D, X, Cs, Es, n_sys,
+                                                                    n_row, h->status);
+        else
+            thomas_f64_kernel<<<grid, THOMAS_BLOCK, 0, st>>>(A, B, C, D, X, Cs, n_sys, n_row,
+                                                             h->status);
+        CK(cudaGetLastError());
+        return BTDMA_OK;
+    }
+
+    SegArgs a = {};
+    a.A = A;
+    a.B = B;
+    a.C = C;
+    a.D = D;
+    a.X = X;
+    a.n_sys = n_sys;
+    a.n_row = n_row;
+    a.P = h->P;
+    a.mcap = seg_mcap(n_row, h->P);
+    a.J = h->J;
+    a.bnd = h->work;
+    a.status = h->status;
+    a.mode = SEG_MODE_SOLVE;
+    if (seg_smem_bytes(a.mcap, a.P, cyclic) > (size_t)max_smem_optin())
+        return fail(BTDMA_ERR_UNSUPPORTED,
+                    "segment of %d rows does not fit in shared memory; use more segments",
+                    a.mcap);
+    CUtensorMap maps[5];
+    std::memset(maps, 0, sizeof maps);
+    a.use_tma = tma_ok(A, n_sys) && tma_ok(B, n_sys) && tma_ok(C, n_sys) && tma_ok(D, n_sys) &&
+                tma_ok(X, n_sys);
+    if (a.use_tma)
+        a.use_tma = make_map(&maps[0], A, n_sys, n_row) && make_map(&maps[1], B, n_sys, n_row) &&
+                    make_map(&maps[2], C, n_sys, n_row) && make_map(&maps[3], D, n_sys, n_row) &&
+                    make_map(&maps[4], X, n_sys, n_row);
+    const int groups = (n_sys + SEG_S - 1) / SEG_S;
+    if (groups > 65535) return fail(BTDMA_ERR_SIZE, "n_sys above %d", 65535 * SEG_S);
+
+    if (h->method == BTDMA_FILTERED_V2) {
+        if ((rc = jmax_launch(h, D, n_sys, n_row, st))) return rc;
+        if ((rc = jfinal_launch(h, n_row, 2, st))) return rc;
+    } else if (h->method == BTDMA_FILTERED_V1) {
+        SegArgs ai = a;
+        ai.mode = SEG_MODE_INTERFACE;
+        rc = cyclic ? launch_seg_method<true>(h->method, maps, ai, groups, st)
+                    : launch_seg_method<false>(h->method, maps, ai, groups, st);
+        if (rc) return rc;
+        if ((rc = jfinal_launch(h, n_row, 1, st))) return rc;
+    }
+    return cyclic ? launch_seg_method<true>(h->method, maps, a, groups, st)
+                  : launch_seg_method<false>(h->method, maps, a, groups, st);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* btdma_last_error(void) { return g_err.c_str(); }
+
+int btdma_create(int method, int n_sys, int n_row, int P, int precision, int flags,
+                 btdma_t* out) {
+    if (!out) return fail(BTDMA_ERR_ARG, "null output handle");
+    *out = nullptr;
+    if (method < BTDMA_PASCAL || method > BTDMA_FILTERED_V2)
+        return fail(BTDMA_ERR_ARG, "unknown method %d", method);
+    if (n_sys <= 0 || n_row <= 0) return fail(BTDMA_ERR_ARG, "n_sys and n_row must be positive");
+    if (precision != BTDMA_FP64)
+        return fail(BTDMA_ERR_UNSUPPORTED, "precision %d not built yet", precision);
+    if (P < 0) return fail(BTDMA_ERR_ARG, "P must be >= 0");
+    if (P == 0) P = auto_segments(n_row);
+    if (P > SEG_MAX_P)
+        return fail(BTDMA_ERR_UNSUPPORTED, "P=%d above the cluster limit %d", P, SEG_MAX_P);
+    if (P > 1 && n_row / P < 3)
+        return fail(BTDMA_ERR_SEGMENT, "n_row %d gives segments shorter than 3 rows at P=%d",
+                    n_row, P);
+    if (P > 1 && seg_smem_bytes(seg_mcap(n_row, P), P, true) > (size_t)max_smem_optin())
+        return fail(BTDMA_ERR_UNSUPPORTED, "segments of %d rows exceed shared memory; raise P",
+                    (n_row + P - 1) / P);
+
+    btdma_handle* h = new btdma_handle();
+    h->method = method;
+    h->P = P;
+    h->precision = precision;
+    h->flags = flags;
+    h->n_sys_cap = n_sys;
+    h->n_row_cap = n_row;
+    h->eps_constant = 1.0e-12;
+    auto cleanup = [&](int code) {
+        btdma_destroy(h);
+        return code;
+    };
+#define CKC(call)                                                                                \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            return cleanup(fail(BTDMA_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)));       \
+    } while (0)
+    CKC(cudaMalloc(&h->rho_row, sizeof(double) * n_row));
+    CKC(cudaMemset(h->rho_row, 0, sizeof(double) * n_row));
+    CKC(cudaMalloc(&h->J, sizeof(int) * P));
+    CKC(cudaMemset(h->J, 0, sizeof(int) * P));
+    CKC(cudaMalloc(&h->work, sizeof(unsigned long long) * 2 * P));
+    CKC(cudaMemset(h->work, 0, sizeof(unsigned long long) * 2 * P));
+    CKC(cudaMalloc(&h->status, sizeof(unsigned)));
+    CKC(cudaMemset(h->status, 0, sizeof(unsigned)));
+    if (P == 1) CKC(cudaMalloc(&h->scratch, sizeof(double) * 2 * (size_t)n_row * n_sys));
+#undef CKC
+    *out = h;
+    return BTDMA_OK;
+}
+
+int btdma_destroy(btdma_t h) {
+    if (!h) return BTDMA_OK;
+    cudaFree(h->rho_row);
+    cudaFree(h->J);
+    cudaFree(h->work);
+    cudaFree(h->status);
+    cudaFree(h->scratch);
+    delete h;
+    return BTDMA_OK;
+}
+
+int btdma_solve(btdma_t h, const double* A, const double* B, const double* C, double* D,
+                int n_sys, int n_row, cudaStream_t stream) {
+    return solve_impl(h, A, B, C, D, D, n_sys, n_row, false, stream);
+}
+
+int btdma_solve_cyclic(btdma_t h, const double* A, const double* B, const double* C, double* D,
+                       int n_sys, int n_row, cudaStream_t stream) {
+    return solve_impl(h, A, B, C, D, D, n_sys, n_row, true, stream);
+}
+
+int btdma_solve_out(btdma_t h, const double* A, const double* B, const double* C,
+                    const double* D, double* X, int n_sys, int n_row, int cyclic,
+                    cudaStream_t stream) {
+    return solve_impl(h, A, B, C, D, X, n_sys, n_row, cyclic != 0, stream);
+}
+
+int btdma_set_eps_constant(btdma_t h, double eps_constant) {
+    if (!h) return fail(BTDMA_ERR_ARG, "null handle");
+    h->eps_constant = eps_constant;
+    return BTDMA_OK;
+}
+
+int btdma_set_rho(btdma_t h, const double* A, const double* B, const double* C, int n_sys,
+                  int n_row, cudaStream_t stream) {
+    int rc = check_sizes(h, n_sys, n_row);
+    if (rc) return rc;
+    if (h->method == BTDMA_PASCAL) return BTDMA_OK;
+    rho_sys0_kernel<<<(n_row + 255) / 256, 256, 0, stream>>>(A, B, C, n_sys, n_row, h->rho_row);
+    CK(cudaGetLastError());
+    return BTDMA_OK;
+}
+
+int btdma_set_rho_all(btdma_t h, const double* A, const double* B, const double* C, int n_sys,
+                      int n_row, cudaStream_t stream) {
+    int rc = check_sizes(h, n_sys, n_row);
+    if (rc) return rc;
+    if (h->method == BTDMA_PASCAL) return BTDMA_OK;
+    CK(cudaMemsetAsync(h->rho_row, 0, sizeof(double) * n_row, stream));
+    int bx = std::max(1, std::min((n_sys + 255) / 256, 32));
+    rho_all_kernel<<<dim3(bx, n_row), 256, 0, stream>>>(
+        A, B, C, n_sys, reinterpret_cast<unsigned long long*>(h->rho_row));
+    CK(cudaGetLastError());
+    return BTDMA_OK;
+}
+
+int btdma_last_J(btdma_t h, int* J, int cap, int* n_out) {
+    if (!h) return fail(BTDMA_ERR_ARG, "null handle");
+    if (n_out) *n_out = h->P;
+    if (!J || cap <= 0) return BTDMA_OK;
+    const int n = std::min(cap, h->P);
+    if (h->P == 1 || h->method == BTDMA_PASCAL) {
+        for (int k = 0; k < n; ++k) J[k] = -1;
+        return BTDMA_OK;
+    }
+    CK(cudaMemcpyAsync(J, h->J, sizeof(int) * n, cudaMemcpyDeviceToHost, h->last_stream));
+    CK(cudaStreamSynchronize(h->last_stream));
+    return BTDMA_OK;
+}
+
+int btdma_status(btdma_t h, unsigned* status) {
+    if (!h || !status) return fail(BTDMA_ERR_ARG, "null argument");
+    CK(cudaMemcpyAsync(status, h->status, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                       h->last_stream));
+    CK(cudaStreamSynchronize(h->last_stream));
+    CK(cudaMemsetAsync(h->status, 0, sizeof(unsigned), h->last_stream));
+    CK(cudaStreamSynchronize(h->last_stream));
+    return BTDMA_OK;
+}
+
+int btdma_set_method(btdma_t h, int method) {
+    if (!h) return fail(BTDMA_ERR_ARG, "null handle");
+    if (method < BTDMA_PASCAL || method > BTDMA_FILTERED_V2)
+        return fail(BTDMA_ERR_ARG, "unknown method %d", method);
+    h->method = method;
+    return BTDMA_OK;
+}
+
+int btdma_segments(btdma_t h, int* P) {
+    if (!h || !P) return fail(BTDMA_ERR_ARG, "null argument");
+    *P = h->P;
+    return BTDMA_OK;
+}
+
+}  // extern "C"

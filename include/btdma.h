@@ -1,0 +1,154 @@
+/*
+ * btdma — batched tridiagonal solves on one NVIDIA B200 (sm_100a).
+ *
+ * C ABI of the library.  Every array is a caller-owned DEVICE pointer in the
+ * reference's row-interleaved layout [n_row x n_sys]: row j of system i at
+ * j*n_sys + i (reference: libs/pascal_tdma/include/pascal_tdma.hpp:13,
+ * libs/filtered_tdma/include/filtered_tdma_cuda.hpp:152-153).  A is the sub-,
+ * B the main- and C the super-diagonal, D the right-hand side.
+ *
+ * Methods (the reference's backend strings, apps/heat_gpu/tdma_backend_gpu.cu:6-13):
+ *   BTDMA_PASCAL       "pascal" | "pascal_tdma"   exact; P segments per system
+ *                      with an exact reduced 2P-row interface solve
+ *                      (PaScaLTDMACUDA, libs/pascal_tdma/gpu/pascal_tdma_cuda.cu)
+ *   BTDMA_FILTERED_V1  "filtered" (any other string)  P segments, adjacent 2x2
+ *                      interface solves, J-truncated correction with J taken after
+ *                      the interface solve (FilteredTDMACUDA::solve_filtered_v1)
+ *   BTDMA_FILTERED_V2  "filtered_v2"  J taken before the sweeps
+ *                      (FilteredTDMACUDA::solve_filtered_v2)
+ * With P = 1 every method is the serial Thomas algorithm, bit-identical to the
+ * reference's tdma_many / tdma_cyclic_many (libs/pascal_tdma/cpu/tdma_local.cpp),
+ * exactly as the reference falls back at nprocs == 1.  In the reference P is the
+ * number of MPI ranks a system is split over; here the P segments of a system
+ * live in the P CTAs of one thread-block cluster on one GPU.
+ *
+ * Semantics that differ from the reference's (all documented in DESIGN.md):
+ *   - D <- x.  A, B and C are left unchanged (the reference leaves elimination
+ *     scratch in A and C).
+ *   - Every segment needs >= 3 rows (the reference's PaScaL is wrong at 2,
+ *     and indexes out of bounds at 1); btdma_create rejects such a P.
+ *   - Calls are stream-ordered and never synchronise the host, except
+ *     btdma_last_J and btdma_status, which read back device values.
+ *
+ * Return value of every function: 0 on success, a negative BTDMA_ERR_* code
+ * otherwise.  Kernels never trap: runtime faults of the data (NaN/Inf solution,
+ * a wait that timed out) are OR-ed into a device status word read by
+ * btdma_status().
+ */
+#ifndef BTDMA_H
+#define BTDMA_H
+
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct btdma_handle* btdma_t;
+
+enum btdma_method {
+    BTDMA_PASCAL = 0,
+    BTDMA_FILTERED_V1 = 1,
+    BTDMA_FILTERED_V2 = 2
+};
+
+enum btdma_precision {
+    BTDMA_FP64 = 0,        /* FP64 storage and arithmetic */
+    BTDMA_FP32_REFINE = 1  /* FP32 storage, FP32 sweeps + FP64 iterative refinement */
+};
+
+enum btdma_flags {
+    /* Filtered J estimator of the reference's CPU library instead of its CUDA
+     * library: v2 takes max|D| over every row of a segment
+     * (libs/filtered_tdma/cpu/filtered_tdma.cpp:75-80) instead of its first and
+     * last rows (libs/filtered_tdma/gpu/filtered_tdma_kernels.cuh:235-238); v1
+     * uses the K bound (filtered_tdma.cpp:110-114) instead of the right-hand-side
+     * bound on the post-interface rows (filtered_tdma_cuda.cu:127-131). */
+    BTDMA_FLAG_J_HOST = 1 << 0
+};
+
+enum btdma_error {
+    BTDMA_OK = 0,
+    BTDMA_ERR_ARG = -1,        /* invalid argument (null handle/pointer, bad size) */
+    BTDMA_ERR_SEGMENT = -2,    /* a segment would have fewer than 3 rows */
+    BTDMA_ERR_CUDA = -3,       /* a CUDA runtime call failed */
+    BTDMA_ERR_SIZE = -4,       /* n_sys / n_row above the handle's capacity */
+    BTDMA_ERR_UNSUPPORTED = -5,/* combination not provided (message via btdma_last_error) */
+    BTDMA_ERR_DEVICE = -6      /* device status word non-zero (see btdma_status) */
+};
+
+/* Create a solver for batches of up to n_sys systems of n_row rows, split into
+ * P segments (P = 0 picks P from the shape).  Replaces the constructors
+ * PaScaLTDMACUDA(n_sys, myrank, nprocs, comm, block_x, block_y)
+ * (libs/pascal_tdma/include/pascal_tdma_cuda.hpp:20-21) and
+ * FilteredTDMACUDA(n_sys, n_row, myrank, nprocs, comm, left, right, eps_constant)
+ * (libs/filtered_tdma/include/filtered_tdma_cuda.hpp:163-166), with nprocs -> P.
+ * Allocates the handle's device scratch; no allocation happens in a solve. */
+int btdma_create(int method, int n_sys, int n_row, int P, int precision, int flags,
+                 btdma_t* out);
+
+/* Release the handle and its device memory (the reference destructors,
+ * pascal_tdma_cuda.cu:153-173, filtered_tdma_cuda.cu:34-54). */
+int btdma_destroy(btdma_t h);
+
+/* Solve in place: D <- x.  Replaces PaScaLTDMACUDA::solve(d_A,d_B,d_C,d_D,n_sys,n_row)
+ * (pascal_tdma_cuda.hpp:28-29) and FilteredTDMACUDA::solve_filtered_v1/v2(d_A,d_B,d_C,d_D)
+ * (filtered_tdma_cuda.hpp:173-174).  n_sys and n_row may be smaller than at
+ * create time (n_row must still give every segment >= 3 rows). */
+int btdma_solve(btdma_t h, const double* A, const double* B, const double* C, double* D,
+                int n_sys, int n_row, cudaStream_t stream);
+
+/* Periodic systems (row 0 couples to row n_row-1 through A[0] and C[n_row-1]).
+ * Replaces PaScaLTDMACUDA::solve_cyclic (pascal_tdma_cuda.hpp:32-33) and
+ * FilteredTDMACUDA::solve_cycl_filtered_v1/v2 (filtered_tdma_cuda.hpp:179-180). */
+int btdma_solve_cyclic(btdma_t h, const double* A, const double* B, const double* C, double* D,
+                       int n_sys, int n_row, cudaStream_t stream);
+
+/* Out-of-place solve: X <- x, D unchanged (X may equal D).  No reference
+ * counterpart; same kernels as btdma_solve. */
+int btdma_solve_out(btdma_t h, const double* A, const double* B, const double* C,
+                    const double* D, double* X, int n_sys, int n_row, int cyclic,
+                    cudaStream_t stream);
+
+/* Filtered: eps = eps_constant / (m * P)^2 per segment of m rows.  Replaces
+ * FilteredTDMACUDA::set_eps_constant (filtered_tdma_cuda.hpp:203-206); no-op for
+ * PASCAL, as in TdmaBackendGPU::set_eps_constant (tdma_backend_gpu.cu:64-66). */
+int btdma_set_eps_constant(btdma_t h, double eps_constant);
+
+/* Filtered: per-row spectral bounds |A_k/B_k|, |C_k/B_k| from system 0's column,
+ * stream-ordered on the device.  Replaces FilteredTDMACUDA::set_rho_device
+ * (filtered_tdma_cuda.hpp:212; kernel k_set_rho, filtered_tdma_kernels.cuh:46-67).
+ * No-op for PASCAL. */
+int btdma_set_rho(btdma_t h, const double* A, const double* B, const double* C, int n_sys,
+                  int n_row, cudaStream_t stream);
+
+/* Filtered: per-row bounds as the maximum over ALL systems (a conservative
+ * estimate for batches whose systems differ; no reference counterpart). */
+int btdma_set_rho_all(btdma_t h, const double* A, const double* B, const double* C, int n_sys,
+                      int n_row, cudaStream_t stream);
+
+/* Filtered: J of every segment from the most recent solve (blocking device->host
+ * read, like FilteredTDMACUDA::last_J, filtered_tdma_cuda.cu:83-87).  Writes
+ * min(P, cap) values; returns the number of segments through *n_out. */
+int btdma_last_J(btdma_t h, int* J, int cap, int* n_out);
+
+/* Device status word OR-ed by the kernels since the last call (blocking read;
+ * resets it to 0).  Bit 0: a wait timed out; bit 1: a non-finite solution. */
+int btdma_status(btdma_t h, unsigned* status);
+
+/* Switch the method of an existing handle (rho, eps and J state are kept).  The
+ * reference's FilteredTDMACUDA object offers v1 and v2 side by side
+ * (filtered_tdma_cuda.hpp:173-180); this lets one handle do the same. */
+int btdma_set_method(btdma_t h, int method);
+
+/* Segments per system used by the handle (after the P = 0 choice). */
+int btdma_segments(btdma_t h, int* P);
+
+/* Message of the most recent failing call on this thread. */
+const char* btdma_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BTDMA_H */

@@ -1,0 +1,194 @@
+"""GPU parity: the CUDA kernels, called through the C ABI, against the oracle.
+
+Bars:
+  * P = 1 (serial Thomas, periodic Thomas): bit-identical to the oracle, which
+    is bit-identical to the reference's tdma_many / tdma_cyclic_many.
+  * PaScaL, P > 1: bit-identical to the oracle's PaScaL (itself bit-identical to
+    the reference's PaScaLTDMA with nprocs = P) and within 1e-12 (relative to
+    max|x|) of the serial Thomas.
+  * Filtered v1/v2: bit-identical to the oracle's Filtered with the same rho
+    and the device J estimator, the same J per segment, and within eps of PaScaL.
+  * A, B, C are not modified; in-place and out-of-place solves agree.
+"""
+import numpy as np
+import pytest
+
+from filtered_tdma_b200 import FilteredTDMACUDA, PaScaLTDMACUDA, Solver, TdmaBackendGPU
+from filtered_tdma_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(cuda, *arrs):
+    import torch
+    return [torch.from_numpy(np.ascontiguousarray(a)).to(cuda) for a in arrs]
+
+
+def host(t):
+    return t.cpu().numpy()
+
+
+def run(cuda, method, A, B, C, D, P, cyclic=False, out=False, rho=None, eps_c=1e-3, flags=0):
+    n_row, n_sys = D.shape
+    s = Solver(method, n_sys, n_row, P, flags=flags)
+    s.set_eps_constant(eps_c)
+    dA, dB, dC, dD = dev(cuda, A, B, C, D)
+    if rho is not None:
+        import torch
+        # the per-row bound goes in through set_rho on a system-0 column
+        # holding exactly rho (A = -rho, B = 1, C = -rho).
+        col = torch.zeros((n_row, 1), dtype=torch.float64, device=cuda)
+        r = torch.from_numpy(np.ascontiguousarray(rho)).to(cuda)[:, None]
+        s.set_rho(-r.contiguous(), (col + 1).contiguous(), -r.contiguous(), 1, n_row)
+    if out:
+        X = dD.clone().zero_()
+        s.solve_out(dA, dB, dC, dD, X, cyclic=cyclic)
+        import torch
+        torch.cuda.synchronize()
+        assert np.array_equal(host(dD), D), "out-of-place solve modified D"
+        res = host(X)
+    else:
+        s.solve(dA, dB, dC, dD, cyclic=cyclic)
+        res = host(dD)
+    assert np.array_equal(host(dA), A) and np.array_equal(host(dB), B) and \
+        np.array_equal(host(dC), C), "A, B or C modified"
+    assert s.status() == 0
+    return res, s
+
+
+SHAPES_P1 = [(1, 1), (3, 2), (5, 3), (31, 17), (64, 64), (4096, 64), (1000, 129), (257, 512)]
+
+
+@pytest.mark.parametrize("n_sys,n_row", SHAPES_P1)
+def test_thomas_bit_exact(cuda, orc, n_sys, n_row):
+    A, B, C, D = W.diag_dominant(n_sys, n_row, seed=n_sys + n_row)
+    x, _ = run(cuda, "pascal", A, B, C, D, 1)
+    assert np.array_equal(x, orc.thomas(A, B, C, D))
+    x2, _ = run(cuda, "pascal", A, B, C, D, 1, out=True)
+    assert np.array_equal(x2, x)
+
+
+@pytest.mark.parametrize("n_sys,n_row", [(5, 3), (31, 17), (4096, 64), (257, 300)])
+def test_thomas_cyclic_bit_exact(cuda, orc, n_sys, n_row):
+    A, B, C, D = W.diag_dominant(n_sys, n_row, seed=7 * n_sys + n_row)
+    x, _ = run(cuda, "pascal", A, B, C, D, 1, cyclic=True)
+    assert np.array_equal(x, orc.thomas_cyclic(A, B, C, D))
+
+
+@pytest.mark.parametrize("n_sys,n_row,P", [
+    (32, 64, 2), (64, 64, 4), (4096, 64, 4), (100, 96, 8), (33, 100, 7), (7, 48, 16),
+    (2048, 512, 8), (96, 515, 16), (130, 37, 3), (64, 1000, 16)])
+def test_pascal_bit_exact(cuda, orc, n_sys, n_row, P):
+    A, B, C, D = W.diag_dominant(n_sys, n_row, seed=P * 1000 + n_row)
+    x, _ = run(cuda, "pascal", A, B, C, D, P)
+    xo = orc.pascal(A, B, C, D, P)
+    assert np.array_equal(x, xo)
+    xt = orc.thomas(A, B, C, D)
+    assert np.max(np.abs(x - xt)) <= 1e-12 * np.max(np.abs(xt))
+    x2, _ = run(cuda, "pascal", A, B, C, D, P, out=True)
+    assert np.array_equal(x2, x)
+
+
+@pytest.mark.parametrize("n_sys,n_row,P", [(32, 64, 2), (100, 96, 8), (33, 100, 7),
+                                           (64, 512, 16)])
+def test_pascal_cyclic_bit_exact(cuda, orc, n_sys, n_row, P):
+    A, B, C, D = W.diag_dominant(n_sys, n_row, seed=P + n_row)
+    x, _ = run(cuda, "pascal", A, B, C, D, P, cyclic=True)
+    assert np.array_equal(x, orc.pascal(A, B, C, D, P, cyclic=True))
+    xt = orc.thomas_cyclic(A, B, C, D)
+    assert np.max(np.abs(x - xt)) <= 1e-12 * np.max(np.abs(xt))
+
+
+@pytest.mark.parametrize("version", [1, 2])
+@pytest.mark.parametrize("cyclic", [False, True])
+@pytest.mark.parametrize("n_sys,n_row,P", [(64, 128, 2), (100, 96, 8), (33, 200, 5),
+                                           (2048, 512, 8)])
+def test_filtered_bit_exact(cuda, orc, version, cyclic, n_sys, n_row, P):
+    A, B, C, D = W.diag_dominant(n_sys, n_row, 0.1, 1.0, seed=version + n_row)
+    rho = orc.rho_rows_all(A, B, C)
+    x, s = run(cuda, f"filtered_v{version}", A, B, C, D, P, cyclic=cyclic, rho=rho)
+    xo, Jo = orc.filtered(A, B, C, D, P, version, cyclic, 1e-3, rho, orc.J_DEVICE)
+    assert s.last_J() == list(Jo)
+    assert np.array_equal(x, xo)
+    # The eps bound holds when the truncation is active in every segment
+    # (J < m-2); the dropped interface couplings then decay below it too.
+    segs = orc.split(n_row, P)
+    if max(Jo) < min(c for _, c in segs) - 2:
+        xp = orc.pascal(A, B, C, D, P, cyclic)
+        eps = 1e-3 / float(min(c for _, c in segs) * P) ** 2
+        assert np.max(np.abs(x - xp)) <= eps
+
+
+@pytest.mark.parametrize("version", [1, 2])
+def test_filtered_host_j_semantics(cuda, orc, version):
+    A, B, C, D = W.diag_dominant(80, 160, 0.1, 1.0, seed=42)
+    rho = orc.rho_rows_all(A, B, C)
+    from filtered_tdma_b200 import _lib as L
+    x, s = run(cuda, f"filtered_v{version}", A, B, C, D, 4, rho=rho, flags=L.FLAG_J_HOST)
+    xo, Jo = orc.filtered(A, B, C, D, 4, version, False, 1e-3, rho, orc.J_HOST)
+    assert np.array_equal(x, xo)
+
+
+def test_filtered_set_rho_system0(cuda, orc):
+    # set_rho reads system 0's column, like the reference's k_set_rho.
+    A, B, C, D = W.diag_dominant(64, 96, seed=3)
+    n_row, n_sys = D.shape
+    s = Solver("filtered_v2", n_sys, n_row, 4)
+    s.set_eps_constant(1e-3)
+    dA, dB, dC, dD = dev(cuda, A, B, C, D)
+    s.set_rho(dA, dB, dC)
+    s.solve(dA, dB, dC, dD)
+    xo, Jo = orc.filtered(A, B, C, D, 4, 2, False, 1e-3, orc.rho_rows(A, B, C, 0), orc.J_DEVICE)
+    assert np.array_equal(host(dD), xo)
+    assert s.last_J() == list(Jo)
+
+
+def test_no_tma_path_odd_systems(cuda, orc):
+    # odd n_sys: the row stride is not a multiple of 16 bytes, plain loads are used
+    A, B, C, D = W.diag_dominant(101, 128, seed=9)
+    x, _ = run(cuda, "pascal", A, B, C, D, 4)
+    assert np.array_equal(x, orc.pascal(A, B, C, D, 4))
+
+
+def test_dropin_classes(cuda, orc):
+    A, B, C, D = W.heat_sweep(4096, 64, r=1.0, seed=1)
+    n_row, n_sys = D.shape
+    xt = orc.thomas(A, B, C, D)
+    # PaScaL with nprocs = 4 segments (config: heat 64^3, P = 4)
+    dA, dB, dC, dD = dev(cuda, A, B, C, D)
+    p = PaScaLTDMACUDA(n_sys, 0, 4, None)
+    p.solve(dA, dB, dC, dD, n_sys, n_row)
+    assert np.array_equal(host(dD), orc.pascal(A, B, C, D, 4))
+    # TdmaBackendGPU strings
+    for kind in ("pascal", "filtered", "filtered_v2"):
+        dA, dB, dC, dD = dev(cuda, A, B, C, D)
+        b = TdmaBackendGPU(kind, n_sys, n_row, 0, 1, None, -2, -2, 1e-3)
+        b.set_rho_device(dA, dB, dC)
+        b.set_eps_constant(1e-3)
+        b.solve(dA, dB, dC, dD)
+        assert np.array_equal(host(dD), xt)  # nprocs = 1: serial Thomas
+        assert b.last_comm_ms() == 0.0 and b.last_gpu_ms() > 0.0
+    f = FilteredTDMACUDA(n_sys, n_row, 0, 4, None, -2, -2, 1e-3)
+    dA, dB, dC, dD = dev(cuda, A, B, C, D)
+    f.set_rho_device(dA, dB, dC)
+    f.solve_filtered_v2(dA, dB, dC, dD)
+    xo, Jo = orc.filtered(A, B, C, D, 4, 2, False, 1e-3, orc.rho_rows(A, B, C, 0), orc.J_DEVICE)
+    assert np.array_equal(host(dD), xo) and f.last_J() == Jo[0]
+
+
+def test_full_size_properties(cuda):
+    """262144 x 512 (the benchmark batch): PaScaL P=8 residual and agreement
+    with the serial Thomas, both on the device."""
+    import torch
+    A, B, C, D = W.diag_dominant(262144, 512, seed=2, device=cuda)
+    n_row, n_sys = D.shape
+    X8 = torch.empty_like(D)
+    X1 = torch.empty_like(D)
+    Solver("pascal", n_sys, n_row, 8).solve_out(A, B, C, D, X8)
+    Solver("pascal", n_sys, n_row, 1).solve_out(A, B, C, D, X1)
+    rel = (X8 - X1).abs().max() / X1.abs().max()
+    assert rel.item() <= 1e-12
+    r = B * X8 - D
+    r[1:] += A[1:] * X8[:-1]
+    r[:-1] += C[:-1] * X8[1:]
+    assert (r.abs().max() / D.abs().max()).item() <= 1e-12
