@@ -74,11 +74,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait: gives up after `limit` polls (each poll may itself suspend the
-// thread for a hardware-chosen time), raising ST_TIMEOUT.  Returns success.
+// thread for a hardware-chosen time), raising ST_TIMEOUT.  Every 4096 polls it
+// also checks the status word and gives up at once if another CTA already timed
+// out, so a systematic failure costs one timeout, not one per CTA.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
-                                                  unsigned* status, uint32_t limit = 1u << 22) {
-    for (uint32_t it = 0; it < limit; ++it)
+                                                  unsigned* status, uint32_t limit = 1u << 20) {
+    for (uint32_t it = 0; it < limit; ++it) {
         if (mbar_try_wait(bar, parity)) return true;
+        if (status && (it & 4095u) == 4095u &&
+            (*reinterpret_cast<volatile unsigned*>(status) & ST_TIMEOUT))
+            return false;
+    }
     raise_status(status, ST_TIMEOUT);
     return false;
 }

@@ -153,8 +153,8 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         }
     }
     auto chunk_ready = [&](int j) {
-        if (args.use_tma && (j % SEG_BOXR) == 0)
-            ok &= mbar_wait_bounded(&bars[j / SEG_BOXR], 0, args.status);
+        if (args.use_tma && ok && (j % SEG_BOXR) == 0)
+            ok = mbar_wait_bounded(&bars[j / SEG_BOXR], 0, args.status);
     };
 
     // J of this segment (Filtered); v1's interface pass runs the full sweeps.
@@ -380,7 +380,7 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     if (!ok && args.use_tma) {
         // A chunk wait gave up: give the copies one more bounded chance to land
         // before this CTA's shared memory is released.
-        for (int c = 0; c < nch; ++c) mbar_wait_bounded(&bars[c], 0, nullptr);
+        for (int c = 0; c < nch; ++c) mbar_wait_bounded(&bars[c], 0, nullptr, 1u << 16);
     }
     __syncwarp();
     cluster_wait();  // the neighbours are done reading this CTA's shared memory
