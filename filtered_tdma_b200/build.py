@@ -25,6 +25,7 @@ NVCC_FLAGS = [
     "-lineinfo", "-O3", "-std=c++17",
     "-Xcompiler", "-fPIC,-Wall",
     "-shared", "-cudart", "static",
+    "-Xlinker", "--exclude-libs=ALL",  # keep the static runtime's symbols private
     "-I" + os.path.join(ROOT, "include"),
 ]
 
