@@ -253,8 +253,8 @@ def main():
     k_ms = sum(per) / len(per)  # one kernel launch per PaScaL step
     achieved = BYTES_PER_ROW_F64 * rows / (k_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": ncu_traffic("seg_pascal_f64_262144x512"),
-                "kernel": "btdma::seg_f64_kernel<PASCAL>", "peak_source": peak_src,
+                "frac": achieved / peak, "traffic": ncu_traffic("tile_pascal_f64_262144x512"),
+                "kernel": "btdma::tile_f64_kernel<16>", "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": BYTES_PER_ROW_F64 * rows}
 
     # ---------------------------------------------------------- variants (rank 0 reports)
@@ -263,9 +263,12 @@ def main():
         def gbps(ms, bpr):
             return bpr * rows / (ms * 1e-3) / 1e9
 
-        for name, method, Pv, lps in (("filtered_v2_P8", "filtered_v2", 8, 3),
-                                      ("thomas_P1", "pascal", 1, 1)):
-            s = Solver(method, N_SYS, N_ROW, Pv)
+        from filtered_tdma_b200 import _lib as L
+        for name, method, Pv, lps, fl in (
+                ("filtered_v2_P8", "filtered_v2", 8, 3, 0),
+                ("pascal_reference_order_P8", "pascal", 8, 1, L.FLAG_REFERENCE_ORDER),
+                ("thomas_P1", "pascal", 1, 1, 0)):
+            s = Solver(method, N_SYS, N_ROW, Pv, flags=fl)
             if method != "pascal":
                 s.set_eps_constant(1e-3)
                 s.set_rho(A, B, C, all_systems=True)

@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(_PKG, "libbtdma.so")
 PASCAL, FILTERED_V1, FILTERED_V2 = 0, 1, 2
 FP64, FP32_REFINE = 0, 1
 FLAG_J_HOST = 1
+FLAG_REFERENCE_ORDER = 2
 OK, ERR_ARG, ERR_SEGMENT, ERR_CUDA, ERR_SIZE, ERR_UNSUPPORTED, ERR_DEVICE = 0, -1, -2, -3, -4, -5, -6
 STATUS_TIMEOUT, STATUS_NONFINITE = 1, 2
 

@@ -16,6 +16,7 @@
 #include "k_filtered_j.cuh"
 #include "k_segment.cuh"
 #include "k_thomas.cuh"
+#include "k_tile.cuh"
 
 using namespace btdma;
 
@@ -138,6 +139,90 @@ int launch_seg(const CUtensorMap* maps, const SegArgs& a, int groups, cudaStream
     return BTDMA_OK;
 }
 
+// 3-D view [nseg][TILE_MT][n_sys] of an [n_row x n_sys] FP64 array; boxes of
+// one row of every sub-segment for `sys` systems.
+bool make_tile_map(CUtensorMap* map, const void* ptr, int n_sys, int nseg, int sys) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)n_sys, (cuuint64_t)TILE_MT, (cuuint64_t)nseg};
+    cuuint64_t strides[2] = {(cuuint64_t)n_sys * sizeof(double),
+                             (cuuint64_t)n_sys * TILE_MT * sizeof(double)};
+    cuuint32_t box[3] = {(cuuint32_t)sys, 1, (cuuint32_t)nseg};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(ptr), dims, strides,
+                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+// Systems per CTA of the tiled kernel: the widest of 128/64/32/16 that keeps
+// SYS * nseg <= 512 threads.
+int tile_sys(int nseg) {
+    for (int sys = 128; sys >= 16; sys >>= 1)
+        if (sys * nseg <= TILE_MAX_THREADS) return sys;
+    return 0;
+}
+
+int num_sms() {
+    static int v = -1;
+    if (v < 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) v = 1;
+    }
+    return v;
+}
+
+template <int SYS>
+int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st) {
+    auto kern = tile_f64_kernel<SYS>;
+    static bool attr_done = false;
+    if (!attr_done) {
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                max_smem_optin()));
+        attr_done = true;
+    }
+    const int threads = SYS * a.nseg;
+    const int grid = std::min(a.n_groups, num_sms());
+    kern<<<grid, threads, tile_smem_bytes(threads), st>>>(maps[0], maps[1], maps[2], maps[3], a);
+    CK(cudaGetLastError());
+    return BTDMA_OK;
+}
+
+// Returns 1 when the tiled kernel was launched, 0 when the shape needs the
+// cluster kernel, < 0 on error.
+int try_tile(const double* A, const double* B, const double* C, const double* D, double* X,
+             int n_sys, int n_row, bool cyclic, unsigned* status, cudaStream_t st) {
+    if (n_row % TILE_MT != 0) return 0;
+    const int nseg = n_row / TILE_MT;
+    const int sys = tile_sys(nseg);
+    if (sys == 0) return 0;
+    if (cyclic && (nseg & (nseg - 1)) != 0) return 0;  // periodic PCR needs 2*nseg = 2^k
+    if (!(tma_ok(A, n_sys) && tma_ok(B, n_sys) && tma_ok(C, n_sys) && tma_ok(D, n_sys)))
+        return 0;
+    if (tile_smem_bytes(sys * nseg) > (size_t)max_smem_optin()) return 0;
+    CUtensorMap maps[4];
+    if (!(make_tile_map(&maps[0], A, n_sys, nseg, sys) && make_tile_map(&maps[1], B, n_sys, nseg, sys) &&
+          make_tile_map(&maps[2], C, n_sys, nseg, sys) && make_tile_map(&maps[3], D, n_sys, nseg, sys)))
+        return 0;
+    TileArgs a = {};
+    a.X = X;
+    a.n_sys = n_sys;
+    a.n_row = n_row;
+    a.nseg = nseg;
+    a.n_groups = (n_sys + sys - 1) / sys;
+    a.cyclic = cyclic ? 1 : 0;
+    a.status = status;
+    int rc;
+    switch (sys) {
+        case 128: rc = launch_tile_sys<128>(maps, a, st); break;
+        case 64: rc = launch_tile_sys<64>(maps, a, st); break;
+        case 32: rc = launch_tile_sys<32>(maps, a, st); break;
+        default: rc = launch_tile_sys<16>(maps, a, st); break;
+    }
+    return rc == BTDMA_OK ? 1 : rc;
+}
+
 template <bool CYCLIC>
 int launch_seg_method(int method, const CUtensorMap* maps, const SegArgs& a, int groups,
                       cudaStream_t st) {
@@ -197,6 +282,12 @@ int solve_impl(btdma_t h, const double* A, const double* B, const double* C, con
                                                              h->status);
         CK(cudaGetLastError());
         return BTDMA_OK;
+    }
+
+    if (h->method == BTDMA_PASCAL && !(h->flags & BTDMA_FLAG_REFERENCE_ORDER)) {
+        rc = try_tile(A, B, C, D, X, n_sys, n_row, cyclic, h->status, st);
+        if (rc < 0) return rc;
+        if (rc == 1) return BTDMA_OK;
     }
 
     SegArgs a = {};

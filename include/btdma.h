@@ -64,7 +64,13 @@ enum btdma_flags {
      * last rows (libs/filtered_tdma/gpu/filtered_tdma_kernels.cuh:235-238); v1
      * uses the K bound (filtered_tdma.cpp:110-114) instead of the right-hand-side
      * bound on the post-interface rows (filtered_tdma_cuda.cu:127-131). */
-    BTDMA_FLAG_J_HOST = 1 << 0
+    BTDMA_FLAG_J_HOST = 1 << 0,
+    /* PaScaL with the reference's operation order: P cluster CTAs per system,
+     * bit-identical to PaScaLTDMA::solve with nprocs = P
+     * (libs/pascal_tdma/cpu/pascal_tdma.cpp:113-227).  Without the flag PaScaL
+     * uses the register-tiled kernel, exact to rounding (<= 1e-12 relative to
+     * the serial Thomas) and faster. */
+    BTDMA_FLAG_REFERENCE_ORDER = 1 << 1
 };
 
 enum btdma_error {

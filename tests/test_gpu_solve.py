@@ -75,28 +75,63 @@ def test_thomas_cyclic_bit_exact(cuda, orc, n_sys, n_row):
     assert np.array_equal(x, orc.thomas_cyclic(A, B, C, D))
 
 
+def rel_err(x, ref):
+    return np.max(np.abs(x - ref)) / np.max(np.abs(ref))
+
+
 @pytest.mark.parametrize("n_sys,n_row,P", [
     (32, 64, 2), (64, 64, 4), (4096, 64, 4), (100, 96, 8), (33, 100, 7), (7, 48, 16),
     (2048, 512, 8), (96, 515, 16), (130, 37, 3), (64, 1000, 16)])
-def test_pascal_bit_exact(cuda, orc, n_sys, n_row, P):
+def test_pascal_reference_order_bit_exact(cuda, orc, n_sys, n_row, P):
+    """Cluster kernel, reference operation order: bit-identical to PaScaLTDMA
+    with nprocs = P (through the oracle, itself pinned to the reference)."""
+    from filtered_tdma_b200 import _lib as L
     A, B, C, D = W.diag_dominant(n_sys, n_row, seed=P * 1000 + n_row)
-    x, _ = run(cuda, "pascal", A, B, C, D, P)
-    xo = orc.pascal(A, B, C, D, P)
-    assert np.array_equal(x, xo)
-    xt = orc.thomas(A, B, C, D)
-    assert np.max(np.abs(x - xt)) <= 1e-12 * np.max(np.abs(xt))
-    x2, _ = run(cuda, "pascal", A, B, C, D, P, out=True)
+    x, _ = run(cuda, "pascal", A, B, C, D, P, flags=L.FLAG_REFERENCE_ORDER)
+    assert np.array_equal(x, orc.pascal(A, B, C, D, P))
+    assert rel_err(x, orc.thomas(A, B, C, D)) <= 1e-12
+    x2, _ = run(cuda, "pascal", A, B, C, D, P, out=True, flags=L.FLAG_REFERENCE_ORDER)
     assert np.array_equal(x2, x)
 
 
 @pytest.mark.parametrize("n_sys,n_row,P", [(32, 64, 2), (100, 96, 8), (33, 100, 7),
                                            (64, 512, 16)])
-def test_pascal_cyclic_bit_exact(cuda, orc, n_sys, n_row, P):
+def test_pascal_cyclic_reference_order_bit_exact(cuda, orc, n_sys, n_row, P):
+    from filtered_tdma_b200 import _lib as L
     A, B, C, D = W.diag_dominant(n_sys, n_row, seed=P + n_row)
-    x, _ = run(cuda, "pascal", A, B, C, D, P, cyclic=True)
+    x, _ = run(cuda, "pascal", A, B, C, D, P, cyclic=True, flags=L.FLAG_REFERENCE_ORDER)
     assert np.array_equal(x, orc.pascal(A, B, C, D, P, cyclic=True))
-    xt = orc.thomas_cyclic(A, B, C, D)
-    assert np.max(np.abs(x - xt)) <= 1e-12 * np.max(np.abs(xt))
+    assert rel_err(x, orc.thomas_cyclic(A, B, C, D)) <= 1e-12
+
+
+# Default PaScaL: the register-tiled kernel where the shape allows it
+# (n_row = 16 * nseg, nseg <= 32, even n_sys), else the cluster kernel.  Exact to
+# rounding: within 1e-12 (relative to max|x|) of the serial Thomas.
+@pytest.mark.parametrize("n_sys,n_row", [
+    (16, 16), (32, 32), (100, 48), (4096, 64), (1000, 128), (2048, 192), (130, 256),
+    (4094, 384), (2048, 512), (98, 512), (33, 64), (64, 100), (64, 1024)])
+def test_pascal_default_within_1e12(cuda, orc, n_sys, n_row):
+    A, B, C, D = W.diag_dominant(n_sys, n_row, seed=n_sys + 3 * n_row)
+    P = 2 if n_row < 64 else 8
+    x, _ = run(cuda, "pascal", A, B, C, D, P)
+    assert rel_err(x, orc.thomas(A, B, C, D)) <= 1e-12
+    x2, _ = run(cuda, "pascal", A, B, C, D, P, out=True)
+    assert np.array_equal(x2, x)
+
+
+@pytest.mark.parametrize("n_sys,n_row", [(16, 16), (64, 32), (1000, 64), (256, 128),
+                                         (2048, 512)])
+def test_pascal_default_cyclic_within_1e12(cuda, orc, n_sys, n_row):
+    A, B, C, D = W.diag_dominant(n_sys, n_row, seed=n_sys + n_row + 1)
+    x, _ = run(cuda, "pascal", A, B, C, D, 4, cyclic=True)
+    assert rel_err(x, orc.thomas_cyclic(A, B, C, D)) <= 1e-12
+
+
+def test_pascal_default_weak_dominance(cuda, orc):
+    # rho up to 0.499: the reduced system is barely dominant
+    A, B, C, D = W.weak_dominance(512, 512, seed=3)
+    x, _ = run(cuda, "pascal", A, B, C, D, 8)
+    assert rel_err(x, orc.thomas(A, B, C, D)) <= 1e-12
 
 
 @pytest.mark.parametrize("version", [1, 2])
@@ -146,8 +181,11 @@ def test_filtered_set_rho_system0(cuda, orc):
 def test_no_tma_path_odd_systems(cuda, orc):
     # odd n_sys: the row stride is not a multiple of 16 bytes, plain loads are used
     A, B, C, D = W.diag_dominant(101, 128, seed=9)
-    x, _ = run(cuda, "pascal", A, B, C, D, 4)
+    from filtered_tdma_b200 import _lib as L
+    x, _ = run(cuda, "pascal", A, B, C, D, 4, flags=L.FLAG_REFERENCE_ORDER)
     assert np.array_equal(x, orc.pascal(A, B, C, D, 4))
+    x, _ = run(cuda, "pascal", A, B, C, D, 4)
+    assert rel_err(x, orc.thomas(A, B, C, D)) <= 1e-12
 
 
 def test_dropin_classes(cuda, orc):
@@ -158,7 +196,7 @@ def test_dropin_classes(cuda, orc):
     dA, dB, dC, dD = dev(cuda, A, B, C, D)
     p = PaScaLTDMACUDA(n_sys, 0, 4, None)
     p.solve(dA, dB, dC, dD, n_sys, n_row)
-    assert np.array_equal(host(dD), orc.pascal(A, B, C, D, 4))
+    assert rel_err(host(dD), xt) <= 1e-12
     # TdmaBackendGPU strings
     for kind in ("pascal", "filtered", "filtered_v2"):
         dA, dB, dC, dD = dev(cuda, A, B, C, D)
