@@ -93,7 +93,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     if (tid == 0) {
         for (int i = 0; i < TILE_NST; ++i) {
             mbar_init(&full[i], 1);
-            mbar_init(&empty[i], T);
+            mbar_init(&empty[i], (T + 31) / 32);  // one arrival per warp
         }
         fence_mbar_init();
     }
@@ -137,7 +137,8 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             if (ok) ok = mbar_wait_bounded(&full[slot], (t / TILE_NST) & 1, args.status);
             const double* st = ring + (size_t)slot * 4 * T;
             const double a = st[tid], b = st[T + tid], c = st[2 * T + tid], d = st[3 * T + tid];
-            mbar_arrive(&empty[slot]);
+            __syncwarp();
+            if ((tid & 31) == 0) mbar_arrive(&empty[slot]);
             if (tid == 0 && ok) {
                 // refill the slot released one row ago (everyone is past it)
                 const int u = t + TILE_NST - 1;
