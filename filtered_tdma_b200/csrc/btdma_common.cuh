@@ -31,6 +31,21 @@ struct Exact64 {
     static __device__ __forceinline__ double rcp(double a) { return __drcp_rn(a); }
 };
 
+// Reciprocal for the kernels that promise rounding-level accuracy, not bit
+// identity: the hardware approximation rcp.approx.ftz.f64 refined by two
+// Newton-Raphson steps e = 1 - x r, r += r e (each step squares the relative
+// error), with no special-case branches.  Accurate to about an ulp for normal,
+// finite, non-zero x; zero, infinite or subnormal pivots are not handled (they
+// are not valid inputs of a diagonally dominant system).
+__device__ __forceinline__ double rcp_nr(double x) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+}
+
 // Status bits OR-ed into the device status word.
 enum : unsigned {
     ST_TIMEOUT = 1u << 0,     // an mbarrier wait hit its iteration limit
@@ -61,27 +76,30 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                  : "memory");
 }
 
+// One poll.  The thread may be suspended until the phase completes or for at
+// most ~kSuspendNs, so a waiting warp sleeps instead of spinning.
+constexpr uint32_t kSuspendNs = 20000;
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendNs)
         : "memory");
     return ok != 0;
 }
 
-// Bounded wait: gives up after `limit` polls (each poll may itself suspend the
-// thread for a hardware-chosen time), raising ST_TIMEOUT.  Every 4096 polls it
-// also checks the status word and gives up at once if another CTA already timed
-// out, so a systematic failure costs one timeout, not one per CTA.
+// Bounded wait: gives up after `limit` polls (each poll suspends the thread for
+// at most kSuspendNs), raising ST_TIMEOUT.  Every 64 polls it also checks the
+// status word and gives up at once if another CTA already timed out, so a
+// systematic failure costs one timeout, not one per CTA.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
-                                                  unsigned* status, uint32_t limit = 1u << 20) {
+                                                  unsigned* status, uint32_t limit = 1u << 16) {
     for (uint32_t it = 0; it < limit; ++it) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (status && (it & 4095u) == 4095u &&
+        if (status && (it & 63u) == 63u &&
             (*reinterpret_cast<volatile unsigned*>(status) & ST_TIMEOUT))
             return false;
     }

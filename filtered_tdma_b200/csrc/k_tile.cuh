@@ -8,8 +8,10 @@
 //   1. Forward pass (one row of every sub-segment per step).  Row k of all NSEG
 //      sub-segments of SYS systems arrives in one TMA box of a 3-D view
 //      [NSEG][TILE_MT][n_sys] of each array, through a TILE_NST-stage shared
-//      memory ring with full/empty mbarriers; thread 0 refills the ring, so the
-//      next group's first rows are in flight while this group finishes.  Each
+//      memory ring (an mbarrier per stage); the last warp to finish reading a
+//      stage refills it, so the ring stays TILE_NST rows ahead of the slowest
+//      warp and the next group's first rows are in flight while this group
+//      finishes.  Each
 //      thread runs the modified Thomas elimination of PaScaL
 //      (libs/pascal_tdma/cpu/pascal_tdma.cpp:131-170) on its 16 rows:
 //          alpha_k x_first + x_k + gamma_k x_{k+1} = delta_k,
@@ -38,7 +40,7 @@
 namespace btdma {
 
 constexpr int TILE_MT = 16;       // rows per sub-segment (per thread)
-constexpr int TILE_NST = 6;       // TMA ring stages
+constexpr int TILE_NST = 10;      // TMA ring stages
 constexpr int TILE_MAX_THREADS = 512;
 
 struct TileArgs {
@@ -51,7 +53,7 @@ struct TileArgs {
 __host__ __device__ __forceinline__ size_t tile_smem_bytes(int threads) {
     size_t ring = (size_t)TILE_NST * 4 * threads * sizeof(double);
     size_t pcr = 2ull * 3 * 2 * threads * sizeof(double);  // 2 buffers x (l,u,r) x 2 rows/thread
-    size_t bars = 2ull * TILE_NST * sizeof(uint64_t);
+    size_t bars = TILE_NST * (sizeof(uint64_t) + sizeof(int));
     return ring + pcr + bars + 128;
 }
 
@@ -82,7 +84,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     double* pcr = ring + (size_t)TILE_NST * 4 * T;  // [2][3][2T]
     uint64_t* full = reinterpret_cast<uint64_t*>(pcr + 2 * 3 * 2 * T);
-    uint64_t* empty = full + TILE_NST;
+    int* readers = reinterpret_cast<int*>(full + TILE_NST);  // warps done with a slot
 
     const int tid = threadIdx.x;
     const int s = tid % SYS;
@@ -90,10 +92,11 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     const int N = 2 * nseg;  // reduced rows per system
     const size_t ns = (size_t)args.n_sys;
 
+    const int nwarps = (T + 31) / 32;
     if (tid == 0) {
         for (int i = 0; i < TILE_NST; ++i) {
             mbar_init(&full[i], 1);
-            mbar_init(&empty[i], (T + 31) / 32);  // one arrival per warp
+            readers[i] = 0;
         }
         fence_mbar_init();
     }
@@ -105,7 +108,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     const int total = n_my * M;  // ring stages this CTA consumes
     const uint32_t stage_bytes = 4u * T * sizeof(double);
 
-    auto issue = [&](int t) {  // thread 0 only
+    auto issue = [&](int t) {  // one thread
         const int slot = t % TILE_NST;
         const int g = (int)blockIdx.x + (t / M) * (int)gridDim.x;
         const int k = t % M;
@@ -137,31 +140,30 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             if (ok) ok = mbar_wait_bounded(&full[slot], (t / TILE_NST) & 1, args.status);
             const double* st = ring + (size_t)slot * 4 * T;
             const double a = st[tid], b = st[T + tid], c = st[2 * T + tid], d = st[3 * T + tid];
+            // The last warp to finish reading the slot refills it with stage
+            // t + TILE_NST: the ring stays TILE_NST rows ahead of the slowest warp.
             __syncwarp();
-            if ((tid & 31) == 0) mbar_arrive(&empty[slot]);
-            if (tid == 0 && ok) {
-                // refill the slot released one row ago (everyone is past it)
-                const int u = t + TILE_NST - 1;
-                if (t >= 1 && u < total) {
-                    const int ps = (t - 1) % TILE_NST;
-                    ok = mbar_wait_bounded(&empty[ps], ((t - 1) / TILE_NST) & 1, args.status);
-                    if (ok) issue(u);
+            if ((tid & 31) == 0) {
+                __threadfence_block();
+                if (atomicAdd(&readers[slot], 1) == nwarps - 1) {
+                    readers[slot] = 0;
+                    if (ok && t + TILE_NST < total) issue(t + TILE_NST);
                 }
             }
             if (k == 0) {
-                const double ib = 1.0 / b;
+                const double ib = rcp_nr(b);
                 ab0 = a * ib;
                 cb0 = c * ib;
                 db0 = d * ib;
             } else if (k == 1) {
-                const double ib = 1.0 / b;
+                const double ib = rcp_nr(b);
                 al[1] = a * ib;
                 ga[1] = c * ib;
                 de[1] = d * ib;
                 sa = al[1];
                 sd = de[1];
             } else {
-                const double inv = 1.0 / (b - a * ga[k - 1]);
+                const double inv = rcp_nr(b - a * ga[k - 1]);
                 ga[k] = c * inv;
                 de[k] = (d - a * de[k - 1]) * inv;
                 al[k] = -a * al[k - 1] * inv;
@@ -174,7 +176,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         }
         // reduced rows of this sub-segment
         const double pi_last = -ga[M - 2] * pi;  // pi_{M-1}
-        const double r0 = 1.0 / (1.0 - cb0 * sa);
+        const double r0 = rcp_nr(1.0 - cb0 * sa);
         double l0 = r0 * ab0;
         double u0 = r0 * cb0 * pi_last;  // -r c0 gamma''_1, gamma''_1 = -pi_{M-1}
         double v0 = r0 * (db0 - cb0 * sd);
@@ -214,7 +216,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                     nl[h] = 0.0;
                     nu[h] = 0.0;
                 } else {
-                    const double ib = 1.0 / (1.0 - li * um - ui * lp);
+                    const double ib = rcp_nr(1.0 - li * um - ui * lp);
                     nl[h] = -li * lm * ib;
                     nu[h] = -ui * up * ib;
                     nr[h] = (ri - li * rm - ui * rp) * ib;
@@ -258,8 +260,9 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     }
     if (!finite) raise_status(args.status, ST_NONFINITE);
     if (!ok && tid == 0) {
-        // a wait gave up: let in-flight copies land before the CTA exits
-        for (int i = 0; i < TILE_NST; ++i) mbar_wait_bounded(&full[i], 0, nullptr, 1u << 14);
+        // a wait gave up: give in-flight copies a bounded chance to land before
+        // the CTA exits
+        for (int i = 0; i < TILE_NST; ++i) mbar_wait_bounded(&full[i], 0, nullptr, 1u << 8);
     }
 }
 
