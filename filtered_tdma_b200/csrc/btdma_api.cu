@@ -173,9 +173,9 @@ int num_sms() {
     return v;
 }
 
-template <int SYS>
+template <int SYS, bool CYCLIC>
 int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st) {
-    auto kern = tile_f64_kernel<SYS>;
+    auto kern = tile_f64_kernel<SYS, CYCLIC>;
     static bool attr_done = false;
     if (!attr_done) {
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -184,7 +184,8 @@ int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st)
     }
     const int threads = SYS * a.nseg;
     const int grid = std::min(a.n_groups, num_sms());
-    kern<<<grid, threads, tile_smem_bytes(threads), st>>>(maps[0], maps[1], maps[2], maps[3], a);
+    kern<<<grid, threads, tile_smem_bytes(threads, SYS), st>>>(maps[0], maps[1], maps[2], maps[3],
+                                                                a);
     CK(cudaGetLastError());
     return BTDMA_OK;
 }
@@ -200,7 +201,7 @@ int try_tile(const double* A, const double* B, const double* C, const double* D,
     if (cyclic && (nseg & (nseg - 1)) != 0) return 0;  // periodic PCR needs 2*nseg = 2^k
     if (!(tma_ok(A, n_sys) && tma_ok(B, n_sys) && tma_ok(C, n_sys) && tma_ok(D, n_sys)))
         return 0;
-    if (tile_smem_bytes(sys * nseg) > (size_t)max_smem_optin()) return 0;
+    if (tile_smem_bytes(sys * nseg, sys) > (size_t)max_smem_optin()) return 0;
     CUtensorMap maps[4];
     if (!(make_tile_map(&maps[0], A, n_sys, nseg, sys) && make_tile_map(&maps[1], B, n_sys, nseg, sys) &&
           make_tile_map(&maps[2], C, n_sys, nseg, sys) && make_tile_map(&maps[3], D, n_sys, nseg, sys)))
@@ -214,11 +215,15 @@ int try_tile(const double* A, const double* B, const double* C, const double* D,
     a.cyclic = cyclic ? 1 : 0;
     a.status = status;
     int rc;
-    switch (sys) {
-        case 128: rc = launch_tile_sys<128>(maps, a, st); break;
-        case 64: rc = launch_tile_sys<64>(maps, a, st); break;
-        case 32: rc = launch_tile_sys<32>(maps, a, st); break;
-        default: rc = launch_tile_sys<16>(maps, a, st); break;
+    switch (sys * 2 + (cyclic ? 1 : 0)) {
+        case 256: rc = launch_tile_sys<128, false>(maps, a, st); break;
+        case 257: rc = launch_tile_sys<128, true>(maps, a, st); break;
+        case 128: rc = launch_tile_sys<64, false>(maps, a, st); break;
+        case 129: rc = launch_tile_sys<64, true>(maps, a, st); break;
+        case 64: rc = launch_tile_sys<32, false>(maps, a, st); break;
+        case 65: rc = launch_tile_sys<32, true>(maps, a, st); break;
+        case 33: rc = launch_tile_sys<16, true>(maps, a, st); break;
+        default: rc = launch_tile_sys<16, false>(maps, a, st); break;
     }
     return rc == BTDMA_OK ? 1 : rc;
 }

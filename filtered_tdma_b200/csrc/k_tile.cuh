@@ -50,9 +50,14 @@ struct TileArgs {
     unsigned* status;
 };
 
-__host__ __device__ __forceinline__ size_t tile_smem_bytes(int threads) {
+// PCR buffers: [2 buffers][3 fields l,u,r][N + 2 rows][SYS], rows -1 and N are
+// zero guard rows so that out-of-range neighbours need no branch.
+__host__ __device__ __forceinline__ size_t tile_pcr_doubles(int threads, int sys) {
+    return 2ull * 3 * (2 * threads + 2 * sys);
+}
+__host__ __device__ __forceinline__ size_t tile_smem_bytes(int threads, int sys) {
     size_t ring = (size_t)TILE_NST * 4 * threads * sizeof(double);
-    size_t pcr = 2ull * 3 * 2 * threads * sizeof(double);  // 2 buffers x (l,u,r) x 2 rows/thread
+    size_t pcr = tile_pcr_doubles(threads, sys) * sizeof(double);
     size_t bars = TILE_NST * (sizeof(uint64_t) + sizeof(int));
     return ring + pcr + bars + 128;
 }
@@ -71,7 +76,7 @@ __device__ __forceinline__ void tma_load_3d(void* smem_dst, const CUtensorMap* m
         : "memory");
 }
 
-template <int SYS>
+template <int SYS, bool CYCLIC>
 __global__ void __launch_bounds__(TILE_MAX_THREADS, 1)
 tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 const __grid_constant__ CUtensorMap tmC, const __grid_constant__ CUtensorMap tmD,
@@ -80,25 +85,37 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     extern __shared__ unsigned char smem_raw[];
     const int nseg = args.nseg;
     const int T = SYS * nseg;  // == blockDim.x
+    const int N = 2 * nseg;    // reduced rows per system
     double* ring = reinterpret_cast<double*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-    double* pcr = ring + (size_t)TILE_NST * 4 * T;  // [2][3][2T]
-    uint64_t* full = reinterpret_cast<uint64_t*>(pcr + 2 * 3 * 2 * T);
+    double* pcr = ring + (size_t)TILE_NST * 4 * T;
+    uint64_t* full = reinterpret_cast<uint64_t*>(pcr + tile_pcr_doubles(T, SYS));
     int* readers = reinterpret_cast<int*>(full + TILE_NST);  // warps done with a slot
 
     const int tid = threadIdx.x;
     const int s = tid % SYS;
     const int q = tid / SYS;
-    const int N = 2 * nseg;  // reduced rows per system
     const size_t ns = (size_t)args.n_sys;
-
     const int nwarps = (T + 31) / 32;
+
+    // PCR field bases for this thread's system column; row r lives at [r * SYS]
+    // from base + SYS (row -1 is the first guard row).
+    const int fs = (N + 2) * SYS;       // field stride
+    double* const pb = pcr + SYS + s;   // buffer 0, field l, row 0
+    auto FB = [&](int b, int f) { return pb + (b * 3 + f) * fs; };
+
     if (tid == 0) {
         for (int i = 0; i < TILE_NST; ++i) {
             mbar_init(&full[i], 1);
             readers[i] = 0;
         }
         fence_mbar_init();
+    }
+    if (tid < SYS) {  // zero guard rows (never written again)
+        for (int bf = 0; bf < 6; ++bf) {
+            pb[bf * fs - SYS] = 0.0;
+            pb[bf * fs + N * SYS] = 0.0;
+        }
     }
     __syncthreads();
 
@@ -124,6 +141,9 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         for (int t = 0; t < TILE_NST && t < total; ++t) issue(t);
 
     bool finite = true;
+    int slot = 0;
+    uint32_t phase = 0;
+    int t = 0;  // stage counter
     for (int it = 0; it < n_my; ++it) {
         const int g = (int)blockIdx.x + it * (int)gridDim.x;
         const int sys = g * SYS + s;
@@ -135,11 +155,9 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         double pi = 1.0, sa = 0.0, sd = 0.0;
 #pragma unroll
         for (int k = 0; k < M; ++k) {
-            const int t = it * M + k;
-            const int slot = t % TILE_NST;
-            if (ok) ok = mbar_wait_bounded(&full[slot], (t / TILE_NST) & 1, args.status);
-            const double* st = ring + (size_t)slot * 4 * T;
-            const double a = st[tid], b = st[T + tid], c = st[2 * T + tid], d = st[3 * T + tid];
+            if (ok) ok = mbar_wait_bounded(&full[slot], phase, args.status);
+            const double* st = ring + (size_t)slot * 4 * T + tid;
+            const double a = st[0], b = st[T], c = st[2 * T], d = st[3 * T];
             // The last warp to finish reading the slot refills it with stage
             // t + TILE_NST: the ring stays TILE_NST rows ahead of the slowest warp.
             __syncwarp();
@@ -149,6 +167,11 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                     readers[slot] = 0;
                     if (ok && t + TILE_NST < total) issue(t + TILE_NST);
                 }
+            }
+            ++t;
+            if (++slot == TILE_NST) {
+                slot = 0;
+                phase ^= 1u;
             }
             if (k == 0) {
                 const double ib = rcp_nr(b);
@@ -177,42 +200,49 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         // reduced rows of this sub-segment
         const double pi_last = -ga[M - 2] * pi;  // pi_{M-1}
         const double r0 = rcp_nr(1.0 - cb0 * sa);
-        double l0 = r0 * ab0;
-        double u0 = r0 * cb0 * pi_last;  // -r c0 gamma''_1, gamma''_1 = -pi_{M-1}
-        double v0 = r0 * (db0 - cb0 * sd);
-        double l1 = al[M - 1], u1 = ga[M - 1], v1 = de[M - 1];
+        const int i0 = 2 * q;
+        {
+            double* w = pb + i0 * SYS;
+            w[0] = r0 * ab0;
+            w[fs] = r0 * cb0 * pi_last;  // -r c0 gamma''_1, gamma''_1 = -pi_{M-1}
+            w[2 * fs] = r0 * (db0 - cb0 * sd);
+            w[SYS] = al[M - 1];
+            w[fs + SYS] = ga[M - 1];
+            w[2 * fs + SYS] = de[M - 1];
+        }
+        __syncthreads();
 
         // ------------------------------------------------- reduced system (PCR)
-        // buffer layout: [buf][field l,u,r][row 0..N-1][SYS]
-        auto P = [&](int buf, int f, int row) -> double& {
-            return pcr[(((size_t)buf * 3 + f) * N + row) * SYS + s];
-        };
-        const int i0 = 2 * q, i1 = 2 * q + 1;
-        P(0, 0, i0) = l0; P(0, 1, i0) = u0; P(0, 2, i0) = v0;
-        P(0, 0, i1) = l1; P(0, 1, i1) = u1; P(0, 2, i1) = v1;
-        __syncthreads();
+        // Row i: l_i x_{i-dl} + x_i + u_i x_{i+dl} = r_i.  Eliminating the rows
+        // i-dl and i+dl doubles the coupling distance; out-of-range neighbours
+        // are the zero guard rows (x = 0 there), or wrap around when periodic.
         int cur = 0;
         double x_first = 0.0, x_last = 0.0;
         bool solved = false;
         for (int dl = 1; dl < N; dl <<= 1) {
-            const bool last_cyclic = args.cyclic && 2 * dl == N;
+            const bool last_cyclic = CYCLIC && 2 * dl == N;
+            const double* L = FB(cur, 0);
+            const double* U = L + fs;
+            const double* R = U + fs;
             double nl[2], nu[2], nr[2];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int i = i0 + h;
-                const double li = P(cur, 0, i), ui = P(cur, 1, i), ri = P(cur, 2, i);
                 int im = i - dl, ip = i + dl;
-                double lm = 0, um = 0, rm = 0, lp = 0, up = 0, rp = 0;
-                if (args.cyclic) {
-                    im = (im + N) % N;
-                    ip = ip % N;
+                if (CYCLIC) {
+                    im = im < 0 ? im + N : im;
+                    ip = ip >= N ? ip - N : ip;
+                } else {
+                    im = im < -1 ? -1 : im;
+                    ip = ip > N ? N : ip;
                 }
-                if (im >= 0) { lm = P(cur, 0, im); um = P(cur, 1, im); rm = P(cur, 2, im); }
-                if (ip < N) { lp = P(cur, 0, ip); up = P(cur, 1, ip); rp = P(cur, 2, ip); }
+                const double li = L[i * SYS], ui = U[i * SYS], ri = R[i * SYS];
+                const double lm = L[im * SYS], um = U[im * SYS], rm = R[im * SYS];
+                const double lp = L[ip * SYS], up = U[ip * SYS], rp = R[ip * SYS];
                 if (last_cyclic) {
                     // i-dl and i+dl are the same row j: 2x2 system in x_i, x_j
                     const double si = li + ui, sj = lm + um;
-                    nr[h] = (ri - si * rm) / (1.0 - si * sj);
+                    nr[h] = (ri - si * rm) * rcp_nr(1.0 - si * sj);
                     nl[h] = 0.0;
                     nu[h] = 0.0;
                 } else {
@@ -223,11 +253,12 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                 }
             }
             const int nxt = cur ^ 1;
+            double* w = FB(nxt, 0) + i0 * SYS;
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-                P(nxt, 0, i0 + h) = nl[h];
-                P(nxt, 1, i0 + h) = nu[h];
-                P(nxt, 2, i0 + h) = nr[h];
+                w[h * SYS] = nl[h];
+                w[fs + h * SYS] = nu[h];
+                w[2 * fs + h * SYS] = nr[h];
             }
             if (last_cyclic) {
                 x_first = nr[0];
@@ -238,8 +269,9 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             cur = nxt;
         }
         if (!solved) {
-            x_first = P(cur, 2, i0);
-            x_last = P(cur, 2, i1);
+            const double* R = FB(cur, 2) + i0 * SYS;
+            x_first = R[0];
+            x_last = R[SYS];
         }
 
         // --------------------------------------------------- back substitution
