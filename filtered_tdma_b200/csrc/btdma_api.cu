@@ -140,27 +140,19 @@ int launch_seg(const CUtensorMap* maps, const SegArgs& a, int groups, cudaStream
 }
 
 // 3-D view [nseg][TILE_MT][n_sys] of an [n_row x n_sys] FP64 array; boxes of
-// one row of every sub-segment for `sys` systems.
-bool make_tile_map(CUtensorMap* map, const void* ptr, int n_sys, int nseg, int sys) {
+// one row of `nsc` consecutive sub-segments for `sys` systems.
+bool make_tile_map(CUtensorMap* map, const void* ptr, int n_sys, int nseg, int sys, int nsc) {
     auto fn = encode_fn();
     if (!fn) return false;
     cuuint64_t dims[3] = {(cuuint64_t)n_sys, (cuuint64_t)TILE_MT, (cuuint64_t)nseg};
     cuuint64_t strides[2] = {(cuuint64_t)n_sys * sizeof(double),
                              (cuuint64_t)n_sys * TILE_MT * sizeof(double)};
-    cuuint32_t box[3] = {(cuuint32_t)sys, 1, (cuuint32_t)nseg};
+    cuuint32_t box[3] = {(cuuint32_t)sys, 1, (cuuint32_t)nsc};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(ptr), dims, strides,
                     box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
-}
-
-// Systems per CTA of the tiled kernel: the widest of 128/64/32/16 that keeps
-// SYS * nseg <= 512 threads.
-int tile_sys(int nseg) {
-    for (int sys = 128; sys >= 16; sys >>= 1)
-        if (sys * nseg <= TILE_MAX_THREADS) return sys;
-    return 0;
 }
 
 int num_sms() {
@@ -173,6 +165,43 @@ int num_sms() {
     return v;
 }
 
+// Shape plan of the tiled kernel: systems per group, CTAs per cluster, ring stages.
+struct TilePlan {
+    int sys = 0, cl = 0, nst = 0, nseg = 0;
+};
+
+TilePlan tile_plan(int n_row, bool cyclic) {
+    TilePlan pl;
+    if (n_row % TILE_MT != 0) return pl;
+    const int nseg = n_row / TILE_MT;
+    if (cyclic && (nseg & (nseg - 1)) != 0) return pl;  // periodic PCR needs 2^k rows
+    int sys, cl = 0;
+    if (nseg <= 4) {
+        sys = 128;
+        cl = 1;
+    } else if (nseg <= 8) {
+        sys = 64;
+        cl = 1;
+    } else {
+        sys = 32;
+        for (int c = 1; c <= 16; c <<= 1)
+            if (nseg % c == 0 && nseg / c <= 16) {
+                cl = c;
+                break;
+            }
+        if (cl == 0) return pl;
+    }
+    const int T = sys * nseg / cl;
+    int nst = TILE_MAX_NST;
+    while (nst >= 3 && tile_smem_bytes(T, nseg, sys / cl, nst) > (size_t)max_smem_optin()) --nst;
+    if (nst < 3) return pl;
+    pl.sys = sys;
+    pl.cl = cl;
+    pl.nst = nst;
+    pl.nseg = nseg;
+    return pl;
+}
+
 template <int SYS, bool CYCLIC>
 int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st) {
     auto kern = tile_f64_kernel<SYS, CYCLIC>;
@@ -180,50 +209,68 @@ int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st)
     if (!attr_done) {
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 max_smem_optin()));
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         attr_done = true;
     }
-    const int threads = SYS * a.nseg;
-    const int grid = std::min(a.n_groups, num_sms());
-    kern<<<grid, threads, tile_smem_bytes(threads, SYS), st>>>(maps[0], maps[1], maps[2], maps[3],
-                                                                a);
-    CK(cudaGetLastError());
+    const int threads = SYS * a.nseg / a.cl;
+    cudaLaunchConfig_t cfg = {};
+    cfg.blockDim = dim3(threads, 1, 1);
+    cfg.dynamicSmemBytes = tile_smem_bytes(threads, a.nseg, SYS / a.cl, a.nst);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = a.cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = num_sms();
+    if (a.cl > 1) {
+        cfg.gridDim = dim3(a.cl * num_sms(), 1, 1);
+        int nc = 0;
+        CK(cudaOccupancyMaxActiveClusters(&nc, kern, &cfg));
+        if (nc <= 0) return fail(BTDMA_ERR_UNSUPPORTED, "no cluster of %d CTAs fits", a.cl);
+        clusters = nc;
+    }
+    clusters = std::min(clusters, a.n_groups);
+    cfg.gridDim = dim3(clusters * a.cl, 1, 1);
+    TileArgs aa = a;
+    CK(cudaLaunchKernelEx(&cfg, kern, maps[0], maps[1], maps[2], maps[3], aa));
     return BTDMA_OK;
 }
 
 // Returns 1 when the tiled kernel was launched, 0 when the shape needs the
-// cluster kernel, < 0 on error.
+// cluster-per-segment kernel, < 0 on error.
 int try_tile(const double* A, const double* B, const double* C, const double* D, double* X,
              int n_sys, int n_row, bool cyclic, unsigned* status, cudaStream_t st) {
-    if (n_row % TILE_MT != 0) return 0;
-    const int nseg = n_row / TILE_MT;
-    const int sys = tile_sys(nseg);
-    if (sys == 0) return 0;
-    if (cyclic && (nseg & (nseg - 1)) != 0) return 0;  // periodic PCR needs 2*nseg = 2^k
+    const TilePlan pl = tile_plan(n_row, cyclic);
+    if (pl.sys == 0) return 0;
     if (!(tma_ok(A, n_sys) && tma_ok(B, n_sys) && tma_ok(C, n_sys) && tma_ok(D, n_sys)))
         return 0;
-    if (tile_smem_bytes(sys * nseg, sys) > (size_t)max_smem_optin()) return 0;
+    const int nsc = pl.nseg / pl.cl;
     CUtensorMap maps[4];
-    if (!(make_tile_map(&maps[0], A, n_sys, nseg, sys) && make_tile_map(&maps[1], B, n_sys, nseg, sys) &&
-          make_tile_map(&maps[2], C, n_sys, nseg, sys) && make_tile_map(&maps[3], D, n_sys, nseg, sys)))
+    if (!(make_tile_map(&maps[0], A, n_sys, pl.nseg, pl.sys, nsc) &&
+          make_tile_map(&maps[1], B, n_sys, pl.nseg, pl.sys, nsc) &&
+          make_tile_map(&maps[2], C, n_sys, pl.nseg, pl.sys, nsc) &&
+          make_tile_map(&maps[3], D, n_sys, pl.nseg, pl.sys, nsc)))
         return 0;
     TileArgs a = {};
     a.X = X;
     a.n_sys = n_sys;
     a.n_row = n_row;
-    a.nseg = nseg;
-    a.n_groups = (n_sys + sys - 1) / sys;
-    a.cyclic = cyclic ? 1 : 0;
+    a.nseg = pl.nseg;
+    a.cl = pl.cl;
+    a.nst = pl.nst;
+    a.n_groups = (n_sys + pl.sys - 1) / pl.sys;
     a.status = status;
     int rc;
-    switch (sys * 2 + (cyclic ? 1 : 0)) {
+    switch (pl.sys * 2 + (cyclic ? 1 : 0)) {
         case 256: rc = launch_tile_sys<128, false>(maps, a, st); break;
         case 257: rc = launch_tile_sys<128, true>(maps, a, st); break;
         case 128: rc = launch_tile_sys<64, false>(maps, a, st); break;
         case 129: rc = launch_tile_sys<64, true>(maps, a, st); break;
-        case 64: rc = launch_tile_sys<32, false>(maps, a, st); break;
         case 65: rc = launch_tile_sys<32, true>(maps, a, st); break;
-        case 33: rc = launch_tile_sys<16, true>(maps, a, st); break;
-        default: rc = launch_tile_sys<16, false>(maps, a, st); break;
+        default: rc = launch_tile_sys<32, false>(maps, a, st); break;
     }
     return rc == BTDMA_OK ? 1 : rc;
 }

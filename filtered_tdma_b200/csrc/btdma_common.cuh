@@ -14,7 +14,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "../../include/btdma.h"
+#include "btdma.h"
 
 #ifndef __CUDA_ARCH__
 #define BTDMA_HOST_ONLY 1

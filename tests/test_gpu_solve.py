@@ -119,8 +119,17 @@ def test_pascal_default_within_1e12(cuda, orc, n_sys, n_row):
     assert np.array_equal(x2, x)
 
 
+@pytest.mark.parametrize("n_sys,n_row", [(96, 768), (64, 1024), (34, 2048), (32, 4096),
+                                         (1000, 384)])
+def test_pascal_default_long_systems(cuda, orc, n_sys, n_row):
+    """Sub-segments split over 2-16 CTAs of a cluster (distributed shared memory)."""
+    A, B, C, D = W.diag_dominant(n_sys, n_row, seed=n_row + 7)
+    x, _ = run(cuda, "pascal", A, B, C, D, 8)
+    assert rel_err(x, orc.thomas(A, B, C, D)) <= 1e-12
+
+
 @pytest.mark.parametrize("n_sys,n_row", [(16, 16), (64, 32), (1000, 64), (256, 128),
-                                         (2048, 512)])
+                                         (2048, 512), (64, 1024), (40, 4096)])
 def test_pascal_default_cyclic_within_1e12(cuda, orc, n_sys, n_row):
     A, B, C, D = W.diag_dominant(n_sys, n_row, seed=n_sys + n_row + 1)
     x, _ = run(cuda, "pascal", A, B, C, D, 4, cyclic=True)
