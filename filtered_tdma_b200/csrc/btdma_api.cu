@@ -408,7 +408,9 @@ int btdma_create(int method, int n_sys, int n_row, int P, int precision, int fla
     if (P > 1 && n_row / P < 3)
         return fail(BTDMA_ERR_SEGMENT, "n_row %d gives segments shorter than 3 rows at P=%d",
                     n_row, P);
-    if (P > 1 && seg_smem_bytes(seg_mcap(n_row, P), P, true) > (size_t)max_smem_optin())
+    const bool tiled = method == BTDMA_PASCAL && !(flags & BTDMA_FLAG_REFERENCE_ORDER) &&
+                       tile_plan(n_row, false).sys != 0;
+    if (P > 1 && !tiled && seg_smem_bytes(seg_mcap(n_row, P), P, true) > (size_t)max_smem_optin())
         return fail(BTDMA_ERR_UNSUPPORTED, "segments of %d rows exceed shared memory; raise P",
                     (n_row + P - 1) / P);
 
