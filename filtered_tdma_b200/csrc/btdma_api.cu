@@ -191,9 +191,9 @@ TilePlan tile_plan(int n_row, bool cyclic) {
             }
         if (cl == 0) return pl;
     }
-    const int T = sys * nseg / cl;
     int nst = TILE_MAX_NST;
-    while (nst >= 3 && tile_smem_bytes(T, nseg, sys / cl, nst) > (size_t)max_smem_optin()) --nst;
+    while (nst >= 3 && tile_smem_bytes(sys, nseg / cl, nseg, sys / cl, nst) > (size_t)max_smem_optin())
+        --nst;
     if (nst < 3) return pl;
     pl.sys = sys;
     pl.cl = cl;
@@ -215,7 +215,7 @@ int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st)
     const int threads = SYS * a.nseg / a.cl;
     cudaLaunchConfig_t cfg = {};
     cfg.blockDim = dim3(threads, 1, 1);
-    cfg.dynamicSmemBytes = tile_smem_bytes(threads, a.nseg, SYS / a.cl, a.nst);
+    cfg.dynamicSmemBytes = tile_smem_bytes(SYS, a.nseg / a.cl, a.nseg, SYS / a.cl, a.nst);
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;

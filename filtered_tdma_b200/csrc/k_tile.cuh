@@ -10,10 +10,12 @@
 //   1. Forward pass (one row of every local sub-segment per step).  Row k of the
 //      CTA's NSC sub-segments of SYS systems arrives in one TMA box of a 3-D view
 //      [NSEG][TILE_MT][n_sys] (SYS * 8 bytes wide, 256 B for SYS = 32) through
-//      an NST-stage shared-memory ring with one mbarrier per stage; the last warp
-//      to finish reading a stage refills it, so the ring stays NST rows ahead of
-//      the slowest warp and the next group's rows are in flight while this group
-//      finishes.  Each thread runs the modified Thomas elimination of PaScaL
+//      an NST-stage shared-memory ring.  Each stage has a "full" mbarrier (TMA
+//      transaction count) and an "empty" mbarrier (one arrival per warp); the
+//      refill of a stage is issued one row later by a rotating producer warp, so
+//      no warp waits for the others on the critical path and the next group's
+//      rows are in flight while this group finishes.  Each thread runs the
+//      modified Thomas elimination of PaScaL
 //      (libs/pascal_tdma/cpu/pascal_tdma.cpp:131-170) on its 16 rows:
 //          alpha_k x_first + x_k + gamma_k x_{k+1} = delta_k,
 //      and, instead of a backward sweep, accumulates the reduced first row in
@@ -25,12 +27,13 @@
 //   2. Reduced system (the reference's all-to-all + serial Thomas on 2P rows,
 //      pascal_tdma.cpp:185-210).  The two reduced rows of every sub-segment are
 //      published in shared memory; after a cluster barrier each CTA gathers, over
-//      distributed shared memory, the whole reduced system of its SYS/CL systems.
-//      One level of cyclic reduction eliminates the first-row unknowns (leaving a
-//      tridiagonal system in the last-row unknowns, one row per thread), parallel
-//      cyclic reduction solves that in log2(NSEG) barrier steps, and the
-//      first-row unknowns follow from their rows.  The results go back to the
-//      owning CTAs over distributed shared memory; a second cluster barrier.
+//      distributed shared memory, the reduced systems of its SYS/CL systems, one
+//      system per group of W = 2^ceil(log2 NSEG) lanes.  One level of cyclic
+//      reduction eliminates the first-row unknowns, parallel cyclic reduction
+//      solves the remaining tridiagonal system in the last-row unknowns with warp
+//      shuffles (no block barrier), and the first-row unknowns follow.  Systems
+//      longer than 512 rows (W > 32) run the same steps through shared memory.
+//      The results go back to the owning CTAs; a second cluster barrier.
 //   3. Back substitution from registers: x_k = delta_k - alpha_k x_first -
 //      gamma_k x_{k+1}, k = M-2..1, stored coalesced, SYS systems wide.
 //
@@ -61,19 +64,29 @@ struct TileArgs {
     unsigned* status;
 };
 
-// Shared memory (doubles unless noted), T = SYS * NSC threads, SUB = SYS / CL:
-//   ring  NST * 4 * T          TMA stages (A, B, C, D of one row per sub-segment)
-//   red   6 * T                this CTA's reduced rows (l0,u0,r0 | l1,u1,r1)
-//   gat   6 * (NSEG + 2) * SUB gathered reduced rows, zero guard rows -1, NSEG
-//   pcr   6 * (NSEG + 2) * SUB two PCR buffers (a, c, d), guard rows
-//   xr    2 * T                x_first / x_last of this CTA's sub-segments
-//   bars  NST mbarriers + NST ints
-__host__ __device__ __forceinline__ size_t tile_fixed_doubles(int T, int nseg, int sub) {
-    return 6ull * T + 6ull * (nseg + 2) * sub + 6ull * (nseg + 2) * sub + 2ull * T;
+__host__ __device__ __forceinline__ int tile_lanes(int nseg) {
+    int w = 1;
+    while (w < nseg) w <<= 1;
+    return w;
 }
-__host__ __device__ __forceinline__ size_t tile_smem_bytes(int T, int nseg, int sub, int nst) {
-    return ((size_t)nst * 4 * T + tile_fixed_doubles(T, nseg, sub)) * sizeof(double) +
-           (size_t)nst * (sizeof(uint64_t) + sizeof(int)) + 128;
+
+// Shared memory (doubles unless noted), T = SYS * NSC threads, SUB = SYS / CL,
+// RP = SYS + 1 (padded pitch of the exchange buffers):
+//   ring  NST * 4 * T             TMA stages (A, B, C, D, one row per sub-segment)
+//   red   6 * NSC * RP            this CTA's reduced rows (l0,u0,r0 | l1,u1,r1)
+//   xr    2 * NSC * RP            x_first / x_last of this CTA's sub-segments
+//   pcr   6 * (NSEG + 2) * SUB    PCR buffers, only when NSEG > 32
+//   bars  2 * NST mbarriers
+__host__ __device__ __forceinline__ size_t tile_fixed_doubles(int sys, int nsc, int nseg, int sub) {
+    size_t f = 8ull * nsc * (sys + 1);
+    if (nseg > 32) f += 6ull * (nseg + 2) * sub;
+    return f;
+}
+__host__ __device__ __forceinline__ size_t tile_smem_bytes(int sys, int nsc, int nseg, int sub,
+                                                           int nst) {
+    const size_t T = (size_t)sys * nsc;
+    return ((size_t)nst * 4 * T + tile_fixed_doubles(sys, nsc, nseg, sub)) * sizeof(double) +
+           2ull * nst * sizeof(uint64_t) + 128;
 }
 
 __device__ __forceinline__ void tma_load_3d(void* smem_dst, const CUtensorMap* map, int x, int y,
@@ -85,6 +98,10 @@ __device__ __forceinline__ void tma_load_3d(void* smem_dst, const CUtensorMap* m
         : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ __forceinline__ void tile_cluster_sync(int cl) {
     if (cl > 1) {
         asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
@@ -94,6 +111,18 @@ __device__ __forceinline__ void tile_cluster_sync(int cl) {
     }
 }
 
+// One PCR row update of  l x_{i-dl} + x_i + u x_{i+dl} = r  with its
+// neighbours (m: row i-dl, p: row i+dl).
+__device__ __forceinline__ void pcr_step(double& l, double& u, double& r, double lm, double um,
+                                         double rm, double lp, double up, double rp) {
+    const double ib = rcp_nr(1.0 - l * um - u * lp);
+    const double nl = -l * lm * ib;
+    const double nu = -u * up * ib;
+    r = (r - l * rm - u * rp) * ib;
+    l = nl;
+    u = nu;
+}
+
 template <int SYS, bool CYCLIC>
 __global__ void __launch_bounds__(TILE_MAX_THREADS, 1)
 tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -101,46 +130,45 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                 const TileArgs args) {
     namespace cg = cooperative_groups;
     constexpr int M = TILE_MT;
+    constexpr int RP = SYS + 1;  // padded pitch of red / xr rows
     extern __shared__ unsigned char smem_raw[];
     const int nseg = args.nseg, cl = args.cl, nst = args.nst;
     const int nsc = nseg / cl;   // sub-segments per CTA
     const int T = SYS * nsc;     // == blockDim.x
     const int sub = SYS / cl;    // systems whose reduced system this CTA solves
-    const int gs = nseg + 2;     // rows per field in gat / pcr (with guards)
+    const int W = tile_lanes(nseg);
+    const bool shuffled = W <= 32;
+    const int fstride = nsc * RP;  // field stride of red / xr
 
     double* ring = reinterpret_cast<double*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     double* red = ring + (size_t)nst * 4 * T;
-    double* gat = red + 6 * T;
-    double* pcr = gat + 6 * gs * sub;
-    double* xr = pcr + 6 * gs * sub;
-    uint64_t* full = reinterpret_cast<uint64_t*>(xr + 2 * T);
-    int* readers = reinterpret_cast<int*>(full + nst);
+    double* xr = red + 6 * fstride;
+    double* pcr = xr + 2 * fstride;  // only when !shuffled
+    const int gs = nseg + 2;
+    uint64_t* full = reinterpret_cast<uint64_t*>(pcr + (shuffled ? 0 : 6 * gs * sub));
+    uint64_t* empty = full + nst;
 
     const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int nwarps = (T + 31) / 32;
     const int c = cl > 1 ? (int)cg::this_cluster().block_rank() : 0;
     const int cluster_id = (int)blockIdx.x / cl;
     const int n_clusters = (int)gridDim.x / cl;
-    // forward / back-substitution mapping: system s, local sub-segment ql
-    const int s = tid % SYS;
+    const int s = tid % SYS;  // forward / back-substitution mapping
     const int ql = tid / SYS;
-    // reduced-system mapping: system sp (of this CTA's slice), global sub-segment p
-    const int sp = tid % sub;
-    const int p = tid / sub;
     const size_t ns = (size_t)args.n_sys;
-    const int nwarps = (T + 31) / 32;
 
     if (tid == 0) {
         for (int i = 0; i < nst; ++i) {
             mbar_init(&full[i], 1);
-            readers[i] = 0;
+            mbar_init(&empty[i], nwarps);
         }
         fence_mbar_init();
     }
-    if (tid < sub) {  // zero guard rows of gat and pcr (never written again)
+    if (!shuffled && tid < sub) {  // zero guard rows of the PCR buffers
         for (int f = 0; f < 6; ++f) {
-            gat[(f * gs + 0) * sub + tid] = 0.0;
-            gat[(f * gs + nseg + 1) * sub + tid] = 0.0;
             pcr[(f * gs + 0) * sub + tid] = 0.0;
             pcr[(f * gs + nseg + 1) * sub + tid] = 0.0;
         }
@@ -169,17 +197,13 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     if (tid == 0)
         for (int t = 0; t < nst && t < total; ++t) issue(t);
 
-    // gat / pcr accessors for this thread's reduced-system column (row -1 is
-    // the first guard row)
-    auto G = [&](int f, int row) -> double& { return gat[(f * gs + row + 1) * sub + sp]; };
-    auto PB = [&](int b, int f, int row) -> double& {
-        return pcr[((b * 3 + f) * gs + row + 1) * sub + sp];
-    };
-
-    bool finite = true;
-    int slot = 0;
-    uint32_t phase = 0;
+    double nonfinite = 0.0;  // becomes NaN if any solution entry is NaN or Inf
+    int slot = 0;            // ring slot of stage t
+    uint32_t phase = 0;      // its phase parity
+    int pslot = nst - 1;     // ring slot of stage t - 1
+    uint32_t pphase = 1;
     int t = 0;
+    int tw = 0;  // t % nwarps
     for (int it = 0; it < n_my; ++it) {
         const int g = cluster_id + it * n_clusters;
         const int sys = g * SYS + s;
@@ -194,17 +218,21 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             if (ok) ok = mbar_wait_bounded(&full[slot], phase, args.status);
             const double* st = ring + (size_t)slot * 4 * T + tid;
             const double a = st[0], b = st[T], cc = st[2 * T], d = st[3 * T];
-            // The last warp to finish reading the slot refills it with stage
-            // t + nst: the ring stays nst rows ahead of the slowest warp.
             __syncwarp();
-            if ((tid & 31) == 0) {
-                __threadfence_block();
-                if (atomicAdd(&readers[slot], 1) == nwarps - 1) {
-                    readers[slot] = 0;
-                    if (ok && t + nst < total) issue(t + nst);
+            if (lane == 0) {
+                mbar_arrive(&empty[slot]);
+                // Rotating producer: one row later, warp (t % nwarps) refills the
+                // slot of stage t - 1 with stage t - 1 + nst once every warp has
+                // released it.
+                if (t >= 1 && warp == tw && t - 1 + nst < total && ok) {
+                    ok = mbar_wait_bounded(&empty[pslot], pphase, args.status);
+                    if (ok) issue(t - 1 + nst);
                 }
             }
+            pslot = slot;
+            pphase = phase;
             ++t;
+            if (++tw == nwarps) tw = 0;
             if (++slot == nst) {
                 slot = 0;
                 phase ^= 1u;
@@ -237,52 +265,130 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         {
             const double pi_last = -ga[M - 2] * pi;
             const double r0 = rcp_nr(1.0 - cb0 * sa);
-            double* w = red + ql * SYS + s;
-            w[0 * T] = r0 * ab0;
-            w[1 * T] = r0 * cb0 * pi_last;  // -r c0 gamma''_1, gamma''_1 = -pi_{M-1}
-            w[2 * T] = r0 * (db0 - cb0 * sd);
-            w[3 * T] = al[M - 1];
-            w[4 * T] = ga[M - 1];
-            w[5 * T] = de[M - 1];
+            double* w = red + ql * RP + s;
+            w[0 * fstride] = r0 * ab0;
+            w[1 * fstride] = r0 * cb0 * pi_last;  // -r c0 gamma''_1, gamma''_1 = -pi_{M-1}
+            w[2 * fstride] = r0 * (db0 - cb0 * sd);
+            w[3 * fstride] = al[M - 1];
+            w[4 * fstride] = ga[M - 1];
+            w[5 * fstride] = de[M - 1];
         }
         tile_cluster_sync(cl);
 
-        // ------------------------------------- gather this CTA's reduced systems
-        {
+        // ------------------------------------------------------ reduced system
+        // Row notation for sub-segment p (of one system):
+        //   first: l0 xL(p-1) + xF(p) + u0 xL(p) = r0
+        //   last:  l1 xF(p) + xL(p) + u1 xF(p+1) = r1
+        // One cyclic-reduction level leaves  a xL(p-1) + xL(p) + c xL(p+1) = d.
+        if (shuffled) {
+            const int per_pass = T / W;  // systems per pass
+            const int p = tid % W;
+            for (int base = 0; base < sub; base += per_pass) {
+                const int sp = base + tid / W;
+                const bool act = sp < sub && p < nseg;
+                double l0 = 0, u0 = 0, r0 = 0, l1 = 0, u1 = 0, r1 = 0;
+                if (act) {
+                    const int owner = p / nsc;
+                    const double* src = red + (p % nsc) * RP + c * sub + sp;
+                    if (cl > 1 && owner != c) src = cg::this_cluster().map_shared_rank(src, owner);
+                    l0 = src[0 * fstride];
+                    u0 = src[1 * fstride];
+                    r0 = src[2 * fstride];
+                    l1 = src[3 * fstride];
+                    u1 = src[4 * fstride];
+                    r1 = src[5 * fstride];
+                }
+                // next sub-segment's first row (zero past the end unless periodic)
+                const int pn = (CYCLIC && p == nseg - 1) ? 0 : p + 1;
+                double l0n = __shfl_sync(0xffffffffu, l0, pn, W);
+                double u0n = __shfl_sync(0xffffffffu, u0, pn, W);
+                double r0n = __shfl_sync(0xffffffffu, r0, pn, W);
+                if (!CYCLIC && p + 1 >= nseg) l0n = u0n = r0n = 0.0;
+                double al_ = 0, cl_ = 0, dl_ = 0;
+                {
+                    const double ib = rcp_nr(1.0 - l1 * u0 - u1 * l0n);
+                    al_ = -l1 * l0 * ib;
+                    cl_ = -u1 * u0n * ib;
+                    dl_ = (r1 - l1 * r0 - u1 * r0n) * ib;
+                }
+                if (!act) al_ = cl_ = dl_ = 0.0;
+                double xl;
+                if (CYCLIC && nseg == 1) {
+                    xl = dl_ * rcp_nr(1.0 + al_ + cl_);
+                } else {
+                    bool solved = false;
+                    xl = 0.0;
+                    for (int dl = 1; dl < nseg; dl <<= 1) {
+                        int im = p - dl, ip = p + dl;
+                        if (CYCLIC) {
+                            im = im < 0 ? im + nseg : im;
+                            ip = ip >= nseg ? ip - nseg : ip;
+                        }
+                        double lm = __shfl_sync(0xffffffffu, al_, im & (W - 1), W);
+                        double um = __shfl_sync(0xffffffffu, cl_, im & (W - 1), W);
+                        double rm = __shfl_sync(0xffffffffu, dl_, im & (W - 1), W);
+                        double lp = __shfl_sync(0xffffffffu, al_, ip & (W - 1), W);
+                        double up = __shfl_sync(0xffffffffu, cl_, ip & (W - 1), W);
+                        double rp = __shfl_sync(0xffffffffu, dl_, ip & (W - 1), W);
+                        if (!CYCLIC) {
+                            if (im < 0) lm = um = rm = 0.0;
+                            if (ip >= nseg) lp = up = rp = 0.0;
+                        }
+                        if (CYCLIC && 2 * dl == nseg) {
+                            // p-dl and p+dl are the same row j: 2x2 system in x_p, x_j
+                            const double si = al_ + cl_, sj = lm + um;
+                            xl = (dl_ - si * rm) * rcp_nr(1.0 - si * sj);
+                            solved = true;
+                        } else {
+                            pcr_step(al_, cl_, dl_, lm, um, rm, lp, up, rp);
+                        }
+                    }
+                    if (!solved) xl = dl_;
+                }
+                // x_first(p) = r0 - l0 xL(p-1) - u0 xL(p)
+                const int pm = (CYCLIC && p == 0) ? nseg - 1 : p - 1;
+                double xlm = __shfl_sync(0xffffffffu, xl, pm & (W - 1), W);
+                if (!CYCLIC && p == 0) xlm = 0.0;
+                const double xf = r0 - l0 * xlm - u0 * xl;
+                if (act) {
+                    const int owner = p / nsc;
+                    double* dst = xr + (p % nsc) * RP + c * sub + sp;
+                    if (cl > 1 && owner != c) dst = cg::this_cluster().map_shared_rank(dst, owner);
+                    dst[0] = xf;
+                    dst[fstride] = xl;
+                }
+            }
+        } else {
+            // NSEG > 32: the same steps through shared memory, one row per thread.
+            const int sp = tid % sub;
+            const int p = tid / sub;
+            auto PB = [&](int b, int f, int row) -> double& {
+                return pcr[((b * 3 + f) * gs + row + 1) * sub + sp];
+            };
             const int owner = p / nsc;
-            const double* src = red + (p % nsc) * SYS + c * sub + sp;
+            const double* src = red + (p % nsc) * RP + c * sub + sp;
             if (cl > 1 && owner != c) src = cg::this_cluster().map_shared_rank(src, owner);
-#pragma unroll
-            for (int f = 0; f < 6; ++f) G(f, p) = src[f * T];
-        }
-        __syncthreads();
-
-        // ------------- one cyclic-reduction level: eliminate the first-row unknowns
-        // first row of p:  l0 xL(p-1) + xF(p) + u0 xL(p) = r0
-        // last row of p:   l1 xF(p) + xL(p) + u1 xF(p+1) = r1
-        const double l0 = G(0, p), u0 = G(1, p), r0 = G(2, p);
-        {
-            const double l1 = G(3, p), u1 = G(4, p), r1 = G(5, p);
+            const double l0 = src[0 * fstride], u0 = src[1 * fstride], r0 = src[2 * fstride];
+            const double l1 = src[3 * fstride], u1 = src[4 * fstride], r1 = src[5 * fstride];
+            // publish the first rows for the neighbour (field 0..2 of buffer 1)
+            PB(1, 0, p) = l0;
+            PB(1, 1, p) = u0;
+            PB(1, 2, p) = r0;
+            __syncthreads();
             int pn = p + 1;
             if (CYCLIC && pn == nseg) pn = 0;
-            const double l0n = G(0, pn), u0n = G(1, pn), r0n = G(2, pn);
-            const double ib = rcp_nr(1.0 - l1 * u0 - u1 * l0n);
-            PB(0, 0, p) = -l1 * l0 * ib;
-            PB(0, 1, p) = -u1 * u0n * ib;
-            PB(0, 2, p) = (r1 - l1 * r0 - u1 * r0n) * ib;
-        }
-        __syncthreads();
-
-        // ------------------------- PCR on the last-row unknowns (one row/thread)
-        int cur = 0;
-        double xl;
-        if (CYCLIC && nseg == 1) {
-            xl = PB(0, 2, 0) * rcp_nr(1.0 + PB(0, 0, 0) + PB(0, 1, 0));
-        } else {
+            const double l0n = PB(1, 0, pn), u0n = PB(1, 1, pn), r0n = PB(1, 2, pn);
+            {
+                const double ib = rcp_nr(1.0 - l1 * u0 - u1 * l0n);
+                PB(0, 0, p) = -l1 * l0 * ib;
+                PB(0, 1, p) = -u1 * u0n * ib;
+                PB(0, 2, p) = (r1 - l1 * r0 - u1 * r0n) * ib;
+            }
+            __syncthreads();
+            int cur = 0;
+            double xl = 0.0;
             bool solved = false;
-            xl = 0.0;
             for (int dl = 1; dl < nseg; dl <<= 1) {
-                const bool last_cyclic = CYCLIC && 2 * dl == nseg;
                 int im = p - dl, ip = p + dl;
                 if (CYCLIC) {
                     im = im < 0 ? im + nseg : im;
@@ -291,48 +397,43 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                     im = im < -1 ? -1 : im;
                     ip = ip > nseg ? nseg : ip;
                 }
-                const double li = PB(cur, 0, p), ui = PB(cur, 1, p), ri = PB(cur, 2, p);
+                double li = PB(cur, 0, p), ui = PB(cur, 1, p), ri = PB(cur, 2, p);
                 const double lm = PB(cur, 0, im), um = PB(cur, 1, im), rm = PB(cur, 2, im);
                 const double lp = PB(cur, 0, ip), up = PB(cur, 1, ip), rp = PB(cur, 2, ip);
                 const int nxt = cur ^ 1;
-                if (last_cyclic) {
-                    // p-dl and p+dl are the same row j: 2x2 system in x_p, x_j
+                if (CYCLIC && 2 * dl == nseg) {
                     const double si = li + ui, sj = lm + um;
                     xl = (ri - si * rm) * rcp_nr(1.0 - si * sj);
                     solved = true;
                 } else {
-                    const double ib = rcp_nr(1.0 - li * um - ui * lp);
-                    PB(nxt, 0, p) = -li * lm * ib;
-                    PB(nxt, 1, p) = -ui * up * ib;
-                    PB(nxt, 2, p) = (ri - li * rm - ui * rp) * ib;
+                    pcr_step(li, ui, ri, lm, um, rm, lp, up, rp);
+                    PB(nxt, 0, p) = li;
+                    PB(nxt, 1, p) = ui;
+                    PB(nxt, 2, p) = ri;
                 }
                 __syncthreads();
                 cur = nxt;
             }
             if (!solved) xl = PB(cur, 2, p);
-        }
-        // publish x_last, then recover x_first(p) = r0 - l0 xL(p-1) - u0 xL(p)
-        PB(cur ^ 1, 2, p) = xl;
-        __syncthreads();
-        const int pm = p - 1;
-        double xlm;
-        if (CYCLIC)
-            xlm = PB(cur ^ 1, 2, pm < 0 ? nseg - 1 : pm);
-        else
-            xlm = pm < 0 ? 0.0 : PB(cur ^ 1, 2, pm);
-        const double xf = r0 - l0 * xlm - u0 * xl;
-        {
-            const int owner = p / nsc;
-            double* dst = xr + (p % nsc) * SYS + c * sub + sp;
+            PB(cur ^ 1, 2, p) = xl;
+            __syncthreads();
+            const int pm = p - 1;
+            double xlm;
+            if (CYCLIC)
+                xlm = PB(cur ^ 1, 2, pm < 0 ? nseg - 1 : pm);
+            else
+                xlm = pm < 0 ? 0.0 : PB(cur ^ 1, 2, pm);
+            const double xf = r0 - l0 * xlm - u0 * xl;
+            double* dst = xr + (p % nsc) * RP + c * sub + sp;
             if (cl > 1 && owner != c) dst = cg::this_cluster().map_shared_rank(dst, owner);
             dst[0] = xf;
-            dst[T] = xl;
+            dst[fstride] = xl;
         }
         tile_cluster_sync(cl);
 
         // --------------------------------------------------- back substitution
-        const double x_first = xr[ql * SYS + s];
-        const double x_last = xr[T + ql * SYS + s];
+        const double x_first = xr[ql * RP + s];
+        const double x_last = xr[fstride + ql * RP + s];
         if (valid) {
             const int q = c * nsc + ql;
             double* xp = args.X + (size_t)(q * M) * ns + sys;
@@ -341,14 +442,14 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 #pragma unroll
             for (int k = M - 2; k >= 1; --k) {
                 xn = de[k] - al[k] * x_first - ga[k] * xn;
-                finite &= isfinite(xn);
+                nonfinite = fma(xn, 0.0, nonfinite);
                 xp[(size_t)k * ns] = xn;
             }
             xp[0] = x_first;
-            finite &= isfinite(x_first) && isfinite(x_last);
+            nonfinite = fma(x_first, 0.0, fma(x_last, 0.0, nonfinite));
         }
     }
-    if (!finite) raise_status(args.status, ST_NONFINITE);
+    if (nonfinite != 0.0) raise_status(args.status, ST_NONFINITE);  // NaN != 0
     if (!ok && tid == 0) {
         // a wait gave up: give in-flight copies a bounded chance to land before
         // the CTA exits
