@@ -182,10 +182,16 @@ TilePlan tile_plan(int n_row, bool cyclic) {
     } else if (nseg <= 8) {
         sys = 64;
         cl = 1;
-    } else {
+    } else if (nseg <= 16) {
         sys = 32;
+        cl = 1;
+    } else {
+        // One CTA up to 32 sub-segments (a 2-CTA cluster with 256-byte boxes
+        // measured slower than one CTA with 128-byte boxes); longer systems split
+        // over the smallest cluster that keeps <= 32 sub-segments per CTA.
+        sys = 16;
         for (int c = 1; c <= 16; c <<= 1)
-            if (nseg % c == 0 && nseg / c <= 16) {
+            if (nseg % c == 0 && nseg / c <= 32) {
                 cl = c;
                 break;
             }
@@ -269,8 +275,10 @@ int try_tile(const double* A, const double* B, const double* C, const double* D,
         case 257: rc = launch_tile_sys<128, true>(maps, a, st); break;
         case 128: rc = launch_tile_sys<64, false>(maps, a, st); break;
         case 129: rc = launch_tile_sys<64, true>(maps, a, st); break;
+        case 64: rc = launch_tile_sys<32, false>(maps, a, st); break;
         case 65: rc = launch_tile_sys<32, true>(maps, a, st); break;
-        default: rc = launch_tile_sys<32, false>(maps, a, st); break;
+        case 33: rc = launch_tile_sys<16, true>(maps, a, st); break;
+        default: rc = launch_tile_sys<16, false>(maps, a, st); break;
     }
     return rc == BTDMA_OK ? 1 : rc;
 }
