@@ -24,7 +24,9 @@ EXPORTS = (
     "btdma_create", "btdma_destroy", "btdma_solve", "btdma_solve_cyclic", "btdma_solve_out",
     "btdma_set_eps_constant", "btdma_set_rho", "btdma_set_rho_all", "btdma_last_J",
     "btdma_status", "btdma_set_method", "btdma_segments", "btdma_last_error",
+    "btdma_solve_noalloc",
 )
+NOALLOC_MAX_ELEMS = 1 << 20
 
 
 class BtdmaError(RuntimeError):
@@ -57,6 +59,7 @@ def lib():
         L.btdma_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint)]
         L.btdma_set_method.argtypes = [vp, i]
         L.btdma_segments.argtypes = [vp, ctypes.POINTER(i)]
+        L.btdma_solve_noalloc.argtypes = [vp, vp, vp, vp, i, i, vp]
         L.btdma_last_error.restype = ctypes.c_char_p
         for name in EXPORTS:
             if name != "btdma_last_error":

@@ -549,3 +549,55 @@ int btdma_segments(btdma_t h, int* P) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free serial Thomas (btdma_solve_noalloc).  The forward sweep's c'
+// goes to this fixed device array instead of handle-owned scratch.  Host code
+// may not pass the array's name to a kernel (on the host it is only a
+// stand-in symbol), so its device address is looked up once per device with
+// that device current and cached here.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) double g_noalloc_scratch[BTDMA_NOALLOC_MAX_ELEMS];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[kMaxDevices] = {};
+
+int noalloc_scratch(double** out) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(BTDMA_ERR_UNSUPPORTED, "device %d", dev);
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return BTDMA_OK;
+}
+
+}  // namespace
+
+extern "C" int btdma_solve_noalloc(const double* A, const double* B, const double* C, double* D,
+                                   int n_sys, int n_row, cudaStream_t stream) {
+    if (!A || !B || !C || !D) return fail(BTDMA_ERR_ARG, "null array");
+    if (n_sys <= 0 || n_row <= 0) return fail(BTDMA_ERR_ARG, "n_sys and n_row must be positive");
+    if ((long long)n_sys * n_row > (long long)BTDMA_NOALLOC_MAX_ELEMS)
+        return fail(BTDMA_ERR_SIZE,
+                    "n_sys * n_row = %lld exceeds the allocation-free limit of %d elements",
+                    (long long)n_sys * n_row, BTDMA_NOALLOC_MAX_ELEMS);
+    double* scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    // c' is written before it is read by the same thread, so the scratch needs
+    // no clearing between calls.
+    const int grid = (n_sys + THOMAS_BLOCK - 1) / THOMAS_BLOCK;
+    thomas_f64_kernel<<<grid, THOMAS_BLOCK, 0, stream>>>(A, B, C, D, D, scratch, n_sys, n_row,
+                                                         nullptr);
+    CK(cudaGetLastError());
+    return BTDMA_OK;
+}
+

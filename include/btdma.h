@@ -150,6 +150,26 @@ int btdma_set_method(btdma_t h, int method);
 /* Segments per system used by the handle (after the P = 0 choice). */
 int btdma_segments(btdma_t h, int* P);
 
+/* Serial Thomas solve (D <- x, bit-identical to btdma_solve with P = 1) that
+ * allocates nothing.  No counterpart in the reference.
+ *
+ * For callers that must not allocate device memory: code running under a
+ * framework that owns the GPU memory pool, loops that cannot afford an
+ * allocation's latency or its implicit synchronisation, and places where
+ * CUDA's allocation calls are not allowed at all.  There is no handle; the
+ * elimination scratch is a fixed array inside the library, BTDMA_NOALLOC_MAX_ELEMS
+ * doubles (8 MiB) that every GPU loading the library keeps until the process
+ * exits.  Batches with n_sys * n_row above that return BTDMA_ERR_SIZE.
+ *
+ * The first call on a device looks up the array's device address (make it
+ * before any stream capture).  All calls share the one array and leave their
+ * scratch in it, so calls that overlap on the GPU (other streams, other host
+ * threads) race with each other: order them on one stream.  A, B, C are
+ * unchanged; no device status word is kept. */
+#define BTDMA_NOALLOC_MAX_ELEMS (1 << 20)
+int btdma_solve_noalloc(const double* A, const double* B, const double* C, double* D,
+                        int n_sys, int n_row, cudaStream_t stream);
+
 /* Message of the most recent failing call on this thread. */
 const char* btdma_last_error(void);
 
