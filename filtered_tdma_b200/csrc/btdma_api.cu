@@ -140,14 +140,14 @@ int launch_seg(const CUtensorMap* maps, const SegArgs& a, int groups, cudaStream
 }
 
 // 3-D view [nseg][TILE_MT][n_sys] of an [n_row x n_sys] FP64 array; boxes of
-// one row of `nsc` consecutive sub-segments for `sys` systems.
+// TILE_RPS rows of `nsc` consecutive sub-segments for `sys` systems.
 bool make_tile_map(CUtensorMap* map, const void* ptr, int n_sys, int nseg, int sys, int nsc) {
     auto fn = encode_fn();
     if (!fn) return false;
     cuuint64_t dims[3] = {(cuuint64_t)n_sys, (cuuint64_t)TILE_MT, (cuuint64_t)nseg};
     cuuint64_t strides[2] = {(cuuint64_t)n_sys * sizeof(double),
                              (cuuint64_t)n_sys * TILE_MT * sizeof(double)};
-    cuuint32_t box[3] = {(cuuint32_t)sys, 1, (cuuint32_t)nsc};
+    cuuint32_t box[3] = {(cuuint32_t)sys, (cuuint32_t)TILE_RPS, (cuuint32_t)nsc};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(ptr), dims, strides,
                     box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,

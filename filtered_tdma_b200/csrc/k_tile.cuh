@@ -7,10 +7,10 @@
 // (CL = 1 for short systems), NSC = NSEG / CL sub-segments per CTA, SYS * NSC
 // <= 512 threads.  Persistent clusters walk over the groups:
 //
-//   1. Forward pass (one row of every local sub-segment per step).  Row k of the
-//      CTA's NSC sub-segments of SYS systems arrives in one TMA box of a 3-D view
-//      [NSEG][TILE_MT][n_sys] (SYS * 8 bytes wide, 256 B for SYS = 32) through
-//      an NST-stage shared-memory ring.  Each stage has a "full" mbarrier (TMA
+//   1. Forward pass (TILE_RPS = 2 rows of every local sub-segment per step).
+//      Rows k, k+1 of the CTA's NSC sub-segments of SYS systems arrive in one TMA
+//      box of a 3-D view [NSEG][TILE_MT][n_sys] (SYS * 8 bytes wide) through an
+//      NST-stage shared-memory ring.  Each stage has a "full" mbarrier (TMA
 //      transaction count) and an "empty" mbarrier (one arrival per warp); the
 //      refill of a stage is issued one row later by a rotating producer warp, so
 //      no warp waits for the others on the critical path and the next group's
@@ -51,8 +51,10 @@
 namespace btdma {
 
 constexpr int TILE_MT = 16;           // rows per sub-segment (per thread)
+constexpr int TILE_RPS = 2;           // rows per ring stage
+constexpr int TILE_SPG = TILE_MT / TILE_RPS;  // stages per group
 constexpr int TILE_MAX_THREADS = 512;
-constexpr int TILE_MAX_NST = 12;      // ring stages (upper bound)
+constexpr int TILE_MAX_NST = 8;       // ring stages (upper bound)
 
 struct TileArgs {
     double* X;
@@ -72,7 +74,7 @@ __host__ __device__ __forceinline__ int tile_lanes(int nseg) {
 
 // Shared memory (doubles unless noted), T = SYS * NSC threads, SUB = SYS / CL,
 // RP = SYS + 1 (padded pitch of the exchange buffers):
-//   ring  NST * 4 * T             TMA stages (A, B, C, D, one row per sub-segment)
+//   ring  NST * 4 * RPS * T       TMA stages (A, B, C, D; RPS rows per sub-segment)
 //   red   6 * NSC * RP            this CTA's reduced rows (l0,u0,r0 | l1,u1,r1)
 //   xr    2 * NSC * RP            x_first / x_last of this CTA's sub-segments
 //   pcr   6 * (NSEG + 2) * SUB    PCR buffers, only when NSEG > 32
@@ -85,7 +87,8 @@ __host__ __device__ __forceinline__ size_t tile_fixed_doubles(int sys, int nsc, 
 __host__ __device__ __forceinline__ size_t tile_smem_bytes(int sys, int nsc, int nseg, int sub,
                                                            int nst) {
     const size_t T = (size_t)sys * nsc;
-    return ((size_t)nst * 4 * T + tile_fixed_doubles(sys, nsc, nseg, sub)) * sizeof(double) +
+    return ((size_t)nst * 4 * TILE_RPS * T + tile_fixed_doubles(sys, nsc, nseg, sub)) *
+               sizeof(double) +
            2ull * nst * sizeof(uint64_t) + 128;
 }
 
@@ -142,7 +145,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 
     double* ring = reinterpret_cast<double*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-    double* red = ring + (size_t)nst * 4 * T;
+    double* red = ring + (size_t)nst * 4 * TILE_RPS * T;
     double* xr = red + 6 * fstride;
     double* pcr = xr + 2 * fstride;  // only when !shuffled
     const int gs = nseg + 2;
@@ -179,23 +182,28 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     const int n_my = args.n_groups > cluster_id
                          ? (args.n_groups - cluster_id + n_clusters - 1) / n_clusters
                          : 0;
-    const int total = n_my * M;
-    const uint32_t stage_bytes = 4u * T * sizeof(double);
+    const int total = n_my * TILE_SPG;  // ring stages this CTA consumes
+    const int sstride = 4 * TILE_RPS * T;  // doubles per stage
+    const uint32_t stage_bytes = (uint32_t)sstride * sizeof(double);
 
     auto issue = [&](int t) {  // one thread
         const int slot = t % nst;
-        const int g = cluster_id + (t / M) * n_clusters;
-        const int k = t % M;
-        double* dst = ring + (size_t)slot * 4 * T;
+        const int g = cluster_id + (t / TILE_SPG) * n_clusters;
+        const int k0 = (t % TILE_SPG) * TILE_RPS;
+        double* dst = ring + (size_t)slot * sstride;
         mbar_expect_tx(&full[slot], stage_bytes);
-        tma_load_3d(dst + 0 * T, &tmA, g * SYS, k, c * nsc, &full[slot]);
-        tma_load_3d(dst + 1 * T, &tmB, g * SYS, k, c * nsc, &full[slot]);
-        tma_load_3d(dst + 2 * T, &tmC, g * SYS, k, c * nsc, &full[slot]);
-        tma_load_3d(dst + 3 * T, &tmD, g * SYS, k, c * nsc, &full[slot]);
+        tma_load_3d(dst + 0 * TILE_RPS * T, &tmA, g * SYS, k0, c * nsc, &full[slot]);
+        tma_load_3d(dst + 1 * TILE_RPS * T, &tmB, g * SYS, k0, c * nsc, &full[slot]);
+        tma_load_3d(dst + 2 * TILE_RPS * T, &tmC, g * SYS, k0, c * nsc, &full[slot]);
+        tma_load_3d(dst + 3 * TILE_RPS * T, &tmD, g * SYS, k0, c * nsc, &full[slot]);
     };
     bool ok = true;
     if (tid == 0)
         for (int t = 0; t < nst && t < total; ++t) issue(t);
+
+    // this thread's element of a stage: array f, row r at st + f*RPS*T + r*SYS
+    const int toff = ql * TILE_RPS * SYS + s;
+    const double* st = ring + toff;  // stage t, this thread's column
 
     double nonfinite = 0.0;  // becomes NaN if any solution entry is NaN or Inf
     int slot = 0;            // ring slot of stage t
@@ -214,16 +222,22 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         double ab0 = 0, cb0 = 0, db0 = 0;
         double pi = 1.0, sa = 0.0, sd = 0.0;
 #pragma unroll
-        for (int k = 0; k < M; ++k) {
+        for (int j = 0; j < TILE_SPG; ++j) {
             if (ok) ok = mbar_wait_bounded(&full[slot], phase, args.status);
-            const double* st = ring + (size_t)slot * 4 * T + tid;
-            const double a = st[0], b = st[T], cc = st[2 * T], d = st[3 * T];
+            double a2[TILE_RPS], b2[TILE_RPS], c2[TILE_RPS], d2[TILE_RPS];
+#pragma unroll
+            for (int r = 0; r < TILE_RPS; ++r) {
+                a2[r] = st[0 * TILE_RPS * T + r * SYS];
+                b2[r] = st[1 * TILE_RPS * T + r * SYS];
+                c2[r] = st[2 * TILE_RPS * T + r * SYS];
+                d2[r] = st[3 * TILE_RPS * T + r * SYS];
+            }
             __syncwarp();
             if (lane == 0) {
                 mbar_arrive(&empty[slot]);
-                // Rotating producer: one row later, warp (t % nwarps) refills the
-                // slot of stage t - 1 with stage t - 1 + nst once every warp has
-                // released it.
+                // Rotating producer: one stage later, warp (t % nwarps) refills
+                // the slot of stage t - 1 with stage t - 1 + nst once every warp
+                // has released it.
                 if (t >= 1 && warp == tw && t - 1 + nst < total && ok) {
                     ok = mbar_wait_bounded(&empty[pslot], pphase, args.status);
                     if (ok) issue(t - 1 + nst);
@@ -233,31 +247,38 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             pphase = phase;
             ++t;
             if (++tw == nwarps) tw = 0;
+            st += sstride;
             if (++slot == nst) {
                 slot = 0;
                 phase ^= 1u;
+                st = ring + toff;
             }
-            if (k == 0) {
-                const double ib = rcp_nr(b);
-                ab0 = a * ib;
-                cb0 = cc * ib;
-                db0 = d * ib;
-            } else if (k == 1) {
-                const double ib = rcp_nr(b);
-                al[1] = a * ib;
-                ga[1] = cc * ib;
-                de[1] = d * ib;
-                sa = al[1];
-                sd = de[1];
-            } else {
-                const double inv = rcp_nr(b - a * ga[k - 1]);
-                ga[k] = cc * inv;
-                de[k] = (d - a * de[k - 1]) * inv;
-                al[k] = -a * al[k - 1] * inv;
-                if (k <= M - 2) {
-                    pi = -ga[k - 1] * pi;
-                    sa += pi * al[k];
-                    sd += pi * de[k];
+#pragma unroll
+            for (int r = 0; r < TILE_RPS; ++r) {
+                const int k = j * TILE_RPS + r;
+                const double a = a2[r], b = b2[r], cc = c2[r], d = d2[r];
+                if (k == 0) {
+                    const double ib = rcp_nr(b);
+                    ab0 = a * ib;
+                    cb0 = cc * ib;
+                    db0 = d * ib;
+                } else if (k == 1) {
+                    const double ib = rcp_nr(b);
+                    al[1] = a * ib;
+                    ga[1] = cc * ib;
+                    de[1] = d * ib;
+                    sa = al[1];
+                    sd = de[1];
+                } else {
+                    const double inv = rcp_nr(b - a * ga[k - 1]);
+                    ga[k] = cc * inv;
+                    de[k] = (d - a * de[k - 1]) * inv;
+                    al[k] = -a * al[k - 1] * inv;
+                    if (k <= M - 2) {
+                        pi = -ga[k - 1] * pi;
+                        sa += pi * al[k];
+                        sd += pi * de[k];
+                    }
                 }
             }
         }
@@ -436,16 +457,18 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         const double x_last = xr[fstride + ql * RP + s];
         if (valid) {
             const int q = c * nsc + ql;
-            double* xp = args.X + (size_t)(q * M) * ns + sys;
-            xp[(size_t)(M - 1) * ns] = x_last;
+            double* xp = args.X + (size_t)(q * M + M - 1) * ns + sys;  // row M-1
+            *xp = x_last;
             double xn = x_last;
 #pragma unroll
             for (int k = M - 2; k >= 1; --k) {
+                xp -= ns;
                 xn = de[k] - al[k] * x_first - ga[k] * xn;
                 nonfinite = fma(xn, 0.0, nonfinite);
-                xp[(size_t)k * ns] = xn;
+                *xp = xn;
             }
-            xp[0] = x_first;
+            xp -= ns;
+            *xp = x_first;
             nonfinite = fma(x_first, 0.0, fma(x_last, 0.0, nonfinite));
         }
     }
