@@ -281,6 +281,43 @@ def main():
                 variants[name]["J"] = s.last_J()
             s.close()
 
+        # FP32 storage (A, B, C, D as float, x as double): 24 B/row
+        from filtered_tdma_b200 import _lib as L
+        A32, B32, C32, D32 = [t.to(torch.float32) for t in (A, B, C, D)]
+        for name, prec in (("fp32_store_P8", L.FP32_STORE),):
+            s = Solver("pascal", N_SYS, N_ROW, P, precision=prec)
+            stream = torch.cuda.current_stream().cuda_stream
+
+            def run_f32():
+                L.check(L.lib().btdma_solve_f32(s._h, A32.data_ptr(), B32.data_ptr(),
+                                                C32.data_ptr(), D32.data_ptr(), X.data_ptr(),
+                                                N_SYS, N_ROW, 0, stream))
+            for _ in range(3):
+                run_f32()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            nrep = max(3, args.steps // 2)
+            e0.record()
+            for _ in range(nrep):
+                run_f32()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / nrep
+            # accuracy against the FP64 solve of the widened values (device, P=1 Thomas)
+            Xr = torch.empty_like(X)
+            ref = Solver("pascal", N_SYS, N_ROW, 1)
+            ref.solve_out(A32.double(), B32.double(), C32.double(), D32.double(), Xr)
+            run_f32()
+            err = ((X - Xr).abs().max() / Xr.abs().max()).item()
+            ref.close()
+            variants[name] = {"rows_per_s": rows / (ms * 1e-3), "ms_per_step": ms,
+                              "hbm_gbs_algorithmic": gbps(ms, 24),
+                              "frac_of_peak": gbps(ms, 24) / peak,
+                              "speedup_vs_fp64_value": (rows / (ms * 1e-3)) / (rows / (ms_step * 1e-3)),
+                              "max_rel_err_vs_fp64_thomas": err, "refinement_sweeps": 0}
+            s.close()
+        del A32, B32, C32, D32
+
     # ---------------------------------------------------------- end to end
     e2e = None
     if not args.no_e2e:

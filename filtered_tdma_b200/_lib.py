@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(_PKG, "libbtdma.so")
 
 # enums of include/btdma.h
 PASCAL, FILTERED_V1, FILTERED_V2 = 0, 1, 2
-FP64, FP32_REFINE = 0, 1
+FP64, FP32_REFINE, FP32_STORE = 0, 1, 2
 FLAG_J_HOST = 1
 FLAG_REFERENCE_ORDER = 2
 OK, ERR_ARG, ERR_SEGMENT, ERR_CUDA, ERR_SIZE, ERR_UNSUPPORTED, ERR_DEVICE = 0, -1, -2, -3, -4, -5, -6
@@ -24,7 +24,7 @@ EXPORTS = (
     "btdma_create", "btdma_destroy", "btdma_solve", "btdma_solve_cyclic", "btdma_solve_out",
     "btdma_set_eps_constant", "btdma_set_rho", "btdma_set_rho_all", "btdma_last_J",
     "btdma_status", "btdma_set_method", "btdma_segments", "btdma_last_error",
-    "btdma_solve_noalloc",
+    "btdma_solve_noalloc", "btdma_solve_f32",
 )
 NOALLOC_MAX_ELEMS = 1 << 20
 
@@ -60,6 +60,7 @@ def lib():
         L.btdma_set_method.argtypes = [vp, i]
         L.btdma_segments.argtypes = [vp, ctypes.POINTER(i)]
         L.btdma_solve_noalloc.argtypes = [vp, vp, vp, vp, i, i, vp]
+        L.btdma_solve_f32.argtypes = [vp, vp, vp, vp, vp, vp, i, i, i, vp]
         L.btdma_last_error.restype = ctypes.c_char_p
         for name in EXPORTS:
             if name != "btdma_last_error":

@@ -141,15 +141,16 @@ int launch_seg(const CUtensorMap* maps, const SegArgs& a, int groups, cudaStream
 
 // 3-D view [nseg][TILE_MT][n_sys] of an [n_row x n_sys] FP64 array; boxes of
 // TILE_RPS rows of `nsc` consecutive sub-segments for `sys` systems.
-bool make_tile_map(CUtensorMap* map, const void* ptr, int n_sys, int nseg, int sys, int nsc) {
+bool make_tile_map(CUtensorMap* map, const void* ptr, int n_sys, int nseg, int sys, int nsc,
+                   int elem = 8) {
     auto fn = encode_fn();
     if (!fn) return false;
     cuuint64_t dims[3] = {(cuuint64_t)n_sys, (cuuint64_t)TILE_MT, (cuuint64_t)nseg};
-    cuuint64_t strides[2] = {(cuuint64_t)n_sys * sizeof(double),
-                             (cuuint64_t)n_sys * TILE_MT * sizeof(double)};
+    cuuint64_t strides[2] = {(cuuint64_t)n_sys * elem, (cuuint64_t)n_sys * TILE_MT * elem};
     cuuint32_t box[3] = {(cuuint32_t)sys, (cuuint32_t)TILE_RPS, (cuuint32_t)nsc};
     cuuint32_t estr[3] = {1, 1, 1};
-    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(ptr), dims, strides,
+    CUresult r = fn(map, elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                    3, const_cast<void*>(ptr), dims, strides,
                     box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
@@ -170,7 +171,7 @@ struct TilePlan {
     int sys = 0, cl = 0, nst = 0, nseg = 0;
 };
 
-TilePlan tile_plan(int n_row, bool cyclic) {
+TilePlan tile_plan(int n_row, bool cyclic, int elem = 8) {
     TilePlan pl;
     if (n_row % TILE_MT != 0) return pl;
     const int nseg = n_row / TILE_MT;
@@ -197,8 +198,9 @@ TilePlan tile_plan(int n_row, bool cyclic) {
             }
         if (cl == 0) return pl;
     }
-    int nst = TILE_MAX_NST;
-    while (nst >= 3 && tile_smem_bytes(sys, nseg / cl, nseg, sys / cl, nst) > (size_t)max_smem_optin())
+    int nst = elem == 8 ? TILE_MAX_NST : 2 * TILE_MAX_NST;
+    while (nst >= 3 &&
+           tile_smem_bytes(sys, nseg / cl, nseg, sys / cl, nst, elem) > (size_t)max_smem_optin())
         --nst;
     if (nst < 3) return pl;
     pl.sys = sys;
@@ -208,9 +210,9 @@ TilePlan tile_plan(int n_row, bool cyclic) {
     return pl;
 }
 
-template <int SYS, bool CYCLIC>
+template <int SYS, bool CYCLIC, typename TIN = double>
 int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st) {
-    auto kern = tile_f64_kernel<SYS, CYCLIC>;
+    auto kern = tile_f64_kernel<SYS, CYCLIC, TIN>;
     static bool attr_done = false;
     if (!attr_done) {
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -221,7 +223,8 @@ int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st)
     const int threads = SYS * a.nseg / a.cl;
     cudaLaunchConfig_t cfg = {};
     cfg.blockDim = dim3(threads, 1, 1);
-    cfg.dynamicSmemBytes = tile_smem_bytes(SYS, a.nseg / a.cl, a.nseg, SYS / a.cl, a.nst);
+    cfg.dynamicSmemBytes =
+        tile_smem_bytes(SYS, a.nseg / a.cl, a.nseg, SYS / a.cl, a.nst, (int)sizeof(TIN));
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -245,20 +248,42 @@ int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st)
     return BTDMA_OK;
 }
 
+template <typename TIN>
+int launch_tile_plan(const TilePlan& pl, const CUtensorMap* maps, const TileArgs& a, bool cyclic,
+                     cudaStream_t st) {
+    switch (pl.sys * 2 + (cyclic ? 1 : 0)) {
+        case 256: return launch_tile_sys<128, false, TIN>(maps, a, st);
+        case 257: return launch_tile_sys<128, true, TIN>(maps, a, st);
+        case 128: return launch_tile_sys<64, false, TIN>(maps, a, st);
+        case 129: return launch_tile_sys<64, true, TIN>(maps, a, st);
+        case 64: return launch_tile_sys<32, false, TIN>(maps, a, st);
+        case 65: return launch_tile_sys<32, true, TIN>(maps, a, st);
+        case 33: return launch_tile_sys<16, true, TIN>(maps, a, st);
+        default: return launch_tile_sys<16, false, TIN>(maps, a, st);
+    }
+}
+
+bool tma_ok_elem(const void* p, int n_sys, int elem) {
+    return ((reinterpret_cast<uintptr_t>(p) & 15) == 0) && ((size_t)n_sys * elem) % 16 == 0;
+}
+
 // Returns 1 when the tiled kernel was launched, 0 when the shape needs the
 // cluster-per-segment kernel, < 0 on error.
-int try_tile(const double* A, const double* B, const double* C, const double* D, double* X,
-             int n_sys, int n_row, bool cyclic, unsigned* status, cudaStream_t st) {
-    const TilePlan pl = tile_plan(n_row, cyclic);
+template <typename TIN>
+int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, int n_sys,
+             int n_row, bool cyclic, unsigned* status, cudaStream_t st) {
+    const int elem = (int)sizeof(TIN);
+    const TilePlan pl = tile_plan(n_row, cyclic, elem);
     if (pl.sys == 0) return 0;
-    if (!(tma_ok(A, n_sys) && tma_ok(B, n_sys) && tma_ok(C, n_sys) && tma_ok(D, n_sys)))
+    if (!(tma_ok_elem(A, n_sys, elem) && tma_ok_elem(B, n_sys, elem) &&
+          tma_ok_elem(C, n_sys, elem) && tma_ok_elem(D, n_sys, elem)))
         return 0;
     const int nsc = pl.nseg / pl.cl;
     CUtensorMap maps[4];
-    if (!(make_tile_map(&maps[0], A, n_sys, pl.nseg, pl.sys, nsc) &&
-          make_tile_map(&maps[1], B, n_sys, pl.nseg, pl.sys, nsc) &&
-          make_tile_map(&maps[2], C, n_sys, pl.nseg, pl.sys, nsc) &&
-          make_tile_map(&maps[3], D, n_sys, pl.nseg, pl.sys, nsc)))
+    if (!(make_tile_map(&maps[0], A, n_sys, pl.nseg, pl.sys, nsc, elem) &&
+          make_tile_map(&maps[1], B, n_sys, pl.nseg, pl.sys, nsc, elem) &&
+          make_tile_map(&maps[2], C, n_sys, pl.nseg, pl.sys, nsc, elem) &&
+          make_tile_map(&maps[3], D, n_sys, pl.nseg, pl.sys, nsc, elem)))
         return 0;
     TileArgs a = {};
     a.X = X;
@@ -269,17 +294,7 @@ int try_tile(const double* A, const double* B, const double* C, const double* D,
     a.nst = pl.nst;
     a.n_groups = (n_sys + pl.sys - 1) / pl.sys;
     a.status = status;
-    int rc;
-    switch (pl.sys * 2 + (cyclic ? 1 : 0)) {
-        case 256: rc = launch_tile_sys<128, false>(maps, a, st); break;
-        case 257: rc = launch_tile_sys<128, true>(maps, a, st); break;
-        case 128: rc = launch_tile_sys<64, false>(maps, a, st); break;
-        case 129: rc = launch_tile_sys<64, true>(maps, a, st); break;
-        case 64: rc = launch_tile_sys<32, false>(maps, a, st); break;
-        case 65: rc = launch_tile_sys<32, true>(maps, a, st); break;
-        case 33: rc = launch_tile_sys<16, true>(maps, a, st); break;
-        default: rc = launch_tile_sys<16, false>(maps, a, st); break;
-    }
+    const int rc = launch_tile_plan<TIN>(pl, maps, a, cyclic, st);
     return rc == BTDMA_OK ? 1 : rc;
 }
 
@@ -345,7 +360,7 @@ int solve_impl(btdma_t h, const double* A, const double* B, const double* C, con
     }
 
     if (h->method == BTDMA_PASCAL && !(h->flags & BTDMA_FLAG_REFERENCE_ORDER)) {
-        rc = try_tile(A, B, C, D, X, n_sys, n_row, cyclic, h->status, st);
+        rc = try_tile<double>(A, B, C, D, X, n_sys, n_row, cyclic, h->status, st);
         if (rc < 0) return rc;
         if (rc == 1) return BTDMA_OK;
     }
@@ -407,8 +422,8 @@ int btdma_create(int method, int n_sys, int n_row, int P, int precision, int fla
     if (method < BTDMA_PASCAL || method > BTDMA_FILTERED_V2)
         return fail(BTDMA_ERR_ARG, "unknown method %d", method);
     if (n_sys <= 0 || n_row <= 0) return fail(BTDMA_ERR_ARG, "n_sys and n_row must be positive");
-    if (precision != BTDMA_FP64)
-        return fail(BTDMA_ERR_UNSUPPORTED, "precision %d not built yet", precision);
+    if (precision < BTDMA_FP64 || precision > BTDMA_FP32_STORE)
+        return fail(BTDMA_ERR_ARG, "unknown precision %d", precision);
     if (P < 0) return fail(BTDMA_ERR_ARG, "P must be >= 0");
     if (P == 0) P = auto_segments(n_row);
     if (P > SEG_MAX_P)
@@ -448,7 +463,8 @@ int btdma_create(int method, int n_sys, int n_row, int P, int precision, int fla
     CKC(cudaMemset(h->work, 0, sizeof(unsigned long long) * 2 * P));
     CKC(cudaMalloc(&h->status, sizeof(unsigned)));
     CKC(cudaMemset(h->status, 0, sizeof(unsigned)));
-    if (P == 1) CKC(cudaMalloc(&h->scratch, sizeof(double) * 2 * (size_t)n_row * n_sys));
+    if (P == 1 && precision == BTDMA_FP64)
+        CKC(cudaMalloc(&h->scratch, sizeof(double) * 2 * (size_t)n_row * n_sys));
 #undef CKC
     *out = h;
     return BTDMA_OK;
@@ -479,6 +495,28 @@ int btdma_solve_out(btdma_t h, const double* A, const double* B, const double* C
                     const double* D, double* X, int n_sys, int n_row, int cyclic,
                     cudaStream_t stream) {
     return solve_impl(h, A, B, C, D, X, n_sys, n_row, cyclic != 0, stream);
+}
+
+int btdma_solve_f32(btdma_t h, const float* A, const float* B, const float* C, const float* D,
+                    double* X, int n_sys, int n_row, int cyclic, cudaStream_t stream) {
+    int rc = check_sizes(h, n_sys, n_row);
+    if (rc) return rc;
+    if (!A || !B || !C || !D || !X) return fail(BTDMA_ERR_ARG, "null array");
+    if (h->precision != BTDMA_FP32_STORE && h->precision != BTDMA_FP32_REFINE)
+        return fail(BTDMA_ERR_ARG, "FP32 arrays passed to an FP64 handle");
+    if (h->method != BTDMA_PASCAL)
+        return fail(BTDMA_ERR_UNSUPPORTED, "FP32 storage is provided for PaScaL only");
+    h->last_stream = stream;
+    if (h->precision == BTDMA_FP32_STORE) {
+        rc = try_tile<float>(A, B, C, D, X, n_sys, n_row, cyclic != 0, h->status, stream);
+        if (rc < 0) return rc;
+        if (rc == 0)
+            return fail(BTDMA_ERR_UNSUPPORTED,
+                        "FP32 storage needs n_row %% 16 == 0, n_sys %% 4 == 0, 16-byte alignment "
+                        "(and a power-of-two n_row/16 when periodic)");
+        return BTDMA_OK;
+    }
+    return fail(BTDMA_ERR_UNSUPPORTED, "FP32 refinement not built yet");
 }
 
 int btdma_set_eps_constant(btdma_t h, double eps_constant) {

@@ -84,11 +84,13 @@ __host__ __device__ __forceinline__ size_t tile_fixed_doubles(int sys, int nsc, 
     if (nseg > 32) f += 6ull * (nseg + 2) * sub;
     return f;
 }
+__host__ __device__ __forceinline__ size_t tile_ring_bytes(int sys, int nsc, int nst, int elem) {
+    return (size_t)nst * 4 * TILE_RPS * sys * nsc * elem;
+}
 __host__ __device__ __forceinline__ size_t tile_smem_bytes(int sys, int nsc, int nseg, int sub,
-                                                           int nst) {
-    const size_t T = (size_t)sys * nsc;
-    return ((size_t)nst * 4 * TILE_RPS * T + tile_fixed_doubles(sys, nsc, nseg, sub)) *
-               sizeof(double) +
+                                                           int nst, int elem = 8) {
+    return tile_ring_bytes(sys, nsc, nst, elem) +
+           tile_fixed_doubles(sys, nsc, nseg, sub) * sizeof(double) +
            2ull * nst * sizeof(uint64_t) + 128;
 }
 
@@ -126,7 +128,9 @@ __device__ __forceinline__ void pcr_step(double& l, double& u, double& r, double
     u = nu;
 }
 
-template <int SYS, bool CYCLIC>
+// TIN: element type of A, B, C, D in HBM (double, or float widened exactly to
+// double on load: FP32 storage, FP64 arithmetic).  x is always FP64.
+template <int SYS, bool CYCLIC, typename TIN = double>
 __global__ void __launch_bounds__(TILE_MAX_THREADS, 1)
 tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 const __grid_constant__ CUtensorMap tmC, const __grid_constant__ CUtensorMap tmD,
@@ -143,9 +147,9 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     const bool shuffled = W <= 32;
     const int fstride = nsc * RP;  // field stride of red / xr
 
-    double* ring = reinterpret_cast<double*>(
+    TIN* ring = reinterpret_cast<TIN*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-    double* red = ring + (size_t)nst * 4 * TILE_RPS * T;
+    double* red = reinterpret_cast<double*>(ring + (size_t)nst * 4 * TILE_RPS * T);
     double* xr = red + 6 * fstride;
     double* pcr = xr + 2 * fstride;  // only when !shuffled
     const int gs = nseg + 2;
@@ -183,14 +187,14 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                          ? (args.n_groups - cluster_id + n_clusters - 1) / n_clusters
                          : 0;
     const int total = n_my * TILE_SPG;  // ring stages this CTA consumes
-    const int sstride = 4 * TILE_RPS * T;  // doubles per stage
-    const uint32_t stage_bytes = (uint32_t)sstride * sizeof(double);
+    const int sstride = 4 * TILE_RPS * T;  // elements per stage
+    const uint32_t stage_bytes = (uint32_t)sstride * sizeof(TIN);
 
     auto issue = [&](int t) {  // one thread
         const int slot = t % nst;
         const int g = cluster_id + (t / TILE_SPG) * n_clusters;
         const int k0 = (t % TILE_SPG) * TILE_RPS;
-        double* dst = ring + (size_t)slot * sstride;
+        TIN* dst = ring + (size_t)slot * sstride;
         mbar_expect_tx(&full[slot], stage_bytes);
         tma_load_3d(dst + 0 * TILE_RPS * T, &tmA, g * SYS, k0, c * nsc, &full[slot]);
         tma_load_3d(dst + 1 * TILE_RPS * T, &tmB, g * SYS, k0, c * nsc, &full[slot]);
@@ -203,7 +207,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 
     // this thread's element of a stage: array f, row r at st + f*RPS*T + r*SYS
     const int toff = ql * TILE_RPS * SYS + s;
-    const double* st = ring + toff;  // stage t, this thread's column
+    const TIN* st = ring + toff;  // stage t, this thread's column
 
     double nonfinite = 0.0;  // becomes NaN if any solution entry is NaN or Inf
     int slot = 0;            // ring slot of stage t
@@ -227,10 +231,10 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             double a2[TILE_RPS], b2[TILE_RPS], c2[TILE_RPS], d2[TILE_RPS];
 #pragma unroll
             for (int r = 0; r < TILE_RPS; ++r) {
-                a2[r] = st[0 * TILE_RPS * T + r * SYS];
-                b2[r] = st[1 * TILE_RPS * T + r * SYS];
-                c2[r] = st[2 * TILE_RPS * T + r * SYS];
-                d2[r] = st[3 * TILE_RPS * T + r * SYS];
+                a2[r] = (double)st[0 * TILE_RPS * T + r * SYS];
+                b2[r] = (double)st[1 * TILE_RPS * T + r * SYS];
+                c2[r] = (double)st[2 * TILE_RPS * T + r * SYS];
+                d2[r] = (double)st[3 * TILE_RPS * T + r * SYS];
             }
             __syncwarp();
             if (lane == 0) {

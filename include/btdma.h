@@ -54,7 +54,8 @@ enum btdma_method {
 
 enum btdma_precision {
     BTDMA_FP64 = 0,        /* FP64 storage and arithmetic */
-    BTDMA_FP32_REFINE = 1  /* FP32 storage, FP32 sweeps + FP64 iterative refinement */
+    BTDMA_FP32_REFINE = 1, /* FP32 storage, FP32 sweeps + FP64 iterative refinement */
+    BTDMA_FP32_STORE = 2   /* FP32 storage widened exactly to FP64, FP64 arithmetic */
 };
 
 enum btdma_flags {
@@ -115,6 +116,16 @@ int btdma_solve_cyclic(btdma_t h, const double* A, const double* B, const double
 int btdma_solve_out(btdma_t h, const double* A, const double* B, const double* C,
                     const double* D, double* X, int n_sys, int n_row, int cyclic,
                     cudaStream_t stream);
+
+/* FP32-stored batch (A, B, C, D float [n_row x n_sys]) solved into an FP64 x:
+ * X <- x, 24 bytes of HBM traffic per row instead of 40.  The reference has no
+ * FP32 path; the result is compared with the FP64 solve of the same values
+ * widened exactly to double.  Handles created with BTDMA_FP32_STORE (FP64
+ * arithmetic on the widened values, no refinement needed) or BTDMA_FP32_REFINE
+ * (FP32 elimination, FP64 residual and correction sweeps).  PaScaL only; needs
+ * n_row a multiple of 16 and n_sys a multiple of 4 (the tiled kernel). */
+int btdma_solve_f32(btdma_t h, const float* A, const float* B, const float* C, const float* D,
+                    double* X, int n_sys, int n_row, int cyclic, cudaStream_t stream);
 
 /* Filtered: eps = eps_constant / (m * P)^2 per segment of m rows.  Replaces
  * FilteredTDMACUDA::set_eps_constant (filtered_tdma_cuda.hpp:203-206); no-op for

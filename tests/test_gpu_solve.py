@@ -239,3 +239,40 @@ def test_full_size_properties(cuda):
     r[1:] += A[1:] * X8[:-1]
     r[:-1] += C[:-1] * X8[1:]
     assert (r.abs().max() / D.abs().max()).item() <= 1e-12
+
+
+# ----------------------------------------------------------------- FP32 storage
+def run_f32(cuda, A, B, C, D, precision, cyclic=False):
+    """FP32-stored inputs, FP64 solution; returns (x, widened inputs)."""
+    import torch
+    from filtered_tdma_b200 import _lib as L
+    A32, B32, C32, D32 = [np.ascontiguousarray(x, dtype=np.float32) for x in (A, B, C, D)]
+    n_row, n_sys = D.shape
+    s = Solver("pascal", n_sys, n_row, 8 if n_row >= 48 else 2, precision=precision)
+    dA, dB, dC, dD = [torch.from_numpy(x).to(cuda) for x in (A32, B32, C32, D32)]
+    X = torch.zeros((n_row, n_sys), dtype=torch.float64, device=cuda)
+    L.check(L.lib().btdma_solve_f32(s._h, dA.data_ptr(), dB.data_ptr(), dC.data_ptr(),
+                                    dD.data_ptr(), X.data_ptr(), n_sys, n_row, int(cyclic),
+                                    torch.cuda.current_stream().cuda_stream))
+    assert s.status() == 0
+    wid = [x.astype(np.float64) for x in (A32, B32, C32, D32)]
+    return host(X), wid
+
+
+@pytest.mark.parametrize("n_sys,n_row", [(64, 64), (1000, 128), (512, 256), (2048, 512),
+                                         (96, 1024)])
+def test_fp32_store_within_1e12(cuda, orc, n_sys, n_row):
+    from filtered_tdma_b200 import _lib as L
+    A, B, C, D = W.diag_dominant(n_sys, n_row, seed=n_row + 5)
+    x, wid = run_f32(cuda, A, B, C, D, L.FP32_STORE)
+    assert rel_err(x, orc.thomas(*wid)) <= 1e-12
+
+
+def test_fp32_store_cyclic_and_weak(cuda, orc):
+    from filtered_tdma_b200 import _lib as L
+    A, B, C, D = W.weak_dominance(1024, 512, seed=3)
+    x, wid = run_f32(cuda, A, B, C, D, L.FP32_STORE)
+    assert rel_err(x, orc.thomas(*wid)) <= 1e-12
+    A, B, C, D = W.diag_dominant(256, 256, seed=4)
+    x, wid = run_f32(cuda, A, B, C, D, L.FP32_STORE, cyclic=True)
+    assert rel_err(x, orc.thomas_cyclic(*wid)) <= 1e-12
