@@ -140,14 +140,14 @@ int launch_seg(const CUtensorMap* maps, const SegArgs& a, int groups, cudaStream
 }
 
 // 3-D view [nseg][TILE_MT][n_sys] of an [n_row x n_sys] FP64 array; boxes of
-// TILE_RPS rows of `nsc` consecutive sub-segments for `sys` systems.
+// tile_rps(elem) rows of `nsc` consecutive sub-segments for `sys` systems.
 bool make_tile_map(CUtensorMap* map, const void* ptr, int n_sys, int nseg, int sys, int nsc,
                    int elem = 8) {
     auto fn = encode_fn();
     if (!fn) return false;
     cuuint64_t dims[3] = {(cuuint64_t)n_sys, (cuuint64_t)TILE_MT, (cuuint64_t)nseg};
     cuuint64_t strides[2] = {(cuuint64_t)n_sys * elem, (cuuint64_t)n_sys * TILE_MT * elem};
-    cuuint32_t box[3] = {(cuuint32_t)sys, (cuuint32_t)TILE_RPS, (cuuint32_t)nsc};
+    cuuint32_t box[3] = {(cuuint32_t)sys, (cuuint32_t)tile_rps(elem), (cuuint32_t)nsc};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = fn(map, elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
                     3, const_cast<void*>(ptr), dims, strides,
@@ -198,7 +198,7 @@ TilePlan tile_plan(int n_row, bool cyclic, int elem = 8) {
             }
         if (cl == 0) return pl;
     }
-    int nst = elem == 8 ? TILE_MAX_NST : 2 * TILE_MAX_NST;
+    int nst = TILE_MAX_NST;
     while (nst >= 3 &&
            tile_smem_bytes(sys, nseg / cl, nseg, sys / cl, nst, elem) > (size_t)max_smem_optin())
         --nst;

@@ -7,7 +7,7 @@
 // (CL = 1 for short systems), NSC = NSEG / CL sub-segments per CTA, SYS * NSC
 // <= 512 threads.  Persistent clusters walk over the groups:
 //
-//   1. Forward pass (TILE_RPS = 2 rows of every local sub-segment per step).
+//   1. Forward pass (RPS = 2 FP64 or 4 FP32 rows of every local sub-segment per step).
 //      Rows k, k+1 of the CTA's NSC sub-segments of SYS systems arrive in one TMA
 //      box of a 3-D view [NSEG][TILE_MT][n_sys] (SYS * 8 bytes wide) through an
 //      NST-stage shared-memory ring.  Each stage has a "full" mbarrier (TMA
@@ -51,8 +51,9 @@
 namespace btdma {
 
 constexpr int TILE_MT = 16;           // rows per sub-segment (per thread)
-constexpr int TILE_RPS = 2;           // rows per ring stage
-constexpr int TILE_SPG = TILE_MT / TILE_RPS;  // stages per group
+// Rows per ring stage: 16 bytes of each array per sub-segment and system, i.e.
+// 2 FP64 rows or 4 FP32 rows, so a stage has the same size for both storages.
+__host__ __device__ constexpr int tile_rps(int elem) { return 16 / elem; }
 constexpr int TILE_MAX_THREADS = 512;
 constexpr int TILE_MAX_NST = 8;       // ring stages (upper bound)
 
@@ -85,7 +86,7 @@ __host__ __device__ __forceinline__ size_t tile_fixed_doubles(int sys, int nsc, 
     return f;
 }
 __host__ __device__ __forceinline__ size_t tile_ring_bytes(int sys, int nsc, int nst, int elem) {
-    return (size_t)nst * 4 * TILE_RPS * sys * nsc * elem;
+    return (size_t)nst * 4 * tile_rps(elem) * sys * nsc * elem;
 }
 __host__ __device__ __forceinline__ size_t tile_smem_bytes(int sys, int nsc, int nseg, int sub,
                                                            int nst, int elem = 8) {
@@ -137,6 +138,8 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                 const TileArgs args) {
     namespace cg = cooperative_groups;
     constexpr int M = TILE_MT;
+    constexpr int RPS = tile_rps((int)sizeof(TIN));  // rows per ring stage
+    constexpr int SPG = M / RPS;                      // stages per group
     constexpr int RP = SYS + 1;  // padded pitch of red / xr rows
     extern __shared__ unsigned char smem_raw[];
     const int nseg = args.nseg, cl = args.cl, nst = args.nst;
@@ -149,7 +152,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 
     TIN* ring = reinterpret_cast<TIN*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-    double* red = reinterpret_cast<double*>(ring + (size_t)nst * 4 * TILE_RPS * T);
+    double* red = reinterpret_cast<double*>(ring + (size_t)nst * 4 * RPS * T);
     double* xr = red + 6 * fstride;
     double* pcr = xr + 2 * fstride;  // only when !shuffled
     const int gs = nseg + 2;
@@ -186,27 +189,27 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     const int n_my = args.n_groups > cluster_id
                          ? (args.n_groups - cluster_id + n_clusters - 1) / n_clusters
                          : 0;
-    const int total = n_my * TILE_SPG;  // ring stages this CTA consumes
-    const int sstride = 4 * TILE_RPS * T;  // elements per stage
+    const int total = n_my * SPG;  // ring stages this CTA consumes
+    const int sstride = 4 * RPS * T;  // elements per stage
     const uint32_t stage_bytes = (uint32_t)sstride * sizeof(TIN);
 
     auto issue = [&](int t) {  // one thread
         const int slot = t % nst;
-        const int g = cluster_id + (t / TILE_SPG) * n_clusters;
-        const int k0 = (t % TILE_SPG) * TILE_RPS;
+        const int g = cluster_id + (t / SPG) * n_clusters;
+        const int k0 = (t % SPG) * RPS;
         TIN* dst = ring + (size_t)slot * sstride;
         mbar_expect_tx(&full[slot], stage_bytes);
-        tma_load_3d(dst + 0 * TILE_RPS * T, &tmA, g * SYS, k0, c * nsc, &full[slot]);
-        tma_load_3d(dst + 1 * TILE_RPS * T, &tmB, g * SYS, k0, c * nsc, &full[slot]);
-        tma_load_3d(dst + 2 * TILE_RPS * T, &tmC, g * SYS, k0, c * nsc, &full[slot]);
-        tma_load_3d(dst + 3 * TILE_RPS * T, &tmD, g * SYS, k0, c * nsc, &full[slot]);
+        tma_load_3d(dst + 0 * RPS * T, &tmA, g * SYS, k0, c * nsc, &full[slot]);
+        tma_load_3d(dst + 1 * RPS * T, &tmB, g * SYS, k0, c * nsc, &full[slot]);
+        tma_load_3d(dst + 2 * RPS * T, &tmC, g * SYS, k0, c * nsc, &full[slot]);
+        tma_load_3d(dst + 3 * RPS * T, &tmD, g * SYS, k0, c * nsc, &full[slot]);
     };
     bool ok = true;
     if (tid == 0)
         for (int t = 0; t < nst && t < total; ++t) issue(t);
 
     // this thread's element of a stage: array f, row r at st + f*RPS*T + r*SYS
-    const int toff = ql * TILE_RPS * SYS + s;
+    const int toff = ql * RPS * SYS + s;
     const TIN* st = ring + toff;  // stage t, this thread's column
 
     double nonfinite = 0.0;  // becomes NaN if any solution entry is NaN or Inf
@@ -226,15 +229,15 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         double ab0 = 0, cb0 = 0, db0 = 0;
         double pi = 1.0, sa = 0.0, sd = 0.0;
 #pragma unroll
-        for (int j = 0; j < TILE_SPG; ++j) {
+        for (int j = 0; j < SPG; ++j) {
             if (ok) ok = mbar_wait_bounded(&full[slot], phase, args.status);
-            double a2[TILE_RPS], b2[TILE_RPS], c2[TILE_RPS], d2[TILE_RPS];
+            double a2[RPS], b2[RPS], c2[RPS], d2[RPS];
 #pragma unroll
-            for (int r = 0; r < TILE_RPS; ++r) {
-                a2[r] = (double)st[0 * TILE_RPS * T + r * SYS];
-                b2[r] = (double)st[1 * TILE_RPS * T + r * SYS];
-                c2[r] = (double)st[2 * TILE_RPS * T + r * SYS];
-                d2[r] = (double)st[3 * TILE_RPS * T + r * SYS];
+            for (int r = 0; r < RPS; ++r) {
+                a2[r] = (double)st[0 * RPS * T + r * SYS];
+                b2[r] = (double)st[1 * RPS * T + r * SYS];
+                c2[r] = (double)st[2 * RPS * T + r * SYS];
+                d2[r] = (double)st[3 * RPS * T + r * SYS];
             }
             __syncwarp();
             if (lane == 0) {
@@ -258,8 +261,8 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                 st = ring + toff;
             }
 #pragma unroll
-            for (int r = 0; r < TILE_RPS; ++r) {
-                const int k = j * TILE_RPS + r;
+            for (int r = 0; r < RPS; ++r) {
+                const int k = j * RPS + r;
                 const double a = a2[r], b = b2[r], cc = c2[r], d = d2[r];
                 if (k == 0) {
                     const double ib = rcp_nr(b);
