@@ -225,6 +225,7 @@ def main():
 
     from filtered_tdma_b200 import Solver
     from filtered_tdma_b200 import workloads as W
+    from filtered_tdma_b200.replicas import max_over_ranks, whole_job_rate
 
     A, B, C, D = W.diag_dominant(N_SYS, N_ROW, seed=2 + rank, device=dev)
     X = torch.empty_like(D)
@@ -242,12 +243,9 @@ def main():
         total_ms, per, launches = time_variant(torch, pas, A, B, C, D, X, args.steps,
                                                args.warmup, 1)
     barrier()
-    t = torch.tensor([total_ms], device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, device=dev)
     ms_step = total_ms / args.steps
-    value = world * rows / (ms_step * 1e-3)
+    value = whole_job_rate(rows, world, ms_step)
 
     peak, peak_src = measured_peak()
     k_ms = sum(per) / len(per)  # one kernel launch per PaScaL step
@@ -342,11 +340,8 @@ def main():
             e2e_step()
         e1.record()
         torch.cuda.synchronize()
-        t = torch.tensor([e0.elapsed_time(e1) / e2e_steps], device=dev)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        e2e = {"value": world * rows / (ms * 1e-3), "unit": "rows/s",
+        ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, device=dev)
+        e2e = {"value": whole_job_rate(rows, world, ms), "unit": "rows/s",
                "h2d_bytes_per_step": 4 * 8 * rows, "d2h_bytes_per_step": 8 * rows,
                "ms_per_step": ms, "path": "Solver.solve_out (C ABI btdma_solve_out) with "
                                          "pinned host buffers copied in and out every step"}
