@@ -63,61 +63,94 @@ def ncu_traffic(kernel_tag):
 
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    """SM clock and throttle-reason samples taken DURING a timed region.
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NVML is polled from a thread every millisecond between start() and stop()
+    (a solve step lasts about a millisecond, so nvidia-smi's 200 ms loop would
+    miss short regions); nvidia-smi one-shot queries are the fallback when NVML
+    cannot be loaded.  Reason names follow nvidia-smi's clocks_event_reasons."""
 
-    def __init__(self, gpu_index):
-        self.gpu = gpu_index
-        self.proc = None
-        self.lines = []
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40),
+               ("sw_thermal_slowdown", 0x20), ("sw_power_cap", 0x4),
+               ("hw_power_brake_slowdown", 0x80))
 
-    def __enter__(self):
+    def __init__(self, torch_device):
+        self.dev = torch_device
+        self.sm, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        self._ready = threading.Event()
+        self._t = None
+        self._nvml = None
+        self._h = None
+
+    def _open(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self._t = threading.Thread(target=self._read, daemon=True)
-            self._t.start()
-        except OSError:
-            self.proc = None
-        return self
-
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
-    def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
             try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-            self._t.join(timeout=2)
+                self._h = pynvml.nvmlDeviceGetHandleByUUID("GPU-" + uuid)
+            except Exception:
+                self._h = pynvml.nvmlDeviceGetHandleByIndex(self.dev.index or 0)
+            self._nvml = pynvml
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM))
+        except Exception:
+            self._nvml = None
+
+    def _sample(self):
+        if self._nvml is not None:
+            n = self._nvml
+            self.sm.append(float(n.nvmlDeviceGetClockInfo(self._h, n.NVML_CLOCK_SM)))
+            mask = int(n.nvmlDeviceGetCurrentClocksEventReasons(self._h))
+            for name, bit in self.REASONS:
+                if mask & bit:
+                    self.reasons.add(name)
+            return
+        out = subprocess.run(
+            ["nvidia-smi", "-i", str(self.dev.index or 0),
+             "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits"],
+            capture_output=True, text=True, timeout=10).stdout.strip().split(",")
+        if len(out) >= 6:
+            self.sm.append(float(out[0]))
+            self.max_mhz = float(out[1])
+            for (name, _), v in zip(self.REASONS, out[2:6]):
+                if v.strip().lower() == "active":
+                    self.reasons.add(name)
+
+    def _run(self):
+        while True:
+            try:
+                self._sample()
+            except Exception:
+                pass
+            self._ready.set()
+            if self._stop.wait(0.001):
+                break
+
+    def start(self):
+        self._open()
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        self._ready.wait(timeout=10)  # first sample taken before the region starts
+
+    def stop(self):
+        self._stop.set()
+        if self._t is not None:
+            self._t.join(timeout=10)
+        try:
+            self._sample()  # at least one sample at the end of the region
+        except Exception:
+            pass
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if not self.sm:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(self.sm), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.sm),
+                "source": "nvml" if self._nvml is not None else "nvidia-smi"}
 
 
 def cpu_reference_rate(sample_sys, reps, warm=1):
@@ -176,11 +209,13 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def time_variant(torch, solver, A, B, C, D, X, steps, warmup, launches_per_step):
+def time_variant(torch, solver, A, B, C, D, X, steps, warmup, launches_per_step, sampler=None):
     stream = torch.cuda.current_stream()
     for _ in range(warmup):
         solver.solve_out(A, B, C, D, X)
     torch.cuda.synchronize()
+    if sampler is not None:
+        sampler.start()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(steps)]
     t0 = torch.cuda.Event(enable_timing=True)
@@ -192,6 +227,8 @@ def time_variant(torch, solver, A, B, C, D, X, steps, warmup, launches_per_step)
         e1.record(stream)
     t1.record(stream)
     torch.cuda.synchronize()
+    if sampler is not None:
+        sampler.stop()
     per = [e0.elapsed_time(e1) for e0, e1 in ev]
     return t0.elapsed_time(t1), per, steps * launches_per_step
 
@@ -239,9 +276,9 @@ def main():
     # ---------------------------------------------------------- headline
     pas = Solver("pascal", N_SYS, N_ROW, P)
     barrier()
-    with ClockSampler(local) as clk:
-        total_ms, per, launches = time_variant(torch, pas, A, B, C, D, X, args.steps,
-                                               args.warmup, 1)
+    clk = ClockSampler(dev)
+    total_ms, per, launches = time_variant(torch, pas, A, B, C, D, X, args.steps, args.warmup, 1,
+                                           sampler=clk)
     barrier()
     total_ms = max_over_ranks(total_ms, device=dev)
     ms_step = total_ms / args.steps
@@ -279,12 +316,16 @@ def main():
                 variants[name]["J"] = s.last_J()
             s.close()
 
-        # FP32 storage (A, B, C, D as float, x as double): 24 B/row
-        from filtered_tdma_b200 import _lib as L
-        A32, B32, C32, D32 = [t.to(torch.float32) for t in (A, B, C, D)]
-        for name, prec in (("fp32_store_P8", L.FP32_STORE),):
+        # FP32 storage (A, B, C, D as float, x as double): 24 B/row.
+        #   fp32_store: FP64 arithmetic on the exactly widened values (one pass);
+        #   fp32_refine: FP32 sweeps + FP64 residual refinement (config batch A),
+        #   and the same on a weakly dominant batch (rho in [0.45, 0.499], batch B).
+        stream = torch.cuda.current_stream().cuda_stream
+        nrep = max(3, args.steps // 2)
+
+        def f32_variant(name, prec, arrs):
+            A32, B32, C32, D32 = arrs
             s = Solver("pascal", N_SYS, N_ROW, P, precision=prec)
-            stream = torch.cuda.current_stream().cuda_stream
 
             def run_f32():
                 L.check(L.lib().btdma_solve_f32(s._h, A32.data_ptr(), B32.data_ptr(),
@@ -294,7 +335,6 @@ def main():
                 run_f32()
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            nrep = max(3, args.steps // 2)
             e0.record()
             for _ in range(nrep):
                 run_f32()
@@ -308,13 +348,29 @@ def main():
             run_f32()
             err = ((X - Xr).abs().max() / Xr.abs().max()).item()
             ref.close()
-            variants[name] = {"rows_per_s": rows / (ms * 1e-3), "ms_per_step": ms,
-                              "hbm_gbs_algorithmic": gbps(ms, 24),
-                              "frac_of_peak": gbps(ms, 24) / peak,
-                              "speedup_vs_fp64_value": (rows / (ms * 1e-3)) / (rows / (ms_step * 1e-3)),
-                              "max_rel_err_vs_fp64_thomas": err, "refinement_sweeps": 0}
+            del Xr
+            v = {"rows_per_s": rows / (ms * 1e-3), "ms_per_step": ms,
+                 "hbm_gbs_algorithmic": gbps(ms, 24),
+                 "frac_of_peak": gbps(ms, 24) / peak,
+                 "speedup_vs_fp64_value": (rows / (ms * 1e-3)) / (rows / (ms_step * 1e-3)),
+                 "max_rel_err_vs_fp64_thomas": err}
+            if prec == L.FP32_REFINE:
+                v["refinement"] = s.last_stats()
+            else:
+                v["refinement_sweeps"] = 0
+            variants[name] = v
             s.close()
-        del A32, B32, C32, D32
+
+        arrs = [t.to(torch.float32) for t in (A, B, C, D)]
+        f32_variant("fp32_store_P8", L.FP32_STORE, arrs)
+        f32_variant("fp32_refine_P8", L.FP32_REFINE, arrs)
+        del arrs
+        Aw, Bw, Cw, Dw = W.weak_dominance(N_SYS, N_ROW, seed=3, device=dev)
+        arrs = [t.to(torch.float32) for t in (Aw, Bw, Cw, Dw)]
+        del Aw, Bw, Cw, Dw
+        f32_variant("fp32_refine_weak_P8", L.FP32_REFINE, arrs)
+        f32_variant("fp32_store_weak_P8", L.FP32_STORE, arrs)
+        del arrs
 
     # ---------------------------------------------------------- end to end
     e2e = None

@@ -24,9 +24,21 @@ EXPORTS = (
     "btdma_create", "btdma_destroy", "btdma_solve", "btdma_solve_cyclic", "btdma_solve_out",
     "btdma_set_eps_constant", "btdma_set_rho", "btdma_set_rho_all", "btdma_last_J",
     "btdma_status", "btdma_set_method", "btdma_segments", "btdma_last_error",
-    "btdma_solve_noalloc", "btdma_solve_f32",
+    "btdma_solve_noalloc", "btdma_solve_f32", "btdma_set_refine", "btdma_last_stats",
 )
 NOALLOC_MAX_ELEMS = 1 << 20
+REFINE_MAX_SWEEPS = 4
+
+
+class Stats(ctypes.Structure):
+    """btdma_stats of include/btdma.h."""
+    _fields_ = [("n_systems", ctypes.c_int), ("sweeps", ctypes.c_int),
+                ("converged_after", ctypes.c_int * (REFINE_MAX_SWEEPS + 1)),
+                ("n_fallback", ctypes.c_int)]
+
+    def as_dict(self) -> dict:
+        return {"n_systems": self.n_systems, "sweeps": self.sweeps,
+                "converged_after": list(self.converged_after), "n_fallback": self.n_fallback}
 
 
 class BtdmaError(RuntimeError):
@@ -61,6 +73,8 @@ def lib():
         L.btdma_segments.argtypes = [vp, ctypes.POINTER(i)]
         L.btdma_solve_noalloc.argtypes = [vp, vp, vp, vp, i, i, vp]
         L.btdma_solve_f32.argtypes = [vp, vp, vp, vp, vp, vp, i, i, i, vp]
+        L.btdma_set_refine.argtypes = [vp, i, d]
+        L.btdma_last_stats.argtypes = [vp, ctypes.POINTER(Stats)]
         L.btdma_last_error.restype = ctypes.c_char_p
         for name in EXPORTS:
             if name != "btdma_last_error":

@@ -17,7 +17,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libbtdma.so")
 SOURCES = [os.path.join(PKG, "csrc", "btdma_api.cu")]
-DEPS = SOURCES + [os.path.join(PKG, "csrc", f) for f in os.listdir(os.path.join(PKG, "csrc"))] + [
+DEPS = SOURCES + [os.path.join(PKG, "csrc", f) for f in os.listdir(os.path.join(PKG, "csrc"))
+                  if f != "width_probe.cu"] + [
     os.path.join(ROOT, "include", "btdma.h")]
 
 NVCC_FLAGS = [
@@ -28,6 +29,10 @@ NVCC_FLAGS = [
     "-Xlinker", "--exclude-libs=ALL",  # keep the static runtime's symbols private
     "-I" + os.path.join(ROOT, "include"),
 ]
+
+
+PROBE = os.path.join(PKG, "_width_probe")
+PROBE_SRC = os.path.join(PKG, "csrc", "width_probe.cu")
 
 
 def stale() -> bool:
@@ -45,6 +50,14 @@ def build(force: bool = False, verbose: bool = False) -> str:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
     return LIB
+
+
+def build_probe(force: bool = False) -> str:
+    """The access-width bandwidth probe (a standalone executable)."""
+    if force or not os.path.exists(PROBE) or os.path.getmtime(PROBE_SRC) > os.path.getmtime(PROBE):
+        subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17",
+                        "-o", PROBE, PROBE_SRC], check=True)
+    return PROBE
 
 
 if __name__ == "__main__":

@@ -11,9 +11,11 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "btdma_common.cuh"
 #include "k_filtered_j.cuh"
+#include "k_refine.cuh"
 #include "k_segment.cuh"
 #include "k_thomas.cuh"
 #include "k_tile.cuh"
@@ -30,6 +32,15 @@ struct btdma_handle {
     unsigned* status = nullptr;              // device status word
     double* scratch = nullptr;               // P == 1: c' and e' [2][n_row_cap * n_sys_cap]
     cudaStream_t last_stream = nullptr;
+    // FP32_REFINE: residual [n_row_cap * n_sys_cap] (FP32), per-system sweep
+    // counts [n_sys_cap], open-system counters [BTDMA_REFINE_MAX_SWEEPS + 1]
+    float* resid = nullptr;
+    unsigned char* iters = nullptr;
+    unsigned* open = nullptr;
+    int max_sweeps = 3;
+    double eta_tol = 8.0 * 0x1p-53;
+    int last_n_sys = 0;
+    bool last_refined = false;
 };
 
 namespace {
@@ -210,9 +221,9 @@ TilePlan tile_plan(int n_row, bool cyclic, int elem = 8) {
     return pl;
 }
 
-template <int SYS, bool CYCLIC, typename TIN = double>
+template <int SYS, bool CYCLIC, typename TIN = double, typename TC = double>
 int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st) {
-    auto kern = tile_f64_kernel<SYS, CYCLIC, TIN>;
+    auto kern = tile_f64_kernel<SYS, CYCLIC, TIN, TC>;
     static bool attr_done = false;
     if (!attr_done) {
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -248,18 +259,18 @@ int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st)
     return BTDMA_OK;
 }
 
-template <typename TIN>
+template <typename TIN, typename TC>
 int launch_tile_plan(const TilePlan& pl, const CUtensorMap* maps, const TileArgs& a, bool cyclic,
                      cudaStream_t st) {
     switch (pl.sys * 2 + (cyclic ? 1 : 0)) {
-        case 256: return launch_tile_sys<128, false, TIN>(maps, a, st);
-        case 257: return launch_tile_sys<128, true, TIN>(maps, a, st);
-        case 128: return launch_tile_sys<64, false, TIN>(maps, a, st);
-        case 129: return launch_tile_sys<64, true, TIN>(maps, a, st);
-        case 64: return launch_tile_sys<32, false, TIN>(maps, a, st);
-        case 65: return launch_tile_sys<32, true, TIN>(maps, a, st);
-        case 33: return launch_tile_sys<16, true, TIN>(maps, a, st);
-        default: return launch_tile_sys<16, false, TIN>(maps, a, st);
+        case 256: return launch_tile_sys<128, false, TIN, TC>(maps, a, st);
+        case 257: return launch_tile_sys<128, true, TIN, TC>(maps, a, st);
+        case 128: return launch_tile_sys<64, false, TIN, TC>(maps, a, st);
+        case 129: return launch_tile_sys<64, true, TIN, TC>(maps, a, st);
+        case 64: return launch_tile_sys<32, false, TIN, TC>(maps, a, st);
+        case 65: return launch_tile_sys<32, true, TIN, TC>(maps, a, st);
+        case 33: return launch_tile_sys<16, true, TIN, TC>(maps, a, st);
+        default: return launch_tile_sys<16, false, TIN, TC>(maps, a, st);
     }
 }
 
@@ -269,9 +280,12 @@ bool tma_ok_elem(const void* p, int n_sys, int elem) {
 
 // Returns 1 when the tiled kernel was launched, 0 when the shape needs the
 // cluster-per-segment kernel, < 0 on error.
-template <typename TIN>
+// TC: arithmetic of the local sweeps; accumulate: X += solution; gate: the
+// kernel does nothing while *gate == 0.
+template <typename TIN, typename TC = double>
 int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, int n_sys,
-             int n_row, bool cyclic, unsigned* status, cudaStream_t st) {
+             int n_row, bool cyclic, unsigned* status, cudaStream_t st, bool accumulate = false,
+             const unsigned* gate = nullptr) {
     const int elem = (int)sizeof(TIN);
     const TilePlan pl = tile_plan(n_row, cyclic, elem);
     if (pl.sys == 0) return 0;
@@ -293,8 +307,10 @@ int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, 
     a.cl = pl.cl;
     a.nst = pl.nst;
     a.n_groups = (n_sys + pl.sys - 1) / pl.sys;
+    a.accumulate = accumulate ? 1 : 0;
+    a.gate = gate;
     a.status = status;
-    const int rc = launch_tile_plan<TIN>(pl, maps, a, cyclic, st);
+    const int rc = launch_tile_plan<TIN, TC>(pl, maps, a, cyclic, st);
     return rc == BTDMA_OK ? 1 : rc;
 }
 
@@ -465,6 +481,11 @@ int btdma_create(int method, int n_sys, int n_row, int P, int precision, int fla
     CKC(cudaMemset(h->status, 0, sizeof(unsigned)));
     if (P == 1 && precision == BTDMA_FP64)
         CKC(cudaMalloc(&h->scratch, sizeof(double) * 2 * (size_t)n_row * n_sys));
+    if (precision == BTDMA_FP32_REFINE) {
+        CKC(cudaMalloc(&h->resid, sizeof(float) * (size_t)n_row * n_sys));
+        CKC(cudaMalloc(&h->iters, (size_t)n_sys));
+        CKC(cudaMalloc(&h->open, sizeof(unsigned) * (BTDMA_REFINE_MAX_SWEEPS + 1)));
+    }
 #undef CKC
     *out = h;
     return BTDMA_OK;
@@ -477,6 +498,9 @@ int btdma_destroy(btdma_t h) {
     cudaFree(h->work);
     cudaFree(h->status);
     cudaFree(h->scratch);
+    cudaFree(h->resid);
+    cudaFree(h->iters);
+    cudaFree(h->open);
     delete h;
     return BTDMA_OK;
 }
@@ -507,16 +531,76 @@ int btdma_solve_f32(btdma_t h, const float* A, const float* B, const float* C, c
     if (h->method != BTDMA_PASCAL)
         return fail(BTDMA_ERR_UNSUPPORTED, "FP32 storage is provided for PaScaL only");
     h->last_stream = stream;
+    h->last_n_sys = n_sys;
+    h->last_refined = false;
+    const bool cyc = cyclic != 0;
+    const char* shape_msg =
+        "FP32 storage needs n_row % 16 == 0, n_sys % 4 == 0, 16-byte alignment "
+        "(and a power-of-two n_row/16 when periodic)";
     if (h->precision == BTDMA_FP32_STORE) {
-        rc = try_tile<float>(A, B, C, D, X, n_sys, n_row, cyclic != 0, h->status, stream);
+        rc = try_tile<float>(A, B, C, D, X, n_sys, n_row, cyc, h->status, stream);
         if (rc < 0) return rc;
-        if (rc == 0)
-            return fail(BTDMA_ERR_UNSUPPORTED,
-                        "FP32 storage needs n_row %% 16 == 0, n_sys %% 4 == 0, 16-byte alignment "
-                        "(and a power-of-two n_row/16 when periodic)");
+        if (rc == 0) return fail(BTDMA_ERR_UNSUPPORTED, "%s", shape_msg);
         return BTDMA_OK;
     }
-    return fail(BTDMA_ERR_UNSUPPORTED, "FP32 refinement not built yet");
+    // FP32_REFINE: x0 from the FP32 sweeps, then up to max_sweeps of
+    //   r = D - T x (FP64), e = T^-1 r (FP32 sweeps), x += e,
+    // each launch gated on the device count of still-open systems, so the whole
+    // sequence is stream-ordered and capturable (no host round trip).
+    const int S = h->max_sweeps;
+    CK(cudaMemsetAsync(h->open, 0, sizeof(unsigned) * (BTDMA_REFINE_MAX_SWEEPS + 1), stream));
+    rc = try_tile<float, float>(A, B, C, D, X, n_sys, n_row, cyc, h->status, stream);
+    if (rc < 0) return rc;
+    if (rc == 0) return fail(BTDMA_ERR_UNSUPPORTED, "%s", shape_msg);
+    const int rgrid = (n_sys + 255) / 256;
+    for (int s = 0; s <= S; ++s) {
+        refine_residual_kernel<<<rgrid, 256, 0, stream>>>(
+            A, B, C, D, X, h->resid, n_sys, n_row, cyclic ? 1 : 0, s, s == S ? 1 : 0, h->eta_tol,
+            h->iters, s == 0 ? nullptr : &h->open[s - 1], &h->open[s]);
+        CK(cudaGetLastError());
+        if (s == S) break;
+        rc = try_tile<float, float>(A, B, C, h->resid, X, n_sys, n_row, cyc, h->status, stream,
+                                    true, &h->open[s]);
+        if (rc < 0) return rc;
+    }
+    // fallback: the FP64-arithmetic solve of the whole batch while any system is open
+    rc = try_tile<float, double>(A, B, C, D, X, n_sys, n_row, cyc, h->status, stream, false,
+                                 &h->open[S]);
+    if (rc < 0) return rc;
+    h->last_refined = true;
+    return BTDMA_OK;
+}
+
+int btdma_set_refine(btdma_t h, int max_sweeps, double eta_tol) {
+    if (!h) return fail(BTDMA_ERR_ARG, "null handle");
+    if (max_sweeps < 0 || max_sweeps > BTDMA_REFINE_MAX_SWEEPS)
+        return fail(BTDMA_ERR_ARG, "max_sweeps must be in [0, %d]", BTDMA_REFINE_MAX_SWEEPS);
+    if (!(eta_tol > 0.0)) return fail(BTDMA_ERR_ARG, "eta_tol must be positive");
+    h->max_sweeps = max_sweeps;
+    h->eta_tol = eta_tol;
+    return BTDMA_OK;
+}
+
+int btdma_last_stats(btdma_t h, btdma_stats* st) {
+    if (!h || !st) return fail(BTDMA_ERR_ARG, "null argument");
+    std::memset(st, 0, sizeof *st);
+    st->n_systems = h->last_n_sys;
+    if (!h->last_refined) return BTDMA_OK;
+    std::vector<unsigned char> it((size_t)h->last_n_sys);
+    unsigned open[BTDMA_REFINE_MAX_SWEEPS + 1];
+    CK(cudaMemcpyAsync(it.data(), h->iters, it.size(), cudaMemcpyDeviceToHost, h->last_stream));
+    CK(cudaMemcpyAsync(open, h->open, sizeof open, cudaMemcpyDeviceToHost, h->last_stream));
+    CK(cudaStreamSynchronize(h->last_stream));
+    for (unsigned char v : it) {
+        if (v == REFINE_FALLBACK || v == REFINE_OPEN)
+            ++st->n_fallback;
+        else if (v <= BTDMA_REFINE_MAX_SWEEPS)
+            ++st->converged_after[v];
+    }
+    // a correction sweep ran when systems were open before it
+    for (int s = 0; s < h->max_sweeps; ++s)
+        if (open[s] != 0u) st->sweeps = s + 1;
+    return BTDMA_OK;
 }
 
 int btdma_set_eps_constant(btdma_t h, double eps_constant) {

@@ -64,8 +64,19 @@ struct TileArgs {
     int cl;        // CTAs per cluster (sub-segments split over them)
     int nst;       // ring stages
     int n_groups;  // groups of SYS systems
+    int accumulate;        // 1: X += solution (refinement corrections), 0: X = solution
+    const unsigned* gate;  // non-null: the launch does nothing while *gate == 0
     unsigned* status;
 };
+
+// Reciprocal in the arithmetic of the local sweeps: FP64 with Newton steps, or
+// the single-instruction FP32 approximation (the inner solver of refinement).
+__device__ __forceinline__ double rcp_tc(double x) { return rcp_nr(x); }
+__device__ __forceinline__ float rcp_tc(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 
 __host__ __device__ __forceinline__ int tile_lanes(int nseg) {
     int w = 1;
@@ -129,9 +140,11 @@ __device__ __forceinline__ void pcr_step(double& l, double& u, double& r, double
     u = nu;
 }
 
-// TIN: element type of A, B, C, D in HBM (double, or float widened exactly to
-// double on load: FP32 storage, FP64 arithmetic).  x is always FP64.
-template <int SYS, bool CYCLIC, typename TIN = double>
+// TIN: element type of A, B, C, D in HBM (double, or float).  TC: arithmetic of
+// the local sweeps — double (FP32 storage is widened exactly on load), or float
+// (the FP32 inner solve of iterative refinement).  The reduced system, the back
+// substitution and x are always FP64.
+template <int SYS, bool CYCLIC, typename TIN = double, typename TC = double>
 __global__ void __launch_bounds__(TILE_MAX_THREADS, 1)
 tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 const __grid_constant__ CUtensorMap tmC, const __grid_constant__ CUtensorMap tmD,
@@ -186,7 +199,11 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     __syncthreads();
     if (cl > 1) tile_cluster_sync(cl);  // peers' shared memory is live before any DSMEM access
 
-    const int n_my = args.n_groups > cluster_id
+    // a closed gate leaves the CTA without groups (it still runs its setup and
+    // exit barriers, so every CTA of a cluster takes the same path)
+    const bool gated_off =
+        args.gate != nullptr && *static_cast<const volatile unsigned*>(args.gate) == 0u;
+    const int n_my = (!gated_off && args.n_groups > cluster_id)
                          ? (args.n_groups - cluster_id + n_clusters - 1) / n_clusters
                          : 0;
     const int total = n_my * SPG;  // ring stages this CTA consumes
@@ -225,19 +242,19 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         const bool valid = sys < args.n_sys;
 
         // ------------------------------------------------------ forward pass
-        double al[M], ga[M], de[M];  // rows 1..M-1 used (register resident)
-        double ab0 = 0, cb0 = 0, db0 = 0;
-        double pi = 1.0, sa = 0.0, sd = 0.0;
+        TC al[M], ga[M], de[M];  // rows 1..M-1 used (register resident)
+        TC ab0 = 0, cb0 = 0, db0 = 0;
+        TC pi = 1, sa = 0, sd = 0;
 #pragma unroll
         for (int j = 0; j < SPG; ++j) {
             if (ok) ok = mbar_wait_bounded(&full[slot], phase, args.status);
-            double a2[RPS], b2[RPS], c2[RPS], d2[RPS];
+            TIN a2[RPS], b2[RPS], c2[RPS], d2[RPS];  // widened where used
 #pragma unroll
             for (int r = 0; r < RPS; ++r) {
-                a2[r] = (double)st[0 * RPS * T + r * SYS];
-                b2[r] = (double)st[1 * RPS * T + r * SYS];
-                c2[r] = (double)st[2 * RPS * T + r * SYS];
-                d2[r] = (double)st[3 * RPS * T + r * SYS];
+                a2[r] = st[0 * RPS * T + r * SYS];
+                b2[r] = st[1 * RPS * T + r * SYS];
+                c2[r] = st[2 * RPS * T + r * SYS];
+                d2[r] = st[3 * RPS * T + r * SYS];
             }
             __syncwarp();
             if (lane == 0) {
@@ -263,21 +280,21 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 #pragma unroll
             for (int r = 0; r < RPS; ++r) {
                 const int k = j * RPS + r;
-                const double a = a2[r], b = b2[r], cc = c2[r], d = d2[r];
+                const TC a = (TC)a2[r], b = (TC)b2[r], cc = (TC)c2[r], d = (TC)d2[r];
                 if (k == 0) {
-                    const double ib = rcp_nr(b);
+                    const TC ib = rcp_tc(b);
                     ab0 = a * ib;
                     cb0 = cc * ib;
                     db0 = d * ib;
                 } else if (k == 1) {
-                    const double ib = rcp_nr(b);
+                    const TC ib = rcp_tc(b);
                     al[1] = a * ib;
                     ga[1] = cc * ib;
                     de[1] = d * ib;
                     sa = al[1];
                     sd = de[1];
                 } else {
-                    const double inv = rcp_nr(b - a * ga[k - 1]);
+                    const TC inv = rcp_tc(b - a * ga[k - 1]);
                     ga[k] = cc * inv;
                     de[k] = (d - a * de[k - 1]) * inv;
                     al[k] = -a * al[k - 1] * inv;
@@ -291,15 +308,15 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         }
         // reduced rows of this sub-segment -> red[f][ql][s]
         {
-            const double pi_last = -ga[M - 2] * pi;
-            const double r0 = rcp_nr(1.0 - cb0 * sa);
+            const TC pi_last = -ga[M - 2] * pi;
+            const TC r0 = rcp_tc(TC(1) - cb0 * sa);
             double* w = red + ql * RP + s;
-            w[0 * fstride] = r0 * ab0;
-            w[1 * fstride] = r0 * cb0 * pi_last;  // -r c0 gamma''_1, gamma''_1 = -pi_{M-1}
-            w[2 * fstride] = r0 * (db0 - cb0 * sd);
-            w[3 * fstride] = al[M - 1];
-            w[4 * fstride] = ga[M - 1];
-            w[5 * fstride] = de[M - 1];
+            w[0 * fstride] = (double)(r0 * ab0);
+            w[1 * fstride] = (double)(r0 * cb0 * pi_last);  // -r c0 gamma''_1, gamma''_1 = -pi_{M-1}
+            w[2 * fstride] = (double)(r0 * (db0 - cb0 * sd));
+            w[3 * fstride] = (double)al[M - 1];
+            w[4 * fstride] = (double)ga[M - 1];
+            w[5 * fstride] = (double)de[M - 1];
         }
         tile_cluster_sync(cl);
 
@@ -465,17 +482,29 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         if (valid) {
             const int q = c * nsc + ql;
             double* xp = args.X + (size_t)(q * M + M - 1) * ns + sys;  // row M-1
-            *xp = x_last;
+            // corrections are accumulated only by the FP32 inner solve of
+            // refinement (the FP64-arithmetic instantiations keep the plain
+            // store); the old x of all M rows is loaded before any store
+            double xo[M];
+            bool acc = false;
+            if constexpr (sizeof(TC) == 4) {
+                acc = args.accumulate != 0;
+                if (acc) {
+#pragma unroll
+                    for (int k = 0; k < M; ++k) xo[k] = xp[-(ptrdiff_t)(M - 1 - k) * (ptrdiff_t)ns];
+                }
+            }
+            *xp = acc ? xo[M - 1] + x_last : x_last;
             double xn = x_last;
 #pragma unroll
             for (int k = M - 2; k >= 1; --k) {
                 xp -= ns;
-                xn = de[k] - al[k] * x_first - ga[k] * xn;
+                xn = (double)de[k] - (double)al[k] * x_first - (double)ga[k] * xn;
                 nonfinite = fma(xn, 0.0, nonfinite);
-                *xp = xn;
+                *xp = acc ? xo[k] + xn : xn;
             }
             xp -= ns;
-            *xp = x_first;
+            *xp = acc ? xo[0] + x_first : x_first;
             nonfinite = fma(x_first, 0.0, fma(x_last, 0.0, nonfinite));
         }
     }

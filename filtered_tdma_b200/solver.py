@@ -121,6 +121,26 @@ class Solver:
                                         ns, nr, int(cyclic), _stream(stream)))
         return X
 
+    def solve_f32(self, A, B, C, D, X, n_sys=None, n_row=None, stream=None, cyclic=False):
+        """FP32-stored A, B, C, D (handle precision FP32_STORE or FP32_REFINE); X <- x in FP64."""
+        if torch is not None:
+            _check_dtype(A, B, C, D, dtype=torch.float32)
+            _check_dtype(X)
+        ns, nr = _shape(D, n_sys, n_row)
+        L.check(L.lib().btdma_solve_f32(self._h, _ptr(A), _ptr(B), _ptr(C), _ptr(D), _ptr(X),
+                                        ns, nr, int(cyclic), _stream(stream)))
+        return X
+
+    def set_refine(self, max_sweeps=3, eta_tol=8 * 2.0**-53):
+        """Refinement sweeps and backward-error bound of an FP32_REFINE handle."""
+        L.check(L.lib().btdma_set_refine(self._h, int(max_sweeps), float(eta_tol)))
+
+    def last_stats(self) -> dict:
+        """Refinement statistics of the most recent solve (blocking read)."""
+        st = L.Stats()
+        L.check(L.lib().btdma_last_stats(self._h, ctypes.byref(st)))
+        return st.as_dict()
+
     def set_eps_constant(self, eps_constant):
         L.check(L.lib().btdma_set_eps_constant(self._h, float(eps_constant)))
 

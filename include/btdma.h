@@ -153,6 +153,32 @@ int btdma_last_J(btdma_t h, int* J, int cap, int* n_out);
  * resets it to 0).  Bit 0: a wait timed out; bit 1: a non-finite solution. */
 int btdma_status(btdma_t h, unsigned* status);
 
+/* Iterative refinement (BTDMA_FP32_REFINE handles): at most max_sweeps
+ * correction sweeps (0..BTDMA_REFINE_MAX_SWEEPS, default 3); a system has
+ * converged when its normwise backward error
+ *     max|D - T x| / (max_j(|A_j| + |B_j| + |C_j|) * max|x| + max|D|)
+ * is at most eta_tol (default 8 * 2^-53 ~ 8.9e-16; the forward error is then at
+ * most cond(T) * eta_tol).  Systems still above it after the last sweep make
+ * the whole batch fall back to the FP64-arithmetic solve of BTDMA_FP32_STORE.
+ * No reference counterpart. */
+#define BTDMA_REFINE_MAX_SWEEPS 4
+int btdma_set_refine(btdma_t h, int max_sweeps, double eta_tol);
+
+/* Statistics of the most recent solve (blocking device->host read).
+ * For FP32_REFINE solves: converged_after[k] = systems that met the bound after
+ * k corrections (k = 0: the FP32 solve alone), n_fallback = systems that did not
+ * meet it after the last sweep (the batch was then solved again with FP64
+ * arithmetic), sweeps = correction sweeps that ran.  Other solves report zeros
+ * except n_systems.  Replaces nothing in the reference; the counterpart of its
+ * J report for the refinement path. */
+typedef struct btdma_stats {
+    int n_systems;
+    int sweeps;
+    int converged_after[BTDMA_REFINE_MAX_SWEEPS + 1];
+    int n_fallback;
+} btdma_stats;
+int btdma_last_stats(btdma_t h, btdma_stats* stats);
+
 /* Switch the method of an existing handle (rho, eps and J state are kept).  The
  * reference's FilteredTDMACUDA object offers v1 and v2 side by side
  * (filtered_tdma_cuda.hpp:173-180); this lets one handle do the same. */

@@ -45,6 +45,19 @@ def test_argument_checks(lib):
     assert _create(lib, 0, 10, 4096, 17)[0] == L.ERR_UNSUPPORTED  # above the cluster limit
     assert lib.btdma_solve(None, None, None, None, None, 1, 1, None) == L.ERR_ARG
     assert b"null" in lib.btdma_last_error()
+    assert lib.btdma_set_refine(None, 3, 1e-15) == L.ERR_ARG
+    assert lib.btdma_last_stats(None, None) == L.ERR_ARG
+
+
+def test_stats_struct_layout():
+    # btdma_stats: n_systems, sweeps, converged_after[BTDMA_REFINE_MAX_SWEEPS + 1], n_fallback
+    import os
+    import re
+    from filtered_tdma_b200 import _lib as L
+    hdr = open(os.path.join(os.path.dirname(__file__), "..", "include", "btdma.h")).read()
+    m = re.search(r"#define BTDMA_REFINE_MAX_SWEEPS (\d+)", hdr)
+    assert m and int(m.group(1)) == L.REFINE_MAX_SWEEPS
+    assert ctypes.sizeof(L.Stats) == 4 * (3 + L.REFINE_MAX_SWEEPS + 1)
 
 
 def test_backend_strings():

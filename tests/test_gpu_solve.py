@@ -242,19 +242,25 @@ def test_full_size_properties(cuda):
 
 
 # ----------------------------------------------------------------- FP32 storage
-def run_f32(cuda, A, B, C, D, precision, cyclic=False):
-    """FP32-stored inputs, FP64 solution; returns (x, widened inputs)."""
+def run_f32(cuda, A, B, C, D, precision, cyclic=False, refine=None, stats=None):
+    """FP32-stored inputs, FP64 solution; returns (x, widened inputs).  refine:
+    (max_sweeps, eta_tol) for FP32_REFINE; stats: a dict filled with the
+    refinement statistics."""
     import torch
     from filtered_tdma_b200 import _lib as L
     A32, B32, C32, D32 = [np.ascontiguousarray(x, dtype=np.float32) for x in (A, B, C, D)]
     n_row, n_sys = D.shape
     s = Solver("pascal", n_sys, n_row, 8 if n_row >= 48 else 2, precision=precision)
+    if refine is not None:
+        s.set_refine(*refine)
     dA, dB, dC, dD = [torch.from_numpy(x).to(cuda) for x in (A32, B32, C32, D32)]
     X = torch.zeros((n_row, n_sys), dtype=torch.float64, device=cuda)
     L.check(L.lib().btdma_solve_f32(s._h, dA.data_ptr(), dB.data_ptr(), dC.data_ptr(),
                                     dD.data_ptr(), X.data_ptr(), n_sys, n_row, int(cyclic),
                                     torch.cuda.current_stream().cuda_stream))
     assert s.status() == 0
+    if stats is not None:
+        stats.update(s.last_stats())
     wid = [x.astype(np.float64) for x in (A32, B32, C32, D32)]
     return host(X), wid
 
@@ -276,3 +282,56 @@ def test_fp32_store_cyclic_and_weak(cuda, orc):
     A, B, C, D = W.diag_dominant(256, 256, seed=4)
     x, wid = run_f32(cuda, A, B, C, D, L.FP32_STORE, cyclic=True)
     assert rel_err(x, orc.thomas_cyclic(*wid)) <= 1e-12
+
+
+# ---------------------------------------------- FP32 storage + iterative refinement
+@pytest.mark.parametrize("n_sys,n_row", [(1000, 128), (2048, 512), (96, 1024)])
+def test_fp32_refine_within_1e12(cuda, orc, n_sys, n_row):
+    """FP32 sweeps + FP64 residual refinement reach the FP64 solve of the widened
+    values; every system converges without the fallback, in at most 3 sweeps."""
+    from filtered_tdma_b200 import _lib as L
+    A, B, C, D = W.diag_dominant(n_sys, n_row, seed=n_row + 6)
+    st = {}
+    x, wid = run_f32(cuda, A, B, C, D, L.FP32_REFINE, stats=st)
+    assert rel_err(x, orc.thomas(*wid)) <= 1e-12
+    assert st["n_systems"] == n_sys
+    assert st["n_fallback"] == 0
+    assert sum(st["converged_after"]) == n_sys
+    assert st["converged_after"][0] == 0  # the FP32 solve alone is not FP64-accurate
+    assert 1 <= st["sweeps"] <= 3
+
+
+def test_fp32_refine_weak_dominance_needs_more_sweeps(cuda, orc):
+    """rho in [0.45, 0.499] (cond(T) up to ~1e3): refinement still converges,
+    with at least as many sweeps as the strongly dominant batch."""
+    from filtered_tdma_b200 import _lib as L
+    strong, weak = {}, {}
+    A, B, C, D = W.diag_dominant(2048, 512, seed=31)
+    run_f32(cuda, A, B, C, D, L.FP32_REFINE, stats=strong)
+    A, B, C, D = W.weak_dominance(2048, 512, seed=32)
+    x, wid = run_f32(cuda, A, B, C, D, L.FP32_REFINE, stats=weak)
+    assert rel_err(x, orc.thomas(*wid)) <= 1e-12
+    assert weak["n_fallback"] == 0
+    assert weak["sweeps"] >= strong["sweeps"]
+
+
+def test_fp32_refine_fallback(cuda, orc):
+    """No sweep allowed, or an unreachable bound: every system falls back to the
+    FP64-arithmetic solve, which still meets 1e-12."""
+    from filtered_tdma_b200 import _lib as L
+    A, B, C, D = W.diag_dominant(512, 256, seed=33)
+    for refine in ((0, 8 * 2.0**-53), (2, 1e-30)):
+        st = {}
+        x, wid = run_f32(cuda, A, B, C, D, L.FP32_REFINE, refine=refine, stats=st)
+        assert rel_err(x, orc.thomas(*wid)) <= 1e-12
+        assert st["n_fallback"] == 512
+        assert st["sweeps"] == refine[0]
+
+
+def test_fp32_refine_cyclic(cuda, orc):
+    from filtered_tdma_b200 import _lib as L
+    A, B, C, D = W.diag_dominant(256, 256, seed=34)
+    st = {}
+    x, wid = run_f32(cuda, A, B, C, D, L.FP32_REFINE, cyclic=True, stats=st)
+    assert rel_err(x, orc.thomas_cyclic(*wid)) <= 1e-12
+    assert st["n_fallback"] == 0
