@@ -485,7 +485,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             // corrections are accumulated only by the FP32 inner solve of
             // refinement (the FP64-arithmetic instantiations keep the plain
             // store); the old x of all M rows is loaded before any store
-            double xo[M];
+            double xo[M] = {};
             bool acc = false;
             if constexpr (sizeof(TC) == 4) {
                 acc = args.accumulate != 0;
