@@ -252,6 +252,7 @@ def main():
         run_reference(args, rank, world)
         return
 
+    import numpy as np
     import torch
     import torch.distributed as dist
     torch.cuda.set_device(local)
@@ -371,6 +372,44 @@ def main():
         f32_variant("fp32_refine_weak_P8", L.FP32_REFINE, arrs)
         f32_variant("fp32_store_weak_P8", L.FP32_STORE, arrs)
         del arrs
+
+        # Ragged batch: 10000 systems, n log-uniform in [16, 4096] (CSR offsets),
+        # 25 % periodic, r log-uniform in [0.05, 20]; autotuned per length bucket.
+        # (FP32-stored values, widened for the FP64 solve, so both solve one system)
+        rA, rB, rC, rD, roff, rper = W.ragged_batch(10000, seed=5, dtype=np.float32)
+        rrows = int(roff[-1])
+        rX = torch.empty(rrows, dtype=torch.float64, device=dev)
+        ref_x = None
+        for name, prec, dt, bpr in (("ragged_fp64", L.FP64, torch.float64, 40),
+                                    ("ragged_fp32_store", L.FP32_STORE, torch.float32, 24)):
+            dA, dB, dC, dD = [torch.from_numpy(v).to(dev).to(dt) for v in (rA, rB, rC, rD)]
+            s = Solver("pascal", 10000, 64, 2, precision=prec)
+            plan = s.ragged_autotune(dA, dB, dC, dD, rX, roff, rper)
+            for _ in range(3):
+                s.solve_ragged(dA, dB, dC, dD, rX, roff, rper)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(nrep):
+                s.solve_ragged(dA, dB, dC, dD, rX, roff, rper)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / nrep
+            v = {"rows_per_s": rrows / (ms * 1e-3), "ms_per_step": ms, "rows": rrows,
+                 "hbm_gbs_algorithmic": bpr * rrows / (ms * 1e-3) / 1e9,
+                 "frac_of_peak": bpr * rrows / (ms * 1e-3) / 1e9 / peak,
+                 "launches_per_step": len(plan),
+                 "plan": [{k: b[k] for k in ("periodic", "n_systems", "n_row_min", "n_row_max",
+                                             "lanes_per_system", "warps_per_cta")} for b in plan]}
+            if ref_x is None:
+                ref_x = rX.clone()
+            else:
+                v["max_rel_err_vs_ragged_fp64"] = ((rX - ref_x).abs().max()
+                                                    / ref_x.abs().max()).item()
+            variants[name] = v
+            s.close()
+            del dA, dB, dC, dD
+        del rX, ref_x
 
     # ---------------------------------------------------------- end to end
     e2e = None

@@ -25,6 +25,8 @@ EXPORTS = (
     "btdma_set_eps_constant", "btdma_set_rho", "btdma_set_rho_all", "btdma_last_J",
     "btdma_status", "btdma_set_method", "btdma_segments", "btdma_last_error",
     "btdma_solve_noalloc", "btdma_solve_f32", "btdma_set_refine", "btdma_last_stats",
+    "btdma_solve_ragged", "btdma_solve_ragged_f32", "btdma_ragged_autotune",
+    "btdma_ragged_plan_info",
 )
 NOALLOC_MAX_ELEMS = 1 << 20
 REFINE_MAX_SWEEPS = 4
@@ -39,6 +41,17 @@ class Stats(ctypes.Structure):
     def as_dict(self) -> dict:
         return {"n_systems": self.n_systems, "sweeps": self.sweeps,
                 "converged_after": list(self.converged_after), "n_fallback": self.n_fallback}
+
+
+class RaggedBucket(ctypes.Structure):
+    """btdma_ragged_bucket of include/btdma.h."""
+    _fields_ = [("periodic", ctypes.c_int), ("n_systems", ctypes.c_int),
+                ("n_row_min", ctypes.c_int), ("n_row_max", ctypes.c_int),
+                ("lanes_per_system", ctypes.c_int), ("warps_per_cta", ctypes.c_int),
+                ("tuned_ms", ctypes.c_float)]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
 
 
 class BtdmaError(RuntimeError):
@@ -75,6 +88,11 @@ def lib():
         L.btdma_solve_f32.argtypes = [vp, vp, vp, vp, vp, vp, i, i, i, vp]
         L.btdma_set_refine.argtypes = [vp, i, d]
         L.btdma_last_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+        L.btdma_solve_ragged.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i, vp]
+        L.btdma_solve_ragged_f32.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i, vp]
+        L.btdma_ragged_autotune.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i, vp]
+        L.btdma_ragged_plan_info.argtypes = [vp, ctypes.POINTER(RaggedBucket), i,
+                                             ctypes.POINTER(i)]
         L.btdma_last_error.restype = ctypes.c_char_p
         for name in EXPORTS:
             if name != "btdma_last_error":

@@ -15,6 +15,7 @@
 
 #include "btdma_common.cuh"
 #include "k_filtered_j.cuh"
+#include "k_ragged.cuh"
 #include "k_refine.cuh"
 #include "k_segment.cuh"
 #include "k_thomas.cuh"
@@ -41,6 +42,16 @@ struct btdma_handle {
     double eta_tol = 8.0 * 0x1p-53;
     int last_n_sys = 0;
     bool last_refined = false;
+    // ragged batches: the plan of the most recent row-offset layout
+    struct RagBucket {
+        int cyc, first, count, nmin, nmax, P, warps, mcap;
+        float best_ms;
+    };
+    std::vector<long long> rag_off;        // host copy of the offsets of the plan
+    std::vector<unsigned char> rag_per;    // host copy of the periodic flags
+    std::vector<RagBucket> rag_buckets;
+    long long* rag_d_off = nullptr;        // device offsets [n_sys + 1]
+    int* rag_d_list = nullptr;             // device system lists, bucket by bucket
 };
 
 namespace {
@@ -501,6 +512,8 @@ int btdma_destroy(btdma_t h) {
     cudaFree(h->resid);
     cudaFree(h->iters);
     cudaFree(h->open);
+    cudaFree(h->rag_d_off);
+    cudaFree(h->rag_d_list);
     delete h;
     return BTDMA_OK;
 }
@@ -723,3 +736,238 @@ extern "C" int btdma_solve_noalloc(const double* A, const double* B, const doubl
     return BTDMA_OK;
 }
 
+
+// ------------------------------------------------------------------ ragged
+namespace {
+
+// Lanes per system for a bucket whose systems have nmin..nmax rows: about
+// 12 rows per lane, a power of two, at most 32, and at least 3 rows per lane
+// for the shortest system.
+int rag_default_P(int nmin, int nmax) {
+    int P = 1;
+    while (P < 32 && nmax / (2 * P) >= 12 && nmin / (2 * P) >= 3) P <<= 1;
+    return P;
+}
+
+int rag_mcap(int nmax, int P) { return (nmax + P - 1) / P; }
+
+// Largest warps-per-CTA (<= 8) whose shared memory fits.
+int rag_fit_warps(int want, int mcap) {
+    int w = want;
+    while (w > 1 && rag_smem_bytes(w, mcap) > (size_t)max_smem_optin()) w >>= 1;
+    return rag_smem_bytes(w, mcap) <= (size_t)max_smem_optin() ? w : 0;
+}
+
+int rag_plan(btdma_t h, const long long* off, const unsigned char* per, int n_sys) {
+    if (n_sys <= 0) return fail(BTDMA_ERR_ARG, "n_sys must be positive");
+    if (!off) return fail(BTDMA_ERR_ARG, "null row offsets");
+    if (off[0] != 0) return fail(BTDMA_ERR_ARG, "row_offsets[0] must be 0");
+    const bool same = (int)h->rag_off.size() == n_sys + 1 &&
+                      std::equal(off, off + n_sys + 1, h->rag_off.begin()) &&
+                      (per ? (h->rag_per.size() == (size_t)n_sys &&
+                              std::equal(per, per + n_sys, h->rag_per.begin()))
+                           : h->rag_per.empty());
+    if (same && h->rag_d_off) return BTDMA_OK;
+    // bucket key: (periodic, ceil(log2 n))
+    std::vector<int> key(n_sys);
+    for (int i = 0; i < n_sys; ++i) {
+        const long long n = off[i + 1] - off[i];
+        if (n < 3) return fail(BTDMA_ERR_SEGMENT, "system %d has %lld rows (needs >= 3)", i, n);
+        if (n > (1 << 20)) return fail(BTDMA_ERR_SIZE, "system %d has %lld rows (> 2^20)", i, n);
+        int lg = 0;
+        while ((1LL << lg) < n) ++lg;
+        key[i] = (per && per[i] ? 64 : 0) + lg;
+    }
+    std::vector<int> order(n_sys);
+    for (int i = 0; i < n_sys; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return key[x] < key[y]; });
+    std::vector<btdma_handle::RagBucket> bk;
+    for (int i = 0; i < n_sys;) {
+        int j = i;
+        int nmin = INT32_MAX, nmax = 0;
+        while (j < n_sys && key[order[j]] == key[order[i]]) {
+            const int n = (int)(off[order[j] + 1] - off[order[j]]);
+            nmin = std::min(nmin, n);
+            nmax = std::max(nmax, n);
+            ++j;
+        }
+        btdma_handle::RagBucket b{};
+        b.cyc = key[order[i]] >= 64 ? 1 : 0;
+        b.first = i;
+        b.count = j - i;
+        b.nmin = nmin;
+        b.nmax = nmax;
+        b.P = rag_default_P(nmin, nmax);
+        b.mcap = rag_mcap(nmax, b.P);
+        b.warps = rag_fit_warps(4, b.mcap);
+        if (b.warps == 0)
+            return fail(BTDMA_ERR_UNSUPPORTED, "systems of %d rows exceed shared memory", nmax);
+        b.best_ms = 0.f;
+        bk.push_back(b);
+        i = j;
+    }
+    cudaFree(h->rag_d_off);
+    cudaFree(h->rag_d_list);
+    h->rag_d_off = nullptr;
+    h->rag_d_list = nullptr;
+    h->rag_off.clear();
+    CK(cudaMalloc(&h->rag_d_off, sizeof(long long) * (n_sys + 1)));
+    CK(cudaMalloc(&h->rag_d_list, sizeof(int) * n_sys));
+    CK(cudaMemcpy(h->rag_d_off, off, sizeof(long long) * (n_sys + 1), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->rag_d_list, order.data(), sizeof(int) * n_sys, cudaMemcpyHostToDevice));
+    h->rag_off.assign(off, off + n_sys + 1);
+    if (per)
+        h->rag_per.assign(per, per + n_sys);
+    else
+        h->rag_per.clear();
+    h->rag_buckets = bk;
+    return BTDMA_OK;
+}
+
+template <typename TIN, bool CYC>
+int rag_launch_t(const RagArgs& a, int warps, cudaStream_t st) {
+    auto kern = ragged_kernel<TIN, CYC>;
+    static bool attr_done = false;
+    if (!attr_done) {
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                max_smem_optin()));
+        attr_done = true;
+    }
+    const int per_cta = warps * (32 / a.P);
+    const int grid = (a.count + per_cta - 1) / per_cta;
+    kern<<<grid, 32 * warps, rag_smem_bytes(warps, a.mcap), st>>>(a);
+    CK(cudaGetLastError());
+    return BTDMA_OK;
+}
+
+template <typename TIN>
+int rag_launch_bucket(btdma_t h, const btdma_handle::RagBucket& b, int P, int warps,
+                      const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X,
+                      cudaStream_t st) {
+    RagArgs a{};
+    a.A = A;
+    a.B = B;
+    a.C = C;
+    a.D = D;
+    a.X = X;
+    a.off = h->rag_d_off;
+    a.list = h->rag_d_list + b.first;
+    a.count = b.count;
+    a.P = P;
+    a.mcap = rag_mcap(b.nmax, P);
+    a.status = h->status;
+    return b.cyc ? rag_launch_t<TIN, true>(a, warps, st) : rag_launch_t<TIN, false>(a, warps, st);
+}
+
+template <typename TIN>
+int rag_solve(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X,
+              const long long* off, const unsigned char* per, int n_sys, cudaStream_t st) {
+    if (!h) return fail(BTDMA_ERR_ARG, "null handle");
+    if (!A || !B || !C || !D || !X) return fail(BTDMA_ERR_ARG, "null array");
+    if (h->method != BTDMA_PASCAL)
+        return fail(BTDMA_ERR_UNSUPPORTED, "ragged batches are solved by PaScaL only");
+    const bool f32 = sizeof(TIN) == 4;
+    if (f32 != (h->precision != BTDMA_FP64))
+        return fail(BTDMA_ERR_ARG, "array type does not match the handle's precision");
+    int rc = rag_plan(h, off, per, n_sys);
+    if (rc) return rc;
+    h->last_stream = st;
+    h->last_n_sys = n_sys;
+    h->last_refined = false;
+    for (const auto& b : h->rag_buckets) {
+        rc = rag_launch_bucket<TIN>(h, b, b.P, b.warps, A, B, C, D, X, st);
+        if (rc) return rc;
+    }
+    return BTDMA_OK;
+}
+
+// Times every (P, warps) candidate of every bucket on the given batch and keeps
+// the fastest (CUDA events on the stream; the batch's X is overwritten).
+template <typename TIN>
+int rag_tune(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X,
+             const long long* off, const unsigned char* per, int n_sys, cudaStream_t st) {
+    int rc = rag_solve<TIN>(h, A, B, C, D, X, off, per, n_sys, st);  // plan + warm-up
+    if (rc) return rc;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    for (auto& b : h->rag_buckets) {
+        float best = 1e30f;
+        int bestP = b.P, bestW = b.warps;
+        for (int P = 1; P <= 32; P <<= 1) {
+            if (b.nmin / P < 3) break;
+            for (int w = 1; w <= 8; w <<= 1) {
+                if (rag_fit_warps(w, rag_mcap(b.nmax, P)) != w) break;
+                float ms = 0.f;
+                for (int rep = 0; rep < 3; ++rep) {  // best of 3
+                    CK(cudaEventRecord(e0, st));
+                    rc = rag_launch_bucket<TIN>(h, b, P, w, A, B, C, D, X, st);
+                    if (rc) break;
+                    CK(cudaEventRecord(e1, st));
+                    CK(cudaEventSynchronize(e1));
+                    float t = 0.f;
+                    CK(cudaEventElapsedTime(&t, e0, e1));
+                    ms = rep == 0 ? t : std::min(ms, t);
+                }
+                if (rc) break;
+                if (ms < best) {
+                    best = ms;
+                    bestP = P;
+                    bestW = w;
+                }
+            }
+            if (rc) break;
+        }
+        if (rc) break;
+        b.P = bestP;
+        b.warps = bestW;
+        b.mcap = rag_mcap(b.nmax, bestP);
+        b.best_ms = best;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
+
+}  // namespace
+
+int btdma_solve_ragged(btdma_t h, const double* A, const double* B, const double* C,
+                       const double* D, double* X, const long long* row_offsets,
+                       const unsigned char* is_periodic, int n_sys, cudaStream_t stream) {
+    return rag_solve<double>(h, A, B, C, D, X, row_offsets, is_periodic, n_sys, stream);
+}
+
+int btdma_solve_ragged_f32(btdma_t h, const float* A, const float* B, const float* C,
+                           const float* D, double* X, const long long* row_offsets,
+                           const unsigned char* is_periodic, int n_sys, cudaStream_t stream) {
+    return rag_solve<float>(h, A, B, C, D, X, row_offsets, is_periodic, n_sys, stream);
+}
+
+int btdma_ragged_autotune(btdma_t h, const void* A, const void* B, const void* C, const void* D,
+                          double* X, const long long* row_offsets,
+                          const unsigned char* is_periodic, int n_sys, cudaStream_t stream) {
+    if (!h) return fail(BTDMA_ERR_ARG, "null handle");
+    if (h->precision == BTDMA_FP64)
+        return rag_tune<double>(h, static_cast<const double*>(A), static_cast<const double*>(B),
+                                static_cast<const double*>(C), static_cast<const double*>(D), X,
+                                row_offsets, is_periodic, n_sys, stream);
+    return rag_tune<float>(h, static_cast<const float*>(A), static_cast<const float*>(B),
+                           static_cast<const float*>(C), static_cast<const float*>(D), X,
+                           row_offsets, is_periodic, n_sys, stream);
+}
+
+int btdma_ragged_plan_info(btdma_t h, btdma_ragged_bucket* out, int cap, int* n_out) {
+    if (!h || !n_out) return fail(BTDMA_ERR_ARG, "null argument");
+    *n_out = (int)h->rag_buckets.size();
+    for (int i = 0; i < cap && i < *n_out; ++i) {
+        const auto& b = h->rag_buckets[i];
+        out[i].periodic = b.cyc;
+        out[i].n_systems = b.count;
+        out[i].n_row_min = b.nmin;
+        out[i].n_row_max = b.nmax;
+        out[i].lanes_per_system = b.P;
+        out[i].warps_per_cta = b.warps;
+        out[i].tuned_ms = b.best_ms;
+    }
+    return BTDMA_OK;
+}

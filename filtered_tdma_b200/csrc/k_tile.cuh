@@ -47,6 +47,7 @@
 #include <cooperative_groups.h>
 
 #include "btdma_common.cuh"
+#include "k_reduced.cuh"
 
 namespace btdma {
 
@@ -126,18 +127,6 @@ __device__ __forceinline__ void tile_cluster_sync(int cl) {
     } else {
         __syncthreads();
     }
-}
-
-// One PCR row update of  l x_{i-dl} + x_i + u x_{i+dl} = r  with its
-// neighbours (m: row i-dl, p: row i+dl).
-__device__ __forceinline__ void pcr_step(double& l, double& u, double& r, double lm, double um,
-                                         double rm, double lp, double up, double rp) {
-    const double ib = rcp_nr(1.0 - l * um - u * lp);
-    const double nl = -l * lm * ib;
-    const double nu = -u * up * ib;
-    r = (r - l * rm - u * rp) * ib;
-    l = nl;
-    u = nu;
 }
 
 // TIN: element type of A, B, C, D in HBM (double, or float).  TC: arithmetic of
@@ -343,58 +332,8 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                     u1 = src[4 * fstride];
                     r1 = src[5 * fstride];
                 }
-                // next sub-segment's first row (zero past the end unless periodic)
-                const int pn = (CYCLIC && p == nseg - 1) ? 0 : p + 1;
-                double l0n = __shfl_sync(0xffffffffu, l0, pn, W);
-                double u0n = __shfl_sync(0xffffffffu, u0, pn, W);
-                double r0n = __shfl_sync(0xffffffffu, r0, pn, W);
-                if (!CYCLIC && p + 1 >= nseg) l0n = u0n = r0n = 0.0;
-                double al_ = 0, cl_ = 0, dl_ = 0;
-                {
-                    const double ib = rcp_nr(1.0 - l1 * u0 - u1 * l0n);
-                    al_ = -l1 * l0 * ib;
-                    cl_ = -u1 * u0n * ib;
-                    dl_ = (r1 - l1 * r0 - u1 * r0n) * ib;
-                }
-                if (!act) al_ = cl_ = dl_ = 0.0;
-                double xl;
-                if (CYCLIC && nseg == 1) {
-                    xl = dl_ * rcp_nr(1.0 + al_ + cl_);
-                } else {
-                    bool solved = false;
-                    xl = 0.0;
-                    for (int dl = 1; dl < nseg; dl <<= 1) {
-                        int im = p - dl, ip = p + dl;
-                        if (CYCLIC) {
-                            im = im < 0 ? im + nseg : im;
-                            ip = ip >= nseg ? ip - nseg : ip;
-                        }
-                        double lm = __shfl_sync(0xffffffffu, al_, im & (W - 1), W);
-                        double um = __shfl_sync(0xffffffffu, cl_, im & (W - 1), W);
-                        double rm = __shfl_sync(0xffffffffu, dl_, im & (W - 1), W);
-                        double lp = __shfl_sync(0xffffffffu, al_, ip & (W - 1), W);
-                        double up = __shfl_sync(0xffffffffu, cl_, ip & (W - 1), W);
-                        double rp = __shfl_sync(0xffffffffu, dl_, ip & (W - 1), W);
-                        if (!CYCLIC) {
-                            if (im < 0) lm = um = rm = 0.0;
-                            if (ip >= nseg) lp = up = rp = 0.0;
-                        }
-                        if (CYCLIC && 2 * dl == nseg) {
-                            // p-dl and p+dl are the same row j: 2x2 system in x_p, x_j
-                            const double si = al_ + cl_, sj = lm + um;
-                            xl = (dl_ - si * rm) * rcp_nr(1.0 - si * sj);
-                            solved = true;
-                        } else {
-                            pcr_step(al_, cl_, dl_, lm, um, rm, lp, up, rp);
-                        }
-                    }
-                    if (!solved) xl = dl_;
-                }
-                // x_first(p) = r0 - l0 xL(p-1) - u0 xL(p)
-                const int pm = (CYCLIC && p == 0) ? nseg - 1 : p - 1;
-                double xlm = __shfl_sync(0xffffffffu, xl, pm & (W - 1), W);
-                if (!CYCLIC && p == 0) xlm = 0.0;
-                const double xf = r0 - l0 * xlm - u0 * xl;
+                double xf, xl;
+                reduced_solve_shfl<CYCLIC>(l0, u0, r0, l1, u1, r1, p, nseg, W, act, xf, xl);
                 if (act) {
                     const int owner = p / nsc;
                     double* dst = xr + (p % nsc) * RP + c * sub + sp;

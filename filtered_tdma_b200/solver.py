@@ -72,6 +72,18 @@ def _check_dtype(*xs, dtype=None):
             raise TypeError(f"expected {want} arrays, got {x.dtype}")
 
 
+def _ragged_host(row_offsets, periodic):
+    import numpy as np
+    off = np.ascontiguousarray(row_offsets, dtype=np.int64)
+    n_sys = off.shape[0] - 1
+    per = None
+    if periodic is not None:
+        per = np.ascontiguousarray(periodic, dtype=np.uint8)
+        if per.shape[0] != n_sys:
+            raise ValueError("periodic needs one flag per system")
+    return off, per, n_sys
+
+
 class Solver:
     """One btdma handle: method, capacity (n_sys, n_row), segments P."""
 
@@ -130,6 +142,36 @@ class Solver:
         L.check(L.lib().btdma_solve_f32(self._h, _ptr(A), _ptr(B), _ptr(C), _ptr(D), _ptr(X),
                                         ns, nr, int(cyclic), _stream(stream)))
         return X
+
+    def solve_ragged(self, A, B, C, D, X, row_offsets, periodic=None, stream=None):
+        """Ragged batch (CSR layout, see btdma_solve_ragged): A..D are 1-D device
+        arrays (float64, or float32 with an FP32 handle), X float64; row_offsets
+        (n_sys + 1, int64) and periodic (n_sys, uint8 or None) are host arrays."""
+        off, per, n_sys = _ragged_host(row_offsets, periodic)
+        f32 = torch is not None and isinstance(A, torch.Tensor) and A.dtype == torch.float32
+        if torch is not None:
+            _check_dtype(A, B, C, D, dtype=torch.float32 if f32 else torch.float64)
+            _check_dtype(X)
+        f = L.lib().btdma_solve_ragged_f32 if f32 else L.lib().btdma_solve_ragged
+        L.check(f(self._h, _ptr(A), _ptr(B), _ptr(C), _ptr(D), _ptr(X), off.ctypes.data,
+                  per.ctypes.data if per is not None else None, n_sys, _stream(stream)))
+        return X
+
+    def ragged_autotune(self, A, B, C, D, X, row_offsets, periodic=None, stream=None):
+        """Pick lanes per system and warps per CTA for every length bucket by
+        timing them on this batch (X is overwritten); returns the plan."""
+        off, per, n_sys = _ragged_host(row_offsets, periodic)
+        L.check(L.lib().btdma_ragged_autotune(
+            self._h, _ptr(A), _ptr(B), _ptr(C), _ptr(D), _ptr(X), off.ctypes.data,
+            per.ctypes.data if per is not None else None, n_sys, _stream(stream)))
+        return self.ragged_plan()
+
+    def ragged_plan(self) -> list:
+        n = ctypes.c_int()
+        L.check(L.lib().btdma_ragged_plan_info(self._h, None, 0, ctypes.byref(n)))
+        arr = (L.RaggedBucket * max(1, n.value))()
+        L.check(L.lib().btdma_ragged_plan_info(self._h, arr, n.value, ctypes.byref(n)))
+        return [arr[i].as_dict() for i in range(n.value)]
 
     def set_refine(self, max_sweeps=3, eta_tol=8 * 2.0**-53):
         """Refinement sweeps and backward-error bound of an FP32_REFINE handle."""

@@ -12,6 +12,9 @@ These generators stand in for them:
 * ``diag_dominant``   per-system r drawn log-uniform in [r_lo, r_hi]
                       (A = C = -r, B = 1+2r), D uniform in [-1, 1].
 * ``weak_dominance``  per-system rho uniform in [rho_lo, rho_hi], r = rho/(1-2rho).
+* ``ragged_batch``    systems of different lengths (n log-uniform in
+                      [n_lo, n_hi]) stored back to back with CSR row offsets,
+                      a fraction of them periodic, per-system r log-uniform.
 
 All arrays are [n_row, n_sys] row-interleaved (row j of system i at
 j*n_sys + i), as the reference lays them out.  numpy generation (``device=None``)
@@ -89,3 +92,25 @@ def _torch_batch(_unused, n_sys, n_row, seed, dtype, device, const_r=None, log_r
     C = A.clone()
     B = (1.0 + 2.0 * r).expand(n_row, n_sys).contiguous().to(tdt)
     return A, B, C, D.to(tdt)
+
+
+def ragged_batch(n_sys: int, n_lo: int = 16, n_hi: int = 4096, periodic_frac: float = 0.25,
+                 r_lo: float = 0.05, r_hi: float = 20.0, seed: int = 5, dtype=np.float64):
+    """Ragged batch in the CSR layout: system i occupies rows
+    [off[i], off[i+1]) of the 1-D arrays A, B, C, D (contiguous).  n_i is
+    floor(exp(U[ln n_lo, ln n_hi])), a fraction periodic_frac of the systems is
+    periodic, r_i is log-uniform in [r_lo, r_hi] (A = C = -r_i, B = 1 + 2 r_i) and
+    D is uniform in [-1, 1].  Returns (A, B, C, D, off int64, periodic uint8)."""
+    rng = np.random.default_rng(seed)
+    n = np.floor(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi), size=n_sys))).astype(np.int64)
+    n = np.clip(n, n_lo, n_hi)
+    periodic = (rng.uniform(size=n_sys) < periodic_frac).astype(np.uint8)
+    r = 10.0 ** rng.uniform(np.log10(r_lo), np.log10(r_hi), size=n_sys)
+    off = np.zeros(n_sys + 1, dtype=np.int64)
+    np.cumsum(n, out=off[1:])
+    rr = np.repeat(r, n)
+    A = np.ascontiguousarray(-rr, dtype=dtype)
+    C = np.ascontiguousarray(-rr, dtype=dtype)
+    B = np.ascontiguousarray(1.0 + 2.0 * rr, dtype=dtype)
+    D = np.ascontiguousarray(rng.uniform(-1.0, 1.0, size=int(off[-1])), dtype=dtype)
+    return A, B, C, D, off, periodic

@@ -179,6 +179,46 @@ typedef struct btdma_stats {
 } btdma_stats;
 int btdma_last_stats(btdma_t h, btdma_stats* stats);
 
+/* Ragged batch: n_sys systems of different lengths stored back to back, system
+ * i in rows [row_offsets[i], row_offsets[i+1]) of A, B, C, D (contiguous; the
+ * CSR layout), solved by PaScaL with one group of lanes per system into X
+ * (X may equal D).  row_offsets (n_sys + 1 entries, starting at 0) and
+ * is_periodic (n_sys flags, or NULL for none) are HOST arrays: the first call
+ * with a new layout builds a plan (buckets of similar length, device copies of
+ * the offsets) and later calls with the same layout reuse it, so build it
+ * before capturing a graph.  Every system needs >= 3 rows.  Periodic systems
+ * couple row 0 and the last row through A[first] and C[last]; non-periodic ones
+ * ignore those two entries.  The _f32 form takes FP32-stored arrays (handle
+ * precision FP32_STORE or FP32_REFINE) and computes in FP64 on the widened
+ * values.  PaScaL handles only.  The reference solves one uniform batch per
+ * call; this replaces looping its solve over equal-length groups. */
+int btdma_solve_ragged(btdma_t h, const double* A, const double* B, const double* C,
+                       const double* D, double* X, const long long* row_offsets,
+                       const unsigned char* is_periodic, int n_sys, cudaStream_t stream);
+int btdma_solve_ragged_f32(btdma_t h, const float* A, const float* B, const float* C,
+                           const float* D, double* X, const long long* row_offsets,
+                           const unsigned char* is_periodic, int n_sys, cudaStream_t stream);
+
+/* Autotuner of ragged solves: times, for every bucket of the plan, each choice of
+ * lanes per system (1..32, at least 3 rows per lane) and warps per CTA (1..8)
+ * on this batch and keeps the fastest for later solves of the same layout.
+ * A..D are double or float as the handle's precision says; X is overwritten.
+ * Blocking (it synchronises the stream). */
+int btdma_ragged_autotune(btdma_t h, const void* A, const void* B, const void* C, const void* D,
+                          double* X, const long long* row_offsets,
+                          const unsigned char* is_periodic, int n_sys, cudaStream_t stream);
+
+/* The buckets of the current ragged plan and their launch shapes. */
+typedef struct btdma_ragged_bucket {
+    int periodic;
+    int n_systems;
+    int n_row_min, n_row_max;
+    int lanes_per_system;
+    int warps_per_cta;
+    float tuned_ms; /* fastest time measured by the autotuner (0 before tuning) */
+} btdma_ragged_bucket;
+int btdma_ragged_plan_info(btdma_t h, btdma_ragged_bucket* out, int cap, int* n_out);
+
 /* Switch the method of an existing handle (rho, eps and J state are kept).  The
  * reference's FilteredTDMACUDA object offers v1 and v2 side by side
  * (filtered_tdma_cuda.hpp:173-180); this lets one handle do the same. */

@@ -1,0 +1,117 @@
+"""Ragged batches (CSR row offsets, systems of different lengths, some periodic)
+through the C ABI, against the oracle's serial Thomas / periodic Thomas solved
+system by system (tdma_many / tdma_cyclic_many with n_sys = 1).
+
+PaScaL's segmented elimination is not the serial order, so the bar is the
+1e-12 relative bound of the segmented FP64 paths; FP32-stored batches are
+compared with the oracle on the widened values.
+"""
+import numpy as np
+import pytest
+
+from filtered_tdma_b200 import Solver
+from filtered_tdma_b200 import _lib as L
+from filtered_tdma_b200 import workloads as W
+
+
+def ragged_oracle(orc, A, B, C, D, off, per):
+    x = np.empty_like(np.asarray(D, dtype=np.float64))
+    for i in range(len(off) - 1):
+        s = slice(int(off[i]), int(off[i + 1]))
+        cols = [np.asarray(v[s], dtype=np.float64)[:, None] for v in (A, B, C, D)]
+        f = orc.thomas_cyclic if per[i] else orc.thomas
+        x[s] = f(*cols)[:, 0]
+    return x
+
+
+def per_system_err(x, ref, off):
+    worst = 0.0
+    for i in range(len(off) - 1):
+        s = slice(int(off[i]), int(off[i + 1]))
+        worst = max(worst, float(np.max(np.abs(x[s] - ref[s])) / np.max(np.abs(ref[s]))))
+    return worst
+
+
+def solve_on_device(cuda, arrays, off, per, precision=L.FP64, tune=False, inplace=False):
+    import torch
+    dA, dB, dC, dD = [torch.from_numpy(np.ascontiguousarray(v)).to(cuda) for v in arrays]
+    n_rows = int(off[-1])
+    s = Solver("pascal", len(off) - 1, 64, 2, precision=precision)
+    X = dD if inplace else torch.zeros(n_rows, dtype=torch.float64, device=cuda)
+    if tune:
+        plan = s.ragged_autotune(dA, dB, dC, dD, X, off, per)
+        assert all(b["tuned_ms"] > 0 for b in plan)
+        dD = torch.from_numpy(np.ascontiguousarray(arrays[3])).to(cuda)
+        if inplace:
+            X = dD
+    s.solve_ragged(dA, dB, dC, dD, X, off, per)
+    torch.cuda.synchronize()
+    assert s.status() == 0
+    return X.cpu().numpy(), s.ragged_plan()
+
+
+@pytest.mark.gpu
+def test_ragged_config_shape_fp64(cuda, orc):
+    # the ragged workload's distributions (n log-uniform in [16, 4096], 25 %
+    # periodic, r log-uniform in [0.05, 20]) at 400 systems
+    A, B, C, D, off, per = W.ragged_batch(400, seed=5)
+    ref = ragged_oracle(orc, A, B, C, D, off, per)
+    x, plan = solve_on_device(cuda, (A, B, C, D), off, per)
+    assert per_system_err(x, ref, off) <= 1e-12
+    assert sum(b["n_systems"] for b in plan) == 400
+    assert {b["periodic"] for b in plan} == {0, 1}
+
+
+@pytest.mark.gpu
+def test_ragged_autotuned_and_inplace(cuda, orc):
+    A, B, C, D, off, per = W.ragged_batch(300, seed=51)
+    ref = ragged_oracle(orc, A, B, C, D, off, per)
+    x, plan = solve_on_device(cuda, (A, B, C, D), off, per, tune=True, inplace=True)
+    assert per_system_err(x, ref, off) <= 1e-12
+    for b in plan:
+        assert b["lanes_per_system"] & (b["lanes_per_system"] - 1) == 0
+        assert b["n_row_min"] // b["lanes_per_system"] >= 3
+
+
+@pytest.mark.gpu
+def test_ragged_fp32_storage(cuda, orc):
+    A, B, C, D, off, per = W.ragged_batch(300, seed=52, dtype=np.float32)
+    wid = [v.astype(np.float64) for v in (A, B, C, D)]
+    ref = ragged_oracle(orc, *wid, off, per)
+    x, _ = solve_on_device(cuda, (A, B, C, D), off, per, precision=L.FP32_STORE)
+    assert per_system_err(x, ref, off) <= 1e-12
+
+
+@pytest.mark.gpu
+def test_ragged_short_and_uniform_systems(cuda, orc):
+    # 3..40 rows (one lane per system below 6 rows), every length present, both
+    # kinds; then a uniform batch that fills one bucket
+    rng = np.random.default_rng(53)
+    n = np.repeat(np.arange(3, 41), 3)
+    per = (np.arange(n.size) % 2).astype(np.uint8)
+    off = np.concatenate([[0], np.cumsum(n)]).astype(np.int64)
+    r = np.repeat(10.0 ** rng.uniform(-1, 1, n.size), n)
+    A, C, B = -r, -r, 1 + 2 * r
+    D = rng.uniform(-1, 1, int(off[-1]))
+    ref = ragged_oracle(orc, A, B, C, D, off, per)
+    x, _ = solve_on_device(cuda, (A, B, C, D), off, per)
+    assert per_system_err(x, ref, off) <= 1e-12
+    off2 = np.arange(0, 257 * 128, 128, dtype=np.int64)
+    A2, B2, C2, D2 = [v[:, 0].copy() for v in W.diag_dominant(1, 256 * 128, seed=54)]
+    x2, plan = solve_on_device(cuda, (A2, B2, C2, D2), off2, None)
+    ref2 = ragged_oracle(orc, A2, B2, C2, D2, off2, np.zeros(256, np.uint8))
+    assert per_system_err(x2, ref2, off2) <= 1e-12
+    assert len(plan) == 1
+
+
+def test_ragged_argument_checks():
+    import ctypes
+    lib = L.lib()
+    vp = ctypes.c_void_p(1)
+    off = np.array([0, 2, 10], dtype=np.int64)  # a 2-row system
+    assert lib.btdma_solve_ragged(None, vp, vp, vp, vp, vp, off.ctypes.data, None, 2,
+                                  None) == L.ERR_ARG
+    assert lib.btdma_ragged_autotune(None, vp, vp, vp, vp, vp, off.ctypes.data, None, 2,
+                                     None) == L.ERR_ARG
+    n = ctypes.c_int()
+    assert lib.btdma_ragged_plan_info(None, None, 0, ctypes.byref(n)) == L.ERR_ARG
