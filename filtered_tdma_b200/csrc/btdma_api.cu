@@ -44,7 +44,9 @@ struct btdma_handle {
     bool last_refined = false;
     // ragged batches: the plan of the most recent row-offset layout
     struct RagBucket {
-        int cyc, first, count, nmin, nmax, P, warps, mcap;
+        int cyc, first, count, nmin, nmax;
+        int cta;    // 1: one CTA of P threads per system, 0: P lanes of a warp per system
+        int P, warps, mcap;
         float best_ms;
     };
     std::vector<long long> rag_off;        // host copy of the offsets of the plan
@@ -751,6 +753,15 @@ int rag_default_P(int nmin, int nmax) {
 
 int rag_mcap(int nmax, int P) { return (nmax + P - 1) / P; }
 
+// CTA-per-system shape for long systems: the smallest power of two >= 64 that
+// keeps <= RAG_MT rows per thread (0 when none <= 512 does, or when the
+// shortest system would get fewer than 3 rows per thread).
+int rag_cta_P(int nmin, int nmax) {
+    int P = 64;
+    while (P <= 512 && rag_mcap(nmax, P) > RAG_MT) P <<= 1;
+    return (P <= 512 && nmin / P >= 3) ? P : 0;
+}
+
 // Largest warps-per-CTA (<= 8) whose shared memory fits.
 int rag_fit_warps(int want, int mcap) {
     int w = want;
@@ -797,11 +808,21 @@ int rag_plan(btdma_t h, const long long* off, const unsigned char* per, int n_sy
         b.count = j - i;
         b.nmin = nmin;
         b.nmax = nmax;
-        b.P = rag_default_P(nmin, nmax);
-        b.mcap = rag_mcap(nmax, b.P);
-        b.warps = rag_fit_warps(4, b.mcap);
-        if (b.warps == 0)
-            return fail(BTDMA_ERR_UNSUPPORTED, "systems of %d rows exceed shared memory", nmax);
+        const int Pc = nmax > 32 * RAG_MT ? rag_cta_P(nmin, nmax) : 0;
+        if (Pc) {
+            b.cta = 1;
+            b.P = Pc;
+            b.warps = Pc / 32;
+            b.mcap = rag_mcap(nmax, Pc);
+        } else {
+            b.cta = 0;
+            b.P = rag_default_P(nmin, nmax);
+            b.mcap = rag_mcap(nmax, b.P);
+            b.warps = rag_fit_warps(4, b.mcap);
+            if (b.warps == 0)
+                return fail(BTDMA_ERR_UNSUPPORTED, "systems of %d rows exceed shared memory",
+                            nmax);
+        }
         b.best_ms = 0.f;
         bk.push_back(b);
         i = j;
@@ -840,8 +861,22 @@ int rag_launch_t(const RagArgs& a, int warps, cudaStream_t st) {
     return BTDMA_OK;
 }
 
+template <typename TIN, bool CYC>
+int rag_launch_cta_t(const RagArgs& a, cudaStream_t st) {
+    auto kern = ragged_cta_kernel<TIN, CYC>;
+    static bool attr_done = false;
+    if (!attr_done) {
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                max_smem_optin()));
+        attr_done = true;
+    }
+    kern<<<a.count, a.P, rag_cta_smem_bytes(a.P), st>>>(a);
+    CK(cudaGetLastError());
+    return BTDMA_OK;
+}
+
 template <typename TIN>
-int rag_launch_bucket(btdma_t h, const btdma_handle::RagBucket& b, int P, int warps,
+int rag_launch_bucket(btdma_t h, const btdma_handle::RagBucket& b, int cta, int P, int warps,
                       const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X,
                       cudaStream_t st) {
     RagArgs a{};
@@ -856,6 +891,7 @@ int rag_launch_bucket(btdma_t h, const btdma_handle::RagBucket& b, int P, int wa
     a.P = P;
     a.mcap = rag_mcap(b.nmax, P);
     a.status = h->status;
+    if (cta) return b.cyc ? rag_launch_cta_t<TIN, true>(a, st) : rag_launch_cta_t<TIN, false>(a, st);
     return b.cyc ? rag_launch_t<TIN, true>(a, warps, st) : rag_launch_t<TIN, false>(a, warps, st);
 }
 
@@ -875,7 +911,7 @@ int rag_solve(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D,
     h->last_n_sys = n_sys;
     h->last_refined = false;
     for (const auto& b : h->rag_buckets) {
-        rc = rag_launch_bucket<TIN>(h, b, b.P, b.warps, A, B, C, D, X, st);
+        rc = rag_launch_bucket<TIN>(h, b, b.cta, b.P, b.warps, A, B, C, D, X, st);
         if (rc) return rc;
     }
     return BTDMA_OK;
@@ -892,36 +928,41 @@ int rag_tune(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, 
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     for (auto& b : h->rag_buckets) {
+        // candidates: (cta, P, warps)
+        struct Cand {
+            int cta, P, w;
+        };
+        std::vector<Cand> cands;
+        for (int P = 1; P <= 32 && b.nmin / P >= 3; P <<= 1)
+            for (int w = 1; w <= 8 && rag_fit_warps(w, rag_mcap(b.nmax, P)) == w; w <<= 1)
+                cands.push_back({0, P, w});
+        for (int P = 64; P <= 512 && b.nmin / P >= 3; P <<= 1)
+            if (rag_mcap(b.nmax, P) <= RAG_MT) cands.push_back({1, P, P / 32});
         float best = 1e30f;
-        int bestP = b.P, bestW = b.warps;
-        for (int P = 1; P <= 32; P <<= 1) {
-            if (b.nmin / P < 3) break;
-            for (int w = 1; w <= 8; w <<= 1) {
-                if (rag_fit_warps(w, rag_mcap(b.nmax, P)) != w) break;
-                float ms = 0.f;
-                for (int rep = 0; rep < 3; ++rep) {  // best of 3
-                    CK(cudaEventRecord(e0, st));
-                    rc = rag_launch_bucket<TIN>(h, b, P, w, A, B, C, D, X, st);
-                    if (rc) break;
-                    CK(cudaEventRecord(e1, st));
-                    CK(cudaEventSynchronize(e1));
-                    float t = 0.f;
-                    CK(cudaEventElapsedTime(&t, e0, e1));
-                    ms = rep == 0 ? t : std::min(ms, t);
-                }
+        Cand pick{b.cta, b.P, b.warps};
+        for (const Cand& cd : cands) {
+            float ms = 0.f;
+            for (int rep = 0; rep < 3 && !rc; ++rep) {  // best of 3
+                CK(cudaEventRecord(e0, st));
+                rc = rag_launch_bucket<TIN>(h, b, cd.cta, cd.P, cd.w, A, B, C, D, X, st);
                 if (rc) break;
-                if (ms < best) {
-                    best = ms;
-                    bestP = P;
-                    bestW = w;
-                }
+                CK(cudaEventRecord(e1, st));
+                CK(cudaEventSynchronize(e1));
+                float t = 0.f;
+                CK(cudaEventElapsedTime(&t, e0, e1));
+                ms = rep == 0 ? t : std::min(ms, t);
             }
             if (rc) break;
+            if (ms < best) {
+                best = ms;
+                pick = cd;
+            }
         }
         if (rc) break;
-        b.P = bestP;
-        b.warps = bestW;
-        b.mcap = rag_mcap(b.nmax, bestP);
+        b.cta = pick.cta;
+        b.P = pick.P;
+        b.warps = pick.w;
+        b.mcap = rag_mcap(b.nmax, pick.P);
         b.best_ms = best;
     }
     cudaEventDestroy(e0);
@@ -967,6 +1008,7 @@ int btdma_ragged_plan_info(btdma_t h, btdma_ragged_bucket* out, int cap, int* n_
         out[i].n_row_max = b.nmax;
         out[i].lanes_per_system = b.P;
         out[i].warps_per_cta = b.warps;
+        out[i].cta_per_system = b.cta;
         out[i].tuned_ms = b.best_ms;
     }
     return BTDMA_OK;

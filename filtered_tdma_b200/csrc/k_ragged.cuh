@@ -161,4 +161,169 @@ __global__ void __launch_bounds__(256) ragged_kernel(const RagArgs a) {
     }
 }
 
+// Long systems: one CTA of P threads (P a power of two, 64..512) per system,
+// at most RAG_MT rows per thread, the elimination state in shared memory laid
+// out [field][row][thread] (consecutive threads, consecutive doubles).  The
+// reduced system of the P sub-segments runs through shared memory: one
+// cyclic-reduction level, then parallel cyclic reduction with a block barrier
+// per level (the same steps as reduced_solve_shfl).
+constexpr int RAG_MT = 16;
+
+__host__ __device__ __forceinline__ size_t rag_cta_smem_bytes(int P) {
+    return (2ull * 3 * (P + 2) + 3ull * RAG_MT * P) * sizeof(double);
+}
+
+template <typename TIN, bool CYCLIC>
+__global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
+    extern __shared__ double rsm[];
+    constexpr int M = RAG_MT;
+    const int P = blockDim.x;
+    const int p = threadIdx.x;
+    const int gs = P + 2;  // guard rows at 0 and P + 1 stay zero (non-periodic ends)
+    auto F = [&](int b, int f, int row) -> double& { return rsm[(b * 3 + f) * gs + row + 1]; };
+    if (p < 6) {
+        rsm[p * gs] = 0.0;
+        rsm[p * gs + P + 1] = 0.0;
+    }
+
+    const int sys = a.list[blockIdx.x];
+    const long long o = a.off[sys];
+    const int n = (int)(a.off[sys + 1] - o);
+    const int base = n / P, rem = n % P;
+    const int m = base + (p < rem ? 1 : 0);  // 3 <= m <= M (host's choice of P)
+    const long long row0 = o + (long long)p * base + (p < rem ? p : rem);
+    const TIN* __restrict__ pA = static_cast<const TIN*>(a.A) + row0;
+    const TIN* __restrict__ pB = static_cast<const TIN*>(a.B) + row0;
+    const TIN* __restrict__ pC = static_cast<const TIN*>(a.C) + row0;
+    const TIN* __restrict__ pD = static_cast<const TIN*>(a.D) + row0;
+
+    double* stt = rsm + 2 * 3 * gs + p;  // field f, row k: stt[(f * M + k) * P]
+    auto AL = [&](int k) -> double& { return stt[(0 * M + k) * P]; };
+    auto GA = [&](int k) -> double& { return stt[(1 * M + k) * P]; };
+    auto DE = [&](int k) -> double& { return stt[(2 * M + k) * P]; };
+    double ab0 = 0, cb0 = 0, db0 = 0, pi = 1.0, sa = 0.0, sd = 0.0, pi_last = 0.0;
+    double alp = 0, gap = 0, dep = 0;  // row k-1
+#pragma unroll
+    for (int k0 = 0; k0 < M; k0 += RAG_LOOKAHEAD) {
+        double ra[RAG_LOOKAHEAD], rb[RAG_LOOKAHEAD], rc[RAG_LOOKAHEAD], rd[RAG_LOOKAHEAD];
+#pragma unroll
+        for (int j = 0; j < RAG_LOOKAHEAD; ++j) {  // loads of the next rows (clamped in bounds)
+            const int kk = k0 + j < m ? k0 + j : m - 1;
+            ra[j] = (double)__ldg(pA + kk);
+            rb[j] = (double)__ldg(pB + kk);
+            rc[j] = (double)__ldg(pC + kk);
+            rd[j] = (double)__ldg(pD + kk);
+        }
+#pragma unroll
+        for (int j = 0; j < RAG_LOOKAHEAD; ++j) {
+            const int k = k0 + j;
+            if (k >= m) continue;
+            if (k == 0) {
+                const double ib = rcp_nr(rb[j]);
+                ab0 = ra[j] * ib;
+                cb0 = rc[j] * ib;
+                db0 = rd[j] * ib;
+            } else {
+                double al, ga, de;
+                if (k == 1) {
+                    const double ib = rcp_nr(rb[j]);
+                    al = ra[j] * ib;
+                    ga = rc[j] * ib;
+                    de = rd[j] * ib;
+                    sa = al;
+                    sd = de;
+                } else {
+                    const double inv = rcp_nr(rb[j] - ra[j] * gap);
+                    ga = rc[j] * inv;
+                    de = (rd[j] - ra[j] * dep) * inv;
+                    al = -ra[j] * alp * inv;
+                    if (k <= m - 2) {
+                        pi = -gap * pi;
+                        sa += pi * al;
+                        sd += pi * de;
+                    }
+                    if (k == m - 1) pi_last = -gap * pi;
+                }
+                AL(k) = al;
+                GA(k) = ga;
+                DE(k) = de;
+                alp = al;
+                gap = ga;
+                dep = de;
+            }
+        }
+    }
+    const double l1 = alp, u1 = gap, r1 = dep;  // row m - 1
+    const double rr = rcp_nr(1.0 - cb0 * sa);
+    const double l0 = rr * ab0, u0 = rr * cb0 * pi_last, r0 = rr * (db0 - cb0 * sd);
+
+    // ---------------------------------------------- reduced system (shared memory)
+    F(1, 0, p) = l0;
+    F(1, 1, p) = u0;
+    F(1, 2, p) = r0;
+    __syncthreads();
+    {
+        const int pn = (CYCLIC && p == P - 1) ? 0 : p + 1;  // p + 1 == P: the zero guard
+        const double l0n = F(1, 0, pn), u0n = F(1, 1, pn), r0n = F(1, 2, pn);
+        const double ib = rcp_nr(1.0 - l1 * u0 - u1 * l0n);
+        F(0, 0, p) = -l1 * l0 * ib;
+        F(0, 1, p) = -u1 * u0n * ib;
+        F(0, 2, p) = (r1 - l1 * r0 - u1 * r0n) * ib;
+    }
+    __syncthreads();
+    int cur = 0;
+    double xl = 0.0;
+    bool solved = false;
+    for (int dl = 1; dl < P; dl <<= 1) {
+        int im = p - dl, ip = p + dl;
+        if (CYCLIC) {
+            im = im < 0 ? im + P : im;
+            ip = ip >= P ? ip - P : ip;
+        } else {
+            im = im < -1 ? -1 : im;
+            ip = ip > P ? P : ip;
+        }
+        double li = F(cur, 0, p), ui = F(cur, 1, p), ri = F(cur, 2, p);
+        const double lm = F(cur, 0, im), um = F(cur, 1, im), rm = F(cur, 2, im);
+        const double lp = F(cur, 0, ip), up = F(cur, 1, ip), rp = F(cur, 2, ip);
+        if (CYCLIC && 2 * dl == P) {
+            const double si = li + ui, sj = lm + um;
+            xl = (ri - si * rm) * rcp_nr(1.0 - si * sj);
+            solved = true;
+        } else {
+            pcr_step(li, ui, ri, lm, um, rm, lp, up, rp);
+            F(cur ^ 1, 0, p) = li;
+            F(cur ^ 1, 1, p) = ui;
+            F(cur ^ 1, 2, p) = ri;
+        }
+        __syncthreads();
+        cur ^= 1;
+    }
+    if (!solved) xl = F(cur, 2, p);
+    F(cur ^ 1, 2, p) = xl;
+    __syncthreads();
+    double xlm;
+    if (CYCLIC)
+        xlm = F(cur ^ 1, 2, p == 0 ? P - 1 : p - 1);
+    else
+        xlm = p == 0 ? 0.0 : F(cur ^ 1, 2, p - 1);
+    const double xf = r0 - l0 * xlm - u0 * xl;
+
+    // ------------------------------------------------ back substitution
+    double* xp = a.X + row0;
+    double nonfinite = fma(xf, 0.0, fma(xl, 0.0, 0.0));
+    double xn = xl;
+#pragma unroll
+    for (int k = M - 2; k >= 1; --k) {
+        if (k <= m - 2) {
+            xn = DE(k) - AL(k) * xf - GA(k) * xn;
+            nonfinite = fma(xn, 0.0, nonfinite);
+            xp[k] = xn;
+        }
+    }
+    xp[0] = xf;
+    xp[m - 1] = xl;
+    if (nonfinite != 0.0) raise_status(a.status, ST_NONFINITE);  // NaN != 0
+}
+
 }  // namespace btdma

@@ -199,9 +199,11 @@ int btdma_solve_ragged_f32(btdma_t h, const float* A, const float* B, const floa
                            const float* D, double* X, const long long* row_offsets,
                            const unsigned char* is_periodic, int n_sys, cudaStream_t stream);
 
-/* Autotuner of ragged solves: times, for every bucket of the plan, each choice of
- * lanes per system (1..32, at least 3 rows per lane) and warps per CTA (1..8)
- * on this batch and keeps the fastest for later solves of the same layout.
+/* Autotuner of ragged solves: times, for every bucket of the plan, each launch
+ * shape — P lanes of a warp per system (P = 1..32) with 1..8 warps per CTA, or
+ * one CTA of P = 64..512 threads per system (<= 16 rows per thread) — with at
+ * least 3 rows per thread, on this batch, and keeps the fastest for later
+ * solves of the same layout.
  * A..D are double or float as the handle's precision says; X is overwritten.
  * Blocking (it synchronises the stream). */
 int btdma_ragged_autotune(btdma_t h, const void* A, const void* B, const void* C, const void* D,
@@ -213,9 +215,10 @@ typedef struct btdma_ragged_bucket {
     int periodic;
     int n_systems;
     int n_row_min, n_row_max;
-    int lanes_per_system;
+    int lanes_per_system; /* threads that share one system */
     int warps_per_cta;
-    float tuned_ms; /* fastest time measured by the autotuner (0 before tuning) */
+    int cta_per_system;   /* 1: one CTA per system (long systems), 0: lanes of a warp */
+    float tuned_ms;       /* fastest time measured by the autotuner (0 before tuning) */
 } btdma_ragged_bucket;
 int btdma_ragged_plan_info(btdma_t h, btdma_ragged_bucket* out, int cap, int* n_out);
 

@@ -115,3 +115,21 @@ def test_ragged_argument_checks():
                                      None) == L.ERR_ARG
     n = ctypes.c_int()
     assert lib.btdma_ragged_plan_info(None, None, 0, ctypes.byref(n)) == L.ERR_ARG
+
+
+@pytest.mark.gpu
+def test_ragged_long_systems_cta_path(cuda, orc):
+    # one CTA per system above 512 rows, up to 8192 rows (512 threads x 16 rows)
+    rng = np.random.default_rng(55)
+    n = np.array([513, 600, 1000, 1024, 1025, 2047, 4096, 5000, 8192, 8192, 700, 3000])
+    per = np.array([0, 1, 0, 1, 0, 1, 0, 1, 0, 1, 1, 0], dtype=np.uint8)
+    off = np.concatenate([[0], np.cumsum(n)]).astype(np.int64)
+    r = np.repeat(10.0 ** rng.uniform(-1.3, 1.3, n.size), n)
+    A, C, B = -r, -r, 1 + 2 * r
+    D = rng.uniform(-1, 1, int(off[-1]))
+    ref = ragged_oracle(orc, A, B, C, D, off, per)
+    x, plan = solve_on_device(cuda, (A, B, C, D), off, per)
+    assert per_system_err(x, ref, off) <= 1e-12
+    assert any(b["cta_per_system"] == 1 and b["lanes_per_system"] == 512 for b in plan)
+    x, plan = solve_on_device(cuda, (A, B, C, D), off, per, tune=True)
+    assert per_system_err(x, ref, off) <= 1e-12
