@@ -52,8 +52,19 @@ struct btdma_handle {
     std::vector<long long> rag_off;        // host copy of the offsets of the plan
     std::vector<unsigned char> rag_per;    // host copy of the periodic flags
     std::vector<RagBucket> rag_buckets;
+    std::vector<int> rag_order;            // system ids, bucket by bucket
     long long* rag_d_off = nullptr;        // device offsets [n_sys + 1]
-    int* rag_d_list = nullptr;             // device system lists, bucket by bucket
+    int* rag_d_list = nullptr;             // device copy of rag_order
+    int4* rag_d_tasks = nullptr;           // task tables [2 * n_sys]
+    int4* rag_d_probe = nullptr;           // task table of one bucket being tuned [n_sys]
+    // launches of a solve: warp-kind tasks (one launch), CTA-kind tasks per P
+    struct RagLaunch {
+        int cta, P, first, count, mcap;
+    };
+    std::vector<RagLaunch> rag_launches;
+    static constexpr int RAG_STREAMS = 4;
+    cudaStream_t rag_side[RAG_STREAMS] = {};
+    cudaEvent_t rag_fork = nullptr, rag_join[RAG_STREAMS] = {};
 };
 
 namespace {
@@ -516,6 +527,13 @@ int btdma_destroy(btdma_t h) {
     cudaFree(h->open);
     cudaFree(h->rag_d_off);
     cudaFree(h->rag_d_list);
+    cudaFree(h->rag_d_tasks);
+    cudaFree(h->rag_d_probe);
+    for (int i = 0; i < btdma_handle::RAG_STREAMS; ++i) {
+        if (h->rag_side[i]) cudaStreamDestroy(h->rag_side[i]);
+        if (h->rag_join[i]) cudaEventDestroy(h->rag_join[i]);
+    }
+    if (h->rag_fork) cudaEventDestroy(h->rag_fork);
     delete h;
     return BTDMA_OK;
 }
@@ -742,6 +760,9 @@ extern "C" int btdma_solve_noalloc(const double* A, const double* B, const doubl
 // ------------------------------------------------------------------ ragged
 namespace {
 
+constexpr int RAG_WPC = 4;         // warps per CTA of the warp-kind launch
+constexpr int RAG_WARP_MCAP = 32;  // rows per lane the warp kind accepts
+
 // Lanes per system for a bucket whose systems have nmin..nmax rows: about
 // 12 rows per lane, a power of two, at most 32, and at least 3 rows per lane
 // for the shortest system.
@@ -762,11 +783,42 @@ int rag_cta_P(int nmin, int nmax) {
     return (P <= 512 && nmin / P >= 3) ? P : 0;
 }
 
-// Largest warps-per-CTA (<= 8) whose shared memory fits.
-int rag_fit_warps(int want, int mcap) {
-    int w = want;
-    while (w > 1 && rag_smem_bytes(w, mcap) > (size_t)max_smem_optin()) w >>= 1;
-    return rag_smem_bytes(w, mcap) <= (size_t)max_smem_optin() ? w : 0;
+// Task entries of one bucket with lanes-per-system P (warp kind: 32 / P
+// systems per warp; CTA kind: one system per CTA).
+void rag_bucket_tasks(const btdma_handle::RagBucket& b, int cta, int P, std::vector<int4>& out) {
+    if (cta) {
+        for (int i = 0; i < b.count; ++i) out.push_back(make_int4(b.first + i, b.cyc, 0, 0));
+        return;
+    }
+    const int G = 32 / P;
+    for (int i = 0; i < b.count; i += G)
+        out.push_back(make_int4(b.first + i, std::min(G, b.count - i), P, b.cyc));
+}
+
+// Task tables of the whole plan: one warp-kind launch (buckets longest first)
+// and one CTA-kind launch per P.
+int rag_build_launches(btdma_t h) {
+    std::vector<int4> tasks;
+    h->rag_launches.clear();
+    btdma_handle::RagLaunch wl{0, 0, 0, 0, 1};
+    for (int i = (int)h->rag_buckets.size() - 1; i >= 0; --i) {
+        const auto& b = h->rag_buckets[i];
+        if (b.cta) continue;
+        rag_bucket_tasks(b, 0, b.P, tasks);
+        wl.mcap = std::max(wl.mcap, rag_mcap(b.nmax, b.P));
+    }
+    wl.count = (int)tasks.size();
+    if (wl.count) h->rag_launches.push_back(wl);
+    for (int P = 512; P >= 64; P >>= 1) {
+        btdma_handle::RagLaunch cl{1, P, (int)tasks.size(), 0, 0};
+        for (const auto& b : h->rag_buckets)
+            if (b.cta && b.P == P) rag_bucket_tasks(b, 1, P, tasks);
+        cl.count = (int)tasks.size() - cl.first;
+        if (cl.count) h->rag_launches.push_back(cl);
+    }
+    CK(cudaMemcpy(h->rag_d_tasks, tasks.data(), sizeof(int4) * tasks.size(),
+                  cudaMemcpyHostToDevice));
+    return BTDMA_OK;
 }
 
 int rag_plan(btdma_t h, const long long* off, const unsigned char* per, int n_sys) {
@@ -784,7 +836,9 @@ int rag_plan(btdma_t h, const long long* off, const unsigned char* per, int n_sy
     for (int i = 0; i < n_sys; ++i) {
         const long long n = off[i + 1] - off[i];
         if (n < 3) return fail(BTDMA_ERR_SEGMENT, "system %d has %lld rows (needs >= 3)", i, n);
-        if (n > (1 << 20)) return fail(BTDMA_ERR_SIZE, "system %d has %lld rows (> 2^20)", i, n);
+        if (n > 32 * RAG_WARP_MCAP && n > 512 * RAG_MT)
+            return fail(BTDMA_ERR_SIZE, "system %d has %lld rows (at most %d)", i, n,
+                        512 * RAG_MT);
         int lg = 0;
         while ((1LL << lg) < n) ++lg;
         key[i] = (per && per[i] ? 64 : 0) + lg;
@@ -812,73 +866,56 @@ int rag_plan(btdma_t h, const long long* off, const unsigned char* per, int n_sy
         if (Pc) {
             b.cta = 1;
             b.P = Pc;
-            b.warps = Pc / 32;
-            b.mcap = rag_mcap(nmax, Pc);
         } else {
             b.cta = 0;
             b.P = rag_default_P(nmin, nmax);
-            b.mcap = rag_mcap(nmax, b.P);
-            b.warps = rag_fit_warps(4, b.mcap);
-            if (b.warps == 0)
-                return fail(BTDMA_ERR_UNSUPPORTED, "systems of %d rows exceed shared memory",
-                            nmax);
+            if (rag_mcap(nmax, b.P) > RAG_WARP_MCAP)
+                return fail(BTDMA_ERR_UNSUPPORTED, "no launch shape for systems of %d..%d rows",
+                            nmin, nmax);
         }
+        b.warps = b.cta ? b.P / 32 : RAG_WPC;
+        b.mcap = rag_mcap(nmax, b.P);
         b.best_ms = 0.f;
         bk.push_back(b);
         i = j;
     }
     cudaFree(h->rag_d_off);
     cudaFree(h->rag_d_list);
+    cudaFree(h->rag_d_tasks);
+    cudaFree(h->rag_d_probe);
     h->rag_d_off = nullptr;
     h->rag_d_list = nullptr;
+    h->rag_d_tasks = h->rag_d_probe = nullptr;
     h->rag_off.clear();
     CK(cudaMalloc(&h->rag_d_off, sizeof(long long) * (n_sys + 1)));
     CK(cudaMalloc(&h->rag_d_list, sizeof(int) * n_sys));
+    CK(cudaMalloc(&h->rag_d_tasks, sizeof(int4) * 2 * n_sys));
+    CK(cudaMalloc(&h->rag_d_probe, sizeof(int4) * n_sys));
     CK(cudaMemcpy(h->rag_d_off, off, sizeof(long long) * (n_sys + 1), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->rag_d_list, order.data(), sizeof(int) * n_sys, cudaMemcpyHostToDevice));
+    if (!h->rag_fork) {
+        CK(cudaEventCreateWithFlags(&h->rag_fork, cudaEventDisableTiming));
+        for (int i = 0; i < btdma_handle::RAG_STREAMS; ++i) {
+            CK(cudaStreamCreateWithFlags(&h->rag_side[i], cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&h->rag_join[i], cudaEventDisableTiming));
+        }
+    }
+    h->rag_buckets = bk;
+    h->rag_order = order;
+    const int rc = rag_build_launches(h);
+    if (rc) return rc;
     h->rag_off.assign(off, off + n_sys + 1);
     if (per)
         h->rag_per.assign(per, per + n_sys);
     else
         h->rag_per.clear();
-    h->rag_buckets = bk;
-    return BTDMA_OK;
-}
-
-template <typename TIN, bool CYC>
-int rag_launch_t(const RagArgs& a, int warps, cudaStream_t st) {
-    auto kern = ragged_kernel<TIN, CYC>;
-    static bool attr_done = false;
-    if (!attr_done) {
-        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                max_smem_optin()));
-        attr_done = true;
-    }
-    const int per_cta = warps * (32 / a.P);
-    const int grid = (a.count + per_cta - 1) / per_cta;
-    kern<<<grid, 32 * warps, rag_smem_bytes(warps, a.mcap), st>>>(a);
-    CK(cudaGetLastError());
-    return BTDMA_OK;
-}
-
-template <typename TIN, bool CYC>
-int rag_launch_cta_t(const RagArgs& a, cudaStream_t st) {
-    auto kern = ragged_cta_kernel<TIN, CYC>;
-    static bool attr_done = false;
-    if (!attr_done) {
-        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                max_smem_optin()));
-        attr_done = true;
-    }
-    kern<<<a.count, a.P, rag_cta_smem_bytes(a.P), st>>>(a);
-    CK(cudaGetLastError());
     return BTDMA_OK;
 }
 
 template <typename TIN>
-int rag_launch_bucket(btdma_t h, const btdma_handle::RagBucket& b, int cta, int P, int warps,
-                      const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X,
-                      cudaStream_t st) {
+int rag_launch(btdma_t h, int cta, int P, int mcap, const int4* tasks, int n_tasks,
+               const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X,
+               cudaStream_t st) {
     RagArgs a{};
     a.A = A;
     a.B = B;
@@ -886,13 +923,58 @@ int rag_launch_bucket(btdma_t h, const btdma_handle::RagBucket& b, int cta, int 
     a.D = D;
     a.X = X;
     a.off = h->rag_d_off;
-    a.list = h->rag_d_list + b.first;
-    a.count = b.count;
-    a.P = P;
-    a.mcap = rag_mcap(b.nmax, P);
+    a.list = h->rag_d_list;
+    a.tasks = tasks;
+    a.n_tasks = n_tasks;
+    a.mcap = mcap;
     a.status = h->status;
-    if (cta) return b.cyc ? rag_launch_cta_t<TIN, true>(a, st) : rag_launch_cta_t<TIN, false>(a, st);
-    return b.cyc ? rag_launch_t<TIN, true>(a, warps, st) : rag_launch_t<TIN, false>(a, warps, st);
+    if (cta) {
+        auto kern = ragged_cta_kernel<TIN>;
+        static bool attr_done = false;
+        if (!attr_done) {
+            CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    max_smem_optin()));
+            attr_done = true;
+        }
+        kern<<<n_tasks, P, rag_cta_smem_bytes(P), st>>>(a);
+    } else {
+        auto kern = ragged_kernel<TIN>;
+        static bool attr_done = false;
+        if (!attr_done) {
+            CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    max_smem_optin()));
+            attr_done = true;
+        }
+        kern<<<(n_tasks + RAG_WPC - 1) / RAG_WPC, 32 * RAG_WPC, rag_smem_bytes(RAG_WPC, mcap),
+               st>>>(a);
+    }
+    CK(cudaGetLastError());
+    return BTDMA_OK;
+}
+
+// All launches of the plan: the first on the caller's stream, the others on
+// side streams forked from it and joined back (graph-capturable).
+template <typename TIN>
+int rag_run(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X,
+            cudaStream_t st) {
+    const auto& L = h->rag_launches;
+    const int n = (int)L.size();
+    const int side = std::min(n - 1, (int)btdma_handle::RAG_STREAMS);
+    if (side > 0) {
+        CK(cudaEventRecord(h->rag_fork, st));
+        for (int i = 0; i < side; ++i) CK(cudaStreamWaitEvent(h->rag_side[i], h->rag_fork, 0));
+    }
+    for (int i = 0; i < n; ++i) {
+        const cudaStream_t s = i == 0 ? st : h->rag_side[(i - 1) % btdma_handle::RAG_STREAMS];
+        const int rc = rag_launch<TIN>(h, L[i].cta, L[i].P, L[i].mcap, h->rag_d_tasks + L[i].first,
+                                       L[i].count, A, B, C, D, X, s);
+        if (rc) return rc;
+    }
+    for (int i = 0; i < side; ++i) {
+        CK(cudaEventRecord(h->rag_join[i], h->rag_side[i]));
+        CK(cudaStreamWaitEvent(st, h->rag_join[i], 0));
+    }
+    return BTDMA_OK;
 }
 
 template <typename TIN>
@@ -910,15 +992,12 @@ int rag_solve(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D,
     h->last_stream = st;
     h->last_n_sys = n_sys;
     h->last_refined = false;
-    for (const auto& b : h->rag_buckets) {
-        rc = rag_launch_bucket<TIN>(h, b, b.cta, b.P, b.warps, A, B, C, D, X, st);
-        if (rc) return rc;
-    }
-    return BTDMA_OK;
+    return rag_run<TIN>(h, A, B, C, D, X, st);
 }
 
-// Times every (P, warps) candidate of every bucket on the given batch and keeps
-// the fastest (CUDA events on the stream; the batch's X is overwritten).
+// Times, bucket by bucket, every launch shape on the given batch (the bucket
+// alone, best of 3, CUDA events on the stream) and keeps the fastest; then
+// rebuilds the merged task tables.  X is overwritten.
 template <typename TIN>
 int rag_tune(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X,
              const long long* off, const unsigned char* per, int n_sys, cudaStream_t st) {
@@ -927,24 +1006,32 @@ int rag_tune(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, 
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
+    std::vector<int4> tasks;
     for (auto& b : h->rag_buckets) {
-        // candidates: (cta, P, warps)
         struct Cand {
-            int cta, P, w;
+            int cta, P;
         };
         std::vector<Cand> cands;
         for (int P = 1; P <= 32 && b.nmin / P >= 3; P <<= 1)
-            for (int w = 1; w <= 8 && rag_fit_warps(w, rag_mcap(b.nmax, P)) == w; w <<= 1)
-                cands.push_back({0, P, w});
+            if (rag_mcap(b.nmax, P) <= RAG_WARP_MCAP) cands.push_back({0, P});
         for (int P = 64; P <= 512 && b.nmin / P >= 3; P <<= 1)
-            if (rag_mcap(b.nmax, P) <= RAG_MT) cands.push_back({1, P, P / 32});
+            if (rag_mcap(b.nmax, P) <= RAG_MT) cands.push_back({1, P});
         float best = 1e30f;
-        Cand pick{b.cta, b.P, b.warps};
+        Cand pick{b.cta, b.P};
         for (const Cand& cd : cands) {
+            tasks.clear();
+            rag_bucket_tasks(b, cd.cta, cd.P, tasks);
+            if (cudaMemcpyAsync(h->rag_d_probe, tasks.data(), sizeof(int4) * tasks.size(),
+                                cudaMemcpyHostToDevice, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess) {
+                rc = fail(BTDMA_ERR_CUDA, "autotune upload failed");
+                break;
+            }
             float ms = 0.f;
-            for (int rep = 0; rep < 3 && !rc; ++rep) {  // best of 3
+            for (int rep = 0; rep < 3 && !rc; ++rep) {
                 CK(cudaEventRecord(e0, st));
-                rc = rag_launch_bucket<TIN>(h, b, cd.cta, cd.P, cd.w, A, B, C, D, X, st);
+                rc = rag_launch<TIN>(h, cd.cta, cd.P, rag_mcap(b.nmax, cd.P), h->rag_d_probe,
+                                     (int)tasks.size(), A, B, C, D, X, st);
                 if (rc) break;
                 CK(cudaEventRecord(e1, st));
                 CK(cudaEventSynchronize(e1));
@@ -961,13 +1048,14 @@ int rag_tune(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, 
         if (rc) break;
         b.cta = pick.cta;
         b.P = pick.P;
-        b.warps = pick.w;
+        b.warps = pick.cta ? pick.P / 32 : RAG_WPC;
         b.mcap = rag_mcap(b.nmax, pick.P);
         b.best_ms = best;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    return rc;
+    if (rc) return rc;
+    return rag_build_launches(h);
 }
 
 }  // namespace

@@ -14,9 +14,10 @@
 // warp shuffles (reduced_solve_shfl), then every lane back-substitutes its rows
 // and stores x (FP64).
 //
-// The host sorts the systems into buckets of similar length (and separates
-// periodic from non-periodic ones, so the shuffles of a warp are uniform); one
-// launch per bucket, whose P and warps per CTA the autotuner picks.
+// The host sorts the systems into buckets of similar length and periodicity
+// (so the shuffles of a warp are uniform), picks P per bucket (autotuner), and
+// lays the work out as a task table: one entry per warp (this kernel) or per
+// CTA (ragged_cta_kernel), so all buckets of one kind run in one launch.
 #pragma once
 
 #include "btdma_common.cuh"
@@ -31,10 +32,13 @@ struct RagArgs {
     const void* D;
     double* X;
     const long long* off;  // [n_sys + 1] row offsets
-    const int* list;       // systems of this bucket
-    int count;             // entries of list
-    int P;                 // lanes per system (power of two <= 32)
-    int mcap;              // state slots per lane (>= longest sub-segment of the bucket)
+    const int* list;       // system ids, bucket by bucket
+    // Task table.  ragged_kernel: one entry per warp, {first list index, systems
+    // (<= 32 / P), P, cyclic}; ragged_cta_kernel: one per CTA, {list index,
+    // cyclic, 0, 0} (P = blockDim.x).
+    const int4* tasks;
+    int n_tasks;
+    int mcap;              // ragged_kernel: state slots per lane (>= every task's rows per lane)
     unsigned* status;
 };
 
@@ -45,24 +49,26 @@ __host__ __device__ __forceinline__ size_t rag_smem_bytes(int warps, int mcap) {
     return (size_t)warps * 3 * mcap * 32 * sizeof(double);
 }
 
-template <typename TIN, bool CYCLIC>
+template <typename TIN>
 __global__ void __launch_bounds__(256) ragged_kernel(const RagArgs a) {
     extern __shared__ double rsm[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const int P = a.P;
-    const int G = 32 / P;  // systems per warp
+    const int gw = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (gw >= a.n_tasks) return;  // the whole warp
+    const int4 task = a.tasks[gw];
+    const int P = task.z;
     const int g = lane / P;
     const int p = lane % P;
+    const bool cyclic = task.w != 0;  // uniform over the warp
     const int mcap = a.mcap;
     double* st = rsm + (size_t)warp * 3 * mcap * 32 + lane;  // field f, row k: st[(f*mcap+k)*32]
 
-    const int sidx = (blockIdx.x * (blockDim.x >> 5) + warp) * G + g;
-    const bool have = sidx < a.count;
+    const bool have = g < task.y;
     int m = 0;
     long long row0 = 0;
     if (have) {
-        const int sys = a.list[sidx];
+        const int sys = a.list[task.x + g];
         const long long o = a.off[sys];
         const int n = (int)(a.off[sys + 1] - o);
         const int base = n / P, rem = n % P;  // para_range: the first rem parts get one more row
@@ -142,7 +148,10 @@ __global__ void __launch_bounds__(256) ragged_kernel(const RagArgs a) {
         r1 = dep;
     }
     double xf, xl;
-    reduced_solve_shfl<CYCLIC>(l0, u0, r0, l1, u1, r1, p, P, P, act, xf, xl);
+    if (cyclic)
+        reduced_solve_shfl<true>(l0, u0, r0, l1, u1, r1, p, P, P, act, xf, xl);
+    else
+        reduced_solve_shfl<false>(l0, u0, r0, l1, u1, r1, p, P, P, act, xf, xl);
 
     // ------------------------------------------------ back substitution
     if (act) {
@@ -173,7 +182,7 @@ __host__ __device__ __forceinline__ size_t rag_cta_smem_bytes(int P) {
     return (2ull * 3 * (P + 2) + 3ull * RAG_MT * P) * sizeof(double);
 }
 
-template <typename TIN, bool CYCLIC>
+template <typename TIN>
 __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
     extern __shared__ double rsm[];
     constexpr int M = RAG_MT;
@@ -186,7 +195,9 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
         rsm[p * gs + P + 1] = 0.0;
     }
 
-    const int sys = a.list[blockIdx.x];
+    const int4 task = a.tasks[blockIdx.x];
+    const bool cyclic = task.y != 0;  // uniform over the CTA
+    const int sys = a.list[task.x];
     const long long o = a.off[sys];
     const int n = (int)(a.off[sys + 1] - o);
     const int base = n / P, rem = n % P;
@@ -263,7 +274,7 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
     F(1, 2, p) = r0;
     __syncthreads();
     {
-        const int pn = (CYCLIC && p == P - 1) ? 0 : p + 1;  // p + 1 == P: the zero guard
+        const int pn = (cyclic && p == P - 1) ? 0 : p + 1;  // p + 1 == P: the zero guard
         const double l0n = F(1, 0, pn), u0n = F(1, 1, pn), r0n = F(1, 2, pn);
         const double ib = rcp_nr(1.0 - l1 * u0 - u1 * l0n);
         F(0, 0, p) = -l1 * l0 * ib;
@@ -276,7 +287,7 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
     bool solved = false;
     for (int dl = 1; dl < P; dl <<= 1) {
         int im = p - dl, ip = p + dl;
-        if (CYCLIC) {
+        if (cyclic) {
             im = im < 0 ? im + P : im;
             ip = ip >= P ? ip - P : ip;
         } else {
@@ -286,7 +297,7 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
         double li = F(cur, 0, p), ui = F(cur, 1, p), ri = F(cur, 2, p);
         const double lm = F(cur, 0, im), um = F(cur, 1, im), rm = F(cur, 2, im);
         const double lp = F(cur, 0, ip), up = F(cur, 1, ip), rp = F(cur, 2, ip);
-        if (CYCLIC && 2 * dl == P) {
+        if (cyclic && 2 * dl == P) {
             const double si = li + ui, sj = lm + um;
             xl = (ri - si * rm) * rcp_nr(1.0 - si * sj);
             solved = true;
@@ -303,7 +314,7 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
     F(cur ^ 1, 2, p) = xl;
     __syncthreads();
     double xlm;
-    if (CYCLIC)
+    if (cyclic)
         xlm = F(cur ^ 1, 2, p == 0 ? P - 1 : p - 1);
     else
         xlm = p == 0 ? 0.0 : F(cur ^ 1, 2, p - 1);
