@@ -26,7 +26,8 @@ EXPORTS = (
     "btdma_status", "btdma_set_method", "btdma_segments", "btdma_last_error",
     "btdma_solve_noalloc", "btdma_solve_f32", "btdma_set_refine", "btdma_last_stats",
     "btdma_solve_ragged", "btdma_solve_ragged_f32", "btdma_ragged_autotune",
-    "btdma_ragged_plan_info",
+    "btdma_ragged_plan_info", "btdma_heat_create", "btdma_heat_destroy", "btdma_heat_init",
+    "btdma_heat_step", "btdma_heat_l2_error",
 )
 NOALLOC_MAX_ELEMS = 1 << 20
 REFINE_MAX_SWEEPS = 4
@@ -93,6 +94,11 @@ def lib():
         L.btdma_ragged_autotune.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i, vp]
         L.btdma_ragged_plan_info.argtypes = [vp, ctypes.POINTER(RaggedBucket), i,
                                              ctypes.POINTER(i)]
+        L.btdma_heat_create.argtypes = [i, i, i, d, ctypes.POINTER(vp)]
+        L.btdma_heat_destroy.argtypes = [vp]
+        L.btdma_heat_init.argtypes = [vp, vp, vp]
+        L.btdma_heat_step.argtypes = [vp, vp, i, i, vp]
+        L.btdma_heat_l2_error.argtypes = [vp, vp, d, ctypes.POINTER(d)]
         L.btdma_last_error.restype = ctypes.c_char_p
         for name in EXPORTS:
             if name != "btdma_last_error":

@@ -15,6 +15,7 @@
 
 #include "btdma_common.cuh"
 #include "k_filtered_j.cuh"
+#include "k_heat.cuh"
 #include "k_ragged.cuh"
 #include "k_refine.cuh"
 #include "k_segment.cuh"
@@ -206,7 +207,8 @@ struct TilePlan {
     int sys = 0, cl = 0, nst = 0, nseg = 0;
 };
 
-TilePlan tile_plan(int n_row, bool cyclic, int elem = 8) {
+// na: arrays per ring stage (4, or 1 for the constant-coefficient D-only ring).
+TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4) {
     TilePlan pl;
     if (n_row % TILE_MT != 0) return pl;
     const int nseg = n_row / TILE_MT;
@@ -233,9 +235,9 @@ TilePlan tile_plan(int n_row, bool cyclic, int elem = 8) {
             }
         if (cl == 0) return pl;
     }
-    int nst = TILE_MAX_NST;
-    while (nst >= 3 &&
-           tile_smem_bytes(sys, nseg / cl, nseg, sys / cl, nst, elem) > (size_t)max_smem_optin())
+    int nst = na == 4 ? TILE_MAX_NST : TILE_MAX_NST_CONST;
+    while (nst >= 3 && tile_smem_bytes(sys, nseg / cl, nseg, sys / cl, nst, elem, na) >
+                           (size_t)max_smem_optin())
         --nst;
     if (nst < 3) return pl;
     pl.sys = sys;
@@ -245,9 +247,9 @@ TilePlan tile_plan(int n_row, bool cyclic, int elem = 8) {
     return pl;
 }
 
-template <int SYS, bool CYCLIC, typename TIN = double, typename TC = double>
+template <int SYS, bool CYCLIC, typename TIN = double, typename TC = double, bool CONSTC = false>
 int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st) {
-    auto kern = tile_f64_kernel<SYS, CYCLIC, TIN, TC>;
+    auto kern = tile_f64_kernel<SYS, CYCLIC, TIN, TC, CONSTC>;
     static bool attr_done = false;
     if (!attr_done) {
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -258,8 +260,8 @@ int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st)
     const int threads = SYS * a.nseg / a.cl;
     cudaLaunchConfig_t cfg = {};
     cfg.blockDim = dim3(threads, 1, 1);
-    cfg.dynamicSmemBytes =
-        tile_smem_bytes(SYS, a.nseg / a.cl, a.nseg, SYS / a.cl, a.nst, (int)sizeof(TIN));
+    cfg.dynamicSmemBytes = tile_smem_bytes(SYS, a.nseg / a.cl, a.nseg, SYS / a.cl, a.nst,
+                                           (int)sizeof(TIN), CONSTC ? 1 : 4);
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -335,6 +337,38 @@ int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, 
     a.gate = gate;
     a.status = status;
     const int rc = launch_tile_plan<TIN, TC>(pl, maps, a, cyclic, st);
+    return rc == BTDMA_OK ? 1 : rc;
+}
+
+// Constant-coefficient batch (every row -cs, 1 + 2 cs, -cs; cs more on the
+// diagonal of the first and last row when cbound): only D is read.  Returns 1
+// when launched, 0 when the shape is not tiled, < 0 on error.
+int try_tile_const(const double* D, double* X, int n_sys, int n_row, double cs, bool cbound,
+                   unsigned* status, cudaStream_t st) {
+    const TilePlan pl = tile_plan(n_row, false, 8, 1);
+    if (pl.sys == 0 || !tma_ok_elem(D, n_sys, 8)) return 0;
+    const int nsc = pl.nseg / pl.cl;
+    CUtensorMap maps[4];
+    if (!make_tile_map(&maps[3], D, n_sys, pl.nseg, pl.sys, nsc, 8)) return 0;
+    maps[0] = maps[1] = maps[2] = maps[3];  // not read in this mode
+    TileArgs a = {};
+    a.X = X;
+    a.n_sys = n_sys;
+    a.n_row = n_row;
+    a.nseg = pl.nseg;
+    a.cl = pl.cl;
+    a.nst = pl.nst;
+    a.n_groups = (n_sys + pl.sys - 1) / pl.sys;
+    a.cs = cs;
+    a.cbound = cbound ? 1 : 0;
+    a.status = status;
+    int rc;
+    switch (pl.sys) {
+        case 128: rc = launch_tile_sys<128, false, double, double, true>(maps, a, st); break;
+        case 64: rc = launch_tile_sys<64, false, double, double, true>(maps, a, st); break;
+        case 32: rc = launch_tile_sys<32, false, double, double, true>(maps, a, st); break;
+        default: rc = launch_tile_sys<16, false, double, double, true>(maps, a, st); break;
+    }
     return rc == BTDMA_OK ? 1 : rc;
 }
 
@@ -1099,5 +1133,200 @@ int btdma_ragged_plan_info(btdma_t h, btdma_ragged_bucket* out, int cap, int* n_
         out[i].cta_per_system = b.cta;
         out[i].tuned_ms = b.best_ms;
     }
+    return BTDMA_OK;
+}
+
+// ------------------------------------------------------------- heat ADI step
+struct btdma_heat {
+    HeatGeom g{};
+    double* xc = nullptr;  // device coordinates (ghosts included)
+    double* yc = nullptr;
+    double* zc = nullptr;
+    double* buf0 = nullptr;  // Z and X sweep layouts
+    double* buf1 = nullptr;  // Y sweep layout
+    double* err = nullptr;   // L2 accumulator
+    double* scratch = nullptr;  // full grid, the warm-up step before graph capture
+    unsigned* status = nullptr;
+    cudaStream_t cap = nullptr;  // private stream the step graph is captured on
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    double* graph_theta = nullptr;  // theta the graph was captured for
+    cudaStream_t last_stream = nullptr;
+};
+
+namespace {
+
+// One step as a kernel sequence on stream st (seven launches, no host sync).
+int heat_enqueue(btdma_heat_t h, double* theta, cudaStream_t st) {
+    const HeatGeom& g = h->g;
+    const dim3 b1(128, 1, 1);
+    const dim3 gr((g.ix + 127) / 128, g.iy, g.iz);
+    heat_rhs_z_kernel<<<gr, b1, 0, st>>>(theta, h->buf0, g);
+    CK(cudaGetLastError());
+    int rc = try_tile_const(h->buf0, h->buf0, g.ix * g.iy, g.iz, g.bz, true, h->status, st);
+    if (rc != 1) return rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "Z sweep not tileable");
+    heat_z_to_y_kernel<<<gr, b1, 0, st>>>(theta, h->buf0, h->buf1, g);
+    CK(cudaGetLastError());
+    rc = try_tile_const(h->buf1, h->buf1, g.ix * g.iz, g.iy, g.by, true, h->status, st);
+    if (rc != 1) return rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "Y sweep not tileable");
+    const dim3 bt(HEAT_TILE, 8, 1);
+    heat_y_to_x_kernel<<<dim3((g.ix + HEAT_TILE - 1) / HEAT_TILE, (g.iy + HEAT_TILE - 1) / HEAT_TILE,
+                              g.iz), bt, 0, st>>>(theta, h->buf1, h->buf0, g);
+    CK(cudaGetLastError());
+    rc = try_tile_const(h->buf0, h->buf0, g.iy * g.iz, g.ix, g.bx, true, h->status, st);
+    if (rc != 1) return rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "X sweep not tileable");
+    heat_update_kernel<<<dim3((g.iy + HEAT_TILE - 1) / HEAT_TILE, (g.ix + HEAT_TILE - 1) / HEAT_TILE,
+                              g.iz), bt, 0, st>>>(theta, h->buf0, g);
+    CK(cudaGetLastError());
+    return BTDMA_OK;
+}
+
+}  // namespace
+
+int btdma_heat_create(int ix, int iy, int iz, double dt, btdma_heat_t* out) {
+    if (!out) return fail(BTDMA_ERR_ARG, "null output handle");
+    *out = nullptr;
+    if (ix <= 0 || iy <= 0 || iz <= 0 || !(dt > 0.0))
+        return fail(BTDMA_ERR_ARG, "grid sizes and dt must be positive");
+    if (ix % 16 || iy % 16 || iz % 16)
+        return fail(BTDMA_ERR_UNSUPPORTED, "the fused step needs ix, iy, iz multiples of 16");
+    if (!tile_plan(iz, false, 8, 1).sys || !tile_plan(iy, false, 8, 1).sys ||
+        !tile_plan(ix, false, 8, 1).sys)
+        return fail(BTDMA_ERR_UNSUPPORTED, "grid not supported by the tiled solve");
+    btdma_heat* h = new btdma_heat();
+    auto cleanup = [&](int code) {
+        btdma_heat_destroy(h);
+        return code;
+    };
+#define CKH(call)                                                                          \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return cleanup(fail(BTDMA_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_))); \
+    } while (0)
+    // cell centres with one ghost each side, x_c[i] = x0 + dd/2 + (i - 1) dd on
+    // [-1, 1] with dd = 2 / n (mpi_subdomain.cpp mesh(), one rank)
+    auto coords = [](int n) {
+        std::vector<double> c(n + 2);
+        const double dd = 2.0 / n;
+        for (int i = 0; i < n + 2; ++i) c[i] = -1.0 + dd / 2.0 + (i - 1) * dd;
+        return c;
+    };
+    const auto hx = coords(ix), hy = coords(iy), hz = coords(iz);
+    CKH(cudaMalloc(&h->xc, sizeof(double) * hx.size()));
+    CKH(cudaMalloc(&h->yc, sizeof(double) * hy.size()));
+    CKH(cudaMalloc(&h->zc, sizeof(double) * hz.size()));
+    CKH(cudaMemcpy(h->xc, hx.data(), sizeof(double) * hx.size(), cudaMemcpyHostToDevice));
+    CKH(cudaMemcpy(h->yc, hy.data(), sizeof(double) * hy.size(), cudaMemcpyHostToDevice));
+    CKH(cudaMemcpy(h->zc, hz.data(), sizeof(double) * hz.size(), cudaMemcpyHostToDevice));
+    const size_t inner = (size_t)ix * iy * iz;
+    CKH(cudaMalloc(&h->buf0, sizeof(double) * inner));
+    CKH(cudaMalloc(&h->buf1, sizeof(double) * inner));
+    CKH(cudaMalloc(&h->err, sizeof(double)));
+    CKH(cudaMalloc(&h->scratch, sizeof(double) * (size_t)(ix + 2) * (iy + 2) * (iz + 2)));
+    CKH(cudaMalloc(&h->status, sizeof(unsigned)));
+    CKH(cudaMemset(h->status, 0, sizeof(unsigned)));
+    CKH(cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking));
+#undef CKH
+    HeatGeom& g = h->g;
+    g.ix = ix;
+    g.iy = iy;
+    g.iz = iz;
+    g.dt = dt;
+    const double dx = 2.0 / ix, dy = 2.0 / iy, dz = 2.0 / iz;
+    g.bx = dt / (2.0 * dx * dx);  // stencil base, stencil_coeffs.hpp:10-13
+    g.by = dt / (2.0 * dy * dy);
+    g.bz = dt / (2.0 * dz * dz);
+    g.xc = h->xc;
+    g.yc = h->yc;
+    g.zc = h->zc;
+    *out = h;
+    return BTDMA_OK;
+}
+
+int btdma_heat_destroy(btdma_heat_t h) {
+    if (!h) return BTDMA_OK;
+    if (h->exec) cudaGraphExecDestroy(h->exec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    if (h->cap) cudaStreamDestroy(h->cap);
+    cudaFree(h->xc);
+    cudaFree(h->yc);
+    cudaFree(h->zc);
+    cudaFree(h->buf0);
+    cudaFree(h->buf1);
+    cudaFree(h->err);
+    cudaFree(h->scratch);
+    cudaFree(h->status);
+    delete h;
+    return BTDMA_OK;
+}
+
+int btdma_heat_init(btdma_heat_t h, double* theta, cudaStream_t stream) {
+    if (!h || !theta) return fail(BTDMA_ERR_ARG, "null argument");
+    const HeatGeom& g = h->g;
+    heat_init_kernel<<<dim3((g.ix + 2 + 127) / 128, g.iy + 2, g.iz + 2), 128, 0, stream>>>(theta,
+                                                                                           g);
+    CK(cudaGetLastError());
+    h->last_stream = stream;
+    return BTDMA_OK;
+}
+
+int btdma_heat_step(btdma_heat_t h, double* theta, int n_steps, int use_graph,
+                    cudaStream_t stream) {
+    if (!h || !theta) return fail(BTDMA_ERR_ARG, "null argument");
+    if (n_steps < 0) return fail(BTDMA_ERR_ARG, "n_steps must be >= 0");
+    h->last_stream = stream;
+    if (!use_graph) {
+        for (int s = 0; s < n_steps; ++s) {
+            const int rc = heat_enqueue(h, theta, stream);
+            if (rc) return rc;
+        }
+        return BTDMA_OK;
+    }
+    if (!h->exec || h->graph_theta != theta) {
+        if (h->exec) cudaGraphExecDestroy(h->exec);
+        if (h->graph) cudaGraphDestroy(h->graph);
+        h->exec = nullptr;
+        h->graph = nullptr;
+        // one uncaptured step on a zeroed scratch field first, so the kernels'
+        // first-use attribute calls stay out of the capture (theta is untouched)
+        const HeatGeom& g = h->g;
+        CK(cudaMemsetAsync(h->scratch, 0, sizeof(double) * (size_t)(g.ix + 2) * (g.iy + 2) *
+                                              (g.iz + 2), h->cap));
+        int rc = heat_enqueue(h, h->scratch, h->cap);
+        if (rc) return rc;
+        CK(cudaStreamSynchronize(h->cap));
+        // capture on the private stream, after the caller's stream has reached
+        // this point (the graph is launched on the caller's stream below)
+        CK(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
+        rc = heat_enqueue(h, theta, h->cap);
+        cudaGraph_t gr = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(h->cap, &gr);
+        if (rc) {
+            if (gr) cudaGraphDestroy(gr);
+            return rc;
+        }
+        CK(e);
+        h->graph = gr;
+        CK(cudaGraphInstantiate(&h->exec, gr, 0));
+        h->graph_theta = theta;
+    }
+    for (int s = 0; s < n_steps; ++s) CK(cudaGraphLaunch(h->exec, stream));
+    return BTDMA_OK;
+}
+
+int btdma_heat_l2_error(btdma_heat_t h, const double* theta, double t_phys, double* l2) {
+    if (!h || !theta || !l2) return fail(BTDMA_ERR_ARG, "null argument");
+    const HeatGeom& g = h->g;
+    const cudaStream_t st = h->last_stream;
+    CK(cudaMemsetAsync(h->err, 0, sizeof(double), st));
+    const double decay = exp(-3.0 * HEAT_PI * HEAT_PI * t_phys);
+    heat_err_kernel<<<dim3((g.ix + 127) / 128, g.iy, g.iz), 128, 0, st>>>(theta, g, decay, h->err);
+    CK(cudaGetLastError());
+    double sum = 0.0;
+    CK(cudaMemcpyAsync(&sum, h->err, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // normalised by (ix + 1)(iy + 1)(iz + 1), the reference's params.nx * ny * nz
+    *l2 = sqrt(sum / ((double)(g.ix + 1) * (g.iy + 1) * (g.iz + 1)));
     return BTDMA_OK;
 }

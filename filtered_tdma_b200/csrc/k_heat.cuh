@@ -1,0 +1,183 @@
+// One theta-scheme ADI step of the reference's 3-D heat application
+// (apps/heat_gpu/solve_theta.cu:121-351 and its step loop at :499-600), fused
+// around the constant-coefficient tiled solve.
+//
+// Grid: ix x iy x iz interior cells on [-1, 1]^3 with one ghost layer; theta is
+// the full grid, theta[(k * ny + j) * nx + i], nx = ix + 2 (i = ii + 1 for
+// interior index ii).  Stencil per direction (stencil_coeffs.hpp:10-13):
+// base = dt / (2 dd^2), a = c = base, b = -2 base.  Dirichlet walls use the
+// reflection ghost u_ghost = 2 u_BC - u_adjacent (mpi_subdomain.cpp boundary()),
+// folded fully implicitly: the wall row of each sweep gets base more on the
+// diagonal and base * (ghost + adjacent) on the right-hand side
+// (solve_theta.cu:185-201).
+//
+// Differences from the reference's kernel sequence, none of which changes the
+// arithmetic of a cell:
+//   * ghosts are not stored: a stencil neighbour outside the interior is
+//     computed as 2 u_BC - theta(cell), exactly the value the reference's ghost
+//     kernels write there;
+//   * A, B, C are never materialised (the solve generates them);
+//   * the Y sweep reads the Z solution in place ([kk][jj][ii] -> [jj][kk][ii]
+//     is a copy with ii fastest on both sides), and only the X sweep and the
+//     final update transpose through shared-memory tiles.
+#pragma once
+
+#include "btdma_common.cuh"
+
+namespace btdma {
+
+struct HeatGeom {
+    int ix, iy, iz;        // interior cells
+    double dt;
+    double bx, by, bz;     // stencil base per direction: dt / (2 dd^2)
+    const double* xc;      // cell centres incl. ghosts [ix + 2]
+    const double* yc;      // [iy + 2]
+    const double* zc;      // [iz + 2]
+};
+
+__device__ __forceinline__ size_t heat_full(const HeatGeom& g, int i, int j, int k) {
+    return ((size_t)k * (g.iy + 2) + j) * (g.ix + 2) + i;
+}
+
+constexpr double HEAT_PI = 3.14159265358979323846;
+
+// Right-hand side of the step (all directions' explicit half) plus the Z wall
+// folds, written in the Z-sweep layout D[(kk * iy + jj) * ix + ii]
+// (solve_theta.cu:121-160 and build_lhs_z_kernel :168-202).
+__global__ void __launch_bounds__(256) heat_rhs_z_kernel(const double* __restrict__ theta,
+                                                         double* __restrict__ D,
+                                                         const HeatGeom g) {
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    const int jj = blockIdx.y;
+    const int kk = blockIdx.z;
+    if (ii >= g.ix) return;
+    const int i = ii + 1, j = jj + 1, k = kk + 1;
+    const double t = theta[heat_full(g, i, j, k)];
+    const double cxk = cos(HEAT_PI * g.zc[k]);
+    double tip, tim, tjp, tjm, tkp, tkm;
+    {
+        const double ubc = -cos(HEAT_PI * g.yc[j]) * cxk;  // x walls
+        tip = ii + 1 < g.ix ? theta[heat_full(g, i + 1, j, k)] : 2.0 * ubc - t;
+        tim = ii > 0 ? theta[heat_full(g, i - 1, j, k)] : 2.0 * ubc - t;
+    }
+    {
+        const double ubc = -cos(HEAT_PI * g.xc[i]) * cxk;  // y walls
+        tjp = jj + 1 < g.iy ? theta[heat_full(g, i, j + 1, k)] : 2.0 * ubc - t;
+        tjm = jj > 0 ? theta[heat_full(g, i, j - 1, k)] : 2.0 * ubc - t;
+    }
+    const double ubz = -cos(HEAT_PI * g.xc[i]) * cos(HEAT_PI * g.yc[j]);  // z walls
+    tkp = kk + 1 < g.iz ? theta[heat_full(g, i, j, k + 1)] : 2.0 * ubz - t;
+    tkm = kk > 0 ? theta[heat_full(g, i, j, k - 1)] : 2.0 * ubz - t;
+    const double src = g.dt * 3.0 * HEAT_PI * HEAT_PI * cos(HEAT_PI * g.xc[i]) *
+                       cos(HEAT_PI * g.yc[j]) * cxk;
+    double rhs = (g.bx * tip + g.bx * tim) + (g.by * tjp + g.by * tjm) +
+                 (g.bz * tkp + g.bz * tkm) +
+                 (1.0 + (-2.0 * g.bx) + (-2.0 * g.by) + (-2.0 * g.bz)) * t + src;
+    // fully implicit Z walls: base * (ghost + boundary cell) to the right-hand side
+    if (kk == 0) rhs += g.bz * ((2.0 * ubz - t) + t);
+    if (kk == g.iz - 1) rhs += g.bz * ((2.0 * ubz - t) + t);
+    D[((size_t)kk * g.iy + jj) * g.ix + ii] = rhs;
+}
+
+// Z solution [kk][jj][ii] -> Y-sweep layout [jj][kk][ii] plus the Y wall folds
+// (copy_z_to_rhs + build_lhs_y_kernel, solve_theta.cu:205-253).
+__global__ void __launch_bounds__(256) heat_z_to_y_kernel(const double* __restrict__ theta,
+                                                          const double* __restrict__ Dz,
+                                                          double* __restrict__ Dy,
+                                                          const HeatGeom g) {
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    const int jj = blockIdx.y;
+    const int kk = blockIdx.z;
+    if (ii >= g.ix) return;
+    double v = Dz[((size_t)kk * g.iy + jj) * g.ix + ii];
+    if (jj == 0 || jj == g.iy - 1) {
+        const int i = ii + 1, k = kk + 1, j = jj == 0 ? 1 : g.iy;
+        const double t = theta[heat_full(g, i, j, k)];
+        const double ubc = -cos(HEAT_PI * g.xc[i]) * cos(HEAT_PI * g.zc[k]);
+        if (jj == 0) v += g.by * ((2.0 * ubc - t) + t);
+        if (jj == g.iy - 1) v += g.by * ((2.0 * ubc - t) + t);
+    }
+    Dy[((size_t)jj * g.iz + kk) * g.ix + ii] = v;
+}
+
+constexpr int HEAT_TILE = 32;
+
+// Y solution [jj][kk][ii] -> X-sweep layout [ii][kk][jj] plus the X wall folds
+// (copy_y_to_rhs + build_lhs_x_kernel, solve_theta.cu:256-332), through a
+// shared 32 x 32 tile so both sides are coalesced.  Block (32, 8).
+__global__ void __launch_bounds__(256) heat_y_to_x_kernel(const double* __restrict__ theta,
+                                                          const double* __restrict__ Dy,
+                                                          double* __restrict__ Dx,
+                                                          const HeatGeom g) {
+    __shared__ double tile[HEAT_TILE][HEAT_TILE + 1];
+    const int ii0 = blockIdx.x * HEAT_TILE, jj0 = blockIdx.y * HEAT_TILE, kk = blockIdx.z;
+    for (int r = threadIdx.y; r < HEAT_TILE; r += blockDim.y) {
+        const int ii = ii0 + threadIdx.x, jj = jj0 + r;
+        if (ii < g.ix && jj < g.iy) tile[r][threadIdx.x] = Dy[((size_t)jj * g.iz + kk) * g.ix + ii];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < HEAT_TILE; r += blockDim.y) {
+        const int jj = jj0 + threadIdx.x, ii = ii0 + r;
+        if (ii < g.ix && jj < g.iy) {
+            double v = tile[threadIdx.x][r];
+            if (ii == 0 || ii == g.ix - 1) {
+                const int j = jj + 1, k = kk + 1, i = ii == 0 ? 1 : g.ix;
+                const double t = theta[heat_full(g, i, j, k)];
+                const double ubc = -cos(HEAT_PI * g.yc[j]) * cos(HEAT_PI * g.zc[k]);
+                if (ii == 0) v += g.bx * ((2.0 * ubc - t) + t);
+                if (ii == g.ix - 1) v += g.bx * ((2.0 * ubc - t) + t);
+            }
+            Dx[((size_t)ii * g.iz + kk) * g.iy + jj] = v;
+        }
+    }
+}
+
+// theta(i, j, k) = X solution [ii][kk][jj] (update_theta_kernel,
+// solve_theta.cu:335-347), transposed back through a shared tile.
+__global__ void __launch_bounds__(256) heat_update_kernel(double* __restrict__ theta,
+                                                          const double* __restrict__ Dx,
+                                                          const HeatGeom g) {
+    __shared__ double tile[HEAT_TILE][HEAT_TILE + 1];
+    const int jj0 = blockIdx.x * HEAT_TILE, ii0 = blockIdx.y * HEAT_TILE, kk = blockIdx.z;
+    for (int r = threadIdx.y; r < HEAT_TILE; r += blockDim.y) {
+        const int jj = jj0 + threadIdx.x, ii = ii0 + r;
+        if (ii < g.ix && jj < g.iy) tile[r][threadIdx.x] = Dx[((size_t)ii * g.iz + kk) * g.iy + jj];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < HEAT_TILE; r += blockDim.y) {
+        const int ii = ii0 + threadIdx.x, jj = jj0 + r;
+        if (ii < g.ix && jj < g.iy) theta[heat_full(g, ii + 1, jj + 1, kk + 1)] = tile[threadIdx.x][r];
+    }
+}
+
+// Initial field on the full grid, ghosts included (mpi_subdomain.cpp
+// initialization): sin(pi x) sin(pi y) sin(pi z) + cos(pi x) cos(pi y) cos(pi z).
+__global__ void heat_init_kernel(double* __restrict__ theta, const HeatGeom g) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, k = blockIdx.z;
+    if (i >= g.ix + 2) return;
+    const double x = g.xc[i], y = g.yc[j], z = g.zc[k];
+    theta[heat_full(g, i, j, k)] = sin(HEAT_PI * x) * sin(HEAT_PI * y) * sin(HEAT_PI * z) +
+                                   cos(HEAT_PI * x) * cos(HEAT_PI * y) * cos(HEAT_PI * z);
+}
+
+// Sum over interior cells of (theta - exact)^2 with the manufactured solution
+// exact = sin sin sin * exp(-3 pi^2 t) + cos cos cos (heat_cpu/main.cpp:59-79).
+__global__ void heat_err_kernel(const double* __restrict__ theta, const HeatGeom g, double decay,
+                                double* __restrict__ sum) {
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    const int jj = blockIdx.y, kk = blockIdx.z;
+    double e = 0.0;
+    if (ii < g.ix) {
+        const int i = ii + 1, j = jj + 1, k = kk + 1;
+        const double x = g.xc[i], y = g.yc[j], z = g.zc[k];
+        const double ex = sin(HEAT_PI * x) * sin(HEAT_PI * y) * sin(HEAT_PI * z) * decay +
+                          cos(HEAT_PI * x) * cos(HEAT_PI * y) * cos(HEAT_PI * z);
+        const double d = theta[heat_full(g, i, j, k)] - ex;
+        e = d * d;
+    }
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(sum, e);
+}
+
+}  // namespace btdma

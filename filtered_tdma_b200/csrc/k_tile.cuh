@@ -57,6 +57,7 @@ constexpr int TILE_MT = 16;           // rows per sub-segment (per thread)
 __host__ __device__ constexpr int tile_rps(int elem) { return 16 / elem; }
 constexpr int TILE_MAX_THREADS = 512;
 constexpr int TILE_MAX_NST = 8;       // ring stages (upper bound)
+constexpr int TILE_MAX_NST_CONST = 16;  // ring stages of D-only (constant-coefficient) rings
 
 struct TileArgs {
     double* X;
@@ -67,6 +68,12 @@ struct TileArgs {
     int n_groups;  // groups of SYS systems
     int accumulate;        // 1: X += solution (refinement corrections), 0: X = solution
     const unsigned* gate;  // non-null: the launch does nothing while *gate == 0
+    // constant-coefficient instantiations (CONSTC): every row is
+    //   -cs x_{j-1} + (1 + 2 cs) x_j - cs x_{j+1} = d_j,
+    // plus cs on the diagonal of the first and last row when cbound != 0 (the
+    // fully implicit Dirichlet wall of the heat ADI step); only D is read.
+    double cs;
+    int cbound;
     unsigned* status;
 };
 
@@ -97,12 +104,14 @@ __host__ __device__ __forceinline__ size_t tile_fixed_doubles(int sys, int nsc, 
     if (nseg > 32) f += 6ull * (nseg + 2) * sub;
     return f;
 }
-__host__ __device__ __forceinline__ size_t tile_ring_bytes(int sys, int nsc, int nst, int elem) {
-    return (size_t)nst * 4 * tile_rps(elem) * sys * nsc * elem;
+// na: arrays per ring stage (4: A, B, C, D; 1: D only).
+__host__ __device__ __forceinline__ size_t tile_ring_bytes(int sys, int nsc, int nst, int elem,
+                                                           int na = 4) {
+    return (size_t)nst * na * tile_rps(elem) * sys * nsc * elem;
 }
 __host__ __device__ __forceinline__ size_t tile_smem_bytes(int sys, int nsc, int nseg, int sub,
-                                                           int nst, int elem = 8) {
-    return tile_ring_bytes(sys, nsc, nst, elem) +
+                                                           int nst, int elem = 8, int na = 4) {
+    return tile_ring_bytes(sys, nsc, nst, elem, na) +
            tile_fixed_doubles(sys, nsc, nseg, sub) * sizeof(double) +
            2ull * nst * sizeof(uint64_t) + 128;
 }
@@ -133,7 +142,7 @@ __device__ __forceinline__ void tile_cluster_sync(int cl) {
 // the local sweeps — double (FP32 storage is widened exactly on load), or float
 // (the FP32 inner solve of iterative refinement).  The reduced system, the back
 // substitution and x are always FP64.
-template <int SYS, bool CYCLIC, typename TIN = double, typename TC = double>
+template <int SYS, bool CYCLIC, typename TIN = double, typename TC = double, bool CONSTC = false>
 __global__ void __launch_bounds__(TILE_MAX_THREADS, 1)
 tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 const __grid_constant__ CUtensorMap tmC, const __grid_constant__ CUtensorMap tmD,
@@ -142,6 +151,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     constexpr int M = TILE_MT;
     constexpr int RPS = tile_rps((int)sizeof(TIN));  // rows per ring stage
     constexpr int SPG = M / RPS;                      // stages per group
+    constexpr int NA = CONSTC ? 1 : 4;                // arrays per ring stage
     constexpr int RP = SYS + 1;  // padded pitch of red / xr rows
     extern __shared__ unsigned char smem_raw[];
     const int nseg = args.nseg, cl = args.cl, nst = args.nst;
@@ -154,7 +164,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 
     TIN* ring = reinterpret_cast<TIN*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-    double* red = reinterpret_cast<double*>(ring + (size_t)nst * 4 * RPS * T);
+    double* red = reinterpret_cast<double*>(ring + (size_t)nst * NA * RPS * T);
     double* xr = red + 6 * fstride;
     double* pcr = xr + 2 * fstride;  // only when !shuffled
     const int gs = nseg + 2;
@@ -196,7 +206,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                          ? (args.n_groups - cluster_id + n_clusters - 1) / n_clusters
                          : 0;
     const int total = n_my * SPG;  // ring stages this CTA consumes
-    const int sstride = 4 * RPS * T;  // elements per stage
+    const int sstride = NA * RPS * T;  // elements per stage
     const uint32_t stage_bytes = (uint32_t)sstride * sizeof(TIN);
 
     auto issue = [&](int t) {  // one thread
@@ -205,10 +215,12 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         const int k0 = (t % SPG) * RPS;
         TIN* dst = ring + (size_t)slot * sstride;
         mbar_expect_tx(&full[slot], stage_bytes);
-        tma_load_3d(dst + 0 * RPS * T, &tmA, g * SYS, k0, c * nsc, &full[slot]);
-        tma_load_3d(dst + 1 * RPS * T, &tmB, g * SYS, k0, c * nsc, &full[slot]);
-        tma_load_3d(dst + 2 * RPS * T, &tmC, g * SYS, k0, c * nsc, &full[slot]);
-        tma_load_3d(dst + 3 * RPS * T, &tmD, g * SYS, k0, c * nsc, &full[slot]);
+        if constexpr (!CONSTC) {
+            tma_load_3d(dst + 0 * RPS * T, &tmA, g * SYS, k0, c * nsc, &full[slot]);
+            tma_load_3d(dst + 1 * RPS * T, &tmB, g * SYS, k0, c * nsc, &full[slot]);
+            tma_load_3d(dst + 2 * RPS * T, &tmC, g * SYS, k0, c * nsc, &full[slot]);
+        }
+        tma_load_3d(dst + (NA - 1) * RPS * T, &tmD, g * SYS, k0, c * nsc, &full[slot]);
     };
     bool ok = true;
     if (tid == 0)
@@ -240,10 +252,12 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             TIN a2[RPS], b2[RPS], c2[RPS], d2[RPS];  // widened where used
 #pragma unroll
             for (int r = 0; r < RPS; ++r) {
-                a2[r] = st[0 * RPS * T + r * SYS];
-                b2[r] = st[1 * RPS * T + r * SYS];
-                c2[r] = st[2 * RPS * T + r * SYS];
-                d2[r] = st[3 * RPS * T + r * SYS];
+                if constexpr (!CONSTC) {
+                    a2[r] = st[0 * RPS * T + r * SYS];
+                    b2[r] = st[1 * RPS * T + r * SYS];
+                    c2[r] = st[2 * RPS * T + r * SYS];
+                }
+                d2[r] = st[(NA - 1) * RPS * T + r * SYS];
             }
             __syncwarp();
             if (lane == 0) {
@@ -269,7 +283,20 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 #pragma unroll
             for (int r = 0; r < RPS; ++r) {
                 const int k = j * RPS + r;
-                const TC a = (TC)a2[r], b = (TC)b2[r], cc = (TC)c2[r], d = (TC)d2[r];
+                TC a, b, cc;
+                if constexpr (CONSTC) {
+                    const int q = c * nsc + ql;  // sub-segment of this thread
+                    const bool wall = args.cbound != 0 && ((q == 0 && k == 0) ||
+                                                           (q == nseg - 1 && k == M - 1));
+                    a = (TC)-args.cs;
+                    cc = (TC)-args.cs;
+                    b = (TC)(1.0 + 2.0 * args.cs + (wall ? args.cs : 0.0));
+                } else {
+                    a = (TC)a2[r];
+                    b = (TC)b2[r];
+                    cc = (TC)c2[r];
+                }
+                const TC d = (TC)d2[r];
                 if (k == 0) {
                     const TC ib = rcp_tc(b);
                     ab0 = a * ib;

@@ -222,6 +222,27 @@ typedef struct btdma_ragged_bucket {
 } btdma_ragged_bucket;
 int btdma_ragged_plan_info(btdma_t h, btdma_ragged_bucket* out, int cap, int* n_out);
 
+/* Fused 3-D heat ADI step: the theta-scheme step of the reference's heat
+ * application (apps/heat_gpu/solve_theta.cu, SolveTheta::profile's step loop:
+ * ghost fill, right-hand side, Z, Y and X sweeps with fully implicit Dirichlet
+ * walls, update) on ix x iy x iz interior cells of [-1, 1]^3, one GPU, PaScaL
+ * solves.  theta is the caller's device field with one ghost layer,
+ * theta[(k * (iy + 2) + j) * (ix + 2) + i].  Each sweep's tridiagonal
+ * coefficients are generated inside the solve (never stored); ix, iy, iz must
+ * be multiples of 16.  btdma_heat_step runs n_steps steps, as one captured
+ * CUDA graph replayed per step when use_graph != 0 (captured on the first call
+ * for this theta pointer).  btdma_heat_init writes the reference's initial
+ * field; btdma_heat_l2_error returns the reference's global L2 error against
+ * the manufactured solution at physical time t_phys (sum over interior cells
+ * divided by (ix + 1)(iy + 1)(iz + 1), heat_cpu/main.cpp:59-79; blocking). */
+typedef struct btdma_heat* btdma_heat_t;
+int btdma_heat_create(int ix, int iy, int iz, double dt, btdma_heat_t* out);
+int btdma_heat_destroy(btdma_heat_t h);
+int btdma_heat_init(btdma_heat_t h, double* theta, cudaStream_t stream);
+int btdma_heat_step(btdma_heat_t h, double* theta, int n_steps, int use_graph,
+                    cudaStream_t stream);
+int btdma_heat_l2_error(btdma_heat_t h, const double* theta, double t_phys, double* l2);
+
 /* Switch the method of an existing handle (rho, eps and J state are kept).  The
  * reference's FilteredTDMACUDA object offers v1 and v2 side by side
  * (filtered_tdma_cuda.hpp:173-180); this lets one handle do the same. */
