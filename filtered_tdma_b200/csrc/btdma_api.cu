@@ -247,9 +247,9 @@ TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4) {
     return pl;
 }
 
-template <int SYS, bool CYCLIC, typename TIN = double, typename TC = double, bool CONSTC = false>
+template <int SYS, bool CYCLIC, typename TIN = double, typename TC = double, int GEN = 0>
 int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st) {
-    auto kern = tile_f64_kernel<SYS, CYCLIC, TIN, TC, CONSTC>;
+    auto kern = tile_f64_kernel<SYS, CYCLIC, TIN, TC, GEN>;
     static bool attr_done = false;
     if (!attr_done) {
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -261,7 +261,7 @@ int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st)
     cudaLaunchConfig_t cfg = {};
     cfg.blockDim = dim3(threads, 1, 1);
     cfg.dynamicSmemBytes = tile_smem_bytes(SYS, a.nseg / a.cl, a.nseg, SYS / a.cl, a.nst,
-                                           (int)sizeof(TIN), CONSTC ? 1 : 4);
+                                           (int)sizeof(TIN), GEN ? 1 : 4);
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -340,18 +340,19 @@ int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, 
     return rc == BTDMA_OK ? 1 : rc;
 }
 
-// Constant-coefficient batch (every row -cs, 1 + 2 cs, -cs; cs more on the
-// diagonal of the first and last row when cbound): only D is read.  Returns 1
-// when launched, 0 when the shape is not tiled, < 0 on error.
-int try_tile_const(const double* D, double* X, int n_sys, int n_row, double cs, bool cbound,
-                   unsigned* status, cudaStream_t st) {
+// Generated-coefficient batch, only D read (the GEN modes of the tiled
+// kernel; the coefficient fields of `gen` are used, the rest is filled here).
+// Returns 1 when launched, 0 when the shape is not tiled, < 0 on error.
+template <int GEN>
+int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArgs& gen,
+                 unsigned* status, cudaStream_t st) {
     const TilePlan pl = tile_plan(n_row, false, 8, 1);
     if (pl.sys == 0 || !tma_ok_elem(D, n_sys, 8)) return 0;
     const int nsc = pl.nseg / pl.cl;
     CUtensorMap maps[4];
     if (!make_tile_map(&maps[3], D, n_sys, pl.nseg, pl.sys, nsc, 8)) return 0;
     maps[0] = maps[1] = maps[2] = maps[3];  // not read in this mode
-    TileArgs a = {};
+    TileArgs a = gen;
     a.X = X;
     a.n_sys = n_sys;
     a.n_row = n_row;
@@ -359,17 +360,27 @@ int try_tile_const(const double* D, double* X, int n_sys, int n_row, double cs, 
     a.cl = pl.cl;
     a.nst = pl.nst;
     a.n_groups = (n_sys + pl.sys - 1) / pl.sys;
-    a.cs = cs;
-    a.cbound = cbound ? 1 : 0;
+    a.accumulate = 0;
+    a.gate = nullptr;
     a.status = status;
     int rc;
     switch (pl.sys) {
-        case 128: rc = launch_tile_sys<128, false, double, double, true>(maps, a, st); break;
-        case 64: rc = launch_tile_sys<64, false, double, double, true>(maps, a, st); break;
-        case 32: rc = launch_tile_sys<32, false, double, double, true>(maps, a, st); break;
-        default: rc = launch_tile_sys<16, false, double, double, true>(maps, a, st); break;
+        case 128: rc = launch_tile_sys<128, false, double, double, GEN>(maps, a, st); break;
+        case 64: rc = launch_tile_sys<64, false, double, double, GEN>(maps, a, st); break;
+        case 32: rc = launch_tile_sys<32, false, double, double, GEN>(maps, a, st); break;
+        default: rc = launch_tile_sys<16, false, double, double, GEN>(maps, a, st); break;
     }
     return rc == BTDMA_OK ? 1 : rc;
+}
+
+// Heat sweep: every row -cs, 1 + 2 cs, -cs; cs more on the diagonal of the
+// first and last row when cbound.
+int try_tile_const(const double* D, double* X, int n_sys, int n_row, double cs, bool cbound,
+                   unsigned* status, cudaStream_t st) {
+    TileArgs g = {};
+    g.cs = cs;
+    g.cbound = cbound ? 1 : 0;
+    return try_tile_gen<1>(D, X, n_sys, n_row, g, status, st);
 }
 
 template <bool CYCLIC>
@@ -1328,5 +1339,91 @@ int btdma_heat_l2_error(btdma_heat_t h, const double* theta, double t_phys, doub
     CK(cudaStreamSynchronize(st));
     // normalised by (ix + 1)(iy + 1)(iz + 1), the reference's params.nx * ny * nz
     *l2 = sqrt(sum / ((double)(g.ix + 1) * (g.iy + 1) * (g.iz + 1)));
+    return BTDMA_OK;
+}
+
+// -------------------------------------------- channel Poisson, wall-normal
+struct btdma_poisson {
+    int nz = 0, n_modes = 0, pin = 0;
+    double* ga = nullptr;   // [nz] sub-diagonal per row
+    double* gc = nullptr;   // [nz] super-diagonal per row
+    double* lam = nullptr;  // [n_modes] kx^2 + ky^2 per mode
+    unsigned* status = nullptr;
+};
+
+int btdma_poisson_create(int nz, const double* dz, const double* dmz, int n_modes,
+                         const double* lambda, int pin_mode0, btdma_poisson_t* out) {
+    if (!out) return fail(BTDMA_ERR_ARG, "null output handle");
+    *out = nullptr;
+    if (nz < 3 || n_modes <= 0 || !dz || !dmz || !lambda)
+        return fail(BTDMA_ERR_ARG, "need nz >= 3, n_modes > 0 and the dz, dmz, lambda arrays");
+    if (!tile_plan(nz, false, 8, 1).sys)
+        return fail(BTDMA_ERR_UNSUPPORTED, "nz must be a multiple of 16 (tiled solve)");
+    // row k: a = 1 / (dz[k+1] dmz[k+1]) (0 at the lower wall),
+    //        c = 1 / (dz[k+1] dmz[k+2]) (0 at the upper wall)
+    //   (k_build_poisson_tdma, PressureSolverGPU.cu:183-210)
+    std::vector<double> ha(nz), hc(nz);
+    for (int k = 0; k < nz; ++k) {
+        ha[k] = k == 0 ? 0.0 : 1.0 / (dz[k + 1] * dmz[k + 1]);
+        hc[k] = k == nz - 1 ? 0.0 : 1.0 / (dz[k + 1] * dmz[k + 2]);
+    }
+    btdma_poisson* h = new btdma_poisson();
+    h->nz = nz;
+    h->n_modes = n_modes;
+    h->pin = pin_mode0 ? 1 : 0;
+    auto cleanup = [&](int code) {
+        btdma_poisson_destroy(h);
+        return code;
+    };
+#define CKP(call)                                                                          \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return cleanup(fail(BTDMA_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_))); \
+    } while (0)
+    CKP(cudaMalloc(&h->ga, sizeof(double) * nz));
+    CKP(cudaMalloc(&h->gc, sizeof(double) * nz));
+    CKP(cudaMalloc(&h->lam, sizeof(double) * n_modes));
+    CKP(cudaMalloc(&h->status, sizeof(unsigned)));
+    CKP(cudaMemset(h->status, 0, sizeof(unsigned)));
+    CKP(cudaMemcpy(h->ga, ha.data(), sizeof(double) * nz, cudaMemcpyHostToDevice));
+    CKP(cudaMemcpy(h->gc, hc.data(), sizeof(double) * nz, cudaMemcpyHostToDevice));
+    CKP(cudaMemcpy(h->lam, lambda, sizeof(double) * n_modes, cudaMemcpyHostToDevice));
+#undef CKP
+    *out = h;
+    return BTDMA_OK;
+}
+
+int btdma_poisson_destroy(btdma_poisson_t h) {
+    if (!h) return BTDMA_OK;
+    cudaFree(h->ga);
+    cudaFree(h->gc);
+    cudaFree(h->lam);
+    cudaFree(h->status);
+    delete h;
+    return BTDMA_OK;
+}
+
+int btdma_poisson_solve(btdma_poisson_t h, double* rhs, cudaStream_t stream) {
+    if (!h || !rhs) return fail(BTDMA_ERR_ARG, "null argument");
+    TileArgs g = {};
+    g.ga = h->ga;
+    g.gc = h->gc;
+    g.glam = h->lam;
+    g.gpin = h->pin;
+    // complex rhs [nz][n_modes] = doubles [nz][2 n_modes]: real and imaginary
+    // parts are systems 2m and 2m + 1 with one matrix
+    const int rc = try_tile_gen<2>(rhs, rhs, 2 * h->n_modes, h->nz, g, h->status, stream);
+    if (rc == 0)
+        return fail(BTDMA_ERR_UNSUPPORTED, "rhs must be 16-byte aligned (tiled solve)");
+    return rc < 0 ? rc : BTDMA_OK;
+}
+
+int btdma_poisson_status(btdma_poisson_t h, unsigned* status, cudaStream_t stream) {
+    if (!h || !status) return fail(BTDMA_ERR_ARG, "null argument");
+    CK(cudaMemcpyAsync(status, h->status, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    CK(cudaMemsetAsync(h->status, 0, sizeof(unsigned), stream));
+    CK(cudaStreamSynchronize(stream));
     return BTDMA_OK;
 }

@@ -68,12 +68,20 @@ struct TileArgs {
     int n_groups;  // groups of SYS systems
     int accumulate;        // 1: X += solution (refinement corrections), 0: X = solution
     const unsigned* gate;  // non-null: the launch does nothing while *gate == 0
-    // constant-coefficient instantiations (CONSTC): every row is
-    //   -cs x_{j-1} + (1 + 2 cs) x_j - cs x_{j+1} = d_j,
-    // plus cs on the diagonal of the first and last row when cbound != 0 (the
-    // fully implicit Dirichlet wall of the heat ADI step); only D is read.
+    // Generated-coefficient instantiations read only D:
+    //  GEN == 1 (heat sweep): every row -cs x_{j-1} + (1 + 2 cs) x_j - cs x_{j+1},
+    //    plus cs on the diagonal of the first and last row when cbound != 0
+    //    (the fully implicit Dirichlet wall of the heat ADI step);
+    //  GEN == 2 (channel Poisson, wall-normal): row j is
+    //    ga[j] x_{j-1} - (ga[j] + gc[j] + glam[s / 2]) x_j + gc[j] x_{j+1},
+    //    systems 2m and 2m + 1 being the real and imaginary parts of mode m;
+    //    with gpin, row 0 of mode 0 is x_0 = 0 (the pinned mean pressure).
     double cs;
     int cbound;
+    const double* ga;
+    const double* gc;
+    const double* glam;
+    int gpin;
     unsigned* status;
 };
 
@@ -142,7 +150,7 @@ __device__ __forceinline__ void tile_cluster_sync(int cl) {
 // the local sweeps — double (FP32 storage is widened exactly on load), or float
 // (the FP32 inner solve of iterative refinement).  The reduced system, the back
 // substitution and x are always FP64.
-template <int SYS, bool CYCLIC, typename TIN = double, typename TC = double, bool CONSTC = false>
+template <int SYS, bool CYCLIC, typename TIN = double, typename TC = double, int GEN = 0>
 __global__ void __launch_bounds__(TILE_MAX_THREADS, 1)
 tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 const __grid_constant__ CUtensorMap tmC, const __grid_constant__ CUtensorMap tmD,
@@ -151,6 +159,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     constexpr int M = TILE_MT;
     constexpr int RPS = tile_rps((int)sizeof(TIN));  // rows per ring stage
     constexpr int SPG = M / RPS;                      // stages per group
+    constexpr bool CONSTC = GEN != 0;                 // coefficients generated, D only
     constexpr int NA = CONSTC ? 1 : 4;                // arrays per ring stage
     constexpr int RP = SYS + 1;  // padded pitch of red / xr rows
     extern __shared__ unsigned char smem_raw[];
@@ -244,6 +253,8 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 
         // ------------------------------------------------------ forward pass
         TC al[M], ga[M], de[M];  // rows 1..M-1 used (register resident)
+        double lam = 0.0;        // GEN == 2: this system's diagonal shift
+        if constexpr (GEN == 2) lam = valid ? args.glam[sys >> 1] : 0.0;
         TC ab0 = 0, cb0 = 0, db0 = 0;
         TC pi = 1, sa = 0, sd = 0;
 #pragma unroll
@@ -283,20 +294,31 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 #pragma unroll
             for (int r = 0; r < RPS; ++r) {
                 const int k = j * RPS + r;
-                TC a, b, cc;
-                if constexpr (CONSTC) {
+                TC a, b, cc, d = (TC)d2[r];
+                if constexpr (GEN == 1) {
                     const int q = c * nsc + ql;  // sub-segment of this thread
                     const bool wall = args.cbound != 0 && ((q == 0 && k == 0) ||
                                                            (q == nseg - 1 && k == M - 1));
                     a = (TC)-args.cs;
                     cc = (TC)-args.cs;
                     b = (TC)(1.0 + 2.0 * args.cs + (wall ? args.cs : 0.0));
+                } else if constexpr (GEN == 2) {
+                    const int kg = (c * nsc + ql) * M + k;  // row of the system
+                    const double ta = args.ga[kg], tc = args.gc[kg];
+                    a = (TC)ta;
+                    cc = (TC)tc;
+                    b = (TC)(-(ta + tc) - lam);
+                    if (args.gpin != 0 && kg == 0 && (sys >> 1) == 0) {
+                        a = 0;
+                        b = 1;
+                        cc = 0;
+                        d = 0;
+                    }
                 } else {
                     a = (TC)a2[r];
                     b = (TC)b2[r];
                     cc = (TC)c2[r];
                 }
-                const TC d = (TC)d2[r];
                 if (k == 0) {
                     const TC ib = rcp_tc(b);
                     ab0 = a * ib;

@@ -243,6 +243,28 @@ int btdma_heat_step(btdma_heat_t h, double* theta, int n_steps, int use_graph,
                     cudaStream_t stream);
 int btdma_heat_l2_error(btdma_heat_t h, const double* theta, double t_phys, double* l2);
 
+/* Wall-normal solve of the channel flow's FFT Poisson equation: for every
+ * Fourier mode m (n_modes of them) and row k = 0..nz-1,
+ *     a_k p_{k-1} - (a_k + c_k + lambda_m) p_k + c_k p_{k+1} = rhs_k,
+ *     a_k = 1 / (dz[k+1] dmz[k+1]) (0 for k = 0),
+ *     c_k = 1 / (dz[k+1] dmz[k+2]) (0 for k = nz - 1),
+ * solved for the real and imaginary parts of the complex right-hand side with
+ * one set of coefficients (replaces k_build_poisson_tdma + two TDMA solves of
+ * PressureSolverGPU::solve_tdma_z_, PressureSolverGPU.cu:183-220 and
+ * :514-537, which store every coefficient twice).  With pin_mode0, row 0 of
+ * mode 0 becomes p_0 = 0 (k_zero_mode).  dz and dmz (nz + 2 entries, ghosts
+ * included) and lambda (n_modes, kx^2 + ky^2 of each mode) are HOST arrays read
+ * at create time.  rhs is the device complex array [nz][n_modes] as
+ * interleaved (real, imaginary) doubles (the reference's hat_Y layout with
+ * mode = j * nxh + i), overwritten with the solution.  nz must be a multiple
+ * of 16; coefficients are generated inside the solve, never stored. */
+typedef struct btdma_poisson* btdma_poisson_t;
+int btdma_poisson_create(int nz, const double* dz, const double* dmz, int n_modes,
+                         const double* lambda, int pin_mode0, btdma_poisson_t* out);
+int btdma_poisson_destroy(btdma_poisson_t h);
+int btdma_poisson_solve(btdma_poisson_t h, double* rhs, cudaStream_t stream);
+int btdma_poisson_status(btdma_poisson_t h, unsigned* status, cudaStream_t stream);
+
 /* Switch the method of an existing handle (rho, eps and J state are kept).  The
  * reference's FilteredTDMACUDA object offers v1 and v2 side by side
  * (filtered_tdma_cuda.hpp:173-180); this lets one handle do the same. */
