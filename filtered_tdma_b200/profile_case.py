@@ -28,7 +28,15 @@ def main():
     ap.add_argument("--cyclic", action="store_true")
     ap.add_argument("--storage", choices=["f64", "f32"], default="f64",
                     help="f32: A, B, C, D stored in FP32 (FP32_STORE handle)")
+    ap.add_argument("--case", choices=["batch", "ragged", "heat", "poisson"], default="batch",
+                    help="batch: uniform [n_row x n_sys] solve; ragged: 10000 CSR systems "
+                         "(n log-uniform 16..4096, autotuned); heat: fused ADI steps on "
+                         "--heat-grid; poisson: channel wall-normal solve 128 x 65 x 192")
+    ap.add_argument("--heat-grid", default="256,384,512")
+    ap.add_argument("--no-tune", action="store_true", help="ragged: keep the default plan")
     args = ap.parse_args()
+    if args.case != "batch":
+        return other_case(args)
 
     import torch
 
@@ -63,6 +71,54 @@ def main():
               f"{bpr * rows / ms / 1e6:.1f} GB/s ({bpr} B/row)")
     if s.status() != 0:
         raise SystemExit("device status word set")
+
+
+def other_case(args):
+    import numpy as np
+    import torch
+
+    from filtered_tdma_b200 import Solver
+    from filtered_tdma_b200 import _lib as L
+    from filtered_tdma_b200 import workloads as W
+
+    dev = torch.device("cuda:0")
+
+    def timed(fn, reps):
+        out = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            out.append(e0.elapsed_time(e1))
+        return out
+
+    if args.case == "ragged":
+        f32 = args.storage == "f32"
+        A, B, C, D, off, per = W.ragged_batch(10000, seed=5,
+                                              dtype=np.float32 if f32 else np.float64)
+        dA, dB, dC, dD = [torch.from_numpy(v).to(dev) for v in (A, B, C, D)]
+        X = torch.empty(int(off[-1]), dtype=torch.float64, device=dev)
+        s = Solver("pascal", 10000, 64, 2, precision=L.FP32_STORE if f32 else L.FP64)
+        if not args.no_tune:
+            s.ragged_autotune(dA, dB, dC, dD, X, off, per)
+        ms = timed(lambda: s.solve_ragged(dA, dB, dC, dD, X, off, per), args.reps)
+        print("ragged", ["%.4f ms" % t for t in ms], int(off[-1]), "rows")
+    elif args.case == "heat":
+        from filtered_tdma_b200.heat import HeatADI, dt_from_rho
+        ix, iy, iz = (int(v) for v in args.heat_grid.split(","))
+        h = HeatADI(ix, iy, iz, dt=dt_from_rho(1.0 / 3.0, iz, option="strong"))
+        th = h.field(dev)
+        ms = timed(lambda: h.step(th, 1), args.reps)
+        print("heat step", ["%.4f ms" % t for t in ms], ix * iy * iz, "cells")
+    else:
+        from filtered_tdma_b200.poisson import ChannelPoisson
+        cp = ChannelPoisson(128, 128, 192, gamma=2.0)
+        hat = torch.complex(torch.rand((192, cp.n_modes), dtype=torch.float64, device=dev),
+                            torch.rand((192, cp.n_modes), dtype=torch.float64, device=dev))
+        ms = timed(lambda: cp.solve(hat), args.reps)
+        print("poisson", ["%.4f ms" % t for t in ms], cp.n_modes, "modes")
 
 
 if __name__ == "__main__":
