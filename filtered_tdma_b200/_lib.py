@@ -27,7 +27,7 @@ EXPORTS = (
     "btdma_solve_noalloc", "btdma_solve_f32", "btdma_set_refine", "btdma_last_stats",
     "btdma_solve_ragged", "btdma_solve_ragged_f32", "btdma_ragged_autotune",
     "btdma_ragged_plan_info", "btdma_heat_create", "btdma_heat_destroy", "btdma_heat_init",
-    "btdma_heat_step", "btdma_heat_l2_error", "btdma_poisson_create", "btdma_poisson_destroy",
+    "btdma_heat_step", "btdma_heat_l2_error", "btdma_heat_step_profile", "btdma_poisson_create", "btdma_poisson_destroy",
     "btdma_poisson_solve", "btdma_poisson_status",
 )
 NOALLOC_MAX_ELEMS = 1 << 20
@@ -100,6 +100,7 @@ def lib():
         L.btdma_heat_init.argtypes = [vp, vp, vp]
         L.btdma_heat_step.argtypes = [vp, vp, i, i, vp]
         L.btdma_heat_l2_error.argtypes = [vp, vp, d, ctypes.POINTER(d)]
+        L.btdma_heat_step_profile.argtypes = [vp, vp, ctypes.POINTER(d), vp]
         L.btdma_poisson_create.argtypes = [i, vp, vp, i, vp, i, ctypes.POINTER(vp)]
         L.btdma_poisson_destroy.argtypes = [vp]
         L.btdma_poisson_solve.argtypes = [vp, vp, vp]

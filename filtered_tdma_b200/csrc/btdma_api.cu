@@ -1326,6 +1326,55 @@ int btdma_heat_step(btdma_heat_t h, double* theta, int n_steps, int use_graph,
     return BTDMA_OK;
 }
 
+int btdma_heat_step_profile(btdma_heat_t h, double* theta, double* times, cudaStream_t stream) {
+    if (!h || !theta || !times) return fail(BTDMA_ERR_ARG, "null argument");
+    const HeatGeom& g = h->g;
+    cudaEvent_t ev[8];
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    auto done = [&](int code) {
+        for (auto& e : ev) cudaEventDestroy(e);
+        return code;
+    };
+    const dim3 b1(128, 1, 1);
+    const dim3 gr((g.ix + 127) / 128, g.iy, g.iz);
+    const dim3 bt(HEAT_TILE, 8, 1);
+    int rc = BTDMA_OK;
+    cudaEventRecord(ev[0], stream);
+    heat_rhs_z_kernel<<<gr, b1, 0, stream>>>(theta, h->buf0, g);
+    cudaEventRecord(ev[1], stream);
+    if ((rc = try_tile_const(h->buf0, h->buf0, g.ix * g.iy, g.iz, g.bz, true, h->status, stream)) != 1)
+        return done(rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "Z sweep not tileable"));
+    cudaEventRecord(ev[2], stream);
+    heat_z_to_y_kernel<<<gr, b1, 0, stream>>>(theta, h->buf0, h->buf1, g);
+    cudaEventRecord(ev[3], stream);
+    if ((rc = try_tile_const(h->buf1, h->buf1, g.ix * g.iz, g.iy, g.by, true, h->status, stream)) != 1)
+        return done(rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "Y sweep not tileable"));
+    cudaEventRecord(ev[4], stream);
+    heat_y_to_x_kernel<<<dim3((g.ix + HEAT_TILE - 1) / HEAT_TILE, (g.iy + HEAT_TILE - 1) / HEAT_TILE,
+                              g.iz), bt, 0, stream>>>(theta, h->buf1, h->buf0, g);
+    cudaEventRecord(ev[5], stream);
+    if ((rc = try_tile_const(h->buf0, h->buf0, g.iy * g.iz, g.ix, g.bx, true, h->status, stream)) != 1)
+        return done(rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "X sweep not tileable"));
+    cudaEventRecord(ev[6], stream);
+    heat_update_kernel<<<dim3((g.iy + HEAT_TILE - 1) / HEAT_TILE, (g.ix + HEAT_TILE - 1) / HEAT_TILE,
+                              g.iz), bt, 0, stream>>>(theta, h->buf0, g);
+    cudaEventRecord(ev[7], stream);
+    if (cudaGetLastError() != cudaSuccess || cudaEventSynchronize(ev[7]) != cudaSuccess)
+        return done(fail(BTDMA_ERR_CUDA, "profiled heat step failed"));
+    auto sec = [&](int a, int b) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[a], ev[b]);
+        return 1e-3 * ms;
+    };
+    // the reference's 12 events (solve_theta.cu:436-439): rhs, solve_z, solve_y,
+    // solve_x, etc, comm, tdma_{z,y,x}_comm, tdma_{z,y,x}_gpu
+    const double t[12] = {sec(0, 1), sec(1, 3), sec(3, 5), sec(5, 7), 0.0, 0.0,
+                          0.0,       0.0,       0.0,       sec(1, 2), sec(3, 4), sec(5, 6)};
+    std::memcpy(times, t, sizeof t);
+    h->last_stream = stream;
+    return done(BTDMA_OK);
+}
+
 int btdma_heat_l2_error(btdma_heat_t h, const double* theta, double t_phys, double* l2) {
     if (!h || !theta || !l2) return fail(BTDMA_ERR_ARG, "null argument");
     const HeatGeom& g = h->g;

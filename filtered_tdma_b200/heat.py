@@ -68,6 +68,12 @@ class HeatADI:
         L.check(L.lib().btdma_heat_step(self._h, theta.data_ptr(), int(n_steps), int(graph),
                                         stream))
 
+    def step_profile(self, theta, stream=0):
+        """One step timed phase by phase: the reference's 12 timing events (seconds)."""
+        t = (ctypes.c_double * 12)()
+        L.check(L.lib().btdma_heat_step_profile(self._h, theta.data_ptr(), t, stream))
+        return list(t)
+
     def l2_error(self, theta, t_phys):
         out = ctypes.c_double()
         L.check(L.lib().btdma_heat_l2_error(self._h, theta.data_ptr(), float(t_phys),

@@ -242,6 +242,14 @@ int btdma_heat_init(btdma_heat_t h, double* theta, cudaStream_t stream);
 int btdma_heat_step(btdma_heat_t h, double* theta, int n_steps, int use_graph,
                     cudaStream_t stream);
 int btdma_heat_l2_error(btdma_heat_t h, const double* theta, double t_phys, double* l2);
+/* One step launched phase by phase with CUDA events between the phases
+ * (blocking); writes the 12 per-step times in seconds of the reference's timing
+ * events, in its order (solve_theta.cu:436-439): rhs, solve_z, solve_y,
+ * solve_x, etc, comm, tdma_z_comm, tdma_y_comm, tdma_x_comm, tdma_z_gpu,
+ * tdma_y_gpu, tdma_x_gpu.  solve_d spans a sweep's solve and the re-layout that
+ * follows it; etc, comm and the *_comm events are 0 (one GPU, ghosts computed
+ * in the right-hand-side kernel). */
+int btdma_heat_step_profile(btdma_heat_t h, double* theta, double* times, cudaStream_t stream);
 
 /* Wall-normal solve of the channel flow's FFT Poisson equation: for every
  * Fourier mode m (n_modes of them) and row k = 0..nz-1,

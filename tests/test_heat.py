@@ -66,3 +66,29 @@ def test_heat_argument_checks():
     assert L.lib().btdma_heat_create(30, 32, 32, 1e-3, ctypes.byref(h)) == L.ERR_UNSUPPORTED
     assert L.lib().btdma_heat_create(32, 32, 32, -1.0, ctypes.byref(h)) == L.ERR_ARG
     assert L.lib().btdma_heat_step(None, None, 1, 1, None) == L.ERR_ARG
+
+
+def test_timing_csv_format(tmp_path):
+    from filtered_tdma_b200 import timing_csv as T
+    p = str(tmp_path / "timing_513_111_pascal.csv")
+    rows = [[1e-4 * (e + 1) + s for e in range(12)] for s in range(3)]
+    T.write_csv(p, rows, T.meta_line(513, 513, 513, 1.25e-5, 13))
+    lines = open(p).read().splitlines()
+    assert lines[0] == "# grid=513x513x513, np=1 (1,1,1), dt= 1.250E-05, Nt=13, solver_kind=pascal"
+    assert lines[1] == "rank,t_step,event,time_sec"
+    assert lines[2] == "0,1,rhs, 1.000000000E-04"  # %16.9E, as timing_csv.hpp writes
+    assert len(lines) == 2 + 3 * 12
+    meta, vals = T.read_csv(p)
+    assert vals[(0, 3, "tdma_x_gpu")] == rows[2][11]
+
+
+@pytest.mark.gpu
+def test_timing_csv_from_profiled_steps(cuda, tmp_path):
+    from filtered_tdma_b200 import timing_csv as T
+    p = T.profile_run(64, 48, 32, steps=3, warmup=1, path=str(tmp_path / "t.csv"))
+    meta, vals = T.read_csv(p)
+    assert meta.startswith("grid=65x49x33, np=1 (1,1,1)")
+    assert len(vals) == 3 * 12
+    for t in (1, 2, 3):
+        assert vals[(0, t, "solve_z")] >= vals[(0, t, "tdma_z_gpu")] > 0
+        assert vals[(0, t, "comm")] == 0.0
