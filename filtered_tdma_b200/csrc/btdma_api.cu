@@ -6,6 +6,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -1153,6 +1154,9 @@ struct btdma_heat {
     double* xc = nullptr;  // device coordinates (ghosts included)
     double* yc = nullptr;
     double* zc = nullptr;
+    double* cosx = nullptr;  // cos(pi x) etc. at the cell centres
+    double* cosy = nullptr;
+    double* cosz = nullptr;
     double* buf0 = nullptr;  // Z and X sweep layouts
     double* buf1 = nullptr;  // Y sweep layout
     double* err = nullptr;   // L2 accumulator
@@ -1224,12 +1228,24 @@ int btdma_heat_create(int ix, int iy, int iz, double dt, btdma_heat_t* out) {
         return c;
     };
     const auto hx = coords(ix), hy = coords(iy), hz = coords(iz);
-    CKH(cudaMalloc(&h->xc, sizeof(double) * hx.size()));
-    CKH(cudaMalloc(&h->yc, sizeof(double) * hy.size()));
-    CKH(cudaMalloc(&h->zc, sizeof(double) * hz.size()));
-    CKH(cudaMemcpy(h->xc, hx.data(), sizeof(double) * hx.size(), cudaMemcpyHostToDevice));
-    CKH(cudaMemcpy(h->yc, hy.data(), sizeof(double) * hy.size(), cudaMemcpyHostToDevice));
-    CKH(cudaMemcpy(h->zc, hz.data(), sizeof(double) * hz.size(), cudaMemcpyHostToDevice));
+    auto cosines = [](const std::vector<double>& c) {
+        std::vector<double> o(c.size());
+        for (size_t i = 0; i < c.size(); ++i) o[i] = std::cos(HEAT_PI * c[i]);
+        return o;
+    };
+    const auto kx = cosines(hx), ky = cosines(hy), kz = cosines(hz);
+    auto upload = [&](double** dst, const std::vector<double>& v) {
+        cudaError_t e = cudaMalloc(dst, sizeof(double) * v.size());
+        if (e == cudaSuccess)
+            e = cudaMemcpy(*dst, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice);
+        return e;
+    };
+    CKH(upload(&h->xc, hx));
+    CKH(upload(&h->yc, hy));
+    CKH(upload(&h->zc, hz));
+    CKH(upload(&h->cosx, kx));
+    CKH(upload(&h->cosy, ky));
+    CKH(upload(&h->cosz, kz));
     const size_t inner = (size_t)ix * iy * iz;
     CKH(cudaMalloc(&h->buf0, sizeof(double) * inner));
     CKH(cudaMalloc(&h->buf1, sizeof(double) * inner));
@@ -1251,6 +1267,9 @@ int btdma_heat_create(int ix, int iy, int iz, double dt, btdma_heat_t* out) {
     g.xc = h->xc;
     g.yc = h->yc;
     g.zc = h->zc;
+    g.cx = h->cosx;
+    g.cy = h->cosy;
+    g.cz = h->cosz;
     *out = h;
     return BTDMA_OK;
 }
@@ -1263,6 +1282,9 @@ int btdma_heat_destroy(btdma_heat_t h) {
     cudaFree(h->xc);
     cudaFree(h->yc);
     cudaFree(h->zc);
+    cudaFree(h->cosx);
+    cudaFree(h->cosy);
+    cudaFree(h->cosz);
     cudaFree(h->buf0);
     cudaFree(h->buf1);
     cudaFree(h->err);

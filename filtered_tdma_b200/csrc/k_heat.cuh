@@ -33,6 +33,9 @@ struct HeatGeom {
     const double* xc;      // cell centres incl. ghosts [ix + 2]
     const double* yc;      // [iy + 2]
     const double* zc;      // [iz + 2]
+    const double* cx;      // cos(pi xc) [ix + 2] (host-computed once)
+    const double* cy;      // cos(pi yc) [iy + 2]
+    const double* cz;      // cos(pi zc) [iz + 2]
 };
 
 __device__ __forceinline__ size_t heat_full(const HeatGeom& g, int i, int j, int k) {
@@ -53,23 +56,22 @@ __global__ void __launch_bounds__(256) heat_rhs_z_kernel(const double* __restric
     if (ii >= g.ix) return;
     const int i = ii + 1, j = jj + 1, k = kk + 1;
     const double t = theta[heat_full(g, i, j, k)];
-    const double cxk = cos(HEAT_PI * g.zc[k]);
+    const double cxi = g.cx[i], cyj = g.cy[j], czk = g.cz[k];
     double tip, tim, tjp, tjm, tkp, tkm;
     {
-        const double ubc = -cos(HEAT_PI * g.yc[j]) * cxk;  // x walls
+        const double ubc = -cyj * czk;  // x walls
         tip = ii + 1 < g.ix ? theta[heat_full(g, i + 1, j, k)] : 2.0 * ubc - t;
         tim = ii > 0 ? theta[heat_full(g, i - 1, j, k)] : 2.0 * ubc - t;
     }
     {
-        const double ubc = -cos(HEAT_PI * g.xc[i]) * cxk;  // y walls
+        const double ubc = -cxi * czk;  // y walls
         tjp = jj + 1 < g.iy ? theta[heat_full(g, i, j + 1, k)] : 2.0 * ubc - t;
         tjm = jj > 0 ? theta[heat_full(g, i, j - 1, k)] : 2.0 * ubc - t;
     }
-    const double ubz = -cos(HEAT_PI * g.xc[i]) * cos(HEAT_PI * g.yc[j]);  // z walls
+    const double ubz = -cxi * cyj;  // z walls
     tkp = kk + 1 < g.iz ? theta[heat_full(g, i, j, k + 1)] : 2.0 * ubz - t;
     tkm = kk > 0 ? theta[heat_full(g, i, j, k - 1)] : 2.0 * ubz - t;
-    const double src = g.dt * 3.0 * HEAT_PI * HEAT_PI * cos(HEAT_PI * g.xc[i]) *
-                       cos(HEAT_PI * g.yc[j]) * cxk;
+    const double src = g.dt * 3.0 * HEAT_PI * HEAT_PI * cxi * cyj * czk;
     double rhs = (g.bx * tip + g.bx * tim) + (g.by * tjp + g.by * tjm) +
                  (g.bz * tkp + g.bz * tkm) +
                  (1.0 + (-2.0 * g.bx) + (-2.0 * g.by) + (-2.0 * g.bz)) * t + src;
@@ -93,7 +95,7 @@ __global__ void __launch_bounds__(256) heat_z_to_y_kernel(const double* __restri
     if (jj == 0 || jj == g.iy - 1) {
         const int i = ii + 1, k = kk + 1, j = jj == 0 ? 1 : g.iy;
         const double t = theta[heat_full(g, i, j, k)];
-        const double ubc = -cos(HEAT_PI * g.xc[i]) * cos(HEAT_PI * g.zc[k]);
+        const double ubc = -g.cx[i] * g.cz[k];
         if (jj == 0) v += g.by * ((2.0 * ubc - t) + t);
         if (jj == g.iy - 1) v += g.by * ((2.0 * ubc - t) + t);
     }
@@ -123,7 +125,7 @@ __global__ void __launch_bounds__(256) heat_y_to_x_kernel(const double* __restri
             if (ii == 0 || ii == g.ix - 1) {
                 const int j = jj + 1, k = kk + 1, i = ii == 0 ? 1 : g.ix;
                 const double t = theta[heat_full(g, i, j, k)];
-                const double ubc = -cos(HEAT_PI * g.yc[j]) * cos(HEAT_PI * g.zc[k]);
+                const double ubc = -g.cy[j] * g.cz[k];
                 if (ii == 0) v += g.bx * ((2.0 * ubc - t) + t);
                 if (ii == g.ix - 1) v += g.bx * ((2.0 * ubc - t) + t);
             }
