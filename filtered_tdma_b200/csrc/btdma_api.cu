@@ -975,14 +975,16 @@ int rag_launch(btdma_t h, int cta, int P, int mcap, const int4* tasks, int n_tas
     a.mcap = mcap;
     a.status = h->status;
     if (cta) {
-        auto kern = ragged_cta_kernel<TIN>;
-        static bool attr_done = false;
-        if (!attr_done) {
+        // staged through shared memory where the whole system fits
+        const bool staged = rag_cta_smem_bytes(P, true) <= (size_t)max_smem_optin();
+        auto kern = staged ? ragged_cta_kernel<TIN, true> : ragged_cta_kernel<TIN, false>;
+        static bool attr_done[2] = {false, false};
+        if (!attr_done[staged]) {
             CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     max_smem_optin()));
-            attr_done = true;
+            attr_done[staged] = true;
         }
-        kern<<<n_tasks, P, rag_cta_smem_bytes(P), st>>>(a);
+        kern<<<n_tasks, P, rag_cta_smem_bytes(P, staged), st>>>(a);
     } else {
         auto kern = ragged_kernel<TIN>;
         static bool attr_done = false;
@@ -1205,6 +1207,9 @@ int btdma_heat_create(int ix, int iy, int iz, double dt, btdma_heat_t* out) {
         return fail(BTDMA_ERR_ARG, "grid sizes and dt must be positive");
     if (ix % 16 || iy % 16 || iz % 16)
         return fail(BTDMA_ERR_UNSUPPORTED, "the fused step needs ix, iy, iz multiples of 16");
+    if ((long long)(ix + 2) * (iy + 2) >= (1LL << 31) || (long long)ix * iy >= (1LL << 31) ||
+        (long long)ix * iz >= (1LL << 31) || (long long)iy * iz >= (1LL << 31))
+        return fail(BTDMA_ERR_SIZE, "grid planes above 2^31 cells");
     if (!tile_plan(iz, false, 8, 1).sys || !tile_plan(iy, false, 8, 1).sys ||
         !tile_plan(ix, false, 8, 1).sys)
         return fail(BTDMA_ERR_UNSUPPORTED, "grid not supported by the tiled solve");

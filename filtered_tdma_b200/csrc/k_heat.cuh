@@ -55,22 +55,25 @@ __global__ void __launch_bounds__(256) heat_rhs_z_kernel(const double* __restric
     const int kk = blockIdx.z;
     if (ii >= g.ix) return;
     const int i = ii + 1, j = jj + 1, k = kk + 1;
-    const double t = theta[heat_full(g, i, j, k)];
+    const int sy = g.ix + 2;               // j stride of the full grid
+    const int sz = (g.iy + 2) * (g.ix + 2);  // k stride (< 2^31 for grids this library takes)
+    const double* c0 = theta + heat_full(g, i, j, k);
+    const double t = c0[0];
     const double cxi = g.cx[i], cyj = g.cy[j], czk = g.cz[k];
     double tip, tim, tjp, tjm, tkp, tkm;
     {
         const double ubc = -cyj * czk;  // x walls
-        tip = ii + 1 < g.ix ? theta[heat_full(g, i + 1, j, k)] : 2.0 * ubc - t;
-        tim = ii > 0 ? theta[heat_full(g, i - 1, j, k)] : 2.0 * ubc - t;
+        tip = ii + 1 < g.ix ? c0[1] : 2.0 * ubc - t;
+        tim = ii > 0 ? c0[-1] : 2.0 * ubc - t;
     }
     {
         const double ubc = -cxi * czk;  // y walls
-        tjp = jj + 1 < g.iy ? theta[heat_full(g, i, j + 1, k)] : 2.0 * ubc - t;
-        tjm = jj > 0 ? theta[heat_full(g, i, j - 1, k)] : 2.0 * ubc - t;
+        tjp = jj + 1 < g.iy ? c0[sy] : 2.0 * ubc - t;
+        tjm = jj > 0 ? c0[-sy] : 2.0 * ubc - t;
     }
     const double ubz = -cxi * cyj;  // z walls
-    tkp = kk + 1 < g.iz ? theta[heat_full(g, i, j, k + 1)] : 2.0 * ubz - t;
-    tkm = kk > 0 ? theta[heat_full(g, i, j, k - 1)] : 2.0 * ubz - t;
+    tkp = kk + 1 < g.iz ? c0[sz] : 2.0 * ubz - t;
+    tkm = kk > 0 ? c0[-sz] : 2.0 * ubz - t;
     const double src = g.dt * 3.0 * HEAT_PI * HEAT_PI * cxi * cyj * czk;
     double rhs = (g.bx * tip + g.bx * tim) + (g.by * tjp + g.by * tjm) +
                  (g.bz * tkp + g.bz * tkm) +

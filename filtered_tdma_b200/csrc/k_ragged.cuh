@@ -178,11 +178,37 @@ __global__ void __launch_bounds__(256) ragged_kernel(const RagArgs a) {
 // per level (the same steps as reduced_solve_shfl).
 constexpr int RAG_MT = 16;
 
-__host__ __device__ __forceinline__ size_t rag_cta_smem_bytes(int P) {
-    return (2ull * 3 * (P + 2) + 3ull * RAG_MT * P) * sizeof(double);
+// STAGED: the whole system is first copied into shared memory with coalesced
+// loads, laid out [array][row of segment][thread] (A, B, C, D widened to
+// FP64), the elimination state then overwrites A, C, D in place and x goes
+// through B on its way out (coalesced stores).  Without staging each thread
+// reads its contiguous rows straight from global memory, which leaves L1 to
+// hold four lines per thread.
+__host__ __device__ __forceinline__ size_t rag_cta_smem_bytes(int P, bool staged) {
+    return (2ull * 3 * (P + 2) + (staged ? 4ull : 3ull) * RAG_MT * P) * sizeof(double);
 }
 
-template <typename TIN>
+// (segment, row in segment) of row r of a system split by para_range into P
+// parts of base or base + 1 rows (the first rem parts longer).
+__device__ __forceinline__ void rag_locate(int r, int base, int rem, float inv0, float inv1,
+                                           int& q, int& k) {
+    const int split = rem * (base + 1);
+    if (r < split) {
+        q = (int)((float)r * inv1);
+        if (q * (base + 1) > r) --q;
+        else if ((q + 1) * (base + 1) <= r) ++q;
+        k = r - q * (base + 1);
+    } else {
+        const int r2 = r - split;
+        q = (int)((float)r2 * inv0);
+        if (q * base > r2) --q;
+        else if ((q + 1) * base <= r2) ++q;
+        k = r2 - q * base;
+        q += rem;
+    }
+}
+
+template <typename TIN, bool STAGED>
 __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
     extern __shared__ double rsm[];
     constexpr int M = RAG_MT;
@@ -208,10 +234,29 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
     const TIN* __restrict__ pC = static_cast<const TIN*>(a.C) + row0;
     const TIN* __restrict__ pD = static_cast<const TIN*>(a.D) + row0;
 
-    double* stt = rsm + 2 * 3 * gs + p;  // field f, row k: stt[(f * M + k) * P]
+    double* const stg = rsm + 2 * 3 * gs;  // [field][row][thread] area
+    double* stt = stg + p;                  // this thread's column: stt[(f * M + k) * P]
+    const float inv0 = 1.0f / (float)(base > 0 ? base : 1), inv1 = 1.0f / (float)(base + 1);
+    if constexpr (STAGED) {
+        // fields 0..3 = A, B, C, D; coalesced over the system's rows
+        const TIN* __restrict__ gA = static_cast<const TIN*>(a.A) + o;
+        const TIN* __restrict__ gB = static_cast<const TIN*>(a.B) + o;
+        const TIN* __restrict__ gC = static_cast<const TIN*>(a.C) + o;
+        const TIN* __restrict__ gD = static_cast<const TIN*>(a.D) + o;
+        for (int r = p; r < n; r += P) {
+            int q, k;
+            rag_locate(r, base, rem, inv0, inv1, q, k);
+            stg[(0 * M + k) * P + q] = (double)gA[r];
+            stg[(1 * M + k) * P + q] = (double)gB[r];
+            stg[(2 * M + k) * P + q] = (double)gC[r];
+            stg[(3 * M + k) * P + q] = (double)gD[r];
+        }
+        __syncthreads();
+    }
+    // state: alpha, gamma, delta (in place of A, C, D when staged)
     auto AL = [&](int k) -> double& { return stt[(0 * M + k) * P]; };
-    auto GA = [&](int k) -> double& { return stt[(1 * M + k) * P]; };
-    auto DE = [&](int k) -> double& { return stt[(2 * M + k) * P]; };
+    auto GA = [&](int k) -> double& { return stt[((STAGED ? 2 : 1) * M + k) * P]; };
+    auto DE = [&](int k) -> double& { return stt[((STAGED ? 3 : 2) * M + k) * P]; };
     double ab0 = 0, cb0 = 0, db0 = 0, pi = 1.0, sa = 0.0, sd = 0.0, pi_last = 0.0;
     double alp = 0, gap = 0, dep = 0;  // row k-1
 #pragma unroll
@@ -220,10 +265,17 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
 #pragma unroll
         for (int j = 0; j < RAG_LOOKAHEAD; ++j) {  // loads of the next rows (clamped in bounds)
             const int kk = k0 + j < m ? k0 + j : m - 1;
-            ra[j] = (double)__ldg(pA + kk);
-            rb[j] = (double)__ldg(pB + kk);
-            rc[j] = (double)__ldg(pC + kk);
-            rd[j] = (double)__ldg(pD + kk);
+            if constexpr (STAGED) {
+                ra[j] = stt[(0 * M + kk) * P];
+                rb[j] = stt[(1 * M + kk) * P];
+                rc[j] = stt[(2 * M + kk) * P];
+                rd[j] = stt[(3 * M + kk) * P];
+            } else {
+                ra[j] = (double)__ldg(pA + kk);
+                rb[j] = (double)__ldg(pB + kk);
+                rc[j] = (double)__ldg(pC + kk);
+                rd[j] = (double)__ldg(pD + kk);
+            }
         }
 #pragma unroll
         for (int j = 0; j < RAG_LOOKAHEAD; ++j) {
@@ -324,16 +376,33 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
     double* xp = a.X + row0;
     double nonfinite = fma(xf, 0.0, fma(xl, 0.0, 0.0));
     double xn = xl;
+    // staged: x goes into the B field (no longer read) and leaves coalesced
+    auto XO = [&](int k) -> double& { return stt[(1 * M + k) * P]; };
 #pragma unroll
     for (int k = M - 2; k >= 1; --k) {
         if (k <= m - 2) {
             xn = DE(k) - AL(k) * xf - GA(k) * xn;
             nonfinite = fma(xn, 0.0, nonfinite);
-            xp[k] = xn;
+            if constexpr (STAGED)
+                XO(k) = xn;
+            else
+                xp[k] = xn;
         }
     }
-    xp[0] = xf;
-    xp[m - 1] = xl;
+    if constexpr (STAGED) {
+        XO(0) = xf;
+        XO(m - 1) = xl;
+        __syncthreads();
+        double* gX = a.X + o;
+        for (int r = p; r < n; r += P) {
+            int q, k;
+            rag_locate(r, base, rem, inv0, inv1, q, k);
+            gX[r] = stg[(1 * M + k) * P + q];
+        }
+    } else {
+        xp[0] = xf;
+        xp[m - 1] = xl;
+    }
     if (nonfinite != 0.0) raise_status(a.status, ST_NONFINITE);  // NaN != 0
 }
 
