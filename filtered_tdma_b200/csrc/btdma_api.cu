@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -48,6 +49,7 @@ struct btdma_handle {
     struct RagBucket {
         int cyc, first, count, nmin, nmax;
         int cta;    // 1: one CTA of P threads per system, 0: P lanes of a warp per system
+        int staged; // CTA kind: system staged through shared memory (autotuner's choice)
         int P, warps, mcap;
         float best_ms;
     };
@@ -61,7 +63,7 @@ struct btdma_handle {
     int4* rag_d_probe = nullptr;           // task table of one bucket being tuned [n_sys]
     // launches of a solve: warp-kind tasks (one launch), CTA-kind tasks per P
     struct RagLaunch {
-        int cta, P, first, count, mcap;
+        int cta, P, first, count, mcap, staged;
     };
     std::vector<RagLaunch> rag_launches;
     static constexpr int RAG_STREAMS = 4;
@@ -206,7 +208,25 @@ int num_sms() {
 // Shape plan of the tiled kernel: systems per group, CTAs per cluster, ring stages.
 struct TilePlan {
     int sys = 0, cl = 0, nst = 0, nseg = 0;
+    int pair = 1;  // CTAs whose loads are issued together (cl == 1 only)
 };
+
+// Paired loads (opt-in): enough neighbouring CTAs that their row pieces add up
+// to 256 bytes, at most BTDMA_TILE_PAIR (environment, default 1 = off).  On
+// B200 the DRAM streams two 128-byte pieces requested together nearly as fast
+// as one 256-byte piece, but coupling every ring-slot refill to the slowest
+// warp of 2-4 SMs cost more than that gained (262144 x 512: FP64 1.12 ms
+// unpaired, 2.08 ms paired by 2), so pairing stays off unless asked for.
+int tile_pair(int sys, int elem) {
+    static int cap = -1;
+    if (cap < 0) {
+        const char* e = getenv("BTDMA_TILE_PAIR");
+        cap = e ? std::max(1, std::min(4, atoi(e))) : 1;
+    }
+    int pr = 1;
+    while (pr < cap && pr * sys * elem < 256) pr <<= 1;
+    return pr;
+}
 
 // na: arrays per ring stage (4, or 1 for the constant-coefficient D-only ring).
 TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4) {
@@ -245,6 +265,7 @@ TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4) {
     pl.cl = cl;
     pl.nst = nst;
     pl.nseg = nseg;
+    pl.pair = cl == 1 ? tile_pair(sys, elem) : 1;
     return pl;
 }
 
@@ -266,21 +287,23 @@ int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st)
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = a.cl;
+    const int pr = a.cl == 1 && a.pair > 1 ? a.pair : 1;
+    const int cdim = a.cl * pr;  // CTAs per cluster: split system (cl) or paired loads (pr)
+    attr[0].val.clusterDim.x = cdim;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int clusters = num_sms();
-    if (a.cl > 1) {
-        cfg.gridDim = dim3(a.cl * num_sms(), 1, 1);
+    if (cdim > 1) {
+        cfg.gridDim = dim3(cdim * num_sms(), 1, 1);
         int nc = 0;
         CK(cudaOccupancyMaxActiveClusters(&nc, kern, &cfg));
-        if (nc <= 0) return fail(BTDMA_ERR_UNSUPPORTED, "no cluster of %d CTAs fits", a.cl);
+        if (nc <= 0) return fail(BTDMA_ERR_UNSUPPORTED, "no cluster of %d CTAs fits", cdim);
         clusters = nc;
     }
-    clusters = std::min(clusters, a.n_groups);
-    cfg.gridDim = dim3(clusters * a.cl, 1, 1);
+    clusters = std::min(clusters, (a.n_groups + pr - 1) / pr);
+    cfg.gridDim = dim3(clusters * cdim, 1, 1);
     TileArgs aa = a;
     CK(cudaLaunchKernelEx(&cfg, kern, maps[0], maps[1], maps[2], maps[3], aa));
     return BTDMA_OK;
@@ -334,6 +357,7 @@ int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, 
     a.cl = pl.cl;
     a.nst = pl.nst;
     a.n_groups = (n_sys + pl.sys - 1) / pl.sys;
+    a.pair = pl.pair;
     a.accumulate = accumulate ? 1 : 0;
     a.gate = gate;
     a.status = status;
@@ -361,6 +385,7 @@ int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArg
     a.cl = pl.cl;
     a.nst = pl.nst;
     a.n_groups = (n_sys + pl.sys - 1) / pl.sys;
+    a.pair = pl.pair;
     a.accumulate = 0;
     a.gate = nullptr;
     a.status = status;
@@ -846,7 +871,7 @@ void rag_bucket_tasks(const btdma_handle::RagBucket& b, int cta, int P, std::vec
 int rag_build_launches(btdma_t h) {
     std::vector<int4> tasks;
     h->rag_launches.clear();
-    btdma_handle::RagLaunch wl{0, 0, 0, 0, 1};
+    btdma_handle::RagLaunch wl{0, 0, 0, 0, 1, 0};
     for (int i = (int)h->rag_buckets.size() - 1; i >= 0; --i) {
         const auto& b = h->rag_buckets[i];
         if (b.cta) continue;
@@ -855,13 +880,14 @@ int rag_build_launches(btdma_t h) {
     }
     wl.count = (int)tasks.size();
     if (wl.count) h->rag_launches.push_back(wl);
-    for (int P = 512; P >= 64; P >>= 1) {
-        btdma_handle::RagLaunch cl{1, P, (int)tasks.size(), 0, 0};
-        for (const auto& b : h->rag_buckets)
-            if (b.cta && b.P == P) rag_bucket_tasks(b, 1, P, tasks);
-        cl.count = (int)tasks.size() - cl.first;
-        if (cl.count) h->rag_launches.push_back(cl);
-    }
+    for (int P = 512; P >= 64; P >>= 1)
+        for (int stg = 0; stg < 2; ++stg) {
+            btdma_handle::RagLaunch cl{1, P, (int)tasks.size(), 0, 0, stg};
+            for (const auto& b : h->rag_buckets)
+                if (b.cta && b.P == P && b.staged == stg) rag_bucket_tasks(b, 1, P, tasks);
+            cl.count = (int)tasks.size() - cl.first;
+            if (cl.count) h->rag_launches.push_back(cl);
+        }
     CK(cudaMemcpy(h->rag_d_tasks, tasks.data(), sizeof(int4) * tasks.size(),
                   cudaMemcpyHostToDevice));
     return BTDMA_OK;
@@ -959,7 +985,7 @@ int rag_plan(btdma_t h, const long long* off, const unsigned char* per, int n_sy
 }
 
 template <typename TIN>
-int rag_launch(btdma_t h, int cta, int P, int mcap, const int4* tasks, int n_tasks,
+int rag_launch(btdma_t h, int cta, int P, int mcap, int staged, const int4* tasks, int n_tasks,
                const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X,
                cudaStream_t st) {
     RagArgs a{};
@@ -975,8 +1001,7 @@ int rag_launch(btdma_t h, int cta, int P, int mcap, const int4* tasks, int n_tas
     a.mcap = mcap;
     a.status = h->status;
     if (cta) {
-        // staged through shared memory where the whole system fits
-        const bool staged = rag_cta_smem_bytes(P, true) <= (size_t)max_smem_optin();
+        if (staged && rag_cta_smem_bytes(P, true) > (size_t)max_smem_optin()) staged = 0;
         auto kern = staged ? ragged_cta_kernel<TIN, true> : ragged_cta_kernel<TIN, false>;
         static bool attr_done[2] = {false, false};
         if (!attr_done[staged]) {
@@ -1014,8 +1039,9 @@ int rag_run(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, d
     }
     for (int i = 0; i < n; ++i) {
         const cudaStream_t s = i == 0 ? st : h->rag_side[(i - 1) % btdma_handle::RAG_STREAMS];
-        const int rc = rag_launch<TIN>(h, L[i].cta, L[i].P, L[i].mcap, h->rag_d_tasks + L[i].first,
-                                       L[i].count, A, B, C, D, X, s);
+        const int rc = rag_launch<TIN>(h, L[i].cta, L[i].P, L[i].mcap, L[i].staged,
+                                       h->rag_d_tasks + L[i].first, L[i].count, A, B, C, D, X,
+                                       s);
         if (rc) return rc;
     }
     for (int i = 0; i < side; ++i) {
@@ -1057,15 +1083,19 @@ int rag_tune(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, 
     std::vector<int4> tasks;
     for (auto& b : h->rag_buckets) {
         struct Cand {
-            int cta, P;
+            int cta, P, staged;
         };
         std::vector<Cand> cands;
         for (int P = 1; P <= 32 && b.nmin / P >= 3; P <<= 1)
-            if (rag_mcap(b.nmax, P) <= RAG_WARP_MCAP) cands.push_back({0, P});
+            if (rag_mcap(b.nmax, P) <= RAG_WARP_MCAP) cands.push_back({0, P, 0});
         for (int P = 64; P <= 512 && b.nmin / P >= 3; P <<= 1)
-            if (rag_mcap(b.nmax, P) <= RAG_MT) cands.push_back({1, P});
+            if (rag_mcap(b.nmax, P) <= RAG_MT) {
+                cands.push_back({1, P, 0});
+                if (rag_cta_smem_bytes(P, true) <= (size_t)max_smem_optin())
+                    cands.push_back({1, P, 1});
+            }
         float best = 1e30f;
-        Cand pick{b.cta, b.P};
+        Cand pick{b.cta, b.P, b.staged};
         for (const Cand& cd : cands) {
             tasks.clear();
             rag_bucket_tasks(b, cd.cta, cd.P, tasks);
@@ -1078,8 +1108,8 @@ int rag_tune(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, 
             float ms = 0.f;
             for (int rep = 0; rep < 3 && !rc; ++rep) {
                 CK(cudaEventRecord(e0, st));
-                rc = rag_launch<TIN>(h, cd.cta, cd.P, rag_mcap(b.nmax, cd.P), h->rag_d_probe,
-                                     (int)tasks.size(), A, B, C, D, X, st);
+                rc = rag_launch<TIN>(h, cd.cta, cd.P, rag_mcap(b.nmax, cd.P), cd.staged,
+                                     h->rag_d_probe, (int)tasks.size(), A, B, C, D, X, st);
                 if (rc) break;
                 CK(cudaEventRecord(e1, st));
                 CK(cudaEventSynchronize(e1));
@@ -1095,6 +1125,7 @@ int rag_tune(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, 
         }
         if (rc) break;
         b.cta = pick.cta;
+        b.staged = pick.staged;
         b.P = pick.P;
         b.warps = pick.cta ? pick.P / 32 : RAG_WPC;
         b.mcap = rag_mcap(b.nmax, pick.P);
@@ -1144,7 +1175,7 @@ int btdma_ragged_plan_info(btdma_t h, btdma_ragged_bucket* out, int cap, int* n_
         out[i].n_row_max = b.nmax;
         out[i].lanes_per_system = b.P;
         out[i].warps_per_cta = b.warps;
-        out[i].cta_per_system = b.cta;
+        out[i].cta_per_system = b.cta + b.staged;
         out[i].tuned_ms = b.best_ms;
     }
     return BTDMA_OK;

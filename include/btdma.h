@@ -217,7 +217,9 @@ typedef struct btdma_ragged_bucket {
     int n_row_min, n_row_max;
     int lanes_per_system; /* threads that share one system */
     int warps_per_cta;
-    int cta_per_system;   /* 1: one CTA per system (long systems), 0: lanes of a warp */
+    int cta_per_system;   /* 0: lanes of a warp per system; 1: one CTA per system
+                             (long systems); 2: one CTA per system staged through
+                             shared memory */
     float tuned_ms;       /* fastest time measured by the autotuner (0 before tuning) */
 } btdma_ragged_bucket;
 int btdma_ragged_plan_info(btdma_t h, btdma_ragged_bucket* out, int cap, int* n_out);
