@@ -208,25 +208,7 @@ int num_sms() {
 // Shape plan of the tiled kernel: systems per group, CTAs per cluster, ring stages.
 struct TilePlan {
     int sys = 0, cl = 0, nst = 0, nseg = 0;
-    int pair = 1;  // CTAs whose loads are issued together (cl == 1 only)
 };
-
-// Paired loads (opt-in): enough neighbouring CTAs that their row pieces add up
-// to 256 bytes, at most BTDMA_TILE_PAIR (environment, default 1 = off).  On
-// B200 the DRAM streams two 128-byte pieces requested together nearly as fast
-// as one 256-byte piece, but coupling every ring-slot refill to the slowest
-// warp of 2-4 SMs cost more than that gained (262144 x 512: FP64 1.12 ms
-// unpaired, 2.08 ms paired by 2), so pairing stays off unless asked for.
-int tile_pair(int sys, int elem) {
-    static int cap = -1;
-    if (cap < 0) {
-        const char* e = getenv("BTDMA_TILE_PAIR");
-        cap = e ? std::max(1, std::min(4, atoi(e))) : 1;
-    }
-    int pr = 1;
-    while (pr < cap && pr * sys * elem < 256) pr <<= 1;
-    return pr;
-}
 
 // na: arrays per ring stage (4, or 1 for the constant-coefficient D-only ring).
 TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4) {
@@ -265,7 +247,6 @@ TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4) {
     pl.cl = cl;
     pl.nst = nst;
     pl.nseg = nseg;
-    pl.pair = cl == 1 ? tile_pair(sys, elem) : 1;
     return pl;
 }
 
@@ -287,23 +268,21 @@ int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st)
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    const int pr = a.cl == 1 && a.pair > 1 ? a.pair : 1;
-    const int cdim = a.cl * pr;  // CTAs per cluster: split system (cl) or paired loads (pr)
-    attr[0].val.clusterDim.x = cdim;
+    attr[0].val.clusterDim.x = a.cl;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int clusters = num_sms();
-    if (cdim > 1) {
-        cfg.gridDim = dim3(cdim * num_sms(), 1, 1);
+    if (a.cl > 1) {
+        cfg.gridDim = dim3(a.cl * num_sms(), 1, 1);
         int nc = 0;
         CK(cudaOccupancyMaxActiveClusters(&nc, kern, &cfg));
-        if (nc <= 0) return fail(BTDMA_ERR_UNSUPPORTED, "no cluster of %d CTAs fits", cdim);
+        if (nc <= 0) return fail(BTDMA_ERR_UNSUPPORTED, "no cluster of %d CTAs fits", a.cl);
         clusters = nc;
     }
-    clusters = std::min(clusters, (a.n_groups + pr - 1) / pr);
-    cfg.gridDim = dim3(clusters * cdim, 1, 1);
+    clusters = std::min(clusters, a.n_groups);
+    cfg.gridDim = dim3(clusters * a.cl, 1, 1);
     TileArgs aa = a;
     CK(cudaLaunchKernelEx(&cfg, kern, maps[0], maps[1], maps[2], maps[3], aa));
     return BTDMA_OK;
@@ -357,7 +336,6 @@ int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, 
     a.cl = pl.cl;
     a.nst = pl.nst;
     a.n_groups = (n_sys + pl.sys - 1) / pl.sys;
-    a.pair = pl.pair;
     a.accumulate = accumulate ? 1 : 0;
     a.gate = gate;
     a.status = status;
@@ -385,7 +363,6 @@ int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArg
     a.cl = pl.cl;
     a.nst = pl.nst;
     a.n_groups = (n_sys + pl.sys - 1) / pl.sys;
-    a.pair = pl.pair;
     a.accumulate = 0;
     a.gate = nullptr;
     a.status = status;

@@ -95,50 +95,6 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 // at most kSuspendNs), raising ST_TIMEOUT.  Every 64 polls it also checks the
 // status word and gives up at once if another CTA already timed out, so a
 // systematic failure costs one timeout, not one per CTA.
-// ---------------------------------------------------- cluster-scope helpers
-// Shared-memory address of the same variable in CTA `rank` of the cluster.
-__device__ __forceinline__ uint32_t cluster_addr(const void* p, int rank) {
-    uint32_t r;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
-    return r;
-}
-// arrive + expect_tx on an mbarrier of any CTA of the cluster
-__device__ __forceinline__ void mbar_expect_tx_remote(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.release.cluster.shared::cluster.b64 _, [%0], %1;" ::"r"(
-                     bar),
-                 "r"(bytes)
-                 : "memory");
-}
-// plain arrival on an mbarrier of any CTA of the cluster
-__device__ __forceinline__ void mbar_arrive_remote(uint32_t bar) {
-    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar)
-                 : "memory");
-}
-// wait (cluster-scope acquire) on a local mbarrier that other CTAs arrive on
-__device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t* bar, uint32_t parity) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendNs)
-        : "memory");
-    return done != 0;
-}
-__device__ __forceinline__ bool mbar_wait_cluster_bounded(uint64_t* bar, uint32_t parity,
-                                                          unsigned* status,
-                                                          uint32_t limit = 1u << 16) {
-    for (uint32_t it = 0; it < limit; ++it) {
-        if (mbar_try_wait_cluster(bar, parity)) return true;
-        if (status && (it & 63u) == 63u &&
-            (*reinterpret_cast<volatile unsigned*>(status) & ST_TIMEOUT))
-            return false;
-    }
-    raise_status(status, ST_TIMEOUT);
-    return false;
-}
-
 __device__ __noinline__ bool mbar_wait_slow(uint64_t* bar, uint32_t parity, unsigned* status,
                                             uint32_t limit);
 

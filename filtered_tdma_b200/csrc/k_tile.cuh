@@ -78,11 +78,6 @@ struct TileArgs {
     //    with gpin, row 0 of mode 0 is x_0 = 0 (the pinned mean pressure).
     double cs;
     int cbound;
-    // pair > 1 (only with cl == 1): a cluster of `pair` CTAs solving adjacent
-    // groups, whose TMA boxes the cluster's first CTA issues back to back (each
-    // into its own CTA's ring), so the DRAM sees neighbouring row pieces
-    // together; members release ring slots by arriving on the leader's barriers
-    int pair;
     const double* ga;
     const double* gc;
     const double* glam;
@@ -138,17 +133,6 @@ __device__ __forceinline__ void tma_load_3d(void* smem_dst, const CUtensorMap* m
         : "memory");
 }
 
-// The same load into shared memory of any CTA of the cluster (dst and bar are
-// shared::cluster addresses of that CTA; no multicast).
-__device__ __forceinline__ void tma_load_3d_to(uint32_t dst, const CUtensorMap* map, int x, int y,
-                                               int z, uint32_t bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
-        : "memory");
-}
-
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
@@ -201,11 +185,8 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     const int warp = tid >> 5;
     const int nwarps = (T + 31) / 32;
     const int c = cl > 1 ? (int)cg::this_cluster().block_rank() : 0;
-    const int pr = (cl == 1 && args.pair > 1) ? args.pair : 1;  // paired-load cluster size
-    const bool paired = pr > 1;
-    const int cr = paired ? (int)cg::this_cluster().block_rank() : 0;
-    const int cluster_id = (int)blockIdx.x / (cl * pr);
-    const int n_clusters = (int)gridDim.x / (cl * pr);
+    const int cluster_id = (int)blockIdx.x / cl;
+    const int n_clusters = (int)gridDim.x / cl;
     const int s = tid % SYS;  // forward / back-substitution mapping
     const int ql = tid / SYS;
     const size_t ns = (size_t)args.n_sys;
@@ -213,8 +194,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     if (tid == 0) {
         for (int i = 0; i < nst; ++i) {
             mbar_init(&full[i], 1);
-            // paired: the leader's empty barriers collect every member's warps
-            mbar_init(&empty[i], paired ? pr * nwarps : nwarps);
+            mbar_init(&empty[i], nwarps);
         }
         fence_mbar_init();
     }
@@ -225,16 +205,14 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         }
     }
     __syncthreads();
-    // peers' shared memory and barriers are live before any remote access
-    if (cl > 1 || paired) tile_cluster_sync(cl * pr);
+    if (cl > 1) tile_cluster_sync(cl);  // peers' shared memory is live before any DSMEM access
 
     // a closed gate leaves the CTA without groups (it still runs its setup and
     // exit barriers, so every CTA of a cluster takes the same path)
     const bool gated_off =
         args.gate != nullptr && *static_cast<const volatile unsigned*>(args.gate) == 0u;
-    const int n_units = (args.n_groups + pr - 1) / pr;  // groups, or pairs of groups
-    const int n_my = (!gated_off && n_units > cluster_id)
-                         ? (n_units - cluster_id + n_clusters - 1) / n_clusters
+    const int n_my = (!gated_off && args.n_groups > cluster_id)
+                         ? (args.n_groups - cluster_id + n_clusters - 1) / n_clusters
                          : 0;
     const int total = n_my * SPG;  // ring stages this CTA consumes
     const int sstride = NA * RPS * T;  // elements per stage
@@ -245,21 +223,6 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         const int g = cluster_id + (t / SPG) * n_clusters;
         const int k0 = (t % SPG) * RPS;
         TIN* dst = ring + (size_t)slot * sstride;
-        if (paired) {  // the leader loads every member's stage, back to back
-            for (int m = 0; m < pr; ++m) {
-                const uint32_t bar = cluster_addr(&full[slot], m);
-                const uint32_t d0 = cluster_addr(dst, m);
-                const int gx = (g * pr + m) * SYS;
-                mbar_expect_tx_remote(bar, stage_bytes);
-                if constexpr (!CONSTC) {
-                    tma_load_3d_to(d0 + 0 * RPS * T * sizeof(TIN), &tmA, gx, k0, 0, bar);
-                    tma_load_3d_to(d0 + 1 * RPS * T * sizeof(TIN), &tmB, gx, k0, 0, bar);
-                    tma_load_3d_to(d0 + 2 * RPS * T * sizeof(TIN), &tmC, gx, k0, 0, bar);
-                }
-                tma_load_3d_to(d0 + (NA - 1) * RPS * T * sizeof(TIN), &tmD, gx, k0, 0, bar);
-            }
-            return;
-        }
         mbar_expect_tx(&full[slot], stage_bytes);
         if constexpr (!CONSTC) {
             tma_load_3d(dst + 0 * RPS * T, &tmA, g * SYS, k0, c * nsc, &full[slot]);
@@ -269,7 +232,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         tma_load_3d(dst + (NA - 1) * RPS * T, &tmD, g * SYS, k0, c * nsc, &full[slot]);
     };
     bool ok = true;
-    if (tid == 0 && cr == 0)
+    if (tid == 0)
         for (int t = 0; t < nst && t < total; ++t) issue(t);
 
     // this thread's element of a stage: array f, row r at st + f*RPS*T + r*SYS
@@ -284,7 +247,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     int t = 0;
     int tw = 0;  // t % nwarps
     for (int it = 0; it < n_my; ++it) {
-        const int g = (cluster_id + it * n_clusters) * pr + cr;
+        const int g = cluster_id + it * n_clusters;
         const int sys = g * SYS + s;
         const bool valid = sys < args.n_sys;
 
@@ -309,16 +272,12 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             }
             __syncwarp();
             if (lane == 0) {
-                if (paired)
-                    mbar_arrive_remote(cluster_addr(&empty[slot], 0));  // the leader's
-                else
-                    mbar_arrive(&empty[slot]);
+                mbar_arrive(&empty[slot]);
                 // Rotating producer: one stage later, warp (t % nwarps) refills
                 // the slot of stage t - 1 with stage t - 1 + nst once every warp
-                // (of every member, when paired) has released it.
-                if (t >= 1 && warp == tw && t - 1 + nst < total && ok && cr == 0) {
-                    ok = paired ? mbar_wait_cluster_bounded(&empty[pslot], pphase, args.status)
-                                : mbar_wait_bounded(&empty[pslot], pphase, args.status);
+                // has released it.
+                if (t >= 1 && warp == tw && t - 1 + nst < total && ok) {
+                    ok = mbar_wait_bounded(&empty[pslot], pphase, args.status);
                     if (ok) issue(t - 1 + nst);
                 }
             }
@@ -543,8 +502,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         // the CTA exits
         for (int i = 0; i < nst; ++i) mbar_wait_bounded(&full[i], 0, nullptr, 1u << 8);
     }
-    // no CTA leaves while peers may touch its memory or barriers
-    if (cl > 1 || paired) tile_cluster_sync(cl * pr);
+    if (cl > 1) tile_cluster_sync(cl);  // no CTA leaves while peers may touch its memory
 }
 
 }  // namespace btdma
