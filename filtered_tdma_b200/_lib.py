@@ -28,7 +28,8 @@ EXPORTS = (
     "btdma_solve_ragged", "btdma_solve_ragged_f32", "btdma_ragged_autotune",
     "btdma_ragged_plan_info", "btdma_heat_create", "btdma_heat_destroy", "btdma_heat_init",
     "btdma_heat_step", "btdma_heat_l2_error", "btdma_heat_step_profile", "btdma_poisson_create", "btdma_poisson_destroy",
-    "btdma_poisson_solve", "btdma_poisson_status",
+    "btdma_poisson_solve", "btdma_poisson_status", "btdma_momentum_create",
+    "btdma_momentum_destroy", "btdma_momentum_sweep", "btdma_momentum_adi", "btdma_momentum_status",
 )
 NOALLOC_MAX_ELEMS = 1 << 20
 REFINE_MAX_SWEEPS = 4
@@ -105,6 +106,12 @@ def lib():
         L.btdma_poisson_destroy.argtypes = [vp]
         L.btdma_poisson_solve.argtypes = [vp, vp, vp]
         L.btdma_poisson_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint), vp]
+        L.btdma_momentum_create.argtypes = [i, i, i, vp, vp, vp, vp, vp, vp, i, i,
+                                            ctypes.POINTER(vp)]
+        L.btdma_momentum_destroy.argtypes = [vp]
+        L.btdma_momentum_sweep.argtypes = [vp, i, i, vp, vp, d, vp]
+        L.btdma_momentum_adi.argtypes = [vp, i, vp, vp, d, vp]
+        L.btdma_momentum_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint), vp]
         L.btdma_last_error.restype = ctypes.c_char_p
         for name in EXPORTS:
             if name != "btdma_last_error":

@@ -18,6 +18,7 @@
 #include "btdma_common.cuh"
 #include "k_filtered_j.cuh"
 #include "k_heat.cuh"
+#include "k_momentum.cuh"
 #include "k_ragged.cuh"
 #include "k_refine.cuh"
 #include "k_segment.cuh"
@@ -346,10 +347,10 @@ int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, 
 // Generated-coefficient batch, only D read (the GEN modes of the tiled
 // kernel; the coefficient fields of `gen` are used, the rest is filled here).
 // Returns 1 when launched, 0 when the shape is not tiled, < 0 on error.
-template <int GEN>
+template <int GEN, bool CYC = false>
 int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArgs& gen,
                  unsigned* status, cudaStream_t st) {
-    const TilePlan pl = tile_plan(n_row, false, 8, 1);
+    const TilePlan pl = tile_plan(n_row, CYC, 8, 1);
     if (pl.sys == 0 || !tma_ok_elem(D, n_sys, 8)) return 0;
     const int nsc = pl.nseg / pl.cl;
     CUtensorMap maps[4];
@@ -368,10 +369,10 @@ int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArg
     a.status = status;
     int rc;
     switch (pl.sys) {
-        case 128: rc = launch_tile_sys<128, false, double, double, GEN>(maps, a, st); break;
-        case 64: rc = launch_tile_sys<64, false, double, double, GEN>(maps, a, st); break;
-        case 32: rc = launch_tile_sys<32, false, double, double, GEN>(maps, a, st); break;
-        default: rc = launch_tile_sys<16, false, double, double, GEN>(maps, a, st); break;
+        case 128: rc = launch_tile_sys<128, CYC, double, double, GEN>(maps, a, st); break;
+        case 64: rc = launch_tile_sys<64, CYC, double, double, GEN>(maps, a, st); break;
+        case 32: rc = launch_tile_sys<32, CYC, double, double, GEN>(maps, a, st); break;
+        default: rc = launch_tile_sys<16, CYC, double, double, GEN>(maps, a, st); break;
     }
     return rc == BTDMA_OK ? 1 : rc;
 }
@@ -1504,6 +1505,168 @@ int btdma_poisson_solve(btdma_poisson_t h, double* rhs, cudaStream_t stream) {
 }
 
 int btdma_poisson_status(btdma_poisson_t h, unsigned* status, cudaStream_t stream) {
+    if (!h || !status) return fail(BTDMA_ERR_ARG, "null argument");
+    CK(cudaMemcpyAsync(status, h->status, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    CK(cudaMemsetAsync(h->status, 0, sizeof(unsigned), stream));
+    CK(cudaStreamSynchronize(stream));
+    return BTDMA_OK;
+}
+
+// ------------------------------------------------ channel momentum ADI sweeps
+struct btdma_momentum {
+    MomGeom g{};
+    int pbc[2] = {0, 0};
+    double* tab = nullptr;  // [dir][comp][ta, tb, tc][n_dir rows]
+    size_t tab_off[3][3] = {};
+    double* buf = nullptr;  // nx * ny * nz, the sweep layout
+    unsigned* status = nullptr;
+};
+
+int btdma_momentum_create(int nx, int ny, int nz, const double* dx0, const double* dmx0,
+                          const double* dx1, const double* dmx1, const double* dx2,
+                          const double* dmx2, int pbc_x, int pbc_y, btdma_momentum_t* out) {
+    if (!out) return fail(BTDMA_ERR_ARG, "null output handle");
+    *out = nullptr;
+    if (nx <= 0 || ny <= 0 || nz <= 0 || !dx0 || !dmx0 || !dx1 || !dmx1 || !dx2 || !dmx2)
+        return fail(BTDMA_ERR_ARG, "grid sizes and the six metric arrays are required");
+    const int n[3] = {nx, ny, nz};
+    for (int d = 0; d < 3; ++d) {
+        const bool cyc = d < 2 && (d == 0 ? pbc_x : pbc_y);
+        if (!tile_plan(n[d], cyc, 8, 1).sys)
+            return fail(BTDMA_ERR_UNSUPPORTED,
+                        "sweep %d: n must be a multiple of 16 (n / 16 a power of two when "
+                        "periodic)", d);
+    }
+    if ((long long)nx * ny * nz >= (1LL << 31))
+        return fail(BTDMA_ERR_SIZE, "grid above 2^31 cells");
+    // row tables (MomentumSolverGPU.cu:135-155, :176-180, :205-209): for row
+    // r = 1..n, staggered when comp == dir;  a = -c ta, c = -c tc, b = 1 + c tb
+    const double* dxs[3] = {dx0, dx1, dx2};
+    const double* dms[3] = {dmx0, dmx1, dmx2};
+    std::vector<double> tab;
+    size_t off[3][3];
+    for (int d = 0; d < 3; ++d)
+        for (int comp = 0; comp < 3; ++comp) {
+            off[d][comp] = tab.size();
+            const int m = n[d];
+            std::vector<double> ta(m), tb(m), tc(m);
+            const double* dx = dxs[d];
+            const double* dm = dms[d];
+            for (int r = 1; r <= m; ++r) {
+                const double ar = comp == d ? 1.0 / (dm[r] * dx[r - 1]) : 1.0 / (dx[r] * dm[r]);
+                const double cr = comp == d ? 1.0 / (dm[r] * dx[r]) : 1.0 / (dx[r] * dm[r + 1]);
+                double a_ = ar, b_ = ar + cr, c_ = cr;
+                if (d == 2) {  // no-slip walls at both ends (one rank holds all of z)
+                    const bool is_w = comp == 2;
+                    if (r == 1) {
+                        a_ = 0.0;
+                        if (!is_w) b_ += ar;
+                    }
+                    if (r == m) {
+                        c_ = 0.0;
+                        if (!is_w) b_ += cr;
+                    }
+                    if (is_w && r == 1) a_ = b_ = c_ = 0.0;  // w = 0 on the wall
+                }
+                ta[r - 1] = a_;
+                tb[r - 1] = b_;
+                tc[r - 1] = c_;
+            }
+            tab.insert(tab.end(), ta.begin(), ta.end());
+            tab.insert(tab.end(), tb.begin(), tb.end());
+            tab.insert(tab.end(), tc.begin(), tc.end());
+        }
+    btdma_momentum* h = new btdma_momentum();
+    h->g.nx = nx;
+    h->g.ny = ny;
+    h->g.nz = nz;
+    h->pbc[0] = pbc_x ? 1 : 0;
+    h->pbc[1] = pbc_y ? 1 : 0;
+    std::memcpy(h->tab_off, off, sizeof off);
+    auto cleanup = [&](int code) {
+        btdma_momentum_destroy(h);
+        return code;
+    };
+    if (cudaMalloc(&h->tab, sizeof(double) * tab.size()) != cudaSuccess ||
+        cudaMemcpy(h->tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice) !=
+            cudaSuccess ||
+        cudaMalloc(&h->buf, sizeof(double) * (size_t)nx * ny * nz) != cudaSuccess ||
+        cudaMalloc(&h->status, sizeof(unsigned)) != cudaSuccess ||
+        cudaMemset(h->status, 0, sizeof(unsigned)) != cudaSuccess)
+        return cleanup(fail(BTDMA_ERR_CUDA, "momentum buffers: %s",
+                            cudaGetErrorString(cudaGetLastError())));
+    *out = h;
+    return BTDMA_OK;
+}
+
+int btdma_momentum_destroy(btdma_momentum_t h) {
+    if (!h) return BTDMA_OK;
+    cudaFree(h->tab);
+    cudaFree(h->buf);
+    cudaFree(h->status);
+    delete h;
+    return BTDMA_OK;
+}
+
+int btdma_momentum_sweep(btdma_momentum_t h, int dir, int comp, const double* q, double* dst,
+                         double c, cudaStream_t stream) {
+    if (!h || !q || !dst) return fail(BTDMA_ERR_ARG, "null argument");
+    if (dir < 0 || dir > 2 || comp < 0 || comp > 2)
+        return fail(BTDMA_ERR_ARG, "dir and comp must be 0, 1 or 2");
+    const MomGeom& g = h->g;
+    const int n[3] = {g.nx, g.ny, g.nz};
+    const int n_sys = g.nx * g.ny * g.nz / n[dir];
+    TileArgs t = {};
+    t.cs = c;
+    t.ga = h->tab + h->tab_off[dir][comp];
+    t.gb = t.ga + n[dir];
+    t.gc = t.gb + n[dir];
+    const dim3 b1(128, 1, 1), bt(MOM_TILE, 8, 1);
+    int rc;
+    if (dir == 2) {
+        mom_gather_kernel<2><<<dim3((g.nx + 127) / 128, g.ny, g.nz), b1, 0, stream>>>(
+            q, h->buf, g, comp == 2 ? 1 : 0);
+        CK(cudaGetLastError());
+        rc = try_tile_gen<3, false>(h->buf, h->buf, n_sys, g.nz, t, h->status, stream);
+    } else if (dir == 1) {
+        mom_gather_kernel<1><<<dim3((g.nx + 127) / 128, g.nz, g.ny), b1, 0, stream>>>(q, h->buf,
+                                                                                   g, 0);
+        CK(cudaGetLastError());
+        rc = h->pbc[1] ? try_tile_gen<3, true>(h->buf, h->buf, n_sys, g.ny, t, h->status, stream)
+                       : try_tile_gen<3, false>(h->buf, h->buf, n_sys, g.ny, t, h->status, stream);
+    } else {
+        mom_gather_x_kernel<<<dim3((g.nx + MOM_TILE - 1) / MOM_TILE,
+                                   (g.ny + MOM_TILE - 1) / MOM_TILE, g.nz), bt, 0, stream>>>(
+            q, h->buf, g);
+        CK(cudaGetLastError());
+        rc = h->pbc[0] ? try_tile_gen<3, true>(h->buf, h->buf, n_sys, g.nx, t, h->status, stream)
+                       : try_tile_gen<3, false>(h->buf, h->buf, n_sys, g.nx, t, h->status, stream);
+    }
+    if (rc != 1) return rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "sweep not tileable");
+    if (dir == 2)
+        mom_scatter_kernel<2><<<dim3((g.nx + 127) / 128, g.ny, g.nz), b1, 0, stream>>>(h->buf,
+                                                                                     dst, g);
+    else if (dir == 1)
+        mom_scatter_kernel<1><<<dim3((g.nx + 127) / 128, g.nz, g.ny), b1, 0, stream>>>(h->buf,
+                                                                                     dst, g);
+    else
+        mom_scatter_x_kernel<<<dim3((g.ny + MOM_TILE - 1) / MOM_TILE,
+                                    (g.nx + MOM_TILE - 1) / MOM_TILE, g.nz), bt, 0, stream>>>(
+            h->buf, dst, g);
+    CK(cudaGetLastError());
+    return BTDMA_OK;
+}
+
+int btdma_momentum_adi(btdma_momentum_t h, int comp, double* rhs, double* q_out, double c,
+                       cudaStream_t stream) {
+    int rc = btdma_momentum_sweep(h, 2, comp, rhs, rhs, c, stream);
+    if (!rc) rc = btdma_momentum_sweep(h, 1, comp, rhs, rhs, c, stream);
+    if (!rc) rc = btdma_momentum_sweep(h, 0, comp, rhs, q_out, c, stream);
+    return rc;
+}
+
+int btdma_momentum_status(btdma_momentum_t h, unsigned* status, cudaStream_t stream) {
     if (!h || !status) return fail(BTDMA_ERR_ARG, "null argument");
     CK(cudaMemcpyAsync(status, h->status, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));

@@ -1,0 +1,92 @@
+// Channel momentum ADI sweeps (apps/channel_gpu/MomentumSolverGPU.cu:135-220
+// k_build_{x,y,z} + solve + k_scatter_{x,y,z}, called by adi_{z,y,x}_ at
+// :261-313), with the coefficients generated inside the tiled solve (GEN = 3
+// row tables) instead of stored: the build is a gather of the ghosted field
+// into the sweep layout, the scatter its inverse.
+//
+// Field: q[i + (nx + 2) * (j + (ny + 2) * k)] (DeviceField.hpp df_idx), interior
+// i = 1..nx, j = 1..ny, k = 1..nz.  Sweep layouts (system index fastest):
+//   z: D[(k-1) * nx*ny + (j-1) * nx + (i-1)]     rows k, systems (j, i)
+//   y: D[(j-1) * nx*nz + (k-1) * nx + (i-1)]     rows j, systems (k, i)
+//   x: D[(i-1) * ny*nz + (k-1) * ny + (j-1)]     rows i, systems (k, j)
+// (the reference orders the systems the other way round, s = (i-1) * ny +
+// (j-1) etc.; a system's rows and coefficients are the same).
+#pragma once
+
+#include "btdma_common.cuh"
+
+namespace btdma {
+
+struct MomGeom {
+    int nx, ny, nz;
+};
+
+__device__ __forceinline__ size_t mom_fld(const MomGeom& g, int i, int j, int k) {
+    return (size_t)i + (size_t)(g.nx + 2) * ((size_t)j + (size_t)(g.ny + 2) * k);
+}
+
+// z and y sweeps: i fastest on both sides, no transpose.  pin: row k = 1 of
+// the z sweep is the w wall (D = 0, k_build_z :150-152).
+template <int DIR>
+__global__ void __launch_bounds__(256) mom_gather_kernel(const double* __restrict__ q,
+                                                         double* __restrict__ D, const MomGeom g,
+                                                         int pin) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int a = blockIdx.y + 1, b = blockIdx.z + 1;  // z: (j, k); y: (k, j)
+    if (i > g.nx) return;
+    const int j = DIR == 2 ? a : b, k = DIR == 2 ? b : a;
+    const size_t o = DIR == 2 ? ((size_t)(k - 1) * g.ny + (j - 1)) * g.nx + (i - 1)
+                              : ((size_t)(j - 1) * g.nz + (k - 1)) * g.nx + (i - 1);
+    D[o] = (DIR == 2 && pin && k == 1) ? 0.0 : q[mom_fld(g, i, j, k)];
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(256) mom_scatter_kernel(const double* __restrict__ D,
+                                                          double* __restrict__ q, const MomGeom g) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int a = blockIdx.y + 1, b = blockIdx.z + 1;
+    if (i > g.nx) return;
+    const int j = DIR == 2 ? a : b, k = DIR == 2 ? b : a;
+    const size_t o = DIR == 2 ? ((size_t)(k - 1) * g.ny + (j - 1)) * g.nx + (i - 1)
+                              : ((size_t)(j - 1) * g.nz + (k - 1)) * g.nx + (i - 1);
+    q[mom_fld(g, i, j, k)] = D[o];
+}
+
+constexpr int MOM_TILE = 32;
+
+// x sweep: (i, j) transposed through a shared 32 x 32 tile per k; block (32, 8).
+__global__ void __launch_bounds__(256) mom_gather_x_kernel(const double* __restrict__ q,
+                                                           double* __restrict__ D,
+                                                           const MomGeom g) {
+    __shared__ double tile[MOM_TILE][MOM_TILE + 1];
+    const int i0 = blockIdx.x * MOM_TILE, j0 = blockIdx.y * MOM_TILE, k = blockIdx.z + 1;
+    for (int r = threadIdx.y; r < MOM_TILE; r += blockDim.y) {
+        const int i = i0 + threadIdx.x + 1, j = j0 + r + 1;
+        if (i <= g.nx && j <= g.ny) tile[r][threadIdx.x] = q[mom_fld(g, i, j, k)];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < MOM_TILE; r += blockDim.y) {
+        const int j = j0 + threadIdx.x + 1, i = i0 + r + 1;
+        if (i <= g.nx && j <= g.ny)
+            D[((size_t)(i - 1) * g.nz + (k - 1)) * g.ny + (j - 1)] = tile[threadIdx.x][r];
+    }
+}
+
+__global__ void __launch_bounds__(256) mom_scatter_x_kernel(const double* __restrict__ D,
+                                                            double* __restrict__ q,
+                                                            const MomGeom g) {
+    __shared__ double tile[MOM_TILE][MOM_TILE + 1];
+    const int j0 = blockIdx.x * MOM_TILE, i0 = blockIdx.y * MOM_TILE, k = blockIdx.z + 1;
+    for (int r = threadIdx.y; r < MOM_TILE; r += blockDim.y) {
+        const int j = j0 + threadIdx.x + 1, i = i0 + r + 1;
+        if (i <= g.nx && j <= g.ny)
+            tile[r][threadIdx.x] = D[((size_t)(i - 1) * g.nz + (k - 1)) * g.ny + (j - 1)];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < MOM_TILE; r += blockDim.y) {
+        const int i = i0 + threadIdx.x + 1, j = j0 + r + 1;
+        if (i <= g.nx && j <= g.ny) q[mom_fld(g, i, j, k)] = tile[threadIdx.x][r];
+    }
+}
+
+}  // namespace btdma

@@ -75,10 +75,14 @@ struct TileArgs {
     //  GEN == 2 (channel Poisson, wall-normal): row j is
     //    ga[j] x_{j-1} - (ga[j] + gc[j] + glam[s / 2]) x_j + gc[j] x_{j+1},
     //    systems 2m and 2m + 1 being the real and imaginary parts of mode m;
-    //    with gpin, row 0 of mode 0 is x_0 = 0 (the pinned mean pressure).
+    //    with gpin, row 0 of mode 0 is x_0 = 0 (the pinned mean pressure);
+    //  GEN == 3 (channel momentum ADI): row j is
+    //    -cs ga[j] x_{j-1} + (1 + cs gb[j]) x_j - cs gc[j] x_{j+1}
+    //    (staggered metrics and wall terms folded into the row tables).
     double cs;
     int cbound;
     const double* ga;
+    const double* gb;
     const double* gc;
     const double* glam;
     int gpin;
@@ -302,6 +306,11 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                     a = (TC)-args.cs;
                     cc = (TC)-args.cs;
                     b = (TC)(1.0 + 2.0 * args.cs + (wall ? args.cs : 0.0));
+                } else if constexpr (GEN == 3) {
+                    const int kg = (c * nsc + ql) * M + k;  // row of the system
+                    a = (TC)(-args.cs * args.ga[kg]);
+                    cc = (TC)(-args.cs * args.gc[kg]);
+                    b = (TC)(1.0 + args.cs * args.gb[kg]);
                 } else if constexpr (GEN == 2) {
                     const int kg = (c * nsc + ql) * M + k;  // row of the system
                     const double ta = args.ga[kg], tc = args.gc[kg];

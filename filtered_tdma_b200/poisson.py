@@ -15,45 +15,13 @@ from __future__ import annotations
 import ctypes
 import math
 
-import numpy as np
-
 from . import _lib as L
+from .channel_grid import axis_metrics, mode_lambdas  # noqa: F401  (re-exported)
 
 
 def wall_normal_grid(n: int, gamma: float, length: float):
-    """(dz, dmz), nz + 2 entries each, ghosts included (Grid::build_axis, one rank,
-    non-periodic axis)."""
-    if abs(gamma) < 1e-14:
-        xf = [length * i / n for i in range(n + 1)]
-    else:
-        th = math.tanh(gamma)
-        xf = [0.5 * length * (1.0 - math.tanh(gamma * (1.0 - 2.0 * (i / n))) / th)
-              for i in range(n + 1)]
-    xc = [0.0] * (n + 2)
-    for i in range(1, n + 1):
-        xc[i] = 0.5 * (xf[i - 1] + xf[i])
-    xc[0] = xf[0] - (xc[1] - xf[0])
-    xc[n + 1] = xf[n] + (xf[n] - xc[n])
-    dz = [0.0] * (n + 2)
-    for i in range(1, n + 1):
-        dz[i] = xf[i] - xf[i - 1]
-    dz[0], dz[n + 1] = dz[1], dz[n]
-    dmz = [0.0] * (n + 2)
-    for i in range(1, n + 2):
-        dmz[i] = xc[i] - xc[i - 1]
-    dmz[0] = dmz[1]
-    return np.array(dz), np.array(dmz)
-
-
-def mode_lambdas(n1m: int, n2m: int, lx: float, ly: float) -> np.ndarray:
-    """lambda per mode m = j * (n1m // 2 + 1) + i."""
-    nxh = n1m // 2 + 1
-    dx, dy = lx / n1m, ly / n2m
-    kx2 = np.array([2.0 * (1.0 - math.cos(2.0 * math.pi * i / n1m)) / (dx * dx)
-                    for i in range(nxh)])
-    ky2 = np.array([2.0 * (1.0 - math.cos(2.0 * math.pi * (j if j <= n2m // 2 else j - n2m)
-                                          / n2m)) / (dy * dy) for j in range(n2m)])
-    return (ky2[:, None] + kx2[None, :]).reshape(-1)
+    """(dz, dmz), nz + 2 entries each, ghosts included (non-periodic axis)."""
+    return axis_metrics(n, length, gamma, uniform=abs(gamma) < 1e-14, periodic=False)
 
 
 class ChannelPoisson:

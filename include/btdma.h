@@ -275,6 +275,32 @@ int btdma_poisson_destroy(btdma_poisson_t h);
 int btdma_poisson_solve(btdma_poisson_t h, double* rhs, cudaStream_t stream);
 int btdma_poisson_status(btdma_poisson_t h, unsigned* status, cudaStream_t stream);
 
+/* Channel momentum ADI sweeps (apps/channel_gpu/MomentumSolverGPU.cu: adi_z_,
+ * adi_y_, adi_x_ at :261-313 with k_build_* / k_scatter_* at :135-220): the
+ * implicit viscous half-step of velocity component comp (0 u, 1 v, 2 w) along
+ * direction dir (0 x, 1 y, 2 z) on an nx x ny x nz grid, field
+ * q[i + (nx+2) * (j + (ny+2) * k)] with one ghost layer.  Row r of a sweep is
+ *     -c ar_r x_{r-1} + (1 + c (ar_r + cr_r)) x_r - c cr_r x_{r+1} = q_r
+ * with ar, cr from the cell sizes dx and centre spacings dmx of that axis
+ * (staggered when comp == dir), no-slip walls at both z ends (u, v: the
+ * ghost folded onto the diagonal; w: w = 0 on the first face) and periodic x
+ * / y sweeps when pbc_x / pbc_y.  dx*, dmx* are HOST arrays of n + 2 entries
+ * (ghosts included), read at create time.  Coefficients are generated inside
+ * the solve, never stored.  btdma_momentum_sweep reads q and writes dst (may
+ * be q); btdma_momentum_adi runs z and y in place on rhs and x into q_out, as
+ * MomentumSolverGPU::advance's diffuse step does after k_lap.  PaScaL (exact)
+ * solves; n a multiple of 16, n / 16 a power of two for periodic sweeps. */
+typedef struct btdma_momentum* btdma_momentum_t;
+int btdma_momentum_create(int nx, int ny, int nz, const double* dx0, const double* dmx0,
+                          const double* dx1, const double* dmx1, const double* dx2,
+                          const double* dmx2, int pbc_x, int pbc_y, btdma_momentum_t* out);
+int btdma_momentum_destroy(btdma_momentum_t h);
+int btdma_momentum_sweep(btdma_momentum_t h, int dir, int comp, const double* q, double* dst,
+                         double c, cudaStream_t stream);
+int btdma_momentum_adi(btdma_momentum_t h, int comp, double* rhs, double* q_out, double c,
+                       cudaStream_t stream);
+int btdma_momentum_status(btdma_momentum_t h, unsigned* status, cudaStream_t stream);
+
 /* Switch the method of an existing handle (rho, eps and J state are kept).  The
  * reference's FilteredTDMACUDA object offers v1 and v2 side by side
  * (filtered_tdma_cuda.hpp:173-180); this lets one handle do the same. */
