@@ -347,9 +347,11 @@ int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, 
 // Generated-coefficient batch, only D read (the GEN modes of the tiled
 // kernel; the coefficient fields of `gen` are used, the rest is filled here).
 // Returns 1 when launched, 0 when the shape is not tiled, < 0 on error.
+// GEN 1 and 3 (one matrix for every system): `tab` is device scratch of
+// n_row * 5 + (n_row / 16) * 6 doubles for the shared elimination factors.
 template <int GEN, bool CYC = false>
 int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArgs& gen,
-                 unsigned* status, cudaStream_t st) {
+                 unsigned* status, cudaStream_t st, double* tab = nullptr) {
     const TilePlan pl = tile_plan(n_row, CYC, 8, 1);
     if (pl.sys == 0 || !tma_ok_elem(D, n_sys, 8)) return 0;
     const int nsc = pl.nseg / pl.cl;
@@ -367,6 +369,12 @@ int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArg
     a.accumulate = 0;
     a.gate = nullptr;
     a.status = status;
+    if constexpr (GEN == 1 || GEN == 3) {
+        if (!tab) return fail(BTDMA_ERR_ARG, "shared-matrix sweep without a factor table");
+        tile_table_kernel<GEN><<<(pl.nseg + 127) / 128, 128, 0, st>>>(a, tab);
+        CK(cudaGetLastError());
+        a.gtab = tab;
+    }
     int rc;
     switch (pl.sys) {
         case 128: rc = launch_tile_sys<128, CYC, double, double, GEN>(maps, a, st); break;
@@ -380,12 +388,14 @@ int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArg
 // Heat sweep: every row -cs, 1 + 2 cs, -cs; cs more on the diagonal of the
 // first and last row when cbound.
 int try_tile_const(const double* D, double* X, int n_sys, int n_row, double cs, bool cbound,
-                   unsigned* status, cudaStream_t st) {
+                   unsigned* status, cudaStream_t st, double* tab) {
     TileArgs g = {};
     g.cs = cs;
     g.cbound = cbound ? 1 : 0;
-    return try_tile_gen<1>(D, X, n_sys, n_row, g, status, st);
+    return try_tile_gen<1>(D, X, n_sys, n_row, g, status, st, tab);
 }
+
+size_t gen_table_doubles(int n_row) { return (size_t)n_row * 5 + (size_t)(n_row / 16 + 1) * 6; }
 
 template <bool CYCLIC>
 int launch_seg_method(int method, const CUtensorMap* maps, const SegArgs& a, int groups,
@@ -1172,6 +1182,7 @@ struct btdma_heat {
     double* buf1 = nullptr;  // Y sweep layout
     double* err = nullptr;   // L2 accumulator
     double* scratch = nullptr;  // full grid, the warm-up step before graph capture
+    double* tab = nullptr;      // shared elimination factors of one sweep
     unsigned* status = nullptr;
     cudaStream_t cap = nullptr;  // private stream the step graph is captured on
     cudaGraph_t graph = nullptr;
@@ -1189,17 +1200,17 @@ int heat_enqueue(btdma_heat_t h, double* theta, cudaStream_t st) {
     const dim3 gr((g.ix + 127) / 128, g.iy, g.iz);
     heat_rhs_z_kernel<<<gr, b1, 0, st>>>(theta, h->buf0, g);
     CK(cudaGetLastError());
-    int rc = try_tile_const(h->buf0, h->buf0, g.ix * g.iy, g.iz, g.bz, true, h->status, st);
+    int rc = try_tile_const(h->buf0, h->buf0, g.ix * g.iy, g.iz, g.bz, true, h->status, st, h->tab);
     if (rc != 1) return rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "Z sweep not tileable");
     heat_z_to_y_kernel<<<gr, b1, 0, st>>>(theta, h->buf0, h->buf1, g);
     CK(cudaGetLastError());
-    rc = try_tile_const(h->buf1, h->buf1, g.ix * g.iz, g.iy, g.by, true, h->status, st);
+    rc = try_tile_const(h->buf1, h->buf1, g.ix * g.iz, g.iy, g.by, true, h->status, st, h->tab);
     if (rc != 1) return rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "Y sweep not tileable");
     const dim3 bt(HEAT_TILE, 8, 1);
     heat_y_to_x_kernel<<<dim3((g.ix + HEAT_TILE - 1) / HEAT_TILE, (g.iy + HEAT_TILE - 1) / HEAT_TILE,
                               g.iz), bt, 0, st>>>(theta, h->buf1, h->buf0, g);
     CK(cudaGetLastError());
-    rc = try_tile_const(h->buf0, h->buf0, g.iy * g.iz, g.ix, g.bx, true, h->status, st);
+    rc = try_tile_const(h->buf0, h->buf0, g.iy * g.iz, g.ix, g.bx, true, h->status, st, h->tab);
     if (rc != 1) return rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "X sweep not tileable");
     heat_update_kernel<<<dim3((g.iy + HEAT_TILE - 1) / HEAT_TILE, (g.ix + HEAT_TILE - 1) / HEAT_TILE,
                               g.iz), bt, 0, st>>>(theta, h->buf0, g);
@@ -1265,6 +1276,7 @@ int btdma_heat_create(int ix, int iy, int iz, double dt, btdma_heat_t* out) {
     CKH(cudaMalloc(&h->buf1, sizeof(double) * inner));
     CKH(cudaMalloc(&h->err, sizeof(double)));
     CKH(cudaMalloc(&h->scratch, sizeof(double) * (size_t)(ix + 2) * (iy + 2) * (iz + 2)));
+    CKH(cudaMalloc(&h->tab, sizeof(double) * gen_table_doubles(std::max(ix, std::max(iy, iz)))));
     CKH(cudaMalloc(&h->status, sizeof(unsigned)));
     CKH(cudaMemset(h->status, 0, sizeof(unsigned)));
     CKH(cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking));
@@ -1303,6 +1315,7 @@ int btdma_heat_destroy(btdma_heat_t h) {
     cudaFree(h->buf1);
     cudaFree(h->err);
     cudaFree(h->scratch);
+    cudaFree(h->tab);
     cudaFree(h->status);
     delete h;
     return BTDMA_OK;
@@ -1378,18 +1391,18 @@ int btdma_heat_step_profile(btdma_heat_t h, double* theta, double* times, cudaSt
     cudaEventRecord(ev[0], stream);
     heat_rhs_z_kernel<<<gr, b1, 0, stream>>>(theta, h->buf0, g);
     cudaEventRecord(ev[1], stream);
-    if ((rc = try_tile_const(h->buf0, h->buf0, g.ix * g.iy, g.iz, g.bz, true, h->status, stream)) != 1)
+    if ((rc = try_tile_const(h->buf0, h->buf0, g.ix * g.iy, g.iz, g.bz, true, h->status, stream, h->tab)) != 1)
         return done(rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "Z sweep not tileable"));
     cudaEventRecord(ev[2], stream);
     heat_z_to_y_kernel<<<gr, b1, 0, stream>>>(theta, h->buf0, h->buf1, g);
     cudaEventRecord(ev[3], stream);
-    if ((rc = try_tile_const(h->buf1, h->buf1, g.ix * g.iz, g.iy, g.by, true, h->status, stream)) != 1)
+    if ((rc = try_tile_const(h->buf1, h->buf1, g.ix * g.iz, g.iy, g.by, true, h->status, stream, h->tab)) != 1)
         return done(rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "Y sweep not tileable"));
     cudaEventRecord(ev[4], stream);
     heat_y_to_x_kernel<<<dim3((g.ix + HEAT_TILE - 1) / HEAT_TILE, (g.iy + HEAT_TILE - 1) / HEAT_TILE,
                               g.iz), bt, 0, stream>>>(theta, h->buf1, h->buf0, g);
     cudaEventRecord(ev[5], stream);
-    if ((rc = try_tile_const(h->buf0, h->buf0, g.iy * g.iz, g.ix, g.bx, true, h->status, stream)) != 1)
+    if ((rc = try_tile_const(h->buf0, h->buf0, g.iy * g.iz, g.ix, g.bx, true, h->status, stream, h->tab)) != 1)
         return done(rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "X sweep not tileable"));
     cudaEventRecord(ev[6], stream);
     heat_update_kernel<<<dim3((g.iy + HEAT_TILE - 1) / HEAT_TILE, (g.ix + HEAT_TILE - 1) / HEAT_TILE,
@@ -1520,6 +1533,7 @@ struct btdma_momentum {
     double* tab = nullptr;  // [dir][comp][ta, tb, tc][n_dir rows]
     size_t tab_off[3][3] = {};
     double* buf = nullptr;  // nx * ny * nz, the sweep layout
+    double* gtab = nullptr; // shared elimination factors of one sweep
     unsigned* status = nullptr;
 };
 
@@ -1592,6 +1606,8 @@ int btdma_momentum_create(int nx, int ny, int nz, const double* dx0, const doubl
         cudaMemcpy(h->tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice) !=
             cudaSuccess ||
         cudaMalloc(&h->buf, sizeof(double) * (size_t)nx * ny * nz) != cudaSuccess ||
+        cudaMalloc(&h->gtab, sizeof(double) * gen_table_doubles(std::max(nx, std::max(ny, nz)))) !=
+            cudaSuccess ||
         cudaMalloc(&h->status, sizeof(unsigned)) != cudaSuccess ||
         cudaMemset(h->status, 0, sizeof(unsigned)) != cudaSuccess)
         return cleanup(fail(BTDMA_ERR_CUDA, "momentum buffers: %s",
@@ -1604,6 +1620,7 @@ int btdma_momentum_destroy(btdma_momentum_t h) {
     if (!h) return BTDMA_OK;
     cudaFree(h->tab);
     cudaFree(h->buf);
+    cudaFree(h->gtab);
     cudaFree(h->status);
     delete h;
     return BTDMA_OK;
@@ -1628,20 +1645,20 @@ int btdma_momentum_sweep(btdma_momentum_t h, int dir, int comp, const double* q,
         mom_gather_kernel<2><<<dim3((g.nx + 127) / 128, g.ny, g.nz), b1, 0, stream>>>(
             q, h->buf, g, comp == 2 ? 1 : 0);
         CK(cudaGetLastError());
-        rc = try_tile_gen<3, false>(h->buf, h->buf, n_sys, g.nz, t, h->status, stream);
+        rc = try_tile_gen<3, false>(h->buf, h->buf, n_sys, g.nz, t, h->status, stream, h->gtab);
     } else if (dir == 1) {
         mom_gather_kernel<1><<<dim3((g.nx + 127) / 128, g.nz, g.ny), b1, 0, stream>>>(q, h->buf,
                                                                                    g, 0);
         CK(cudaGetLastError());
-        rc = h->pbc[1] ? try_tile_gen<3, true>(h->buf, h->buf, n_sys, g.ny, t, h->status, stream)
-                       : try_tile_gen<3, false>(h->buf, h->buf, n_sys, g.ny, t, h->status, stream);
+        rc = h->pbc[1] ? try_tile_gen<3, true>(h->buf, h->buf, n_sys, g.ny, t, h->status, stream, h->gtab)
+                       : try_tile_gen<3, false>(h->buf, h->buf, n_sys, g.ny, t, h->status, stream, h->gtab);
     } else {
         mom_gather_x_kernel<<<dim3((g.nx + MOM_TILE - 1) / MOM_TILE,
                                    (g.ny + MOM_TILE - 1) / MOM_TILE, g.nz), bt, 0, stream>>>(
             q, h->buf, g);
         CK(cudaGetLastError());
-        rc = h->pbc[0] ? try_tile_gen<3, true>(h->buf, h->buf, n_sys, g.nx, t, h->status, stream)
-                       : try_tile_gen<3, false>(h->buf, h->buf, n_sys, g.nx, t, h->status, stream);
+        rc = h->pbc[0] ? try_tile_gen<3, true>(h->buf, h->buf, n_sys, g.nx, t, h->status, stream, h->gtab)
+                       : try_tile_gen<3, false>(h->buf, h->buf, n_sys, g.nx, t, h->status, stream, h->gtab);
     }
     if (rc != 1) return rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "sweep not tileable");
     if (dir == 2)

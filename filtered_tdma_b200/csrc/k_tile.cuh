@@ -85,6 +85,12 @@ struct TileArgs {
     const double* gb;
     const double* gc;
     const double* glam;
+    // GEN 1 and 3: every system of the batch has the same matrix, so the
+    // elimination of each sub-segment is computed once (tile_table_kernel) into
+    // gtab: per row [inv pivot, a * inv, pi, alpha, gamma] (n_row x 5), then
+    // per sub-segment [r, r c0, l0, u0, l1, u1] (nseg x 6); the solve runs the
+    // right-hand-side recurrences only
+    const double* gtab;
     int gpin;
     unsigned* status;
 };
@@ -164,6 +170,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     constexpr int RPS = tile_rps((int)sizeof(TIN));  // rows per ring stage
     constexpr int SPG = M / RPS;                      // stages per group
     constexpr bool CONSTC = GEN != 0;                 // coefficients generated, D only
+    constexpr bool SH = GEN == 1 || GEN == 3;         // one matrix for all systems (gtab)
     constexpr int NA = CONSTC ? 1 : 4;                // arrays per ring stage
     constexpr int RP = SYS + 1;  // padded pitch of red / xr rows
     extern __shared__ unsigned char smem_raw[];
@@ -298,6 +305,20 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 #pragma unroll
             for (int r = 0; r < RPS; ++r) {
                 const int k = j * RPS + r;
+                if constexpr (SH) {  // right-hand side only, factors from gtab
+                    const double* tr = args.gtab + (size_t)((c * nsc + ql) * M + k) * 5;
+                    const double d = (double)d2[r];
+                    if (k == 0) {
+                        db0 = d * tr[0];
+                    } else if (k == 1) {
+                        de[1] = d * tr[0];
+                        sd = de[1];
+                    } else {
+                        de[k] = d * tr[0] - tr[1] * de[k - 1];
+                        if (k <= M - 2) sd += tr[2] * de[k];
+                    }
+                    continue;
+                }
                 TC a, b, cc, d = (TC)d2[r];
                 if constexpr (GEN == 1) {
                     const int q = c * nsc + ql;  // sub-segment of this thread
@@ -354,7 +375,16 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             }
         }
         // reduced rows of this sub-segment -> red[f][ql][s]
-        {
+        if constexpr (SH) {
+            const double* sb = args.gtab + (size_t)args.n_row * 5 + (size_t)(c * nsc + ql) * 6;
+            double* w = red + ql * RP + s;
+            w[0 * fstride] = sb[2];
+            w[1 * fstride] = sb[3];
+            w[2 * fstride] = sb[0] * (double)db0 - sb[1] * (double)sd;
+            w[3 * fstride] = sb[4];
+            w[4 * fstride] = sb[5];
+            w[5 * fstride] = (double)de[M - 1];
+        } else {
             const TC pi_last = -ga[M - 2] * pi;
             const TC r0 = rcp_tc(TC(1) - cb0 * sa);
             double* w = red + ql * RP + s;
@@ -496,7 +526,12 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 #pragma unroll
             for (int k = M - 2; k >= 1; --k) {
                 xp -= ns;
-                xn = (double)de[k] - (double)al[k] * x_first - (double)ga[k] * xn;
+                if constexpr (SH) {
+                    const double* tr = args.gtab + (size_t)(q * M + k) * 5;
+                    xn = (double)de[k] - tr[3] * x_first - tr[4] * xn;
+                } else {
+                    xn = (double)de[k] - (double)al[k] * x_first - (double)ga[k] * xn;
+                }
                 nonfinite = fma(xn, 0.0, nonfinite);
                 *xp = acc ? xo[k] + xn : xn;
             }
@@ -512,6 +547,83 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         for (int i = 0; i < nst; ++i) mbar_wait_bounded(&full[i], 0, nullptr, 1u << 8);
     }
     if (cl > 1) tile_cluster_sync(cl);  // no CTA leaves while peers may touch its memory
+}
+
+// Coefficients (a, b, c) of row k of sub-segment q for the shared-matrix modes,
+// as the solve generates them.
+template <int GEN>
+__device__ __forceinline__ void tile_gen_row(const TileArgs& args, int q, int k, double& a,
+                                             double& b, double& c) {
+    if constexpr (GEN == 1) {
+        const bool wall =
+            args.cbound != 0 && ((q == 0 && k == 0) || (q == args.nseg - 1 && k == TILE_MT - 1));
+        a = -args.cs;
+        c = -args.cs;
+        b = 1.0 + 2.0 * args.cs + (wall ? args.cs : 0.0);
+    } else {
+        const int kg = q * TILE_MT + k;
+        a = -args.cs * args.ga[kg];
+        c = -args.cs * args.gc[kg];
+        b = 1.0 + args.cs * args.gb[kg];
+    }
+}
+
+// The elimination of every sub-segment of the shared matrix (the steps of the
+// tiled kernel's forward pass and reduced-row formation without the right-hand
+// side): one thread per sub-segment.
+template <int GEN>
+__global__ void tile_table_kernel(const TileArgs args, double* __restrict__ tab) {
+    constexpr int M = TILE_MT;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= args.nseg) return;
+    double* sub = tab + (size_t)args.n_row * 5 + (size_t)q * 6;
+    double ab0 = 0, cb0 = 0, sa = 0, pi = 1.0, alp = 0, gap = 0, gm2 = 0;
+    for (int k = 0; k < M; ++k) {
+        double a, b, c;
+        tile_gen_row<GEN>(args, q, k, a, b, c);
+        double* tr = tab + (size_t)(q * M + k) * 5;
+        if (k == 0) {
+            const double ib = rcp_nr(b);
+            ab0 = a * ib;
+            cb0 = c * ib;
+            tr[0] = ib;
+            tr[1] = tr[2] = tr[3] = tr[4] = 0.0;
+            continue;
+        }
+        double al, ga, inv;
+        if (k == 1) {
+            inv = rcp_nr(b);
+            al = a * inv;
+            ga = c * inv;
+            sa = al;
+            tr[1] = 0.0;
+            tr[2] = 1.0;
+        } else {
+            inv = rcp_nr(b - a * gap);
+            ga = c * inv;
+            al = -a * alp * inv;
+            tr[1] = a * inv;
+            if (k <= M - 2) {
+                pi = -gap * pi;
+                sa += pi * al;
+            }
+            tr[2] = pi;
+        }
+        tr[0] = inv;
+        tr[3] = al;
+        tr[4] = ga;
+        if (k == M - 2) gm2 = ga;
+        alp = al;
+        gap = ga;
+    }
+    const double pi_last = -gm2 * pi;
+    const double rr = rcp_nr(1.0 - cb0 * sa);
+    sub[0] = rr;
+    sub[1] = rr * cb0;
+    sub[2] = rr * ab0;
+    sub[3] = rr * cb0 * pi_last;
+    sub[4] = alp;
+    sub[5] = gap;
 }
 
 }  // namespace btdma

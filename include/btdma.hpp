@@ -277,3 +277,90 @@ class TdmaBackendGPU {
     std::unique_ptr<FilteredTDMACUDA> filt_;
     std::unique_ptr<PaScaLTDMACUDA> pasc_;
 };
+
+// ------------------------------------------------------------------------
+// RAII wrappers of the components with no reference class of their own
+// (ragged batches, the fused heat step, the channel Poisson and momentum
+// sweeps); each owns one C-ABI handle and throws btdma::Error on failure.
+namespace btdma {
+
+class HeatADI {
+   public:
+    HeatADI(int ix, int iy, int iz, double dt) { check(btdma_heat_create(ix, iy, iz, dt, &h_)); }
+    ~HeatADI() { btdma_heat_destroy(h_); }
+    HeatADI(const HeatADI&) = delete;
+    HeatADI& operator=(const HeatADI&) = delete;
+    void init(double* d_theta, cudaStream_t s = 0) { check(btdma_heat_init(h_, d_theta, s)); }
+    void step(double* d_theta, int n_steps, bool graph = true, cudaStream_t s = 0) {
+        check(btdma_heat_step(h_, d_theta, n_steps, graph ? 1 : 0, s));
+    }
+    double l2_error(const double* d_theta, double t_phys) {
+        double l2 = 0.0;
+        check(btdma_heat_l2_error(h_, d_theta, t_phys, &l2));
+        return l2;
+    }
+
+   private:
+    btdma_heat_t h_ = nullptr;
+};
+
+class ChannelPoisson {
+   public:
+    ChannelPoisson(int nz, const double* dz, const double* dmz, int n_modes, const double* lambda,
+                   bool pin_mode0 = true) {
+        check(btdma_poisson_create(nz, dz, dmz, n_modes, lambda, pin_mode0 ? 1 : 0, &h_));
+    }
+    ~ChannelPoisson() { btdma_poisson_destroy(h_); }
+    ChannelPoisson(const ChannelPoisson&) = delete;
+    ChannelPoisson& operator=(const ChannelPoisson&) = delete;
+    // d_hat: complex [nz][n_modes] as interleaved doubles, in place
+    void solve(double* d_hat, cudaStream_t s = 0) { check(btdma_poisson_solve(h_, d_hat, s)); }
+
+   private:
+    btdma_poisson_t h_ = nullptr;
+};
+
+class ChannelMomentum {
+   public:
+    ChannelMomentum(int nx, int ny, int nz, const double* dx0, const double* dmx0,
+                    const double* dx1, const double* dmx1, const double* dx2, const double* dmx2,
+                    bool pbc_x, bool pbc_y) {
+        check(btdma_momentum_create(nx, ny, nz, dx0, dmx0, dx1, dmx1, dx2, dmx2, pbc_x ? 1 : 0,
+                                    pbc_y ? 1 : 0, &h_));
+    }
+    ~ChannelMomentum() { btdma_momentum_destroy(h_); }
+    ChannelMomentum(const ChannelMomentum&) = delete;
+    ChannelMomentum& operator=(const ChannelMomentum&) = delete;
+    void adi(int comp, double* d_rhs, double* d_q, double nu_dt_half, cudaStream_t s = 0) {
+        check(btdma_momentum_adi(h_, comp, d_rhs, d_q, nu_dt_half, s));
+    }
+
+   private:
+    btdma_momentum_t h_ = nullptr;
+};
+
+// Ragged (CSR) batches through a PaScaL handle of the given storage precision.
+class RaggedSolver {
+   public:
+    explicit RaggedSolver(int n_sys, int precision = BTDMA_FP64) {
+        check(btdma_create(BTDMA_PASCAL, n_sys, 64, 2, precision, 0, &h_));
+    }
+    ~RaggedSolver() { btdma_destroy(h_); }
+    RaggedSolver(const RaggedSolver&) = delete;
+    RaggedSolver& operator=(const RaggedSolver&) = delete;
+    void solve(const double* A, const double* B, const double* C, const double* D, double* X,
+               const long long* row_offsets, const unsigned char* periodic, int n_sys,
+               cudaStream_t s = 0) {
+        check(btdma_solve_ragged(h_, A, B, C, D, X, row_offsets, periodic, n_sys, s));
+    }
+    void autotune(const double* A, const double* B, const double* C, const double* D, double* X,
+                  const long long* row_offsets, const unsigned char* periodic, int n_sys,
+                  cudaStream_t s = 0) {
+        check(btdma_ragged_autotune(h_, A, B, C, D, X, row_offsets, periodic, n_sys, s));
+    }
+
+   private:
+    btdma_t h_ = nullptr;
+};
+
+}  // namespace btdma

@@ -1,8 +1,9 @@
 // Compiles the C++ drop-in header the way a reference caller would use it and,
 // when run on a GPU, solves the heat 64-row sweep through TdmaBackendGPU,
-// PaScaLTDMACUDA and FilteredTDMACUDA.  Prints one line per solve:
+// PaScaLTDMACUDA and FilteredTDMACUDA, then the fused heat step and a ragged
+// batch through the RAII wrappers.  Prints one line per solve:
 //   <name> <max |x|> <status>
-// tests/test_gpu_dropin.py compares the solutions with the oracle.
+// tests/test_cpp_dropin.py compares the solutions with the oracle.
 #include <cuda_runtime_api.h>
 
 #include <cmath>
@@ -79,6 +80,39 @@ int main(int argc, char** argv) {
         f.solve_cycl_filtered_v2(dA, dB, dC, dD);
         report("filtered_v2_cyclic");
         std::printf("J %d\n", f.last_J());
+
+        // the fused heat step of the reference's order-accuracy run (32^3,
+        // rho = 0.25, one step) through the C++ wrapper
+        {
+            const int g = 32;
+            const double dx = 2.0 / g, rho = 0.25;
+            const double dt = rho / (1.0 - 2.0 * rho) * (2.0 * dx * dx);
+            double* th;
+            cudaMalloc((void**)&th, sizeof(double) * (g + 2) * (g + 2) * (g + 2));
+            btdma::HeatADI heat(g, g, g, dt);
+            heat.init(th);
+            heat.step(th, 1);
+            std::printf("heat_l2 %.9g\n", heat.l2_error(th, dt));
+            cudaFree(th);
+        }
+        // a small ragged batch: two systems of 5 and 40 rows, the second periodic
+        {
+            const long long off[3] = {0, 5, 45};
+            const unsigned char per[2] = {0, 1};
+            std::vector<double> ra(45, -1.0), rb(45, 4.0), rc(45, -1.0), rd(45, 1.0), rx(45);
+            double *qa, *qb, *qc, *qd, *qx;
+            for (double** p : {&qa, &qb, &qc, &qd, &qx}) cudaMalloc((void**)p, 45 * 8);
+            cudaMemcpy(qa, ra.data(), 45 * 8, cudaMemcpyHostToDevice);
+            cudaMemcpy(qb, rb.data(), 45 * 8, cudaMemcpyHostToDevice);
+            cudaMemcpy(qc, rc.data(), 45 * 8, cudaMemcpyHostToDevice);
+            cudaMemcpy(qd, rd.data(), 45 * 8, cudaMemcpyHostToDevice);
+            btdma::RaggedSolver rs(2);
+            rs.solve(qa, qb, qc, qd, qx, off, per, 2);
+            cudaMemcpy(rx.data(), qx, 45 * 8, cudaMemcpyDeviceToHost);
+            // periodic system of constant rows: x = 1 / (4 - 2) everywhere
+            std::printf("ragged_periodic_x %.17g\n", rx[20]);
+            for (double* p : {qa, qb, qc, qd, qx}) cudaFree(p);
+        }
     } catch (const btdma::Error& e) {
         std::fprintf(stderr, "%s\n", e.what());
         return 2;
