@@ -211,8 +211,21 @@ struct TilePlan {
     int sys = 0, cl = 0, nst = 0, nseg = 0;
 };
 
+int max_smem_per_sm() {
+    static int v = -1;
+    if (v < 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) !=
+            cudaSuccess)
+            v = 0;
+    }
+    return v;
+}
+
 // na: arrays per ring stage (4, or 1 for the constant-coefficient D-only ring).
-TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4) {
+// sh: shared-matrix sweep (factor table in shared memory, two CTAs per SM).
+TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4, bool sh = false) {
     TilePlan pl;
     if (n_row % TILE_MT != 0) return pl;
     const int nseg = n_row / TILE_MT;
@@ -240,8 +253,11 @@ TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4) {
         if (cl == 0) return pl;
     }
     int nst = na == 4 ? TILE_MAX_NST : TILE_MAX_NST_CONST;
-    while (nst >= 3 && tile_smem_bytes(sys, nseg / cl, nseg, sys / cl, nst, elem, na) >
-                           (size_t)max_smem_optin())
+    // two CTAs per SM for shared-matrix sweeps: half an SM's shared memory each
+    // (less 1 KB the runtime reserves per CTA)
+    const size_t cap = sh && cl == 1 ? (size_t)max_smem_per_sm() / 2 - 1024 : (size_t)max_smem_optin();
+    while (nst >= 3 &&
+           tile_smem_bytes(sys, nseg / cl, nseg, sys / cl, nst, elem, na, sh) > cap)
         --nst;
     if (nst < 3) return pl;
     pl.sys = sys;
@@ -264,8 +280,9 @@ int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st)
     const int threads = SYS * a.nseg / a.cl;
     cudaLaunchConfig_t cfg = {};
     cfg.blockDim = dim3(threads, 1, 1);
+    constexpr bool SHT = GEN == 1 || GEN == 3;
     cfg.dynamicSmemBytes = tile_smem_bytes(SYS, a.nseg / a.cl, a.nseg, SYS / a.cl, a.nst,
-                                           (int)sizeof(TIN), GEN ? 1 : 4);
+                                           (int)sizeof(TIN), GEN ? 1 : 4, SHT);
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -275,6 +292,12 @@ int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st)
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int clusters = num_sms();
+    if (SHT && a.cl == 1) {  // built for two CTAs per SM
+        int nb = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, threads,
+                                                         cfg.dynamicSmemBytes));
+        clusters = num_sms() * std::max(1, nb);
+    }
     if (a.cl > 1) {
         cfg.gridDim = dim3(a.cl * num_sms(), 1, 1);
         int nc = 0;
@@ -352,7 +375,7 @@ int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, 
 template <int GEN, bool CYC = false>
 int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArgs& gen,
                  unsigned* status, cudaStream_t st, double* tab = nullptr) {
-    const TilePlan pl = tile_plan(n_row, CYC, 8, 1);
+    const TilePlan pl = tile_plan(n_row, CYC, 8, 1, GEN == 1 || GEN == 3);
     if (pl.sys == 0 || !tma_ok_elem(D, n_sys, 8)) return 0;
     const int nsc = pl.nseg / pl.cl;
     CUtensorMap maps[4];

@@ -127,9 +127,16 @@ __host__ __device__ __forceinline__ size_t tile_ring_bytes(int sys, int nsc, int
                                                            int na = 4) {
     return (size_t)nst * na * tile_rps(elem) * sys * nsc * elem;
 }
+// Shared-matrix table slice of one CTA (its nsc sub-segments): per row 5 and
+// per sub-segment 6 doubles.
+__host__ __device__ __forceinline__ size_t tile_tab_doubles(int nsc) {
+    return (size_t)nsc * TILE_MT * 5 + (size_t)nsc * 6;
+}
 __host__ __device__ __forceinline__ size_t tile_smem_bytes(int sys, int nsc, int nseg, int sub,
-                                                           int nst, int elem = 8, int na = 4) {
+                                                           int nst, int elem = 8, int na = 4,
+                                                           bool shared_tab = false) {
     return tile_ring_bytes(sys, nsc, nst, elem, na) +
+           (shared_tab ? tile_tab_doubles(nsc) * sizeof(double) : 0) +
            tile_fixed_doubles(sys, nsc, nseg, sub) * sizeof(double) +
            2ull * nst * sizeof(uint64_t) + 128;
 }
@@ -160,8 +167,10 @@ __device__ __forceinline__ void tile_cluster_sync(int cl) {
 // the local sweeps — double (FP32 storage is widened exactly on load), or float
 // (the FP32 inner solve of iterative refinement).  The reduced system, the back
 // substitution and x are always FP64.
+// Shared-matrix instantiations (GEN 1, 3) hold no per-row matrix state, so they
+// are built for two CTAs per SM (64 registers a thread).
 template <int SYS, bool CYCLIC, typename TIN = double, typename TC = double, int GEN = 0>
-__global__ void __launch_bounds__(TILE_MAX_THREADS, 1)
+__global__ void __launch_bounds__(TILE_MAX_THREADS, (GEN == 1 || GEN == 3) ? 2 : 1)
 tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 const __grid_constant__ CUtensorMap tmC, const __grid_constant__ CUtensorMap tmD,
                 const TileArgs args) {
@@ -188,7 +197,8 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     double* xr = red + 6 * fstride;
     double* pcr = xr + 2 * fstride;  // only when !shuffled
     const int gs = nseg + 2;
-    uint64_t* full = reinterpret_cast<uint64_t*>(pcr + (shuffled ? 0 : 6 * gs * sub));
+    double* tabs = pcr + (shuffled ? 0 : 6 * gs * sub);  // SH: this CTA's factor table
+    uint64_t* full = reinterpret_cast<uint64_t*>(tabs + (SH ? tile_tab_doubles(nsc) : 0));
     uint64_t* empty = full + nst;
 
     const int tid = threadIdx.x;
@@ -208,6 +218,13 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             mbar_init(&empty[i], nwarps);
         }
         fence_mbar_init();
+    }
+    if constexpr (SH) {  // rows of this CTA's sub-segments, then their reduced-row factors
+        const int c0 = (cl > 1 ? (int)cg::this_cluster().block_rank() : 0) * nsc;
+        const double* g0 = args.gtab + (size_t)c0 * M * 5;
+        for (int i = threadIdx.x; i < nsc * M * 5; i += blockDim.x) tabs[i] = g0[i];
+        const double* g1 = args.gtab + (size_t)args.n_row * 5 + (size_t)c0 * 6;
+        for (int i = threadIdx.x; i < nsc * 6; i += blockDim.x) tabs[nsc * M * 5 + i] = g1[i];
     }
     if (!shuffled && tid < sub) {  // zero guard rows of the PCR buffers
         for (int f = 0; f < 6; ++f) {
@@ -306,7 +323,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             for (int r = 0; r < RPS; ++r) {
                 const int k = j * RPS + r;
                 if constexpr (SH) {  // right-hand side only, factors from gtab
-                    const double* tr = args.gtab + (size_t)((c * nsc + ql) * M + k) * 5;
+                    const double* tr = tabs + (ql * M + k) * 5;
                     const double d = (double)d2[r];
                     if (k == 0) {
                         db0 = d * tr[0];
@@ -376,7 +393,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         }
         // reduced rows of this sub-segment -> red[f][ql][s]
         if constexpr (SH) {
-            const double* sb = args.gtab + (size_t)args.n_row * 5 + (size_t)(c * nsc + ql) * 6;
+            const double* sb = tabs + nsc * M * 5 + ql * 6;
             double* w = red + ql * RP + s;
             w[0 * fstride] = sb[2];
             w[1 * fstride] = sb[3];
@@ -527,7 +544,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             for (int k = M - 2; k >= 1; --k) {
                 xp -= ns;
                 if constexpr (SH) {
-                    const double* tr = args.gtab + (size_t)(q * M + k) * 5;
+                    const double* tr = tabs + (ql * M + k) * 5;
                     xn = (double)de[k] - tr[3] * x_first - tr[4] * xn;
                 } else {
                     xn = (double)de[k] - (double)al[k] * x_first - (double)ga[k] * xn;
