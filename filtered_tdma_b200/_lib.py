@@ -30,6 +30,7 @@ EXPORTS = (
     "btdma_heat_step", "btdma_heat_l2_error", "btdma_heat_step_profile", "btdma_poisson_create", "btdma_poisson_destroy",
     "btdma_poisson_solve", "btdma_poisson_status", "btdma_momentum_create",
     "btdma_momentum_destroy", "btdma_momentum_sweep", "btdma_momentum_adi", "btdma_momentum_status",
+    "btdma_selftest_wait_timeout",
 )
 NOALLOC_MAX_ELEMS = 1 << 20
 REFINE_MAX_SWEEPS = 4
@@ -112,6 +113,7 @@ def lib():
         L.btdma_momentum_sweep.argtypes = [vp, i, i, vp, vp, d, vp]
         L.btdma_momentum_adi.argtypes = [vp, i, vp, vp, d, vp]
         L.btdma_momentum_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint), vp]
+        L.btdma_selftest_wait_timeout.argtypes = [i, ctypes.POINTER(ctypes.c_uint), vp]
         L.btdma_last_error.restype = ctypes.c_char_p
         for name in EXPORTS:
             if name != "btdma_last_error":

@@ -1714,3 +1714,38 @@ int btdma_momentum_status(btdma_momentum_t h, unsigned* status, cudaStream_t str
     CK(cudaStreamSynchronize(stream));
     return BTDMA_OK;
 }
+
+// ------------------------------------------------------------- self test
+namespace {
+
+// One thread waits, with the library's bounded wait, on an mbarrier that
+// nothing ever arrives at: the wait must give up after `limit` polls and
+// raise ST_TIMEOUT in the status word (the path every pipeline wait takes
+// when a transfer never lands), leaving the context usable.
+__global__ void selftest_wait_kernel(unsigned* status, uint32_t limit) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) (void)mbar_wait_bounded(&bar, 0, status, limit);
+}
+
+}  // namespace
+
+int btdma_selftest_wait_timeout(int limit, unsigned* status_out, cudaStream_t stream) {
+    if (limit <= 0 || limit > (1 << 16) || !status_out)
+        return fail(BTDMA_ERR_ARG, "limit in [1, 65536] and an output word are required");
+    unsigned* d = nullptr;
+    CK(cudaMalloc(&d, sizeof(unsigned)));
+    cudaMemsetAsync(d, 0, sizeof(unsigned), stream);
+    selftest_wait_kernel<<<1, 32, 0, stream>>>(d, (uint32_t)limit);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(status_out, d, sizeof(unsigned),
+                                              cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    cudaFree(d);
+    CK(e);
+    return BTDMA_OK;
+}

@@ -301,6 +301,14 @@ int btdma_momentum_adi(btdma_momentum_t h, int comp, double* rhs, double* q_out,
                        cudaStream_t stream);
 int btdma_momentum_status(btdma_momentum_t h, unsigned* status, cudaStream_t stream);
 
+/* Self test of the failure path of every pipeline wait: a one-thread kernel
+ * waits with the library's bounded wait (at most `limit` polls of up to 20 us)
+ * on an mbarrier nothing arrives at; *status_out receives the device status
+ * word, which must have BTDMA_STATUS_TIMEOUT set.  No fault, no hang. */
+#define BTDMA_STATUS_TIMEOUT 1u
+#define BTDMA_STATUS_NONFINITE 2u
+int btdma_selftest_wait_timeout(int limit, unsigned* status_out, cudaStream_t stream);
+
 /* Switch the method of an existing handle (rho, eps and J state are kept).  The
  * reference's FilteredTDMACUDA object offers v1 and v2 side by side
  * (filtered_tdma_cuda.hpp:173-180); this lets one handle do the same. */
