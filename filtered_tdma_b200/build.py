@@ -16,7 +16,7 @@ import sys
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libbtdma.so")
-SOURCES = [os.path.join(PKG, "csrc", "btdma_api.cu")]
+SOURCES = [os.path.join(PKG, "csrc", f) for f in ("btdma_api.cu", "btdma_ragged.cu", "btdma_apps.cu")]
 DEPS = SOURCES + [os.path.join(PKG, "csrc", f) for f in os.listdir(os.path.join(PKG, "csrc"))
                   if f != "width_probe.cu"] + [
     os.path.join(ROOT, "include", "btdma.h")]
@@ -43,12 +43,30 @@ def stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every translation unit to an object in parallel, then link."""
     if force or stale():
-        cmd = ["nvcc", *NVCC_FLAGS, "-o", LIB, *SOURCES]
-        if verbose:
-            cmd.insert(1, "-Xptxas=-v")
-            print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+        from concurrent.futures import ThreadPoolExecutor
+        obj_dir = os.path.join(PKG, "_build")
+        os.makedirs(obj_dir, exist_ok=True)
+        compile_flags = [f for f in NVCC_FLAGS if f not in ("-shared",)]
+        compile_flags = [f for f in compile_flags if f not in ("-cudart", "static")]
+        compile_flags = [f for f in compile_flags
+                         if f not in ("-Xlinker", "--exclude-libs=ALL")]
+
+        def one(src):
+            obj = os.path.join(obj_dir, os.path.basename(src).replace(".cu", ".o"))
+            cmd = ["nvcc", *compile_flags, "-c", "-o", obj, src]
+            if verbose:
+                cmd.insert(1, "-Xptxas=-v")
+                print(" ".join(cmd))
+            subprocess.run(cmd, check=True)
+            return obj
+
+        with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+            objs = list(ex.map(one, SOURCES))
+        link = ["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-cudart",
+                "static", "-Xlinker", "--exclude-libs=ALL", "-o", LIB, *objs]
+        subprocess.run(link, check=True)
     return LIB
 
 

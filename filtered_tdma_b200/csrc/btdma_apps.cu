@@ -1,0 +1,525 @@
+// C ABI of the application steps built on the tiled solve with generated
+// coefficients: the fused heat ADI step, the channel Poisson wall-normal
+// solve and the channel momentum ADI sweeps (declared in include/btdma.h).
+#include <cmath>
+#include <cstring>
+
+#include "btdma_host.cuh"
+#include "k_heat.cuh"
+#include "k_momentum.cuh"
+
+// ------------------------------------------------------------- heat ADI step
+struct btdma_heat {
+    HeatGeom g{};
+    double* xc = nullptr;  // device coordinates (ghosts included)
+    double* yc = nullptr;
+    double* zc = nullptr;
+    double* cosx = nullptr;  // cos(pi x) etc. at the cell centres
+    double* cosy = nullptr;
+    double* cosz = nullptr;
+    double* buf0 = nullptr;  // Z and X sweep layouts
+    double* buf1 = nullptr;  // Y sweep layout
+    double* err = nullptr;   // L2 accumulator
+    double* scratch = nullptr;  // full grid, the warm-up step before graph capture
+    double* tab = nullptr;      // shared elimination factors of one sweep
+    unsigned* status = nullptr;
+    cudaStream_t cap = nullptr;  // private stream the step graph is captured on
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    double* graph_theta = nullptr;  // theta the graph was captured for
+    cudaStream_t last_stream = nullptr;
+};
+
+namespace {
+
+// One step as a kernel sequence on stream st (no host sync): right-hand side,
+// then per direction a solve with generated coefficients and the re-layout
+// for the next direction.  ev (optional): 8 events recorded around the phases
+// (the profiled step).
+int heat_enqueue(btdma_heat_t h, double* theta, cudaStream_t st, cudaEvent_t* ev = nullptr) {
+    const HeatGeom& g = h->g;
+    auto mark = [&](int i) {
+        if (ev) cudaEventRecord(ev[i], st);
+    };
+    auto sweep = [&](double* buf, int n_sys, int n_row, double base, const char* name) {
+        const int rc = try_tile_const(buf, buf, n_sys, n_row, base, true, h->status, st, h->tab);
+        return rc == 1 ? BTDMA_OK
+                       : (rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "%s sweep not tileable", name));
+    };
+    const dim3 b1(128, 1, 1), gr((g.ix + 127) / 128, g.iy, g.iz), bt(HEAT_TILE, 8, 1);
+    const int tx = (g.ix + HEAT_TILE - 1) / HEAT_TILE, ty = (g.iy + HEAT_TILE - 1) / HEAT_TILE;
+    int rc;
+    mark(0);
+    heat_rhs_z_kernel<<<gr, b1, 0, st>>>(theta, h->buf0, g);
+    CK(cudaGetLastError());
+    mark(1);
+    if ((rc = sweep(h->buf0, g.ix * g.iy, g.iz, g.bz, "Z"))) return rc;
+    mark(2);
+    heat_z_to_y_kernel<<<gr, b1, 0, st>>>(theta, h->buf0, h->buf1, g);
+    CK(cudaGetLastError());
+    mark(3);
+    if ((rc = sweep(h->buf1, g.ix * g.iz, g.iy, g.by, "Y"))) return rc;
+    mark(4);
+    heat_y_to_x_kernel<<<dim3(tx, ty, g.iz), bt, 0, st>>>(theta, h->buf1, h->buf0, g);
+    CK(cudaGetLastError());
+    mark(5);
+    if ((rc = sweep(h->buf0, g.iy * g.iz, g.ix, g.bx, "X"))) return rc;
+    mark(6);
+    heat_update_kernel<<<dim3(ty, tx, g.iz), bt, 0, st>>>(theta, h->buf0, g);
+    CK(cudaGetLastError());
+    mark(7);
+    return BTDMA_OK;
+}
+
+}  // namespace
+
+int btdma_heat_create(int ix, int iy, int iz, double dt, btdma_heat_t* out) {
+    if (!out) return fail(BTDMA_ERR_ARG, "null output handle");
+    *out = nullptr;
+    if (ix <= 0 || iy <= 0 || iz <= 0 || !(dt > 0.0))
+        return fail(BTDMA_ERR_ARG, "grid sizes and dt must be positive");
+    if (ix % 16 || iy % 16 || iz % 16)
+        return fail(BTDMA_ERR_UNSUPPORTED, "the fused step needs ix, iy, iz multiples of 16");
+    if ((long long)(ix + 2) * (iy + 2) >= (1LL << 31) || (long long)ix * iy >= (1LL << 31) ||
+        (long long)ix * iz >= (1LL << 31) || (long long)iy * iz >= (1LL << 31))
+        return fail(BTDMA_ERR_SIZE, "grid planes above 2^31 cells");
+    if (!tile_plan(iz, false, 8, 1).sys || !tile_plan(iy, false, 8, 1).sys ||
+        !tile_plan(ix, false, 8, 1).sys)
+        return fail(BTDMA_ERR_UNSUPPORTED, "grid not supported by the tiled solve");
+    btdma_heat* h = new btdma_heat();
+    auto cleanup = [&](int code) {
+        btdma_heat_destroy(h);
+        return code;
+    };
+#define CKH(call)                                                                          \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return cleanup(fail(BTDMA_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_))); \
+    } while (0)
+    // cell centres with one ghost each side, x_c[i] = x0 + dd/2 + (i - 1) dd on
+    // [-1, 1] with dd = 2 / n (mpi_subdomain.cpp mesh(), one rank)
+    auto coords = [](int n) {
+        std::vector<double> c(n + 2);
+        const double dd = 2.0 / n;
+        for (int i = 0; i < n + 2; ++i) c[i] = -1.0 + dd / 2.0 + (i - 1) * dd;
+        return c;
+    };
+    const auto hx = coords(ix), hy = coords(iy), hz = coords(iz);
+    auto cosines = [](const std::vector<double>& c) {
+        std::vector<double> o(c.size());
+        for (size_t i = 0; i < c.size(); ++i) o[i] = std::cos(HEAT_PI * c[i]);
+        return o;
+    };
+    const auto kx = cosines(hx), ky = cosines(hy), kz = cosines(hz);
+    auto upload = [&](double** dst, const std::vector<double>& v) {
+        cudaError_t e = cudaMalloc(dst, sizeof(double) * v.size());
+        if (e == cudaSuccess)
+            e = cudaMemcpy(*dst, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice);
+        return e;
+    };
+    CKH(upload(&h->xc, hx));
+    CKH(upload(&h->yc, hy));
+    CKH(upload(&h->zc, hz));
+    CKH(upload(&h->cosx, kx));
+    CKH(upload(&h->cosy, ky));
+    CKH(upload(&h->cosz, kz));
+    const size_t inner = (size_t)ix * iy * iz;
+    CKH(cudaMalloc(&h->buf0, sizeof(double) * inner));
+    CKH(cudaMalloc(&h->buf1, sizeof(double) * inner));
+    CKH(cudaMalloc(&h->err, sizeof(double)));
+    CKH(cudaMalloc(&h->scratch, sizeof(double) * (size_t)(ix + 2) * (iy + 2) * (iz + 2)));
+    CKH(cudaMalloc(&h->tab, sizeof(double) * gen_table_doubles(std::max(ix, std::max(iy, iz)))));
+    CKH(cudaMalloc(&h->status, sizeof(unsigned)));
+    CKH(cudaMemset(h->status, 0, sizeof(unsigned)));
+    CKH(cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking));
+#undef CKH
+    HeatGeom& g = h->g;
+    g.ix = ix;
+    g.iy = iy;
+    g.iz = iz;
+    g.dt = dt;
+    const double dx = 2.0 / ix, dy = 2.0 / iy, dz = 2.0 / iz;
+    g.bx = dt / (2.0 * dx * dx);  // stencil base, stencil_coeffs.hpp:10-13
+    g.by = dt / (2.0 * dy * dy);
+    g.bz = dt / (2.0 * dz * dz);
+    g.xc = h->xc;
+    g.yc = h->yc;
+    g.zc = h->zc;
+    g.cx = h->cosx;
+    g.cy = h->cosy;
+    g.cz = h->cosz;
+    *out = h;
+    return BTDMA_OK;
+}
+
+int btdma_heat_destroy(btdma_heat_t h) {
+    if (!h) return BTDMA_OK;
+    if (h->exec) cudaGraphExecDestroy(h->exec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    if (h->cap) cudaStreamDestroy(h->cap);
+    cudaFree(h->xc);
+    cudaFree(h->yc);
+    cudaFree(h->zc);
+    cudaFree(h->cosx);
+    cudaFree(h->cosy);
+    cudaFree(h->cosz);
+    cudaFree(h->buf0);
+    cudaFree(h->buf1);
+    cudaFree(h->err);
+    cudaFree(h->scratch);
+    cudaFree(h->tab);
+    cudaFree(h->status);
+    delete h;
+    return BTDMA_OK;
+}
+
+int btdma_heat_init(btdma_heat_t h, double* theta, cudaStream_t stream) {
+    if (!h || !theta) return fail(BTDMA_ERR_ARG, "null argument");
+    const HeatGeom& g = h->g;
+    heat_init_kernel<<<dim3((g.ix + 2 + 127) / 128, g.iy + 2, g.iz + 2), 128, 0, stream>>>(theta,
+                                                                                           g);
+    CK(cudaGetLastError());
+    h->last_stream = stream;
+    return BTDMA_OK;
+}
+
+int btdma_heat_step(btdma_heat_t h, double* theta, int n_steps, int use_graph,
+                    cudaStream_t stream) {
+    if (!h || !theta) return fail(BTDMA_ERR_ARG, "null argument");
+    if (n_steps < 0) return fail(BTDMA_ERR_ARG, "n_steps must be >= 0");
+    h->last_stream = stream;
+    if (!use_graph) {
+        for (int s = 0; s < n_steps; ++s) {
+            const int rc = heat_enqueue(h, theta, stream);
+            if (rc) return rc;
+        }
+        return BTDMA_OK;
+    }
+    if (!h->exec || h->graph_theta != theta) {
+        if (h->exec) cudaGraphExecDestroy(h->exec);
+        if (h->graph) cudaGraphDestroy(h->graph);
+        h->exec = nullptr;
+        h->graph = nullptr;
+        // one uncaptured step on a zeroed scratch field first, so the kernels'
+        // first-use attribute calls stay out of the capture (theta is untouched)
+        const HeatGeom& g = h->g;
+        CK(cudaMemsetAsync(h->scratch, 0, sizeof(double) * (size_t)(g.ix + 2) * (g.iy + 2) *
+                                              (g.iz + 2), h->cap));
+        int rc = heat_enqueue(h, h->scratch, h->cap);
+        if (rc) return rc;
+        CK(cudaStreamSynchronize(h->cap));
+        // capture on the private stream, after the caller's stream has reached
+        // this point (the graph is launched on the caller's stream below)
+        CK(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
+        rc = heat_enqueue(h, theta, h->cap);
+        cudaGraph_t gr = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(h->cap, &gr);
+        if (rc) {
+            if (gr) cudaGraphDestroy(gr);
+            return rc;
+        }
+        CK(e);
+        h->graph = gr;
+        CK(cudaGraphInstantiate(&h->exec, gr, 0));
+        h->graph_theta = theta;
+    }
+    for (int s = 0; s < n_steps; ++s) CK(cudaGraphLaunch(h->exec, stream));
+    return BTDMA_OK;
+}
+
+int btdma_heat_step_profile(btdma_heat_t h, double* theta, double* times, cudaStream_t stream) {
+    if (!h || !theta || !times) return fail(BTDMA_ERR_ARG, "null argument");
+    cudaEvent_t ev[8] = {};
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    int rc = heat_enqueue(h, theta, stream, ev);
+    if (!rc && cudaEventSynchronize(ev[7]) != cudaSuccess)
+        rc = fail(BTDMA_ERR_CUDA, "profiled heat step failed");
+    if (!rc) {
+        auto sec = [&](int a, int b) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[a], ev[b]);
+            return 1e-3 * ms;
+        };
+        // the reference's 12 events (solve_theta.cu:436-439): rhs, solve_z,
+        // solve_y, solve_x, etc, comm, tdma_{z,y,x}_comm, tdma_{z,y,x}_gpu
+        const double t[12] = {sec(0, 1), sec(1, 3), sec(3, 5), sec(5, 7), 0.0,       0.0,
+                              0.0,       0.0,       0.0,       sec(1, 2), sec(3, 4), sec(5, 6)};
+        std::memcpy(times, t, sizeof t);
+        h->last_stream = stream;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    return rc;
+}
+
+int btdma_heat_l2_error(btdma_heat_t h, const double* theta, double t_phys, double* l2) {
+    if (!h || !theta || !l2) return fail(BTDMA_ERR_ARG, "null argument");
+    const HeatGeom& g = h->g;
+    const cudaStream_t st = h->last_stream;
+    CK(cudaMemsetAsync(h->err, 0, sizeof(double), st));
+    const double decay = exp(-3.0 * HEAT_PI * HEAT_PI * t_phys);
+    heat_err_kernel<<<dim3((g.ix + 127) / 128, g.iy, g.iz), 128, 0, st>>>(theta, g, decay, h->err);
+    CK(cudaGetLastError());
+    double sum = 0.0;
+    CK(cudaMemcpyAsync(&sum, h->err, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // normalised by (ix + 1)(iy + 1)(iz + 1), the reference's params.nx * ny * nz
+    *l2 = sqrt(sum / ((double)(g.ix + 1) * (g.iy + 1) * (g.iz + 1)));
+    return BTDMA_OK;
+}
+
+// -------------------------------------------- channel Poisson, wall-normal
+struct btdma_poisson {
+    int nz = 0, n_modes = 0, pin = 0;
+    double* ga = nullptr;   // [nz] sub-diagonal per row
+    double* gc = nullptr;   // [nz] super-diagonal per row
+    double* lam = nullptr;  // [n_modes] kx^2 + ky^2 per mode
+    unsigned* status = nullptr;
+};
+
+int btdma_poisson_create(int nz, const double* dz, const double* dmz, int n_modes,
+                         const double* lambda, int pin_mode0, btdma_poisson_t* out) {
+    if (!out) return fail(BTDMA_ERR_ARG, "null output handle");
+    *out = nullptr;
+    if (nz < 3 || n_modes <= 0 || !dz || !dmz || !lambda)
+        return fail(BTDMA_ERR_ARG, "need nz >= 3, n_modes > 0 and the dz, dmz, lambda arrays");
+    if (!tile_plan(nz, false, 8, 1).sys)
+        return fail(BTDMA_ERR_UNSUPPORTED, "nz must be a multiple of 16 (tiled solve)");
+    // row k: a = 1 / (dz[k+1] dmz[k+1]) (0 at the lower wall),
+    //        c = 1 / (dz[k+1] dmz[k+2]) (0 at the upper wall)
+    //   (k_build_poisson_tdma, PressureSolverGPU.cu:183-210)
+    std::vector<double> ha(nz), hc(nz);
+    for (int k = 0; k < nz; ++k) {
+        ha[k] = k == 0 ? 0.0 : 1.0 / (dz[k + 1] * dmz[k + 1]);
+        hc[k] = k == nz - 1 ? 0.0 : 1.0 / (dz[k + 1] * dmz[k + 2]);
+    }
+    btdma_poisson* h = new btdma_poisson();
+    h->nz = nz;
+    h->n_modes = n_modes;
+    h->pin = pin_mode0 ? 1 : 0;
+    auto cleanup = [&](int code) {
+        btdma_poisson_destroy(h);
+        return code;
+    };
+#define CKP(call)                                                                          \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return cleanup(fail(BTDMA_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_))); \
+    } while (0)
+    CKP(cudaMalloc(&h->ga, sizeof(double) * nz));
+    CKP(cudaMalloc(&h->gc, sizeof(double) * nz));
+    CKP(cudaMalloc(&h->lam, sizeof(double) * n_modes));
+    CKP(cudaMalloc(&h->status, sizeof(unsigned)));
+    CKP(cudaMemset(h->status, 0, sizeof(unsigned)));
+    CKP(cudaMemcpy(h->ga, ha.data(), sizeof(double) * nz, cudaMemcpyHostToDevice));
+    CKP(cudaMemcpy(h->gc, hc.data(), sizeof(double) * nz, cudaMemcpyHostToDevice));
+    CKP(cudaMemcpy(h->lam, lambda, sizeof(double) * n_modes, cudaMemcpyHostToDevice));
+#undef CKP
+    *out = h;
+    return BTDMA_OK;
+}
+
+int btdma_poisson_destroy(btdma_poisson_t h) {
+    if (!h) return BTDMA_OK;
+    cudaFree(h->ga);
+    cudaFree(h->gc);
+    cudaFree(h->lam);
+    cudaFree(h->status);
+    delete h;
+    return BTDMA_OK;
+}
+
+int btdma_poisson_solve(btdma_poisson_t h, double* rhs, cudaStream_t stream) {
+    if (!h || !rhs) return fail(BTDMA_ERR_ARG, "null argument");
+    TileArgs g = {};
+    g.ga = h->ga;
+    g.gc = h->gc;
+    g.glam = h->lam;
+    g.gpin = h->pin;
+    // complex rhs [nz][n_modes] = doubles [nz][2 n_modes]: real and imaginary
+    // parts are systems 2m and 2m + 1 with one matrix
+    const int rc = try_tile_gen<2>(rhs, rhs, 2 * h->n_modes, h->nz, g, h->status, stream);
+    if (rc == 0)
+        return fail(BTDMA_ERR_UNSUPPORTED, "rhs must be 16-byte aligned (tiled solve)");
+    return rc < 0 ? rc : BTDMA_OK;
+}
+
+int btdma_poisson_status(btdma_poisson_t h, unsigned* status, cudaStream_t stream) {
+    if (!h || !status) return fail(BTDMA_ERR_ARG, "null argument");
+    CK(cudaMemcpyAsync(status, h->status, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    CK(cudaMemsetAsync(h->status, 0, sizeof(unsigned), stream));
+    CK(cudaStreamSynchronize(stream));
+    return BTDMA_OK;
+}
+
+// ------------------------------------------------ channel momentum ADI sweeps
+struct btdma_momentum {
+    MomGeom g{};
+    int pbc[2] = {0, 0};
+    double* tab = nullptr;  // [dir][comp][ta, tb, tc][n_dir rows]
+    size_t tab_off[3][3] = {};
+    double* buf = nullptr;  // nx * ny * nz, the sweep layout
+    double* gtab = nullptr; // shared elimination factors of one sweep
+    unsigned* status = nullptr;
+};
+
+int btdma_momentum_create(int nx, int ny, int nz, const double* dx0, const double* dmx0,
+                          const double* dx1, const double* dmx1, const double* dx2,
+                          const double* dmx2, int pbc_x, int pbc_y, btdma_momentum_t* out) {
+    if (!out) return fail(BTDMA_ERR_ARG, "null output handle");
+    *out = nullptr;
+    if (nx <= 0 || ny <= 0 || nz <= 0 || !dx0 || !dmx0 || !dx1 || !dmx1 || !dx2 || !dmx2)
+        return fail(BTDMA_ERR_ARG, "grid sizes and the six metric arrays are required");
+    const int n[3] = {nx, ny, nz};
+    for (int d = 0; d < 3; ++d) {
+        const bool cyc = d < 2 && (d == 0 ? pbc_x : pbc_y);
+        if (!tile_plan(n[d], cyc, 8, 1).sys)
+            return fail(BTDMA_ERR_UNSUPPORTED,
+                        "sweep %d: n must be a multiple of 16 (n / 16 a power of two when "
+                        "periodic)", d);
+    }
+    if ((long long)nx * ny * nz >= (1LL << 31))
+        return fail(BTDMA_ERR_SIZE, "grid above 2^31 cells");
+    // row tables (MomentumSolverGPU.cu:135-155, :176-180, :205-209): for row
+    // r = 1..n, staggered when comp == dir;  a = -c ta, c = -c tc, b = 1 + c tb
+    const double* dxs[3] = {dx0, dx1, dx2};
+    const double* dms[3] = {dmx0, dmx1, dmx2};
+    std::vector<double> tab;
+    size_t off[3][3];
+    for (int d = 0; d < 3; ++d)
+        for (int comp = 0; comp < 3; ++comp) {
+            off[d][comp] = tab.size();
+            const int m = n[d];
+            std::vector<double> ta(m), tb(m), tc(m);
+            const double* dx = dxs[d];
+            const double* dm = dms[d];
+            for (int r = 1; r <= m; ++r) {
+                const double ar = comp == d ? 1.0 / (dm[r] * dx[r - 1]) : 1.0 / (dx[r] * dm[r]);
+                const double cr = comp == d ? 1.0 / (dm[r] * dx[r]) : 1.0 / (dx[r] * dm[r + 1]);
+                double a_ = ar, b_ = ar + cr, c_ = cr;
+                if (d == 2) {  // no-slip walls at both ends (one rank holds all of z)
+                    const bool is_w = comp == 2;
+                    if (r == 1) {
+                        a_ = 0.0;
+                        if (!is_w) b_ += ar;
+                    }
+                    if (r == m) {
+                        c_ = 0.0;
+                        if (!is_w) b_ += cr;
+                    }
+                    if (is_w && r == 1) a_ = b_ = c_ = 0.0;  // w = 0 on the wall
+                }
+                ta[r - 1] = a_;
+                tb[r - 1] = b_;
+                tc[r - 1] = c_;
+            }
+            tab.insert(tab.end(), ta.begin(), ta.end());
+            tab.insert(tab.end(), tb.begin(), tb.end());
+            tab.insert(tab.end(), tc.begin(), tc.end());
+        }
+    btdma_momentum* h = new btdma_momentum();
+    h->g.nx = nx;
+    h->g.ny = ny;
+    h->g.nz = nz;
+    h->pbc[0] = pbc_x ? 1 : 0;
+    h->pbc[1] = pbc_y ? 1 : 0;
+    std::memcpy(h->tab_off, off, sizeof off);
+    auto cleanup = [&](int code) {
+        btdma_momentum_destroy(h);
+        return code;
+    };
+    if (cudaMalloc(&h->tab, sizeof(double) * tab.size()) != cudaSuccess ||
+        cudaMemcpy(h->tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice) !=
+            cudaSuccess ||
+        cudaMalloc(&h->buf, sizeof(double) * (size_t)nx * ny * nz) != cudaSuccess ||
+        cudaMalloc(&h->gtab, sizeof(double) * gen_table_doubles(std::max(nx, std::max(ny, nz)))) !=
+            cudaSuccess ||
+        cudaMalloc(&h->status, sizeof(unsigned)) != cudaSuccess ||
+        cudaMemset(h->status, 0, sizeof(unsigned)) != cudaSuccess)
+        return cleanup(fail(BTDMA_ERR_CUDA, "momentum buffers: %s",
+                            cudaGetErrorString(cudaGetLastError())));
+    *out = h;
+    return BTDMA_OK;
+}
+
+int btdma_momentum_destroy(btdma_momentum_t h) {
+    if (!h) return BTDMA_OK;
+    cudaFree(h->tab);
+    cudaFree(h->buf);
+    cudaFree(h->gtab);
+    cudaFree(h->status);
+    delete h;
+    return BTDMA_OK;
+}
+
+int btdma_momentum_sweep(btdma_momentum_t h, int dir, int comp, const double* q, double* dst,
+                         double c, cudaStream_t stream) {
+    if (!h || !q || !dst) return fail(BTDMA_ERR_ARG, "null argument");
+    if (dir < 0 || dir > 2 || comp < 0 || comp > 2)
+        return fail(BTDMA_ERR_ARG, "dir and comp must be 0, 1 or 2");
+    const MomGeom& g = h->g;
+    const int n[3] = {g.nx, g.ny, g.nz};
+    const int n_sys = g.nx * g.ny * g.nz / n[dir];
+    TileArgs t = {};
+    t.cs = c;
+    t.ga = h->tab + h->tab_off[dir][comp];
+    t.gb = t.ga + n[dir];
+    t.gc = t.gb + n[dir];
+    const dim3 b1(128, 1, 1), bt(MOM_TILE, 8, 1);
+    int rc;
+    if (dir == 2) {
+        mom_gather_kernel<2><<<dim3((g.nx + 127) / 128, g.ny, g.nz), b1, 0, stream>>>(
+            q, h->buf, g, comp == 2 ? 1 : 0);
+        CK(cudaGetLastError());
+        rc = try_tile_gen<3, false>(h->buf, h->buf, n_sys, g.nz, t, h->status, stream, h->gtab);
+    } else if (dir == 1) {
+        mom_gather_kernel<1><<<dim3((g.nx + 127) / 128, g.nz, g.ny), b1, 0, stream>>>(q, h->buf,
+                                                                                   g, 0);
+        CK(cudaGetLastError());
+        rc = h->pbc[1]
+                 ? try_tile_gen<3, true>(h->buf, h->buf, n_sys, g.ny, t, h->status, stream, h->gtab)
+                 : try_tile_gen<3, false>(h->buf, h->buf, n_sys, g.ny, t, h->status, stream,
+                                          h->gtab);
+    } else {
+        mom_gather_x_kernel<<<dim3((g.nx + MOM_TILE - 1) / MOM_TILE,
+                                   (g.ny + MOM_TILE - 1) / MOM_TILE, g.nz), bt, 0, stream>>>(
+            q, h->buf, g);
+        CK(cudaGetLastError());
+        rc = h->pbc[0]
+                 ? try_tile_gen<3, true>(h->buf, h->buf, n_sys, g.nx, t, h->status, stream, h->gtab)
+                 : try_tile_gen<3, false>(h->buf, h->buf, n_sys, g.nx, t, h->status, stream,
+                                          h->gtab);
+    }
+    if (rc != 1) return rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "sweep not tileable");
+    if (dir == 2)
+        mom_scatter_kernel<2><<<dim3((g.nx + 127) / 128, g.ny, g.nz), b1, 0, stream>>>(h->buf,
+                                                                                     dst, g);
+    else if (dir == 1)
+        mom_scatter_kernel<1><<<dim3((g.nx + 127) / 128, g.nz, g.ny), b1, 0, stream>>>(h->buf,
+                                                                                     dst, g);
+    else
+        mom_scatter_x_kernel<<<dim3((g.ny + MOM_TILE - 1) / MOM_TILE,
+                                    (g.nx + MOM_TILE - 1) / MOM_TILE, g.nz), bt, 0, stream>>>(
+            h->buf, dst, g);
+    CK(cudaGetLastError());
+    return BTDMA_OK;
+}
+
+int btdma_momentum_adi(btdma_momentum_t h, int comp, double* rhs, double* q_out, double c,
+                       cudaStream_t stream) {
+    int rc = btdma_momentum_sweep(h, 2, comp, rhs, rhs, c, stream);
+    if (!rc) rc = btdma_momentum_sweep(h, 1, comp, rhs, rhs, c, stream);
+    if (!rc) rc = btdma_momentum_sweep(h, 0, comp, rhs, q_out, c, stream);
+    return rc;
+}
+
+int btdma_momentum_status(btdma_momentum_t h, unsigned* status, cudaStream_t stream) {
+    if (!h || !status) return fail(BTDMA_ERR_ARG, "null argument");
+    CK(cudaMemcpyAsync(status, h->status, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    CK(cudaMemsetAsync(h->status, 0, sizeof(unsigned), stream));
+    CK(cudaStreamSynchronize(stream));
+    return BTDMA_OK;
+}

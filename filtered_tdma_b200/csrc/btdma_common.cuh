@@ -95,7 +95,7 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 // at most kSuspendNs), raising ST_TIMEOUT.  Every 64 polls it also checks the
 // status word and gives up at once if another CTA already timed out, so a
 // systematic failure costs one timeout, not one per CTA.
-__device__ __noinline__ bool mbar_wait_slow(uint64_t* bar, uint32_t parity, unsigned* status,
+static __device__ __noinline__ bool mbar_wait_slow(uint64_t* bar, uint32_t parity, unsigned* status,
                                             uint32_t limit);
 
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
@@ -105,7 +105,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return mbar_wait_slow(bar, parity, status, limit);
 }
 
-__device__ __noinline__ bool mbar_wait_slow(uint64_t* bar, uint32_t parity, unsigned* status,
+static __device__ __noinline__ bool mbar_wait_slow(uint64_t* bar, uint32_t parity, unsigned* status,
                                             uint32_t limit) {
     for (uint32_t it = 0; it < limit; ++it) {
         if (mbar_try_wait(bar, parity)) return true;

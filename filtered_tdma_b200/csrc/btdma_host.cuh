@@ -1,0 +1,423 @@
+// Host-side internals shared by the library's translation units: the solver
+// handle, error reporting, tensor-map encoding and the launch planning of the
+// tiled and segment kernels.  Not part of the C ABI (include/btdma.h).
+#pragma once
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "btdma_common.cuh"
+#include "k_segment.cuh"
+#include "k_tile.cuh"
+
+using namespace btdma;
+
+struct btdma_handle {
+    int method, P, precision, flags;
+    int n_sys_cap, n_row_cap;
+    double eps_constant;
+    double* rho_row = nullptr;               // [n_row_cap] per-row spectral bound
+    int* J = nullptr;                        // [P]
+    unsigned long long* work = nullptr;      // [2P] J accumulators (kept zero between solves)
+    unsigned* status = nullptr;              // device status word
+    double* scratch = nullptr;               // P == 1: c' and e' [2][n_row_cap * n_sys_cap]
+    cudaStream_t last_stream = nullptr;
+    // FP32_REFINE: residual [n_row_cap * n_sys_cap] (FP32), per-system sweep
+    // counts [n_sys_cap], open-system counters [BTDMA_REFINE_MAX_SWEEPS + 1]
+    float* resid = nullptr;
+    unsigned char* iters = nullptr;
+    unsigned* open = nullptr;
+    int max_sweeps = 3;
+    double eta_tol = 8.0 * 0x1p-53;
+    int last_n_sys = 0;
+    bool last_refined = false;
+    // ragged batches: the plan of the most recent row-offset layout
+    struct RagBucket {
+        int cyc, first, count, nmin, nmax;
+        int cta;    // 1: one CTA of P threads per system, 0: P lanes of a warp per system
+        int staged; // CTA kind: system staged through shared memory (autotuner's choice)
+        int P, warps, mcap;
+        float best_ms;
+    };
+    std::vector<long long> rag_off;        // host copy of the offsets of the plan
+    std::vector<unsigned char> rag_per;    // host copy of the periodic flags
+    std::vector<RagBucket> rag_buckets;
+    std::vector<int> rag_order;            // system ids, bucket by bucket
+    long long* rag_d_off = nullptr;        // device offsets [n_sys + 1]
+    int* rag_d_list = nullptr;             // device copy of rag_order
+    int4* rag_d_tasks = nullptr;           // task tables [2 * n_sys]
+    int4* rag_d_probe = nullptr;           // task table of one bucket being tuned [n_sys]
+    // launches of a solve: warp-kind tasks (one launch), CTA-kind tasks per P
+    struct RagLaunch {
+        int cta, P, first, count, mcap, staged;
+    };
+    std::vector<RagLaunch> rag_launches;
+    static constexpr int RAG_STREAMS = 4;
+    cudaStream_t rag_side[RAG_STREAMS] = {};
+    cudaEvent_t rag_fork = nullptr, rag_join[RAG_STREAMS] = {};
+};
+namespace btdma_host {
+
+extern thread_local std::string g_err;
+
+// Records the message of a failing call (btdma_last_error) and returns code.
+int fail(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(BTDMA_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                              \
+    } while (0)
+
+// ------------------------------------------------------------ tensor maps
+inline PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// [n_row x n_sys] FP64 array, boxes of SEG_BOXR rows x SEG_S systems.
+inline bool make_map(CUtensorMap* map, const void* ptr, int n_sys, int n_row) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)n_sys, (cuuint64_t)n_row};
+    cuuint64_t strides[1] = {(cuuint64_t)n_sys * sizeof(double)};
+    cuuint32_t box[2] = {(cuuint32_t)SEG_S, (cuuint32_t)SEG_BOXR};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void*>(ptr), dims, strides,
+                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+inline bool tma_ok(const void* p, int n_sys) {
+    return ((reinterpret_cast<uintptr_t>(p) & 15) == 0) && (n_sys % 2 == 0);
+}
+
+inline int auto_segments(int n_row) {
+    // ~64 rows per segment, at least 3, at most the cluster limit.
+    if (n_row < 6) return 1;
+    int P = (n_row + 63) / 64;
+    P = std::max(2, std::min(P, SEG_MAX_P));
+    while (P > 1 && n_row / P < 3) --P;
+    return P;
+}
+
+inline int seg_mcap(int n_row, int P) {
+    int mmax = (n_row + P - 1) / P;
+    return (mmax + SEG_BOXR - 1) / SEG_BOXR * SEG_BOXR;
+}
+
+inline int max_smem_optin() {
+    static int v = -1;
+    if (v < 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+            v = 48 * 1024;
+    }
+    return v;
+}
+
+template <int METHOD, bool CYCLIC>
+int launch_seg(const CUtensorMap* maps, const SegArgs& a, int groups, cudaStream_t st) {
+    auto kern = seg_f64_kernel<METHOD, CYCLIC>;
+    static bool attr_done = false;
+    if (!attr_done) {
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                max_smem_optin()));
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        attr_done = true;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(a.P, groups, 1);
+    cfg.blockDim = dim3(SEG_S, 1, 1);
+    cfg.dynamicSmemBytes = seg_smem_bytes(a.mcap, a.P, CYCLIC);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = a.P;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, kern, maps[0], maps[1], maps[2], maps[3], maps[4], a));
+    return BTDMA_OK;
+}
+
+// 3-D view [nseg][TILE_MT][n_sys] of an [n_row x n_sys] FP64 array; boxes of
+// tile_rps(elem) rows of `nsc` consecutive sub-segments for `sys` systems.
+inline bool make_tile_map(CUtensorMap* map, const void* ptr, int n_sys, int nseg, int sys,
+                          int nsc, int elem = 8) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)n_sys, (cuuint64_t)TILE_MT, (cuuint64_t)nseg};
+    cuuint64_t strides[2] = {(cuuint64_t)n_sys * elem, (cuuint64_t)n_sys * TILE_MT * elem};
+    cuuint32_t box[3] = {(cuuint32_t)sys, (cuuint32_t)tile_rps(elem), (cuuint32_t)nsc};
+    cuuint32_t estr[3] = {1, 1, 1};
+    const CUtensorMapDataType dt =
+        elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    CUresult r = fn(map, dt, 3, const_cast<void*>(ptr), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+inline int num_sms() {
+    static int v = -1;
+    if (v < 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) v = 1;
+    }
+    return v;
+}
+
+// Shape plan of the tiled kernel: systems per group, CTAs per cluster, ring stages.
+struct TilePlan {
+    int sys = 0, cl = 0, nst = 0, nseg = 0;
+};
+
+inline int max_smem_per_sm() {
+    static int v = -1;
+    if (v < 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) !=
+            cudaSuccess)
+            v = 0;
+    }
+    return v;
+}
+
+// na: arrays per ring stage (4, or 1 for the constant-coefficient D-only ring).
+// sh: shared-matrix sweep (factor table in shared memory, two CTAs per SM).
+inline TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4, bool sh = false) {
+    TilePlan pl;
+    if (n_row % TILE_MT != 0) return pl;
+    const int nseg = n_row / TILE_MT;
+    if (cyclic && (nseg & (nseg - 1)) != 0) return pl;  // periodic PCR needs 2^k rows
+    int sys, cl = 0;
+    if (nseg <= 4) {
+        sys = 128;
+        cl = 1;
+    } else if (nseg <= 8) {
+        sys = 64;
+        cl = 1;
+    } else if (nseg <= 16) {
+        sys = 32;
+        cl = 1;
+    } else {
+        // One CTA up to 32 sub-segments (a 2-CTA cluster with 256-byte boxes
+        // measured slower than one CTA with 128-byte boxes); longer systems split
+        // over the smallest cluster that keeps <= 32 sub-segments per CTA.
+        sys = 16;
+        for (int c = 1; c <= 16; c <<= 1)
+            if (nseg % c == 0 && nseg / c <= 32) {
+                cl = c;
+                break;
+            }
+        if (cl == 0) return pl;
+    }
+    int nst = na == 4 ? TILE_MAX_NST : TILE_MAX_NST_CONST;
+    // two CTAs per SM for shared-matrix sweeps: half an SM's shared memory each
+    // (less 1 KB the runtime reserves per CTA)
+    const size_t cap =
+        sh && cl == 1 ? (size_t)max_smem_per_sm() / 2 - 1024 : (size_t)max_smem_optin();
+    while (nst >= 3 &&
+           tile_smem_bytes(sys, nseg / cl, nseg, sys / cl, nst, elem, na, sh) > cap)
+        --nst;
+    if (nst < 3) return pl;
+    pl.sys = sys;
+    pl.cl = cl;
+    pl.nst = nst;
+    pl.nseg = nseg;
+    return pl;
+}
+
+template <int SYS, bool CYCLIC, typename TIN = double, typename TC = double, int GEN = 0>
+int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st) {
+    auto kern = tile_f64_kernel<SYS, CYCLIC, TIN, TC, GEN>;
+    static bool attr_done = false;
+    if (!attr_done) {
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                max_smem_optin()));
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        attr_done = true;
+    }
+    const int threads = SYS * a.nseg / a.cl;
+    cudaLaunchConfig_t cfg = {};
+    cfg.blockDim = dim3(threads, 1, 1);
+    constexpr bool SHT = GEN == 1 || GEN == 3;
+    cfg.dynamicSmemBytes = tile_smem_bytes(SYS, a.nseg / a.cl, a.nseg, SYS / a.cl, a.nst,
+                                           (int)sizeof(TIN), GEN ? 1 : 4, SHT);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = a.cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = num_sms();
+    if (SHT && a.cl == 1) {  // built for two CTAs per SM
+        int nb = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, threads,
+                                                         cfg.dynamicSmemBytes));
+        clusters = num_sms() * std::max(1, nb);
+    }
+    if (a.cl > 1) {
+        cfg.gridDim = dim3(a.cl * num_sms(), 1, 1);
+        int nc = 0;
+        CK(cudaOccupancyMaxActiveClusters(&nc, kern, &cfg));
+        if (nc <= 0) return fail(BTDMA_ERR_UNSUPPORTED, "no cluster of %d CTAs fits", a.cl);
+        clusters = nc;
+    }
+    clusters = std::min(clusters, a.n_groups);
+    cfg.gridDim = dim3(clusters * a.cl, 1, 1);
+    TileArgs aa = a;
+    CK(cudaLaunchKernelEx(&cfg, kern, maps[0], maps[1], maps[2], maps[3], aa));
+    return BTDMA_OK;
+}
+
+template <typename TIN, typename TC>
+int launch_tile_plan(const TilePlan& pl, const CUtensorMap* maps, const TileArgs& a, bool cyclic,
+                     cudaStream_t st) {
+    switch (pl.sys * 2 + (cyclic ? 1 : 0)) {
+        case 256: return launch_tile_sys<128, false, TIN, TC>(maps, a, st);
+        case 257: return launch_tile_sys<128, true, TIN, TC>(maps, a, st);
+        case 128: return launch_tile_sys<64, false, TIN, TC>(maps, a, st);
+        case 129: return launch_tile_sys<64, true, TIN, TC>(maps, a, st);
+        case 64: return launch_tile_sys<32, false, TIN, TC>(maps, a, st);
+        case 65: return launch_tile_sys<32, true, TIN, TC>(maps, a, st);
+        case 33: return launch_tile_sys<16, true, TIN, TC>(maps, a, st);
+        default: return launch_tile_sys<16, false, TIN, TC>(maps, a, st);
+    }
+}
+
+inline bool tma_ok_elem(const void* p, int n_sys, int elem) {
+    return ((reinterpret_cast<uintptr_t>(p) & 15) == 0) && ((size_t)n_sys * elem) % 16 == 0;
+}
+
+// Returns 1 when the tiled kernel was launched, 0 when the shape needs the
+// cluster-per-segment kernel, < 0 on error.
+// TC: arithmetic of the local sweeps; accumulate: X += solution; gate: the
+// kernel does nothing while *gate == 0.
+template <typename TIN, typename TC = double>
+int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, int n_sys,
+             int n_row, bool cyclic, unsigned* status, cudaStream_t st, bool accumulate = false,
+             const unsigned* gate = nullptr) {
+    const int elem = (int)sizeof(TIN);
+    const TilePlan pl = tile_plan(n_row, cyclic, elem);
+    if (pl.sys == 0) return 0;
+    if (!(tma_ok_elem(A, n_sys, elem) && tma_ok_elem(B, n_sys, elem) &&
+          tma_ok_elem(C, n_sys, elem) && tma_ok_elem(D, n_sys, elem)))
+        return 0;
+    const int nsc = pl.nseg / pl.cl;
+    CUtensorMap maps[4];
+    if (!(make_tile_map(&maps[0], A, n_sys, pl.nseg, pl.sys, nsc, elem) &&
+          make_tile_map(&maps[1], B, n_sys, pl.nseg, pl.sys, nsc, elem) &&
+          make_tile_map(&maps[2], C, n_sys, pl.nseg, pl.sys, nsc, elem) &&
+          make_tile_map(&maps[3], D, n_sys, pl.nseg, pl.sys, nsc, elem)))
+        return 0;
+    TileArgs a = {};
+    a.X = X;
+    a.n_sys = n_sys;
+    a.n_row = n_row;
+    a.nseg = pl.nseg;
+    a.cl = pl.cl;
+    a.nst = pl.nst;
+    a.n_groups = (n_sys + pl.sys - 1) / pl.sys;
+    a.accumulate = accumulate ? 1 : 0;
+    a.gate = gate;
+    a.status = status;
+    const int rc = launch_tile_plan<TIN, TC>(pl, maps, a, cyclic, st);
+    return rc == BTDMA_OK ? 1 : rc;
+}
+
+// Generated-coefficient batch, only D read (the GEN modes of the tiled
+// kernel; the coefficient fields of `gen` are used, the rest is filled here).
+// Returns 1 when launched, 0 when the shape is not tiled, < 0 on error.
+// GEN 1 and 3 (one matrix for every system): `tab` is device scratch of
+// n_row * 5 + (n_row / 16) * 6 doubles for the shared elimination factors.
+template <int GEN, bool CYC = false>
+int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArgs& gen,
+                 unsigned* status, cudaStream_t st, double* tab = nullptr) {
+    const TilePlan pl = tile_plan(n_row, CYC, 8, 1, GEN == 1 || GEN == 3);
+    if (pl.sys == 0 || !tma_ok_elem(D, n_sys, 8)) return 0;
+    const int nsc = pl.nseg / pl.cl;
+    CUtensorMap maps[4];
+    if (!make_tile_map(&maps[3], D, n_sys, pl.nseg, pl.sys, nsc, 8)) return 0;
+    maps[0] = maps[1] = maps[2] = maps[3];  // not read in this mode
+    TileArgs a = gen;
+    a.X = X;
+    a.n_sys = n_sys;
+    a.n_row = n_row;
+    a.nseg = pl.nseg;
+    a.cl = pl.cl;
+    a.nst = pl.nst;
+    a.n_groups = (n_sys + pl.sys - 1) / pl.sys;
+    a.accumulate = 0;
+    a.gate = nullptr;
+    a.status = status;
+    if constexpr (GEN == 1 || GEN == 3) {
+        if (!tab) return fail(BTDMA_ERR_ARG, "shared-matrix sweep without a factor table");
+        tile_table_kernel<GEN><<<(pl.nseg + 127) / 128, 128, 0, st>>>(a, tab);
+        CK(cudaGetLastError());
+        a.gtab = tab;
+    }
+    int rc;
+    switch (pl.sys) {
+        case 128: rc = launch_tile_sys<128, CYC, double, double, GEN>(maps, a, st); break;
+        case 64: rc = launch_tile_sys<64, CYC, double, double, GEN>(maps, a, st); break;
+        case 32: rc = launch_tile_sys<32, CYC, double, double, GEN>(maps, a, st); break;
+        default: rc = launch_tile_sys<16, CYC, double, double, GEN>(maps, a, st); break;
+    }
+    return rc == BTDMA_OK ? 1 : rc;
+}
+
+// Heat sweep: every row -cs, 1 + 2 cs, -cs; cs more on the diagonal of the
+// first and last row when cbound.
+inline int try_tile_const(const double* D, double* X, int n_sys, int n_row, double cs, bool cbound,
+                   unsigned* status, cudaStream_t st, double* tab) {
+    TileArgs g = {};
+    g.cs = cs;
+    g.cbound = cbound ? 1 : 0;
+    return try_tile_gen<1>(D, X, n_sys, n_row, g, status, st, tab);
+}
+
+inline size_t gen_table_doubles(int n_row) {
+    return (size_t)n_row * 5 + (size_t)(n_row / 16 + 1) * 6;
+}
+
+template <bool CYCLIC>
+int launch_seg_method(int method, const CUtensorMap* maps, const SegArgs& a, int groups,
+                      cudaStream_t st) {
+    switch (method) {
+        case BTDMA_PASCAL: return launch_seg<SEG_PASCAL, CYCLIC>(maps, a, groups, st);
+        case BTDMA_FILTERED_V1: return launch_seg<SEG_FILT_V1, CYCLIC>(maps, a, groups, st);
+        default: return launch_seg<SEG_FILT_V2, CYCLIC>(maps, a, groups, st);
+    }
+}
+
+}  // namespace btdma_host
+
+using namespace btdma_host;

@@ -1,0 +1,360 @@
+// C ABI of ragged (CSR) batches: length buckets, task tables, launches on
+// forked side streams, the autotuner (declared in include/btdma.h).
+#include <algorithm>
+#include <climits>
+
+#include "btdma_host.cuh"
+#include "k_ragged.cuh"
+
+// ------------------------------------------------------------------ ragged
+namespace {
+
+constexpr int RAG_WPC = 4;         // warps per CTA of the warp-kind launch
+constexpr int RAG_WARP_MCAP = 32;  // rows per lane the warp kind accepts
+
+// Lanes per system for a bucket whose systems have nmin..nmax rows: about
+// 12 rows per lane, a power of two, at most 32, and at least 3 rows per lane
+// for the shortest system.
+int rag_default_P(int nmin, int nmax) {
+    int P = 1;
+    while (P < 32 && nmax / (2 * P) >= 12 && nmin / (2 * P) >= 3) P <<= 1;
+    return P;
+}
+
+int rag_mcap(int nmax, int P) { return (nmax + P - 1) / P; }
+
+// CTA-per-system shape for long systems: the smallest power of two >= 64 that
+// keeps <= RAG_MT rows per thread (0 when none <= 512 does, or when the
+// shortest system would get fewer than 3 rows per thread).
+int rag_cta_P(int nmin, int nmax) {
+    int P = 64;
+    while (P <= 512 && rag_mcap(nmax, P) > RAG_MT) P <<= 1;
+    return (P <= 512 && nmin / P >= 3) ? P : 0;
+}
+
+// Task entries of one bucket with lanes-per-system P (warp kind: 32 / P
+// systems per warp; CTA kind: one system per CTA).
+void rag_bucket_tasks(const btdma_handle::RagBucket& b, int cta, int P, std::vector<int4>& out) {
+    if (cta) {
+        for (int i = 0; i < b.count; ++i) out.push_back(make_int4(b.first + i, b.cyc, 0, 0));
+        return;
+    }
+    const int G = 32 / P;
+    for (int i = 0; i < b.count; i += G)
+        out.push_back(make_int4(b.first + i, std::min(G, b.count - i), P, b.cyc));
+}
+
+// Task tables of the whole plan: one warp-kind launch (buckets longest first)
+// and one CTA-kind launch per P.
+int rag_build_launches(btdma_t h) {
+    std::vector<int4> tasks;
+    h->rag_launches.clear();
+    btdma_handle::RagLaunch wl{0, 0, 0, 0, 1, 0};
+    for (int i = (int)h->rag_buckets.size() - 1; i >= 0; --i) {
+        const auto& b = h->rag_buckets[i];
+        if (b.cta) continue;
+        rag_bucket_tasks(b, 0, b.P, tasks);
+        wl.mcap = std::max(wl.mcap, rag_mcap(b.nmax, b.P));
+    }
+    wl.count = (int)tasks.size();
+    if (wl.count) h->rag_launches.push_back(wl);
+    for (int P = 512; P >= 64; P >>= 1)
+        for (int stg = 0; stg < 2; ++stg) {
+            btdma_handle::RagLaunch cl{1, P, (int)tasks.size(), 0, 0, stg};
+            for (const auto& b : h->rag_buckets)
+                if (b.cta && b.P == P && b.staged == stg) rag_bucket_tasks(b, 1, P, tasks);
+            cl.count = (int)tasks.size() - cl.first;
+            if (cl.count) h->rag_launches.push_back(cl);
+        }
+    CK(cudaMemcpy(h->rag_d_tasks, tasks.data(), sizeof(int4) * tasks.size(),
+                  cudaMemcpyHostToDevice));
+    return BTDMA_OK;
+}
+
+int rag_plan(btdma_t h, const long long* off, const unsigned char* per, int n_sys) {
+    if (n_sys <= 0) return fail(BTDMA_ERR_ARG, "n_sys must be positive");
+    if (!off) return fail(BTDMA_ERR_ARG, "null row offsets");
+    if (off[0] != 0) return fail(BTDMA_ERR_ARG, "row_offsets[0] must be 0");
+    const bool same = (int)h->rag_off.size() == n_sys + 1 &&
+                      std::equal(off, off + n_sys + 1, h->rag_off.begin()) &&
+                      (per ? (h->rag_per.size() == (size_t)n_sys &&
+                              std::equal(per, per + n_sys, h->rag_per.begin()))
+                           : h->rag_per.empty());
+    if (same && h->rag_d_off) return BTDMA_OK;
+    // bucket key: (periodic, ceil(log2 n))
+    std::vector<int> key(n_sys);
+    for (int i = 0; i < n_sys; ++i) {
+        const long long n = off[i + 1] - off[i];
+        if (n < 3) return fail(BTDMA_ERR_SEGMENT, "system %d has %lld rows (needs >= 3)", i, n);
+        if (n > 32 * RAG_WARP_MCAP && n > 512 * RAG_MT)
+            return fail(BTDMA_ERR_SIZE, "system %d has %lld rows (at most %d)", i, n,
+                        512 * RAG_MT);
+        int lg = 0;
+        while ((1LL << lg) < n) ++lg;
+        key[i] = (per && per[i] ? 64 : 0) + lg;
+    }
+    std::vector<int> order(n_sys);
+    for (int i = 0; i < n_sys; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return key[x] < key[y]; });
+    std::vector<btdma_handle::RagBucket> bk;
+    for (int i = 0; i < n_sys;) {
+        int j = i;
+        int nmin = INT32_MAX, nmax = 0;
+        while (j < n_sys && key[order[j]] == key[order[i]]) {
+            const int n = (int)(off[order[j] + 1] - off[order[j]]);
+            nmin = std::min(nmin, n);
+            nmax = std::max(nmax, n);
+            ++j;
+        }
+        btdma_handle::RagBucket b{};
+        b.cyc = key[order[i]] >= 64 ? 1 : 0;
+        b.first = i;
+        b.count = j - i;
+        b.nmin = nmin;
+        b.nmax = nmax;
+        const int Pc = nmax > 32 * RAG_MT ? rag_cta_P(nmin, nmax) : 0;
+        if (Pc) {
+            b.cta = 1;
+            b.P = Pc;
+        } else {
+            b.cta = 0;
+            b.P = rag_default_P(nmin, nmax);
+            if (rag_mcap(nmax, b.P) > RAG_WARP_MCAP)
+                return fail(BTDMA_ERR_UNSUPPORTED, "no launch shape for systems of %d..%d rows",
+                            nmin, nmax);
+        }
+        b.warps = b.cta ? b.P / 32 : RAG_WPC;
+        b.mcap = rag_mcap(nmax, b.P);
+        b.best_ms = 0.f;
+        bk.push_back(b);
+        i = j;
+    }
+    cudaFree(h->rag_d_off);
+    cudaFree(h->rag_d_list);
+    cudaFree(h->rag_d_tasks);
+    cudaFree(h->rag_d_probe);
+    h->rag_d_off = nullptr;
+    h->rag_d_list = nullptr;
+    h->rag_d_tasks = h->rag_d_probe = nullptr;
+    h->rag_off.clear();
+    CK(cudaMalloc(&h->rag_d_off, sizeof(long long) * (n_sys + 1)));
+    CK(cudaMalloc(&h->rag_d_list, sizeof(int) * n_sys));
+    CK(cudaMalloc(&h->rag_d_tasks, sizeof(int4) * 2 * n_sys));
+    CK(cudaMalloc(&h->rag_d_probe, sizeof(int4) * n_sys));
+    CK(cudaMemcpy(h->rag_d_off, off, sizeof(long long) * (n_sys + 1), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->rag_d_list, order.data(), sizeof(int) * n_sys, cudaMemcpyHostToDevice));
+    if (!h->rag_fork) {
+        CK(cudaEventCreateWithFlags(&h->rag_fork, cudaEventDisableTiming));
+        for (int i = 0; i < btdma_handle::RAG_STREAMS; ++i) {
+            CK(cudaStreamCreateWithFlags(&h->rag_side[i], cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&h->rag_join[i], cudaEventDisableTiming));
+        }
+    }
+    h->rag_buckets = bk;
+    h->rag_order = order;
+    const int rc = rag_build_launches(h);
+    if (rc) return rc;
+    h->rag_off.assign(off, off + n_sys + 1);
+    if (per)
+        h->rag_per.assign(per, per + n_sys);
+    else
+        h->rag_per.clear();
+    return BTDMA_OK;
+}
+
+template <typename TIN>
+int rag_launch(btdma_t h, int cta, int P, int mcap, int staged, const int4* tasks, int n_tasks,
+               const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X,
+               cudaStream_t st) {
+    RagArgs a{};
+    a.A = A;
+    a.B = B;
+    a.C = C;
+    a.D = D;
+    a.X = X;
+    a.off = h->rag_d_off;
+    a.list = h->rag_d_list;
+    a.tasks = tasks;
+    a.n_tasks = n_tasks;
+    a.mcap = mcap;
+    a.status = h->status;
+    if (cta) {
+        if (staged && rag_cta_smem_bytes(P, true) > (size_t)max_smem_optin()) staged = 0;
+        auto kern = staged ? ragged_cta_kernel<TIN, true> : ragged_cta_kernel<TIN, false>;
+        static bool attr_done[2] = {false, false};
+        if (!attr_done[staged]) {
+            CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    max_smem_optin()));
+            attr_done[staged] = true;
+        }
+        kern<<<n_tasks, P, rag_cta_smem_bytes(P, staged), st>>>(a);
+    } else {
+        auto kern = ragged_kernel<TIN>;
+        static bool attr_done = false;
+        if (!attr_done) {
+            CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    max_smem_optin()));
+            attr_done = true;
+        }
+        kern<<<(n_tasks + RAG_WPC - 1) / RAG_WPC, 32 * RAG_WPC, rag_smem_bytes(RAG_WPC, mcap),
+               st>>>(a);
+    }
+    CK(cudaGetLastError());
+    return BTDMA_OK;
+}
+
+// All launches of the plan: the first on the caller's stream, the others on
+// side streams forked from it and joined back (graph-capturable).
+template <typename TIN>
+int rag_run(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X,
+            cudaStream_t st) {
+    const auto& L = h->rag_launches;
+    const int n = (int)L.size();
+    const int side = std::min(n - 1, (int)btdma_handle::RAG_STREAMS);
+    if (side > 0) {
+        CK(cudaEventRecord(h->rag_fork, st));
+        for (int i = 0; i < side; ++i) CK(cudaStreamWaitEvent(h->rag_side[i], h->rag_fork, 0));
+    }
+    for (int i = 0; i < n; ++i) {
+        const cudaStream_t s = i == 0 ? st : h->rag_side[(i - 1) % btdma_handle::RAG_STREAMS];
+        const int rc = rag_launch<TIN>(h, L[i].cta, L[i].P, L[i].mcap, L[i].staged,
+                                       h->rag_d_tasks + L[i].first, L[i].count, A, B, C, D, X,
+                                       s);
+        if (rc) return rc;
+    }
+    for (int i = 0; i < side; ++i) {
+        CK(cudaEventRecord(h->rag_join[i], h->rag_side[i]));
+        CK(cudaStreamWaitEvent(st, h->rag_join[i], 0));
+    }
+    return BTDMA_OK;
+}
+
+template <typename TIN>
+int rag_solve(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X,
+              const long long* off, const unsigned char* per, int n_sys, cudaStream_t st) {
+    if (!h) return fail(BTDMA_ERR_ARG, "null handle");
+    if (!A || !B || !C || !D || !X) return fail(BTDMA_ERR_ARG, "null array");
+    if (h->method != BTDMA_PASCAL)
+        return fail(BTDMA_ERR_UNSUPPORTED, "ragged batches are solved by PaScaL only");
+    const bool f32 = sizeof(TIN) == 4;
+    if (f32 != (h->precision != BTDMA_FP64))
+        return fail(BTDMA_ERR_ARG, "array type does not match the handle's precision");
+    int rc = rag_plan(h, off, per, n_sys);
+    if (rc) return rc;
+    h->last_stream = st;
+    h->last_n_sys = n_sys;
+    h->last_refined = false;
+    return rag_run<TIN>(h, A, B, C, D, X, st);
+}
+
+// Times, bucket by bucket, every launch shape on the given batch (the bucket
+// alone, best of 3, CUDA events on the stream) and keeps the fastest; then
+// rebuilds the merged task tables.  X is overwritten.
+template <typename TIN>
+int rag_tune(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X,
+             const long long* off, const unsigned char* per, int n_sys, cudaStream_t st) {
+    int rc = rag_solve<TIN>(h, A, B, C, D, X, off, per, n_sys, st);  // plan + warm-up
+    if (rc) return rc;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    std::vector<int4> tasks;
+    for (auto& b : h->rag_buckets) {
+        struct Cand {
+            int cta, P, staged;
+        };
+        std::vector<Cand> cands;
+        for (int P = 1; P <= 32 && b.nmin / P >= 3; P <<= 1)
+            if (rag_mcap(b.nmax, P) <= RAG_WARP_MCAP) cands.push_back({0, P, 0});
+        for (int P = 64; P <= 512 && b.nmin / P >= 3; P <<= 1)
+            if (rag_mcap(b.nmax, P) <= RAG_MT) {
+                cands.push_back({1, P, 0});
+                if (rag_cta_smem_bytes(P, true) <= (size_t)max_smem_optin())
+                    cands.push_back({1, P, 1});
+            }
+        float best = 1e30f;
+        Cand pick{b.cta, b.P, b.staged};
+        for (const Cand& cd : cands) {
+            tasks.clear();
+            rag_bucket_tasks(b, cd.cta, cd.P, tasks);
+            if (cudaMemcpyAsync(h->rag_d_probe, tasks.data(), sizeof(int4) * tasks.size(),
+                                cudaMemcpyHostToDevice, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess) {
+                rc = fail(BTDMA_ERR_CUDA, "autotune upload failed");
+                break;
+            }
+            float ms = 0.f;
+            for (int rep = 0; rep < 3 && !rc; ++rep) {
+                CK(cudaEventRecord(e0, st));
+                rc = rag_launch<TIN>(h, cd.cta, cd.P, rag_mcap(b.nmax, cd.P), cd.staged,
+                                     h->rag_d_probe, (int)tasks.size(), A, B, C, D, X, st);
+                if (rc) break;
+                CK(cudaEventRecord(e1, st));
+                CK(cudaEventSynchronize(e1));
+                float t = 0.f;
+                CK(cudaEventElapsedTime(&t, e0, e1));
+                ms = rep == 0 ? t : std::min(ms, t);
+            }
+            if (rc) break;
+            if (ms < best) {
+                best = ms;
+                pick = cd;
+            }
+        }
+        if (rc) break;
+        b.cta = pick.cta;
+        b.staged = pick.staged;
+        b.P = pick.P;
+        b.warps = pick.cta ? pick.P / 32 : RAG_WPC;
+        b.mcap = rag_mcap(b.nmax, pick.P);
+        b.best_ms = best;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    return rag_build_launches(h);
+}
+
+}  // namespace
+
+int btdma_solve_ragged(btdma_t h, const double* A, const double* B, const double* C,
+                       const double* D, double* X, const long long* row_offsets,
+                       const unsigned char* is_periodic, int n_sys, cudaStream_t stream) {
+    return rag_solve<double>(h, A, B, C, D, X, row_offsets, is_periodic, n_sys, stream);
+}
+
+int btdma_solve_ragged_f32(btdma_t h, const float* A, const float* B, const float* C,
+                           const float* D, double* X, const long long* row_offsets,
+                           const unsigned char* is_periodic, int n_sys, cudaStream_t stream) {
+    return rag_solve<float>(h, A, B, C, D, X, row_offsets, is_periodic, n_sys, stream);
+}
+
+int btdma_ragged_autotune(btdma_t h, const void* A, const void* B, const void* C, const void* D,
+                          double* X, const long long* row_offsets,
+                          const unsigned char* is_periodic, int n_sys, cudaStream_t stream) {
+    if (!h) return fail(BTDMA_ERR_ARG, "null handle");
+    if (h->precision == BTDMA_FP64)
+        return rag_tune<double>(h, static_cast<const double*>(A), static_cast<const double*>(B),
+                                static_cast<const double*>(C), static_cast<const double*>(D), X,
+                                row_offsets, is_periodic, n_sys, stream);
+    return rag_tune<float>(h, static_cast<const float*>(A), static_cast<const float*>(B),
+                           static_cast<const float*>(C), static_cast<const float*>(D), X,
+                           row_offsets, is_periodic, n_sys, stream);
+}
+
+int btdma_ragged_plan_info(btdma_t h, btdma_ragged_bucket* out, int cap, int* n_out) {
+    if (!h || !n_out) return fail(BTDMA_ERR_ARG, "null argument");
+    *n_out = (int)h->rag_buckets.size();
+    for (int i = 0; i < cap && i < *n_out; ++i) {
+        const auto& b = h->rag_buckets[i];
+        out[i].periodic = b.cyc;
+        out[i].n_systems = b.count;
+        out[i].n_row_min = b.nmin;
+        out[i].n_row_max = b.nmax;
+        out[i].lanes_per_system = b.P;
+        out[i].warps_per_cta = b.warps;
+        out[i].cta_per_system = b.cta + b.staged;
+        out[i].tuned_ms = b.best_ms;
+    }
+    return BTDMA_OK;
+}
