@@ -396,8 +396,8 @@ int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArg
 
 // Heat sweep: every row -cs, 1 + 2 cs, -cs; cs more on the diagonal of the
 // first and last row when cbound.
-inline int try_tile_const(const double* D, double* X, int n_sys, int n_row, double cs, bool cbound,
-                   unsigned* status, cudaStream_t st, double* tab) {
+inline int try_tile_const(const double* D, double* X, int n_sys, int n_row, double cs,
+                          bool cbound, unsigned* status, cudaStream_t st, double* tab) {
     TileArgs g = {};
     g.cs = cs;
     g.cbound = cbound ? 1 : 0;
