@@ -18,6 +18,7 @@ FLAG_J_HOST = 1
 FLAG_REFERENCE_ORDER = 2
 OK, ERR_ARG, ERR_SEGMENT, ERR_CUDA, ERR_SIZE, ERR_UNSUPPORTED, ERR_DEVICE = 0, -1, -2, -3, -4, -5, -6
 STATUS_TIMEOUT, STATUS_NONFINITE = 1, 2
+TILE_AUTO, TILE_NARROW, TILE_WIDE = 0, 1, 2
 
 # every exported symbol of include/btdma.h
 EXPORTS = (
@@ -30,7 +31,7 @@ EXPORTS = (
     "btdma_heat_step", "btdma_heat_l2_error", "btdma_heat_step_profile", "btdma_poisson_create", "btdma_poisson_destroy",
     "btdma_poisson_solve", "btdma_poisson_status", "btdma_momentum_create",
     "btdma_momentum_destroy", "btdma_momentum_sweep", "btdma_momentum_adi", "btdma_momentum_status",
-    "btdma_selftest_wait_timeout",
+    "btdma_selftest_wait_timeout", "btdma_set_tile_shape",
 )
 NOALLOC_MAX_ELEMS = 1 << 20
 REFINE_MAX_SWEEPS = 4
@@ -88,6 +89,7 @@ def lib():
         L.btdma_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint)]
         L.btdma_set_method.argtypes = [vp, i]
         L.btdma_segments.argtypes = [vp, ctypes.POINTER(i)]
+        L.btdma_set_tile_shape.argtypes = [vp, i]
         L.btdma_solve_noalloc.argtypes = [vp, vp, vp, vp, i, i, vp]
         L.btdma_solve_f32.argtypes = [vp, vp, vp, vp, vp, vp, i, i, i, vp]
         L.btdma_set_refine.argtypes = [vp, i, d]

@@ -84,7 +84,8 @@ int solve_impl(btdma_t h, const double* A, const double* B, const double* C, con
     }
 
     if (h->method == BTDMA_PASCAL && !(h->flags & BTDMA_FLAG_REFERENCE_ORDER)) {
-        rc = try_tile<double>(A, B, C, D, X, n_sys, n_row, cyclic, h->status, st);
+        rc = try_tile<double>(A, B, C, D, X, n_sys, n_row, cyclic, h->status, st, false,
+                              nullptr, h->tile_shape);
         if (rc < 0) return rc;
         if (rc == 1) return BTDMA_OK;
     }
@@ -255,7 +256,8 @@ int btdma_solve_f32(btdma_t h, const float* A, const float* B, const float* C, c
         "FP32 storage needs n_row % 16 == 0, n_sys % 4 == 0, 16-byte alignment "
         "(and a power-of-two n_row/16 when periodic)";
     if (h->precision == BTDMA_FP32_STORE) {
-        rc = try_tile<float>(A, B, C, D, X, n_sys, n_row, cyc, h->status, stream);
+        rc = try_tile<float>(A, B, C, D, X, n_sys, n_row, cyc, h->status, stream, false,
+                             nullptr, h->tile_shape);
         if (rc < 0) return rc;
         if (rc == 0) return fail(BTDMA_ERR_UNSUPPORTED, "%s", shape_msg);
         return BTDMA_OK;
@@ -378,6 +380,14 @@ int btdma_set_method(btdma_t h, int method) {
     if (method < BTDMA_PASCAL || method > BTDMA_FILTERED_V2)
         return fail(BTDMA_ERR_ARG, "unknown method %d", method);
     h->method = method;
+    return BTDMA_OK;
+}
+
+int btdma_set_tile_shape(btdma_t h, int shape) {
+    if (!h) return fail(BTDMA_ERR_ARG, "null handle");
+    if (shape < BTDMA_TILE_AUTO || shape > BTDMA_TILE_WIDE)
+        return fail(BTDMA_ERR_ARG, "unknown tile shape %d", shape);
+    h->tile_shape = shape;
     return BTDMA_OK;
 }
 

@@ -17,11 +17,13 @@
 #include "btdma_common.cuh"
 #include "k_segment.cuh"
 #include "k_tile.cuh"
+#include "k_tile_wide.cuh"
 
 using namespace btdma;
 
 struct btdma_handle {
     int method, P, precision, flags;
+    int tile_shape = 0;  // BTDMA_TILE_AUTO / NARROW / WIDE (uniform PaScaL batches)
     int n_sys_cap, n_row_cap;
     double eps_constant;
     double* rho_row = nullptr;               // [n_row_cap] per-row spectral bound
@@ -313,6 +315,68 @@ int launch_tile_plan(const TilePlan& pl, const CUtensorMap* maps, const TileArgs
     }
 }
 
+// BTDMA_TILE_AUTO's choice between the kernels for a shape both take, from
+// B200 measurements of 262144 x 512, 524288 x 256 and 1048576 x 128 batches:
+// the wide kernel wins only for FP32 storage above 16 sub-segments (0.85 vs
+// 1.02 ms at 512 rows, where the narrow kernel reads 64-byte row pieces); at 16
+// or fewer sub-segments the narrow kernel already reads 128-byte pieces, and
+// for FP64 it reads 128-byte pieces with all state in registers (1.05 vs
+// 1.23 ms at 512 rows).
+inline bool wide_by_default(int n_row, int elem) {
+    return elem == 4 && n_row / TILE_MT > 16;
+}
+
+// Plan of the wide-box kernel (k_tile_wide.cuh): sys == 0 when the shape does
+// not take it.
+inline TilePlan tile_wide_plan(int n_row, bool cyclic, int elem) {
+    TilePlan pl;
+    if (n_row % TILE_MT != 0) return pl;
+    const int nseg = n_row / TILE_MT;
+    if (nseg < 8 || nseg > 32 || nseg % 2 != 0) return pl;
+    if (cyclic && (nseg & (nseg - 1)) != 0) return pl;
+    const int h = nseg / 2;
+    const int sys = h > 8 ? 32 : (h > 4 ? 64 : 128);
+    int nst = TILE_MAX_NST;
+    while (nst >= 3 && tile_wide_smem_bytes(sys, nseg, nst, elem) > (size_t)max_smem_optin())
+        --nst;
+    if (nst < 3) return pl;
+    pl.sys = sys;
+    pl.cl = 1;
+    pl.nst = nst;
+    pl.nseg = nseg;
+    return pl;
+}
+
+template <int SYS, bool CYCLIC, typename TIN>
+int launch_tile_wide(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st) {
+    auto kern = tile_wide_kernel<SYS, CYCLIC, TIN>;
+    static bool attr_done = false;
+    if (!attr_done) {
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                max_smem_optin()));
+        attr_done = true;
+    }
+    const int threads = SYS * (a.nseg / 2);
+    const size_t smem = tile_wide_smem_bytes(SYS, a.nseg, a.nst, (int)sizeof(TIN));
+    const int grid = std::min(num_sms(), a.n_groups);
+    kern<<<grid, threads, smem, st>>>(maps[0], maps[1], maps[2], maps[3], a);
+    CK(cudaGetLastError());
+    return BTDMA_OK;
+}
+
+template <typename TIN>
+int launch_tile_wide_plan(const TilePlan& pl, const CUtensorMap* maps, const TileArgs& a,
+                          bool cyclic, cudaStream_t st) {
+    switch (pl.sys * 2 + (cyclic ? 1 : 0)) {
+        case 256: return launch_tile_wide<128, false, TIN>(maps, a, st);
+        case 257: return launch_tile_wide<128, true, TIN>(maps, a, st);
+        case 128: return launch_tile_wide<64, false, TIN>(maps, a, st);
+        case 129: return launch_tile_wide<64, true, TIN>(maps, a, st);
+        case 65: return launch_tile_wide<32, true, TIN>(maps, a, st);
+        default: return launch_tile_wide<32, false, TIN>(maps, a, st);
+    }
+}
+
 inline bool tma_ok_elem(const void* p, int n_sys, int elem) {
     return ((reinterpret_cast<uintptr_t>(p) & 15) == 0) && ((size_t)n_sys * elem) % 16 == 0;
 }
@@ -321,17 +385,25 @@ inline bool tma_ok_elem(const void* p, int n_sys, int elem) {
 // cluster-per-segment kernel, < 0 on error.
 // TC: arithmetic of the local sweeps; accumulate: X += solution; gate: the
 // kernel does nothing while *gate == 0.
+// shape: BTDMA_TILE_* (the wide-box kernel serves FP64-arithmetic plain solves).
 template <typename TIN, typename TC = double>
 int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, int n_sys,
              int n_row, bool cyclic, unsigned* status, cudaStream_t st, bool accumulate = false,
-             const unsigned* gate = nullptr) {
+             const unsigned* gate = nullptr, int shape = BTDMA_TILE_NARROW) {
     const int elem = (int)sizeof(TIN);
-    const TilePlan pl = tile_plan(n_row, cyclic, elem);
+    bool wide = false;
+    TilePlan pl;
+    if (shape != BTDMA_TILE_NARROW && sizeof(TC) == 8 && !accumulate && gate == nullptr) {
+        pl = tile_wide_plan(n_row, cyclic, elem);
+        wide = pl.sys != 0 && (shape == BTDMA_TILE_WIDE || wide_by_default(n_row, elem));
+    }
+    if (!wide) pl = tile_plan(n_row, cyclic, elem);
     if (pl.sys == 0) return 0;
     if (!(tma_ok_elem(A, n_sys, elem) && tma_ok_elem(B, n_sys, elem) &&
           tma_ok_elem(C, n_sys, elem) && tma_ok_elem(D, n_sys, elem)))
         return 0;
-    const int nsc = pl.nseg / pl.cl;
+    // sub-segments per TMA box: the CTA's share (narrow), or half a system (wide)
+    const int nsc = wide ? pl.nseg / 2 : pl.nseg / pl.cl;
     CUtensorMap maps[4];
     if (!(make_tile_map(&maps[0], A, n_sys, pl.nseg, pl.sys, nsc, elem) &&
           make_tile_map(&maps[1], B, n_sys, pl.nseg, pl.sys, nsc, elem) &&
@@ -349,7 +421,8 @@ int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, 
     a.accumulate = accumulate ? 1 : 0;
     a.gate = gate;
     a.status = status;
-    const int rc = launch_tile_plan<TIN, TC>(pl, maps, a, cyclic, st);
+    const int rc = wide ? launch_tile_wide_plan<TIN>(pl, maps, a, cyclic, st)
+                        : launch_tile_plan<TIN, TC>(pl, maps, a, cyclic, st);
     return rc == BTDMA_OK ? 1 : rc;
 }
 

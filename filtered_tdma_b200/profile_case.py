@@ -34,6 +34,8 @@ def main():
                          "--heat-grid; poisson: channel wall-normal solve 128 x 65 x 192")
     ap.add_argument("--heat-grid", default="256,384,512")
     ap.add_argument("--no-tune", action="store_true", help="ragged: keep the default plan")
+    ap.add_argument("--tile-shape", choices=["auto", "narrow", "wide"], default="auto",
+                    help="batch: kernel shape of the tiled PaScaL solve")
     args = ap.parse_args()
     if args.case != "batch":
         return other_case(args)
@@ -52,6 +54,8 @@ def main():
         A, B, C, D = [t.float() for t in (A, B, C, D)]
     s = Solver(args.method, args.n_sys, args.n_row, args.P,
                precision=L.FP32_STORE if f32 else L.FP64)
+    s.set_tile_shape({"auto": L.TILE_AUTO, "narrow": L.TILE_NARROW,
+                      "wide": L.TILE_WIDE}[args.tile_shape])
     if args.method != "pascal":
         s.set_eps_constant(1e-3)
         s.set_rho(A, B, C, all_systems=True)

@@ -173,6 +173,11 @@ class Solver:
         L.check(L.lib().btdma_ragged_plan_info(self._h, arr, n.value, ctypes.byref(n)))
         return [arr[i].as_dict() for i in range(n.value)]
 
+    def set_tile_shape(self, shape):
+        """Kernel shape of the tiled PaScaL solves: TILE_AUTO, TILE_NARROW or
+        TILE_WIDE (same results; see btdma_set_tile_shape)."""
+        L.check(L.lib().btdma_set_tile_shape(self._h, int(shape)))
+
     def set_refine(self, max_sweeps=3, eta_tol=8 * 2.0**-53):
         """Refinement sweeps and backward-error bound of an FP32_REFINE handle."""
         L.check(L.lib().btdma_set_refine(self._h, int(max_sweeps), float(eta_tol)))

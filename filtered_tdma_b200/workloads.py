@@ -12,6 +12,10 @@ These generators stand in for them:
 * ``diag_dominant``   per-system r drawn log-uniform in [r_lo, r_hi]
                       (A = C = -r, B = 1+2r), D uniform in [-1, 1].
 * ``weak_dominance``  per-system rho uniform in [rho_lo, rho_hi], r = rho/(1-2rho).
+* ``row_varying``     every coefficient drawn on its own (|A|, |C| log-uniform in
+                      [0.05, 5] with random signs, B = (|A| + |C|) / rho with rho
+                      uniform in [0.3, 0.9] per row), so a kernel that takes a
+                      coefficient from the wrong row or system is caught.
 * ``ragged_batch``    systems of different lengths (n log-uniform in
                       [n_lo, n_hi]) stored back to back with CSR row offsets,
                       a fraction of them periodic, per-system r log-uniform.
@@ -70,6 +74,18 @@ def weak_dominance(n_sys: int, n_row: int, rho_lo: float = 0.45, rho_hi: float =
     r = rho / (1.0 - 2.0 * rho)
     D = rng.uniform(-1.0, 1.0, size=(n_row, n_sys))
     return _np_batch(r, n_row, D, dtype)
+
+
+def row_varying(n_sys: int, n_row: int, seed: int = 7, dtype=np.float64):
+    rng = np.random.default_rng(seed)
+    shape = (n_row, n_sys)
+    a = 10.0 ** rng.uniform(np.log10(0.05), np.log10(5.0), size=shape)
+    c = 10.0 ** rng.uniform(np.log10(0.05), np.log10(5.0), size=shape)
+    a *= rng.choice([-1.0, 1.0], size=shape)
+    c *= rng.choice([-1.0, 1.0], size=shape)
+    b = (np.abs(a) + np.abs(c)) / rng.uniform(0.3, 0.9, size=shape)
+    D = rng.uniform(-1.0, 1.0, size=shape)
+    return tuple(np.ascontiguousarray(v, dtype=dtype) for v in (a, b, c, D))
 
 
 def _torch_batch(_unused, n_sys, n_row, seed, dtype, device, const_r=None, log_r=None, rho=None):

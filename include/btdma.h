@@ -317,6 +317,19 @@ int btdma_set_method(btdma_t h, int method);
 /* Segments per system used by the handle (after the P = 0 choice). */
 int btdma_segments(btdma_t h, int* P);
 
+/* Kernel shape of the PaScaL solves that run the register-tiled kernel
+ * (FP64 and FP32 storage with FP64 arithmetic).  NARROW: SYS systems per CTA
+ * with every row's elimination state in registers.  WIDE: twice the systems
+ * per CTA (wider HBM row pieces), half of each group's rows read a second time
+ * from L2 instead of held.  AUTO: the library's measured choice per shape.
+ * Both return the same bits.  No counterpart in the reference. */
+enum btdma_tile_shape {
+    BTDMA_TILE_AUTO = 0,
+    BTDMA_TILE_NARROW = 1,
+    BTDMA_TILE_WIDE = 2
+};
+int btdma_set_tile_shape(btdma_t h, int shape);
+
 /* Serial Thomas solve (D <- x, bit-identical to btdma_solve with P = 1) that
  * allocates nothing.  No counterpart in the reference.
  *

@@ -47,6 +47,7 @@ def test_argument_checks(lib):
     assert b"null" in lib.btdma_last_error()
     assert lib.btdma_set_refine(None, 3, 1e-15) == L.ERR_ARG
     assert lib.btdma_last_stats(None, None) == L.ERR_ARG
+    assert lib.btdma_set_tile_shape(None, L.TILE_WIDE) == L.ERR_ARG
 
 
 def test_stats_struct_layout():

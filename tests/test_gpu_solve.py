@@ -335,3 +335,49 @@ def test_fp32_refine_cyclic(cuda, orc):
     x, wid = run_f32(cuda, A, B, C, D, L.FP32_REFINE, cyclic=True, stats=st)
     assert rel_err(x, orc.thomas_cyclic(*wid)) <= 1e-12
     assert st["n_fallback"] == 0
+
+
+# ------------------------------------------- coefficients that differ in every row
+# The generators above give each system one coefficient triple; these batches
+# draw A, B, C per row and system, so a kernel that takes a coefficient from the
+# wrong row, sub-segment or system fails by far more than rounding.
+@pytest.mark.parametrize("n_sys,n_row", [(96, 64), (1000, 129), (258, 512)])
+def test_row_varying_thomas_bit_exact(cuda, orc, n_sys, n_row):
+    A, B, C, D = W.row_varying(n_sys, n_row, seed=n_row)
+    x, _ = run(cuda, "pascal", A, B, C, D, 1)
+    assert np.array_equal(x, orc.thomas(A, B, C, D))
+    x, _ = run(cuda, "pascal", A, B, C, D, 1, cyclic=True)
+    assert np.array_equal(x, orc.thomas_cyclic(A, B, C, D))
+
+
+@pytest.mark.parametrize("n_sys,n_row,P", [(64, 64, 4), (100, 96, 8), (64, 1000, 16)])
+def test_row_varying_reference_order_bit_exact(cuda, orc, n_sys, n_row, P):
+    from filtered_tdma_b200 import _lib as L
+    A, B, C, D = W.row_varying(n_sys, n_row, seed=P + n_row)
+    x, _ = run(cuda, "pascal", A, B, C, D, P, flags=L.FLAG_REFERENCE_ORDER)
+    assert np.array_equal(x, orc.pascal(A, B, C, D, P))
+    x, _ = run(cuda, "pascal", A, B, C, D, P, cyclic=True, flags=L.FLAG_REFERENCE_ORDER)
+    assert np.array_equal(x, orc.pascal(A, B, C, D, P, cyclic=True))
+
+
+@pytest.mark.parametrize("n_sys,n_row", [(4096, 64), (1000, 128), (130, 256), (4094, 384),
+                                         (2048, 512), (96, 768), (64, 1024), (34, 2048)])
+def test_row_varying_tiled_within_1e12(cuda, orc, n_sys, n_row):
+    """Every tiled shape: one CTA (16 to 128 systems a CTA) and clusters."""
+    A, B, C, D = W.row_varying(n_sys, n_row, seed=n_sys + n_row)
+    x, _ = run(cuda, "pascal", A, B, C, D, 8)
+    assert rel_err(x, orc.thomas(A, B, C, D)) <= 1e-12
+    if (n_row // 16) & (n_row // 16 - 1) == 0:
+        x, _ = run(cuda, "pascal", A, B, C, D, 8, cyclic=True)
+        assert rel_err(x, orc.thomas_cyclic(A, B, C, D)) <= 1e-12
+
+
+@pytest.mark.parametrize("precision", ["store", "refine"])
+def test_row_varying_fp32(cuda, orc, precision):
+    from filtered_tdma_b200 import _lib as L
+    prec = L.FP32_STORE if precision == "store" else L.FP32_REFINE
+    for n_sys, n_row, cyc in ((2048, 512, False), (520, 256, True), (96, 1024, False)):
+        A, B, C, D = W.row_varying(n_sys, n_row, seed=n_row + 1)
+        x, wid = run_f32(cuda, A, B, C, D, prec, cyclic=cyc)
+        ref = orc.thomas_cyclic(*wid) if cyc else orc.thomas(*wid)
+        assert rel_err(x, ref) <= 1e-12

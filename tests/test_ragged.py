@@ -133,3 +133,18 @@ def test_ragged_long_systems_cta_path(cuda, orc):
     assert any(b["cta_per_system"] == 1 and b["lanes_per_system"] == 512 for b in plan)
     x, plan = solve_on_device(cuda, (A, B, C, D), off, per, tune=True)
     assert per_system_err(x, ref, off) <= 1e-12
+
+
+@pytest.mark.gpu
+def test_ragged_row_varying_coefficients(cuda, orc):
+    # coefficients drawn per row (the other ragged batches hold one triple per
+    # system), lengths across the warp and CTA kinds, both kinds of system
+    n = np.array([3, 5, 17, 40, 64, 100, 255, 256, 511, 600, 1024, 3000, 5000] * 3)
+    per = (np.arange(n.size) % 3 == 1).astype(np.uint8)
+    off = np.concatenate([[0], np.cumsum(n)]).astype(np.int64)
+    A, B, C, D = [v[:, 0].copy() for v in W.row_varying(1, int(off[-1]), seed=57)]
+    ref = ragged_oracle(orc, A, B, C, D, off, per)
+    x, _ = solve_on_device(cuda, (A, B, C, D), off, per)
+    assert per_system_err(x, ref, off) <= 1e-12
+    x, _ = solve_on_device(cuda, (A, B, C, D), off, per, tune=True)
+    assert per_system_err(x, ref, off) <= 1e-12
