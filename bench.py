@@ -289,8 +289,8 @@ def main():
     k_ms = sum(per) / len(per)  # one kernel launch per PaScaL step
     achieved = BYTES_PER_ROW_F64 * rows / (k_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": ncu_traffic("tile_pascal_f64_262144x512"),
-                "kernel": "btdma::tile_f64_kernel<16>", "peak_source": peak_src,
+                "frac": achieved / peak, "traffic": ncu_traffic("tile_wide_f64_262144x512"),
+                "kernel": "btdma::tile_wide_kernel<32, false, double>", "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": BYTES_PER_ROW_F64 * rows}
 
     # ---------------------------------------------------------- variants (rank 0 reports)
@@ -359,6 +359,8 @@ def main():
                 v["refinement"] = s.last_stats()
             else:
                 v["refinement_sweeps"] = 0
+                v["kernel"] = "btdma::tile_wide_kernel<32, false, float>"
+                v["traffic"] = ncu_traffic("tile_wide_f32_262144x512")
             variants[name] = v
             s.close()
 

@@ -465,7 +465,10 @@ __global__ void selftest_wait_kernel(unsigned* status, uint32_t limit) {
         fence_mbar_init();
     }
     __syncthreads();
-    if (threadIdx.x == 0) (void)mbar_wait_bounded(&bar, 0, status, limit);
+    if (threadIdx.x == 0) {
+        (void)mbar_wait_bounded(&bar, 0, &status[0], limit);
+        (void)mbar_wait_bounded_spin(&bar, 0, &status[1], limit);
+    }
 }
 
 }  // namespace
@@ -474,14 +477,18 @@ int btdma_selftest_wait_timeout(int limit, unsigned* status_out, cudaStream_t st
     if (limit <= 0 || limit > (1 << 16) || !status_out)
         return fail(BTDMA_ERR_ARG, "limit in [1, 65536] and an output word are required");
     unsigned* d = nullptr;
-    CK(cudaMalloc(&d, sizeof(unsigned)));
-    cudaMemsetAsync(d, 0, sizeof(unsigned), stream);
-    selftest_wait_kernel<<<1, 32, 0, stream>>>(d, (uint32_t)limit);
-    cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpyAsync(status_out, d, sizeof(unsigned),
-                                              cudaMemcpyDeviceToHost, stream);
+    CK(cudaMalloc(&d, 2 * sizeof(unsigned)));
+    unsigned h[2] = {0, 0};
+    cudaError_t e = cudaMemsetAsync(d, 0, 2 * sizeof(unsigned), stream);
+    if (e == cudaSuccess) {
+        selftest_wait_kernel<<<1, 32, 0, stream>>>(d, (uint32_t)limit);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h, d, sizeof h, cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     cudaFree(d);
     CK(e);
+    *status_out = h[0] & h[1];  // a bit only if both waits raised it
     return BTDMA_OK;
 }

@@ -105,6 +105,43 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return mbar_wait_slow(bar, parity, status, limit);
 }
 
+// One poll without a suspend-time hint: the hardware's own, shorter limit, so a
+// waiting warp polls again sooner.  Measured faster than the hinted poll for the
+// wide tiled kernel (every warp waits on every stage) and slower for the narrow
+// one.
+__device__ __forceinline__ bool mbar_try_wait_spin(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+static __device__ __noinline__ bool mbar_wait_spin_slow(uint64_t* bar, uint32_t parity,
+                                                        unsigned* status, uint32_t limit) {
+    for (uint32_t it = 0; it < limit; ++it) {
+        if (mbar_try_wait_spin(bar, parity)) return true;
+        if (status && (it & 1023u) == 1023u &&
+            (*reinterpret_cast<volatile unsigned*>(status) & ST_TIMEOUT))
+            return false;
+    }
+    raise_status(status, ST_TIMEOUT);
+    return false;
+}
+
+// Bounded wait with unhinted polls (a poll lasts far less than kSuspendNs, so
+// the default limit allows more of them).
+__device__ __forceinline__ bool mbar_wait_bounded_spin(uint64_t* bar, uint32_t parity,
+                                                       unsigned* status,
+                                                       uint32_t limit = 1u << 22) {
+    if (mbar_try_wait_spin(bar, parity)) return true;
+    return mbar_wait_spin_slow(bar, parity, status, limit);
+}
+
 static __device__ __noinline__ bool mbar_wait_slow(uint64_t* bar, uint32_t parity, unsigned* status,
                                             uint32_t limit) {
     for (uint32_t it = 0; it < limit; ++it) {

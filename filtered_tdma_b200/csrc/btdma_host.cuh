@@ -316,14 +316,14 @@ int launch_tile_plan(const TilePlan& pl, const CUtensorMap* maps, const TileArgs
 }
 
 // BTDMA_TILE_AUTO's choice between the kernels for a shape both take, from
-// B200 measurements of 262144 x 512, 524288 x 256 and 1048576 x 128 batches:
-// the wide kernel wins only for FP32 storage above 16 sub-segments (0.85 vs
-// 1.02 ms at 512 rows, where the narrow kernel reads 64-byte row pieces); at 16
-// or fewer sub-segments the narrow kernel already reads 128-byte pieces, and
-// for FP64 it reads 128-byte pieces with all state in registers (1.05 vs
-// 1.23 ms at 512 rows).
+// B200 measurements (262144 x 512, 524288 x 256, 1048576 x 128; ms):
+//   FP32 storage  narrow 1.03 / 0.81 / 0.83   wide 0.82 / 0.73 / 0.72
+//   FP64          narrow 1.06 / 0.97 / 0.96   wide 1.03 / 1.02 / 1.01
+// The narrow kernel reads 64-byte row pieces for FP32 at 512 rows and 128-byte
+// pieces elsewhere; the wide kernel's extra pass over half the rows pays off
+// for FP32 storage everywhere and for FP64 above 16 sub-segments only.
 inline bool wide_by_default(int n_row, int elem) {
-    return elem == 4 && n_row / TILE_MT > 16;
+    return elem == 4 || n_row / TILE_MT > 16;
 }
 
 // Plan of the wide-box kernel (k_tile_wide.cuh): sys == 0 when the shape does

@@ -184,7 +184,7 @@ tile_wide_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
     // Next stage's RPS rows of this thread's sub-segment (widened), then the
     // release of the slot and, one stage later, its refill.
     auto fetch = [&](double (&a2)[RPS], double (&b2)[RPS], double (&c2)[RPS], double (&d2)[RPS]) {
-        if (ok) ok = mbar_wait_bounded(&full[slot], phase, args.status);
+        if (ok) ok = mbar_wait_bounded_spin(&full[slot], phase, args.status);
 #pragma unroll
         for (int r = 0; r < RPS; ++r) {
             a2[r] = (double)st[0 * RPS * T + r * SYS];
@@ -196,7 +196,7 @@ tile_wide_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
         if (lane == 0) {
             mbar_arrive(&empty[slot]);
             if (t >= 1 && warp == tw && t - 1 + nst < total && ok) {
-                ok = mbar_wait_bounded(&empty[pslot], pphase, args.status);
+                ok = mbar_wait_bounded_spin(&empty[pslot], pphase, args.status);
                 if (ok) issue(t - 1 + nst);
             }
         }

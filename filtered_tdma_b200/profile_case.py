@@ -71,7 +71,7 @@ def main():
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
-        print(f"rep {r}: {ms:.4f} ms  {rows / ms / 1e6:.3e} rows/s  "
+        print(f"rep {r}: {ms:.4f} ms  {rows / ms / 1e6:.2f} G rows/s  "
               f"{bpr * rows / ms / 1e6:.1f} GB/s ({bpr} B/row)")
     if s.status() != 0:
         raise SystemExit("device status word set")

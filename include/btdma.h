@@ -302,9 +302,10 @@ int btdma_momentum_adi(btdma_momentum_t h, int comp, double* rhs, double* q_out,
 int btdma_momentum_status(btdma_momentum_t h, unsigned* status, cudaStream_t stream);
 
 /* Self test of the failure path of every pipeline wait: a one-thread kernel
- * waits with the library's bounded wait (at most `limit` polls of up to 20 us)
- * on an mbarrier nothing arrives at; *status_out receives the device status
- * word, which must have BTDMA_STATUS_TIMEOUT set.  No fault, no hang. */
+ * waits with each of the library's bounded waits (at most `limit` polls; a
+ * hinted poll lasts up to 20 us, an unhinted one far less) on an mbarrier
+ * nothing arrives at; *status_out receives the AND of their device status
+ * words, which must have BTDMA_STATUS_TIMEOUT set.  No fault, no hang. */
 #define BTDMA_STATUS_TIMEOUT 1u
 #define BTDMA_STATUS_NONFINITE 2u
 int btdma_selftest_wait_timeout(int limit, unsigned* status_out, cudaStream_t stream);
