@@ -179,13 +179,18 @@ __global__ void __launch_bounds__(256) ragged_kernel(const RagArgs a) {
 constexpr int RAG_MT = 16;
 
 // STAGED: the whole system is first copied into shared memory with coalesced
-// loads, laid out [array][row of segment][thread] (A, B, C, D widened to
-// FP64), the elimination state then overwrites A, C, D in place and x goes
-// through B on its way out (coalesced stores).  Without staging each thread
-// reads its contiguous rows straight from global memory, which leaves L1 to
-// hold four lines per thread.
+// loads, laid out [array][thread][row of segment] with an odd pitch of
+// RAG_MT + 1 doubles (A, B, C, D widened to FP64): consecutive rows of a
+// segment are consecutive words for the coalesced fill, and the threads reading
+// row k of their segments are 17 doubles apart (no bank conflicts either way).
+// The elimination state then overwrites A, C, D in place and x goes through B
+// on its way out (coalesced stores).  Without staging each thread reads its
+// contiguous rows straight from global memory, which leaves L1 to hold four
+// lines per thread.
+constexpr int RAG_MP = RAG_MT + 1;  // staged pitch per thread
 __host__ __device__ __forceinline__ size_t rag_cta_smem_bytes(int P, bool staged) {
-    return (2ull * 3 * (P + 2) + (staged ? 4ull : 3ull) * RAG_MT * P) * sizeof(double);
+    return (2ull * 3 * (P + 2) + (staged ? 4ull * RAG_MP * P : 3ull * RAG_MT * P)) *
+           sizeof(double);
 }
 
 // (segment, row in segment) of row r of a system split by para_range into P
@@ -234,8 +239,12 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
     const TIN* __restrict__ pC = static_cast<const TIN*>(a.C) + row0;
     const TIN* __restrict__ pD = static_cast<const TIN*>(a.D) + row0;
 
-    double* const stg = rsm + 2 * 3 * gs;  // [field][row][thread] area
-    double* stt = stg + p;                  // this thread's column: stt[(f * M + k) * P]
+    double* const stg = rsm + 2 * 3 * gs;  // state / staging area
+    // this thread's slots: unstaged [field][row][thread] -> stt[(f * M + k) * P];
+    // staged [field][thread][row] -> stt[f * P * RAG_MP + k]
+    double* stt = STAGED ? stg + p * RAG_MP : stg + p;
+    const int fs = STAGED ? P * RAG_MP : M * P;  // field stride
+    const int ks = STAGED ? 1 : P;               // row stride
     const float inv0 = 1.0f / (float)(base > 0 ? base : 1), inv1 = 1.0f / (float)(base + 1);
     if constexpr (STAGED) {
         // fields 0..3 = A, B, C, D; coalesced over the system's rows
@@ -246,17 +255,18 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
         for (int r = p; r < n; r += P) {
             int q, k;
             rag_locate(r, base, rem, inv0, inv1, q, k);
-            stg[(0 * M + k) * P + q] = (double)gA[r];
-            stg[(1 * M + k) * P + q] = (double)gB[r];
-            stg[(2 * M + k) * P + q] = (double)gC[r];
-            stg[(3 * M + k) * P + q] = (double)gD[r];
+            double* dst = stg + q * RAG_MP + k;
+            dst[0 * fs] = (double)gA[r];
+            dst[1 * fs] = (double)gB[r];
+            dst[2 * fs] = (double)gC[r];
+            dst[3 * fs] = (double)gD[r];
         }
         __syncthreads();
     }
     // state: alpha, gamma, delta (in place of A, C, D when staged)
-    auto AL = [&](int k) -> double& { return stt[(0 * M + k) * P]; };
-    auto GA = [&](int k) -> double& { return stt[((STAGED ? 2 : 1) * M + k) * P]; };
-    auto DE = [&](int k) -> double& { return stt[((STAGED ? 3 : 2) * M + k) * P]; };
+    auto AL = [&](int k) -> double& { return stt[0 * fs + k * ks]; };
+    auto GA = [&](int k) -> double& { return stt[(STAGED ? 2 : 1) * fs + k * ks]; };
+    auto DE = [&](int k) -> double& { return stt[(STAGED ? 3 : 2) * fs + k * ks]; };
     double ab0 = 0, cb0 = 0, db0 = 0, pi = 1.0, sa = 0.0, sd = 0.0, pi_last = 0.0;
     double alp = 0, gap = 0, dep = 0;  // row k-1
 #pragma unroll
@@ -266,10 +276,10 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
         for (int j = 0; j < RAG_LOOKAHEAD; ++j) {  // loads of the next rows (clamped in bounds)
             const int kk = k0 + j < m ? k0 + j : m - 1;
             if constexpr (STAGED) {
-                ra[j] = stt[(0 * M + kk) * P];
-                rb[j] = stt[(1 * M + kk) * P];
-                rc[j] = stt[(2 * M + kk) * P];
-                rd[j] = stt[(3 * M + kk) * P];
+                ra[j] = stt[0 * fs + kk];
+                rb[j] = stt[1 * fs + kk];
+                rc[j] = stt[2 * fs + kk];
+                rd[j] = stt[3 * fs + kk];
             } else {
                 ra[j] = (double)__ldg(pA + kk);
                 rb[j] = (double)__ldg(pB + kk);
@@ -377,7 +387,7 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
     double nonfinite = fma(xf, 0.0, fma(xl, 0.0, 0.0));
     double xn = xl;
     // staged: x goes into the B field (no longer read) and leaves coalesced
-    auto XO = [&](int k) -> double& { return stt[(1 * M + k) * P]; };
+    auto XO = [&](int k) -> double& { return stt[1 * fs + k * ks]; };
 #pragma unroll
     for (int k = M - 2; k >= 1; --k) {
         if (k <= m - 2) {
@@ -397,7 +407,7 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
         for (int r = p; r < n; r += P) {
             int q, k;
             rag_locate(r, base, rem, inv0, inv1, q, k);
-            gX[r] = stg[(1 * M + k) * P + q];
+            gX[r] = stg[1 * fs + q * RAG_MP + k];
         }
     } else {
         xp[0] = xf;
