@@ -31,7 +31,7 @@ EXPORTS = (
     "btdma_heat_step", "btdma_heat_l2_error", "btdma_heat_step_profile", "btdma_poisson_create", "btdma_poisson_destroy",
     "btdma_poisson_solve", "btdma_poisson_status", "btdma_momentum_create",
     "btdma_momentum_destroy", "btdma_momentum_sweep", "btdma_momentum_adi", "btdma_momentum_status",
-    "btdma_selftest_wait_timeout", "btdma_set_tile_shape",
+    "btdma_selftest_wait_timeout", "btdma_set_tile_shape", "btdma_ragged_set_plan",
 )
 NOALLOC_MAX_ELEMS = 1 << 20
 REFINE_MAX_SWEEPS = 4
@@ -90,6 +90,7 @@ def lib():
         L.btdma_set_method.argtypes = [vp, i]
         L.btdma_segments.argtypes = [vp, ctypes.POINTER(i)]
         L.btdma_set_tile_shape.argtypes = [vp, i]
+        L.btdma_ragged_set_plan.argtypes = [vp, ctypes.POINTER(RaggedBucket), i]
         L.btdma_solve_noalloc.argtypes = [vp, vp, vp, vp, i, i, vp]
         L.btdma_solve_f32.argtypes = [vp, vp, vp, vp, vp, vp, i, i, i, vp]
         L.btdma_set_refine.argtypes = [vp, i, d]

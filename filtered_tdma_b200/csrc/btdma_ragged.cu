@@ -342,6 +342,47 @@ int btdma_ragged_autotune(btdma_t h, const void* A, const void* B, const void* C
                            row_offsets, is_periodic, n_sys, stream);
 }
 
+int btdma_ragged_set_plan(btdma_t h, const btdma_ragged_bucket* in, int n) {
+    if (!h || (!in && n > 0)) return fail(BTDMA_ERR_ARG, "null argument");
+    if (n != (int)h->rag_buckets.size())
+        return fail(BTDMA_ERR_ARG, "the current plan has %d buckets, %d given",
+                    (int)h->rag_buckets.size(), n);
+    for (int i = 0; i < n; ++i) {
+        const auto& b = h->rag_buckets[i];
+        const btdma_ragged_bucket& g = in[i];
+        if (g.periodic != b.cyc || g.n_systems != b.count || g.n_row_min != b.nmin ||
+            g.n_row_max != b.nmax)
+            return fail(BTDMA_ERR_ARG, "bucket %d does not match the current plan", i);
+        const int P = g.lanes_per_system, kind = g.cta_per_system;
+        if (P <= 0 || (P & (P - 1)) != 0 || b.nmin / P < 3)
+            return fail(BTDMA_ERR_ARG, "bucket %d: %d lanes per system", i, P);
+        if (kind == 0) {
+            if (P > 32 || rag_mcap(b.nmax, P) > RAG_WARP_MCAP)
+                return fail(BTDMA_ERR_ARG, "bucket %d: warp kind needs P <= 32 and <= %d rows "
+                            "per lane", i, RAG_WARP_MCAP);
+        } else if (kind == 1 || kind == 2) {
+            if (P < 64 || P > 512 || rag_mcap(b.nmax, P) > RAG_MT)
+                return fail(BTDMA_ERR_ARG, "bucket %d: CTA kind needs 64 <= P <= 512 and <= %d "
+                            "rows per thread", i, RAG_MT);
+            if (kind == 2 && rag_cta_smem_bytes(P, true) > (size_t)max_smem_optin())
+                return fail(BTDMA_ERR_ARG, "bucket %d: a staged system of %d threads does not "
+                            "fit in shared memory", i, P);
+        } else {
+            return fail(BTDMA_ERR_ARG, "bucket %d: cta_per_system %d", i, kind);
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        auto& b = h->rag_buckets[i];
+        b.P = in[i].lanes_per_system;
+        b.cta = in[i].cta_per_system > 0 ? 1 : 0;
+        b.staged = in[i].cta_per_system == 2 ? 1 : 0;
+        b.warps = b.cta ? b.P / 32 : RAG_WPC;
+        b.mcap = rag_mcap(b.nmax, b.P);
+        b.best_ms = in[i].tuned_ms;
+    }
+    return rag_build_launches(h);
+}
+
 int btdma_ragged_plan_info(btdma_t h, btdma_ragged_bucket* out, int cap, int* n_out) {
     if (!h || !n_out) return fail(BTDMA_ERR_ARG, "null argument");
     *n_out = (int)h->rag_buckets.size();

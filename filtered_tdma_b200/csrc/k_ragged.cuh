@@ -86,16 +86,23 @@ __global__ void __launch_bounds__(256) ragged_kernel(const RagArgs a) {
     double alp = 0, gap = 0, dep = 0;  // row k-1
     double pi = 1.0, sa = 0.0, sd = 0.0, pi_last = 0.0;
     if (act) {
-        for (int k0 = 0; k0 < m; k0 += RAG_LOOKAHEAD) {
-            double ra[RAG_LOOKAHEAD], rb[RAG_LOOKAHEAD], rc[RAG_LOOKAHEAD], rd[RAG_LOOKAHEAD];
+        // rows k0 .. k0 + RAG_LOOKAHEAD - 1, clamped (in bounds) at the tail; the
+        // next batch is requested before the current one is eliminated
+        double ra[RAG_LOOKAHEAD], rb[RAG_LOOKAHEAD], rc[RAG_LOOKAHEAD], rd[RAG_LOOKAHEAD];
+        auto fetch = [&](int k0, double* fa, double* fb, double* fc, double* fd) {
 #pragma unroll
             for (int j = 0; j < RAG_LOOKAHEAD; ++j) {
-                const int k = k0 + j < m ? k0 + j : m - 1;  // clamped (in bounds) tail loads
-                ra[j] = (double)__ldg(pA + k);
-                rb[j] = (double)__ldg(pB + k);
-                rc[j] = (double)__ldg(pC + k);
-                rd[j] = (double)__ldg(pD + k);
+                const int k = k0 + j < m ? k0 + j : m - 1;
+                fa[j] = (double)__ldg(pA + k);
+                fb[j] = (double)__ldg(pB + k);
+                fc[j] = (double)__ldg(pC + k);
+                fd[j] = (double)__ldg(pD + k);
             }
+        };
+        fetch(0, ra, rb, rc, rd);
+        for (int k0 = 0; k0 < m; k0 += RAG_LOOKAHEAD) {
+            double na[RAG_LOOKAHEAD], nb[RAG_LOOKAHEAD], nc[RAG_LOOKAHEAD], nd[RAG_LOOKAHEAD];
+            fetch(k0 + RAG_LOOKAHEAD, na, nb, nc, nd);
 #pragma unroll
             for (int j = 0; j < RAG_LOOKAHEAD; ++j) {
                 const int k = k0 + j;
@@ -133,6 +140,13 @@ __global__ void __launch_bounds__(256) ragged_kernel(const RagArgs a) {
                 alp = al;
                 gap = ga;
                 dep = de;
+            }
+#pragma unroll
+            for (int j = 0; j < RAG_LOOKAHEAD; ++j) {
+                ra[j] = na[j];
+                rb[j] = nb[j];
+                rc[j] = nc[j];
+                rd[j] = nd[j];
             }
         }
     }
@@ -191,6 +205,18 @@ constexpr int RAG_MP = RAG_MT + 1;  // staged pitch per thread
 __host__ __device__ __forceinline__ size_t rag_cta_smem_bytes(int P, bool staged) {
     return (2ull * 3 * (P + 2) + (staged ? 4ull * RAG_MP * P : 3ull * RAG_MT * P)) *
            sizeof(double);
+}
+
+// Asynchronous global -> shared copy of one element (completion:
+// cp.async.wait_all) into the 8-byte slot dst: a double fills it, a float its
+// low word.
+__device__ __forceinline__ void cp_async_elem(double* dst, const double* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_elem(double* dst, const float* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src)
+                 : "memory");
 }
 
 // (segment, row in segment) of row r of a system split by para_range into P
@@ -252,16 +278,28 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
         const TIN* __restrict__ gB = static_cast<const TIN*>(a.B) + o;
         const TIN* __restrict__ gC = static_cast<const TIN*>(a.C) + o;
         const TIN* __restrict__ gD = static_cast<const TIN*>(a.D) + o;
+        // asynchronous copies straight into the staged layout, every row of the
+        // thread in flight at once; FP32 values land in the low word of their
+        // 8-byte slot and each thread widens its own rows once they are in
         for (int r = p; r < n; r += P) {
             int q, k;
             rag_locate(r, base, rem, inv0, inv1, q, k);
             double* dst = stg + q * RAG_MP + k;
-            dst[0 * fs] = (double)gA[r];
-            dst[1 * fs] = (double)gB[r];
-            dst[2 * fs] = (double)gC[r];
-            dst[3 * fs] = (double)gD[r];
+            cp_async_elem(dst + 0 * fs, gA + r);
+            cp_async_elem(dst + 1 * fs, gB + r);
+            cp_async_elem(dst + 2 * fs, gC + r);
+            cp_async_elem(dst + 3 * fs, gD + r);
         }
+        asm volatile("cp.async.wait_all;" ::: "memory");
         __syncthreads();
+        if constexpr (sizeof(TIN) == 4) {
+            for (int k = 0; k < m; ++k)
+#pragma unroll
+                for (int f = 0; f < 4; ++f) {
+                    double* sl = stt + f * fs + k;
+                    *sl = (double)*reinterpret_cast<const float*>(sl);
+                }
+        }
     }
     // state: alpha, gamma, delta (in place of A, C, D when staged)
     auto AL = [&](int k) -> double& { return stt[0 * fs + k * ks]; };
@@ -269,24 +307,31 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
     auto DE = [&](int k) -> double& { return stt[(STAGED ? 3 : 2) * fs + k * ks]; };
     double ab0 = 0, cb0 = 0, db0 = 0, pi = 1.0, sa = 0.0, sd = 0.0, pi_last = 0.0;
     double alp = 0, gap = 0, dep = 0;  // row k-1
+    // rows of batch k0 .. k0 + RAG_LOOKAHEAD - 1 (clamped in bounds); the next
+    // batch is requested before the current one is eliminated
+    double ra[RAG_LOOKAHEAD], rb[RAG_LOOKAHEAD], rc[RAG_LOOKAHEAD], rd[RAG_LOOKAHEAD];
+    auto fetch = [&](int k0, double* fa, double* fb, double* fc, double* fd) {
 #pragma unroll
-    for (int k0 = 0; k0 < M; k0 += RAG_LOOKAHEAD) {
-        double ra[RAG_LOOKAHEAD], rb[RAG_LOOKAHEAD], rc[RAG_LOOKAHEAD], rd[RAG_LOOKAHEAD];
-#pragma unroll
-        for (int j = 0; j < RAG_LOOKAHEAD; ++j) {  // loads of the next rows (clamped in bounds)
+        for (int j = 0; j < RAG_LOOKAHEAD; ++j) {
             const int kk = k0 + j < m ? k0 + j : m - 1;
             if constexpr (STAGED) {
-                ra[j] = stt[0 * fs + kk];
-                rb[j] = stt[1 * fs + kk];
-                rc[j] = stt[2 * fs + kk];
-                rd[j] = stt[3 * fs + kk];
+                fa[j] = stt[0 * fs + kk];
+                fb[j] = stt[1 * fs + kk];
+                fc[j] = stt[2 * fs + kk];
+                fd[j] = stt[3 * fs + kk];
             } else {
-                ra[j] = (double)__ldg(pA + kk);
-                rb[j] = (double)__ldg(pB + kk);
-                rc[j] = (double)__ldg(pC + kk);
-                rd[j] = (double)__ldg(pD + kk);
+                fa[j] = (double)__ldg(pA + kk);
+                fb[j] = (double)__ldg(pB + kk);
+                fc[j] = (double)__ldg(pC + kk);
+                fd[j] = (double)__ldg(pD + kk);
             }
         }
+    };
+    fetch(0, ra, rb, rc, rd);
+#pragma unroll
+    for (int k0 = 0; k0 < M; k0 += RAG_LOOKAHEAD) {
+        double na[RAG_LOOKAHEAD], nb[RAG_LOOKAHEAD], nc[RAG_LOOKAHEAD], nd[RAG_LOOKAHEAD];
+        if (k0 + RAG_LOOKAHEAD < M) fetch(k0 + RAG_LOOKAHEAD, na, nb, nc, nd);
 #pragma unroll
         for (int j = 0; j < RAG_LOOKAHEAD; ++j) {
             const int k = k0 + j;
@@ -323,6 +368,15 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
                 alp = al;
                 gap = ga;
                 dep = de;
+            }
+        }
+        if (k0 + RAG_LOOKAHEAD < M) {
+#pragma unroll
+            for (int j = 0; j < RAG_LOOKAHEAD; ++j) {
+                ra[j] = na[j];
+                rb[j] = nb[j];
+                rc[j] = nc[j];
+                rd[j] = nd[j];
             }
         }
     }

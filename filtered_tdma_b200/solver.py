@@ -173,6 +173,15 @@ class Solver:
         L.check(L.lib().btdma_ragged_plan_info(self._h, arr, n.value, ctypes.byref(n)))
         return [arr[i].as_dict() for i in range(n.value)]
 
+    def ragged_set_plan(self, plan):
+        """Apply launch shapes (a list of ragged_plan() dicts, in its order) to the
+        current ragged plan; see btdma_ragged_set_plan."""
+        arr = (L.RaggedBucket * max(1, len(plan)))()
+        for i, b in enumerate(plan):
+            for f, _ in L.RaggedBucket._fields_:
+                setattr(arr[i], f, b[f])
+        L.check(L.lib().btdma_ragged_set_plan(self._h, arr, len(plan)))
+
     def set_tile_shape(self, shape):
         """Kernel shape of the tiled PaScaL solves: TILE_AUTO, TILE_NARROW or
         TILE_WIDE (same results; see btdma_set_tile_shape)."""

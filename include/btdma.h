@@ -224,6 +224,15 @@ typedef struct btdma_ragged_bucket {
 } btdma_ragged_bucket;
 int btdma_ragged_plan_info(btdma_t h, btdma_ragged_bucket* out, int cap, int* n_out);
 
+/* Replace the launch shapes of the current ragged plan (lanes_per_system and
+ * cta_per_system of every bucket; the other fields must match the plan, in
+ * plan_info's order): restores a plan tuned earlier, e.g. by another process,
+ * without timing again.  Every shape is checked against the limits the
+ * autotuner uses (P a power of two, >= 3 rows per thread, per-thread row and
+ * shared-memory caps); a rejected plan leaves the current one in place.  No
+ * counterpart in the reference. */
+int btdma_ragged_set_plan(btdma_t h, const btdma_ragged_bucket* buckets, int n);
+
 /* Fused 3-D heat ADI step: the theta-scheme step of the reference's heat
  * application (apps/heat_gpu/solve_theta.cu, SolveTheta::profile's step loop:
  * ghost fill, right-hand side, Z, Y and X sweeps with fully implicit Dirichlet

@@ -115,6 +115,7 @@ def test_ragged_argument_checks():
                                      None) == L.ERR_ARG
     n = ctypes.c_int()
     assert lib.btdma_ragged_plan_info(None, None, 0, ctypes.byref(n)) == L.ERR_ARG
+    assert lib.btdma_ragged_set_plan(None, None, 0) == L.ERR_ARG
 
 
 @pytest.mark.gpu
@@ -148,3 +149,53 @@ def test_ragged_row_varying_coefficients(cuda, orc):
     assert per_system_err(x, ref, off) <= 1e-12
     x, _ = solve_on_device(cuda, (A, B, C, D), off, per, tune=True)
     assert per_system_err(x, ref, off) <= 1e-12
+
+
+def _shapes(b):
+    """Every launch shape the library accepts for bucket b: (P, cta_per_system)."""
+    out = []
+    for P in (1, 2, 4, 8, 16, 32):
+        if b["n_row_min"] // P >= 3 and -(-b["n_row_max"] // P) <= 32:
+            out.append((P, 0))
+    for P in (64, 128, 256, 512):
+        if b["n_row_min"] // P >= 3 and -(-b["n_row_max"] // P) <= 16:
+            out.append((P, 1))
+            if 4 * P * 17 * 8 + 6 * (P + 2) * 8 <= 227 * 1024:
+                out.append((P, 2))
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_ragged_every_launch_shape(cuda, orc, precision):
+    """Every shape of every bucket (warp lanes, CTA, CTA staged through shared
+    memory), applied with btdma_ragged_set_plan, against the oracle."""
+    import torch
+    dtype = np.float64 if precision == "fp64" else np.float32
+    A, B, C, D, off, per = W.ragged_batch(600, seed=58, dtype=dtype)
+    ref = ragged_oracle(orc, *[v.astype(np.float64) for v in (A, B, C, D)], off, per)
+    dA, dB, dC, dD = [torch.from_numpy(np.ascontiguousarray(v)).to(cuda) for v in (A, B, C, D)]
+    s = Solver("pascal", 600, 64, 2, precision=L.FP64 if precision == "fp64" else L.FP32_STORE)
+    X = torch.zeros(int(off[-1]), dtype=torch.float64, device=cuda)
+    s.solve_ragged(dA, dB, dC, dD, X, off, per)
+    plan = s.ragged_plan()
+    for bad in (dict(plan[0], lanes_per_system=3), dict(plan[-1], cta_per_system=2,
+                                                          lanes_per_system=512),
+                dict(plan[0], n_row_max=plan[0]["n_row_max"] + 1)):
+        with pytest.raises(L.BtdmaError):
+            s.ragged_set_plan([bad] + plan[1:] if bad["n_row_min"] == plan[0]["n_row_min"]
+                              else plan[:-1] + [bad])
+    assert s.ragged_plan() == plan  # a rejected plan leaves the current one
+    opts = [_shapes(b) for b in plan]
+    assert all(opts)
+    assert any((P, 2) in o for o in opts for P in (64, 128, 256))
+    for j in range(max(len(o) for o in opts)):
+        want = [o[j % len(o)] for o in opts]
+        s.ragged_set_plan([dict(b, lanes_per_system=P, cta_per_system=k)
+                           for b, (P, k) in zip(plan, want)])
+        assert [(b["lanes_per_system"], b["cta_per_system"]) for b in s.ragged_plan()] == want
+        X.zero_()
+        s.solve_ragged(dA, dB, dC, dD, X, off, per)
+        torch.cuda.synchronize()
+        assert s.status() == 0
+        assert per_system_err(X.cpu().numpy(), ref, off) <= 1e-12, want
