@@ -41,8 +41,18 @@ int heat_enqueue(btdma_heat_t h, double* theta, cudaStream_t st, cudaEvent_t* ev
     auto mark = [&](int i) {
         if (ev) cudaEventRecord(ev[i], st);
     };
-    auto sweep = [&](double* buf, int n_sys, int n_row, double base, const char* name) {
-        const int rc = try_tile_const(buf, buf, n_sys, n_row, base, true, h->status, st, h->tab);
+    // constant-coefficient sweep of D into X, stored through the layout map
+    // (xblk, xbs, xss, xrs) of the tiled solve (xblk = 0: X in D's layout)
+    auto sweep = [&](const double* D, double* X, int n_sys, int n_row, double base, int xblk,
+                     int xbs, int xss, int xrs, const char* name) {
+        TileArgs ga = {};
+        ga.cs = base;
+        ga.cbound = 1;
+        ga.xblk = xblk;
+        ga.xbs = xbs;
+        ga.xss = xss;
+        ga.xrs = xrs;
+        const int rc = try_tile_gen<1>(D, X, n_sys, n_row, ga, h->status, st, h->tab);
         return rc == 1 ? BTDMA_OK
                        : (rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "%s sweep not tileable", name));
     };
@@ -53,17 +63,19 @@ int heat_enqueue(btdma_heat_t h, double* theta, cudaStream_t st, cudaEvent_t* ev
     heat_rhs_z_kernel<<<gr, b1, 0, st>>>(theta, h->buf0, g);
     CK(cudaGetLastError());
     mark(1);
-    if ((rc = sweep(h->buf0, g.ix * g.iy, g.iz, g.bz, "Z"))) return rc;
+    // Z sweep: system jj * ix + ii, row kk; solution to [jj][kk][ii]
+    if ((rc = sweep(h->buf0, h->buf1, g.ix * g.iy, g.iz, g.bz, g.ix, g.iz * g.ix, 1, g.ix, "Z")))
+        return rc;
     mark(2);
-    heat_z_to_y_kernel<<<gr, b1, 0, st>>>(theta, h->buf0, h->buf1, g);
+    heat_y_fold_kernel<<<dim3((g.ix + 127) / 128, 2, g.iz), b1, 0, st>>>(theta, h->buf1, g);
     CK(cudaGetLastError());
     mark(3);
-    if ((rc = sweep(h->buf1, g.ix * g.iz, g.iy, g.by, "Y"))) return rc;
+    if ((rc = sweep(h->buf1, h->buf1, g.ix * g.iz, g.iy, g.by, 0, 0, 0, 0, "Y"))) return rc;
     mark(4);
     heat_y_to_x_kernel<<<dim3(tx, ty, g.iz), bt, 0, st>>>(theta, h->buf1, h->buf0, g);
     CK(cudaGetLastError());
     mark(5);
-    if ((rc = sweep(h->buf0, g.iy * g.iz, g.ix, g.bx, "X"))) return rc;
+    if ((rc = sweep(h->buf0, h->buf0, g.iy * g.iz, g.ix, g.bx, 0, 0, 0, 0, "X"))) return rc;
     mark(6);
     heat_update_kernel<<<dim3(ty, tx, g.iz), bt, 0, st>>>(theta, h->buf0, g);
     CK(cudaGetLastError());

@@ -448,9 +448,7 @@ int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArg
     a.cl = pl.cl;
     a.nst = pl.nst;
     a.n_groups = (n_sys + pl.sys - 1) / pl.sys;
-    a.accumulate = 0;
-    a.gate = nullptr;
-    a.status = status;
+    a.status = status;  // the layout map (xblk ...) comes with gen
     if constexpr (GEN == 1 || GEN == 3) {
         if (!tab) return fail(BTDMA_ERR_ARG, "shared-matrix sweep without a factor table");
         tile_table_kernel<GEN><<<(pl.nseg + 127) / 128, 128, 0, st>>>(a, tab);
@@ -465,16 +463,6 @@ int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArg
         default: rc = launch_tile_sys<16, CYC, double, double, GEN>(maps, a, st); break;
     }
     return rc == BTDMA_OK ? 1 : rc;
-}
-
-// Heat sweep: every row -cs, 1 + 2 cs, -cs; cs more on the diagonal of the
-// first and last row when cbound.
-inline int try_tile_const(const double* D, double* X, int n_sys, int n_row, double cs,
-                          bool cbound, unsigned* status, cudaStream_t st, double* tab) {
-    TileArgs g = {};
-    g.cs = cs;
-    g.cbound = cbound ? 1 : 0;
-    return try_tile_gen<1>(D, X, n_sys, n_row, g, status, st, tab);
 }
 
 inline size_t gen_table_doubles(int n_row) {

@@ -17,9 +17,12 @@
 //     computed as 2 u_BC - theta(cell), exactly the value the reference's ghost
 //     kernels write there;
 //   * A, B, C are never materialised (the solve generates them);
-//   * the Y sweep reads the Z solution in place ([kk][jj][ii] -> [jj][kk][ii]
-//     is a copy with ii fastest on both sides), and only the X sweep and the
-//     final update transpose through shared-memory tiles.
+//   * the Z sweep stores its solution straight into the Y sweep's layout
+//     ([kk][jj][ii] -> [jj][kk][ii], the tiled solve's mapped store; the Y wall
+//     folds then touch the two wall planes only), so the only copies left are
+//     the two transposes, Y -> X and X -> theta, through shared-memory tiles.
+//     (Storing the X sweep straight into theta was measured slower than the
+//     transpose it saves: its lanes write rows 2 KB apart.)
 #pragma once
 
 #include "btdma_common.cuh"
@@ -84,25 +87,21 @@ __global__ void __launch_bounds__(256) heat_rhs_z_kernel(const double* __restric
     D[((size_t)kk * g.iy + jj) * g.ix + ii] = rhs;
 }
 
-// Z solution [kk][jj][ii] -> Y-sweep layout [jj][kk][ii] plus the Y wall folds
-// (copy_z_to_rhs + build_lhs_y_kernel, solve_theta.cu:205-253).
-__global__ void __launch_bounds__(256) heat_z_to_y_kernel(const double* __restrict__ theta,
-                                                          const double* __restrict__ Dz,
+// Y wall folds on the Z solution, already in the Y-sweep layout [jj][kk][ii]
+// (build_lhs_y_kernel's right-hand-side terms, solve_theta.cu:205-253): planes
+// jj = 0 and jj = iy - 1 get base * (ghost + boundary cell).  Grid (ix / 128,
+// 2, iz).
+__global__ void __launch_bounds__(128) heat_y_fold_kernel(const double* __restrict__ theta,
                                                           double* __restrict__ Dy,
                                                           const HeatGeom g) {
     const int ii = blockIdx.x * blockDim.x + threadIdx.x;
-    const int jj = blockIdx.y;
+    const int jj = blockIdx.y == 0 ? 0 : g.iy - 1;
     const int kk = blockIdx.z;
     if (ii >= g.ix) return;
-    double v = Dz[((size_t)kk * g.iy + jj) * g.ix + ii];
-    if (jj == 0 || jj == g.iy - 1) {
-        const int i = ii + 1, k = kk + 1, j = jj == 0 ? 1 : g.iy;
-        const double t = theta[heat_full(g, i, j, k)];
-        const double ubc = -g.cx[i] * g.cz[k];
-        if (jj == 0) v += g.by * ((2.0 * ubc - t) + t);
-        if (jj == g.iy - 1) v += g.by * ((2.0 * ubc - t) + t);
-    }
-    Dy[((size_t)jj * g.iz + kk) * g.ix + ii] = v;
+    const int i = ii + 1, k = kk + 1, j = jj + 1;
+    const double t = theta[heat_full(g, i, j, k)];
+    const double ubc = -g.cx[i] * g.cz[k];
+    Dy[((size_t)jj * g.iz + kk) * g.ix + ii] += g.by * ((2.0 * ubc - t) + t);
 }
 
 constexpr int HEAT_TILE = 32;

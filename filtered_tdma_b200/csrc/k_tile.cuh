@@ -66,8 +66,22 @@ struct TileArgs {
     int cl;        // CTAs per cluster (sub-segments split over them)
     int nst;       // ring stages
     int n_groups;  // groups of SYS systems
-    int accumulate;        // 1: X += solution (refinement corrections), 0: X = solution
-    const unsigned* gate;  // non-null: the launch does nothing while *gate == 0
+    union {
+        struct {  // modes that read A, B, C (GEN == 0)
+            int accumulate;        // 1: X += solution (refinement corrections), 0: X = solution
+            const unsigned* gate;  // non-null: the launch does nothing while *gate == 0
+        };
+        // Generated-coefficient modes (GEN != 0) may store x through a layout
+        // map instead of the plain [n_row][n_sys]: with xblk > 0, row j of
+        // system s goes to  X + (s / xblk) * xbs + (s % xblk) * xss + j * xrs
+        // (xrs > 0).  The heat step writes its Z sweep in the Y sweep's layout
+        // and its X sweep into the ghosted field, without a copy pass.  (A union
+        // with the refinement fields: a larger argument struct made ptxas spill
+        // more in every instantiation.)
+        struct {
+            int xblk, xbs, xss, xrs;
+        };
+    };
     // Generated-coefficient instantiations read only D:
     //  GEN == 1 (heat sweep): every row -cs x_{j-1} + (1 + 2 cs) x_j - cs x_{j+1},
     //    plus cs on the diagonal of the first and last row when cbound != 0
@@ -210,7 +224,8 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     const int n_clusters = (int)gridDim.x / cl;
     const int s = tid % SYS;  // forward / back-substitution mapping
     const int ql = tid / SYS;
-    const size_t ns = (size_t)args.n_sys;
+    // row stride of x: n_sys, or xrs through the layout map of the generated modes
+    const size_t ns = (CONSTC && args.xblk > 0) ? (size_t)args.xrs : (size_t)args.n_sys;
 
     if (tid == 0) {
         for (int i = 0; i < nst; ++i) {
@@ -237,8 +252,8 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 
     // a closed gate leaves the CTA without groups (it still runs its setup and
     // exit barriers, so every CTA of a cluster takes the same path)
-    const bool gated_off =
-        args.gate != nullptr && *static_cast<const volatile unsigned*>(args.gate) == 0u;
+    const bool gated_off = !CONSTC && args.gate != nullptr &&
+                           *static_cast<const volatile unsigned*>(args.gate) == 0u;
     const int n_my = (!gated_off && args.n_groups > cluster_id)
                          ? (args.n_groups - cluster_id + n_clusters - 1) / n_clusters
                          : 0;
@@ -526,6 +541,12 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         if (valid) {
             const int q = c * nsc + ql;
             double* xp = args.X + (size_t)(q * M + M - 1) * ns + sys;  // row M-1
+            if constexpr (CONSTC) {
+                if (args.xblk > 0)
+                    xp = args.X + (ptrdiff_t)(sys / args.xblk) * (ptrdiff_t)args.xbs +
+                         (ptrdiff_t)(sys % args.xblk) * (ptrdiff_t)args.xss +
+                         (size_t)(q * M + M - 1) * ns;
+            }
             // corrections are accumulated only by the FP32 inner solve of
             // refinement (the FP64-arithmetic instantiations keep the plain
             // store); the old x of all M rows is loaded before any store
