@@ -392,8 +392,8 @@ int btdma_momentum_create(int nx, int ny, int nz, const double* dx0, const doubl
                         "sweep %d: n must be a multiple of 16 (n / 16 a power of two when "
                         "periodic)", d);
     }
-    if ((long long)nx * ny * nz >= (1LL << 31))
-        return fail(BTDMA_ERR_SIZE, "grid above 2^31 cells");
+    if ((long long)(nx + 2) * (ny + 2) * (nz + 2) >= (1LL << 31))
+        return fail(BTDMA_ERR_SIZE, "ghosted grid above 2^31 cells");
     // row tables (MomentumSolverGPU.cu:135-155, :176-180, :205-209): for row
     // r = 1..n, staggered when comp == dir;  a = -c ta, c = -c tc, b = 1 + c tb
     const double* dxs[3] = {dx0, dx1, dx2};
@@ -480,21 +480,33 @@ int btdma_momentum_sweep(btdma_momentum_t h, int dir, int comp, const double* q,
     t.gb = t.ga + n[dir];
     t.gc = t.gb + n[dir];
     const dim3 b1(128, 1, 1), bt(MOM_TILE, 8, 1);
+    // z and y sweeps store straight into dst's interior through the tiled
+    // solve's layout map (system s = (a, i) with i = s % nx fastest, row r):
+    //   z: dst(i, j = s / nx + 1, k = r + 1);  y: dst(i, j = r + 1, k = s / nx + 1)
+    const int sp = (g.nx + 2) * (g.ny + 2);  // plane stride (< 2^31, checked at create)
+    double* const dst_in = dst + sp + (g.nx + 2) + 1;  // dst(1, 1, 1)
+    t.xblk = g.nx;
+    t.xss = 1;
     int rc;
     if (dir == 2) {
         mom_gather_kernel<2><<<dim3((g.nx + 127) / 128, g.ny, g.nz), b1, 0, stream>>>(
             q, h->buf, g, comp == 2 ? 1 : 0);
         CK(cudaGetLastError());
-        rc = try_tile_gen<3, false>(h->buf, h->buf, n_sys, g.nz, t, h->status, stream, h->gtab);
+        t.xbs = g.nx + 2;
+        t.xrs = sp;
+        rc = try_tile_gen<3, false>(h->buf, dst_in, n_sys, g.nz, t, h->status, stream, h->gtab);
     } else if (dir == 1) {
         mom_gather_kernel<1><<<dim3((g.nx + 127) / 128, g.nz, g.ny), b1, 0, stream>>>(q, h->buf,
                                                                                    g, 0);
         CK(cudaGetLastError());
+        t.xbs = sp;
+        t.xrs = g.nx + 2;
         rc = h->pbc[1]
-                 ? try_tile_gen<3, true>(h->buf, h->buf, n_sys, g.ny, t, h->status, stream, h->gtab)
-                 : try_tile_gen<3, false>(h->buf, h->buf, n_sys, g.ny, t, h->status, stream,
+                 ? try_tile_gen<3, true>(h->buf, dst_in, n_sys, g.ny, t, h->status, stream, h->gtab)
+                 : try_tile_gen<3, false>(h->buf, dst_in, n_sys, g.ny, t, h->status, stream,
                                           h->gtab);
     } else {
+        t.xblk = 0;  // x: the plain layout, transposed back below
         mom_gather_x_kernel<<<dim3((g.nx + MOM_TILE - 1) / MOM_TILE,
                                    (g.ny + MOM_TILE - 1) / MOM_TILE, g.nz), bt, 0, stream>>>(
             q, h->buf, g);
@@ -505,17 +517,12 @@ int btdma_momentum_sweep(btdma_momentum_t h, int dir, int comp, const double* q,
                                           h->gtab);
     }
     if (rc != 1) return rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "sweep not tileable");
-    if (dir == 2)
-        mom_scatter_kernel<2><<<dim3((g.nx + 127) / 128, g.ny, g.nz), b1, 0, stream>>>(h->buf,
-                                                                                     dst, g);
-    else if (dir == 1)
-        mom_scatter_kernel<1><<<dim3((g.nx + 127) / 128, g.nz, g.ny), b1, 0, stream>>>(h->buf,
-                                                                                     dst, g);
-    else
+    if (dir == 0) {
         mom_scatter_x_kernel<<<dim3((g.ny + MOM_TILE - 1) / MOM_TILE,
                                     (g.nx + MOM_TILE - 1) / MOM_TILE, g.nz), bt, 0, stream>>>(
             h->buf, dst, g);
-    CK(cudaGetLastError());
+        CK(cudaGetLastError());
+    }
     return BTDMA_OK;
 }
 

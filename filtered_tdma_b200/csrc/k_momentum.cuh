@@ -2,7 +2,9 @@
 // k_build_{x,y,z} + solve + k_scatter_{x,y,z}, called by adi_{z,y,x}_ at
 // :261-313), with the coefficients generated inside the tiled solve (GEN = 3
 // row tables) instead of stored: the build is a gather of the ghosted field
-// into the sweep layout, the scatter its inverse.
+// into the sweep layout; the z and y sweeps store their solutions straight back
+// into the field (the tiled solve's layout map), the x sweep through a
+// transposing scatter.
 //
 // Field: q[i + (nx + 2) * (j + (ny + 2) * k)] (DeviceField.hpp df_idx), interior
 // i = 1..nx, j = 1..ny, k = 1..nz.  Sweep layouts (system index fastest):
@@ -38,18 +40,6 @@ __global__ void __launch_bounds__(256) mom_gather_kernel(const double* __restric
     const size_t o = DIR == 2 ? ((size_t)(k - 1) * g.ny + (j - 1)) * g.nx + (i - 1)
                               : ((size_t)(j - 1) * g.nz + (k - 1)) * g.nx + (i - 1);
     D[o] = (DIR == 2 && pin && k == 1) ? 0.0 : q[mom_fld(g, i, j, k)];
-}
-
-template <int DIR>
-__global__ void __launch_bounds__(256) mom_scatter_kernel(const double* __restrict__ D,
-                                                          double* __restrict__ q, const MomGeom g) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int a = blockIdx.y + 1, b = blockIdx.z + 1;
-    if (i > g.nx) return;
-    const int j = DIR == 2 ? a : b, k = DIR == 2 ? b : a;
-    const size_t o = DIR == 2 ? ((size_t)(k - 1) * g.ny + (j - 1)) * g.nx + (i - 1)
-                              : ((size_t)(j - 1) * g.nz + (k - 1)) * g.nx + (i - 1);
-    q[mom_fld(g, i, j, k)] = D[o];
 }
 
 constexpr int MOM_TILE = 32;
