@@ -27,6 +27,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "btdma.h"
 
@@ -124,6 +125,11 @@ class PaScaLTDMACUDA {
     double last_comm_ms() const { return 0.0; }
     double last_gpu_ms() const { return gpu_ms_; }
     void set_stream(cudaStream_t s) { stream_ = s; }
+    // BTDMA_TILE_AUTO / NARROW / WIDE (btdma_set_tile_shape); kept across handle regrowth.
+    void set_tile_shape(int shape) {
+        tile_shape_ = shape;
+        if (h_) btdma::check(btdma_set_tile_shape(h_->get(), shape));
+    }
 
    private:
     // The handle is sized on the first solve (n_row is not a constructor
@@ -132,9 +138,11 @@ class PaScaLTDMACUDA {
         if (!h_ || n_row > h_->n_row() || n_sys > h_->n_sys()) {
             h_.reset();
             h_.reset(new btdma::Handle(BTDMA_PASCAL, std::max(n_sys, n_sys_), n_row, nprocs_));
+            btdma::check(btdma_set_tile_shape(h_->get(), tile_shape_));
         }
         return h_->get();
     }
+    int tile_shape_ = BTDMA_TILE_AUTO;
     int n_sys_, nprocs_;
     std::unique_ptr<btdma::Handle> h_;
     cudaStream_t stream_ = 0;
@@ -357,6 +365,18 @@ class RaggedSolver {
                   const long long* row_offsets, const unsigned char* periodic, int n_sys,
                   cudaStream_t s = 0) {
         check(btdma_ragged_autotune(h_, A, B, C, D, X, row_offsets, periodic, n_sys, s));
+    }
+    // The current plan (e.g. after autotune), and a stored plan applied again
+    // to the same layout without timing.
+    std::vector<btdma_ragged_bucket> plan() const {
+        int n = 0;
+        check(btdma_ragged_plan_info(h_, nullptr, 0, &n));
+        std::vector<btdma_ragged_bucket> out(n);
+        check(btdma_ragged_plan_info(h_, out.data(), n, &n));
+        return out;
+    }
+    void set_plan(const std::vector<btdma_ragged_bucket>& plan) {
+        check(btdma_ragged_set_plan(h_, plan.data(), (int)plan.size()));
     }
 
    private:

@@ -1,7 +1,8 @@
 // Compiles the C++ drop-in header the way a reference caller would use it and,
 // when run on a GPU, solves the heat 64-row sweep through TdmaBackendGPU,
-// PaScaLTDMACUDA and FilteredTDMACUDA, then the fused heat step and a ragged
-// batch through the RAII wrappers.  Prints one line per solve:
+// PaScaLTDMACUDA and FilteredTDMACUDA (and, read as 512 x 512, both tiled
+// kernel shapes), then the fused heat step and a ragged batch through the RAII
+// wrappers.  Prints one line per solve:
 //   <name> <max |x|> <status>
 // tests/test_cpp_dropin.py compares the solutions with the oracle.
 #include <cuda_runtime_api.h>
@@ -80,6 +81,15 @@ int main(int argc, char** argv) {
         f.solve_cycl_filtered_v2(dA, dB, dC, dD);
         report("filtered_v2_cyclic");
         std::printf("J %d\n", f.last_J());
+        // the same values read as 512 systems of 512 rows, through both tiled
+        // kernel shapes
+        for (int shape : {BTDMA_TILE_NARROW, BTDMA_TILE_WIDE}) {
+            upload();
+            PaScaLTDMACUDA w(512, 0, 8);
+            w.set_tile_shape(shape);
+            w.solve(dA, dB, dC, dD, 512, 512);
+            report(shape == BTDMA_TILE_WIDE ? "pascal512_wide" : "pascal512_narrow");
+        }
 
         // the fused heat step of the reference's order-accuracy run (32^3,
         // rho = 0.25, one step) through the C++ wrapper
@@ -107,6 +117,8 @@ int main(int argc, char** argv) {
             cudaMemcpy(qc, rc.data(), 45 * 8, cudaMemcpyHostToDevice);
             cudaMemcpy(qd, rd.data(), 45 * 8, cudaMemcpyHostToDevice);
             btdma::RaggedSolver rs(2);
+            rs.solve(qa, qb, qc, qd, qx, off, per, 2);
+            rs.set_plan(rs.plan());  // a stored plan applied again
             rs.solve(qa, qb, qc, qd, qx, off, per, 2);
             cudaMemcpy(rx.data(), qx, 45 * 8, cudaMemcpyDeviceToHost);
             // periodic system of constant rows: x = 1 / (4 - 2) everywhere

@@ -54,3 +54,12 @@ def test_cpp_dropin_runs_and_matches_oracle(cuda, orc, tmp_path):
         assert np.array_equal(got(name), x), name
     assert float(lines["heat_l2"]) == pytest.approx(0.00153948, abs=5e-9)
     assert float(lines["ragged_periodic_x"]) == pytest.approx(0.5, rel=1e-13)
+    # the same values as 512 systems x 512 rows through both tiled kernel shapes
+    D5 = D.reshape(512, 512)
+    A5, B5, C5 = (np.full_like(D5, v) for v in (-1.0, 3.0, -1.0))
+    x5 = orc.thomas(A5, B5, C5, D5)
+    w = np.fromfile(f"{prefix}_pascal512_wide.bin", dtype=np.float64).reshape(512, 512)
+    nw = np.fromfile(f"{prefix}_pascal512_narrow.bin", dtype=np.float64).reshape(512, 512)
+    for x in (w, nw):
+        assert np.max(np.abs(x - x5)) / np.max(np.abs(x5)) <= 1e-12
+    assert np.max(np.abs(w - nw)) / np.max(np.abs(x5)) <= 1e-13
