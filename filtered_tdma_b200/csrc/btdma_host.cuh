@@ -152,7 +152,7 @@ int launch_seg(const CUtensorMap* maps, const SegArgs& a, int groups, cudaStream
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(a.P, groups, 1);
     cfg.blockDim = dim3(SEG_S, 1, 1);
-    cfg.dynamicSmemBytes = seg_smem_bytes(a.mcap, a.P, CYCLIC);
+    cfg.dynamicSmemBytes = seg_smem_bytes(a.mcap, a.P, CYCLIC, METHOD == SEG_PASCAL);
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;

@@ -7,10 +7,13 @@
 //
 //   * CTA k of the cluster owns rows [r0_k, r0_k + m_k) (para_range split) of
 //     systems [g*SEG_S, (g+1)*SEG_S); one thread per system.
-//   * The segment tile (A, B, C, D: 4 * m * SEG_S doubles) is staged once into
+//   * The segment tile (A, C, D: 3 * m * SEG_S doubles) is staged once into
 //     shared memory by TMA in chunks of SEG_BOXR rows, each chunk completing on
 //     its own mbarrier, so the forward sweep starts on the first chunk while the
-//     others are still in flight.  A, B, C, D are read from HBM exactly once.
+//     others are still in flight.  B is only read by the forward sweep: it comes
+//     straight from HBM, a chunk ahead into registers, which keeps the tile at
+//     three arrays (4 CTAs per SM at 64 rows instead of 3).  A, B, C, D are read
+//     from HBM exactly once.
 //   * The modified Thomas sweeps run in place on the tile (the reference's
 //     per-rank steps, pascal_tdma.cpp:131-183 / filtered_tdma_kernels.hpp:35-189,
 //     with the same operation order, IEEE round-to-nearest, no FMA).
@@ -63,19 +66,16 @@ struct SegArgs {
     unsigned* status;
 };
 
-// Dynamic shared memory layout of one CTA: the four tiles, the published
-// reduced rows, the reduced-solve scratch and the chunk barriers.  The scratch
-// reuses the B tile (dead after the forward sweep) whenever it fits there.
+// Dynamic shared memory layout of one CTA: the A, C, D tiles, the published
+// reduced rows, the reduced-solve scratch (PaScaL only) and the chunk barriers.
 __host__ __device__ __forceinline__ size_t seg_rsc_bytes(int P, bool cyclic) {
     return (cyclic ? 4ull : 3ull) * 2 * P * SEG_S * sizeof(double);
 }
-__host__ __device__ __forceinline__ bool seg_rsc_in_b(int mcap, int P, bool cyclic) {
-    return seg_rsc_bytes(P, cyclic) <= (size_t)mcap * SEG_S * sizeof(double);
-}
-__host__ __device__ __forceinline__ size_t seg_smem_bytes(int mcap, int P, bool cyclic) {
-    size_t tiles = 4ull * mcap * SEG_S * sizeof(double);
+__host__ __device__ __forceinline__ size_t seg_smem_bytes(int mcap, int P, bool cyclic,
+                                                          bool pascal = true) {
+    size_t tiles = 3ull * mcap * SEG_S * sizeof(double);
     size_t red = 6ull * SEG_S * sizeof(double);
-    size_t rsc = seg_rsc_in_b(mcap, P, cyclic) ? 0 : seg_rsc_bytes(P, cyclic);
+    size_t rsc = pascal ? seg_rsc_bytes(P, cyclic) : 0;
     size_t bars = (size_t)(mcap / SEG_BOXR) * sizeof(uint64_t);
     return tiles + red + rsc + bars + 128;  // +128: alignment slack
 }
@@ -88,7 +88,7 @@ __device__ __forceinline__ void cluster_wait() {
 }
 
 template <int METHOD, bool CYCLIC>
-__global__ void __launch_bounds__(SEG_S)
+__global__ void __launch_bounds__(SEG_S, 4)
 seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                const __grid_constant__ CUtensorMap tmC, const __grid_constant__ CUtensorMap tmD,
                const __grid_constant__ CUtensorMap tmX, const SegArgs args) {
@@ -98,15 +98,12 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     const int mcap = args.mcap;
     double* TA = base;
-    double* TB = TA + (size_t)mcap * SEG_S;
-    double* TC = TB + (size_t)mcap * SEG_S;
+    double* TC = TA + (size_t)mcap * SEG_S;
     double* TD = TC + (size_t)mcap * SEG_S;
-    double* red = TD + (size_t)mcap * SEG_S;              // [6][SEG_S]
-    const bool rsc_in_b = seg_rsc_in_b(mcap, args.P, CYCLIC);
-    double* after_red = red + 6 * SEG_S;
-    double* rsc = rsc_in_b ? TB : after_red;              // reduced-solve scratch
+    double* red = TD + (size_t)mcap * SEG_S;  // [6][SEG_S]
+    double* rsc = red + 6 * SEG_S;            // reduced-solve scratch (PaScaL)
     uint64_t* bars = reinterpret_cast<uint64_t*>(
-        rsc_in_b ? after_red : after_red + seg_rsc_bytes(args.P, CYCLIC) / sizeof(double));
+        rsc + (METHOD == SEG_PASCAL ? seg_rsc_bytes(args.P, CYCLIC) / sizeof(double) : 0));
 
     cg::cluster_group cluster = cg::this_cluster();
     const int P = args.P;
@@ -132,13 +129,12 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         }
         __syncwarp();
         if (s == 0) {
-            const uint32_t bytes = 4u * SEG_BOXR * SEG_S * sizeof(double);
+            const uint32_t bytes = 3u * SEG_BOXR * SEG_S * sizeof(double);
             for (int c = 0; c < nch; ++c) {
                 mbar_expect_tx(&bars[c], bytes);
                 const int y = r0 + c * SEG_BOXR;
                 const size_t o = (size_t)c * SEG_BOXR * SEG_S;
                 tma_load_2d(TA + o, &tmA, g * SEG_S, y, &bars[c]);
-                tma_load_2d(TB + o, &tmB, g * SEG_S, y, &bars[c]);
                 tma_load_2d(TC + o, &tmC, g * SEG_S, y, &bars[c]);
                 tma_load_2d(TD + o, &tmD, g * SEG_S, y, &bars[c]);
             }
@@ -147,11 +143,21 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         for (int j = 0; j < m; ++j) {
             size_t off = (size_t)(r0 + j) * ns + sys;
             T(TA, j) = valid ? args.A[off] : 0.0;
-            T(TB, j) = valid ? args.B[off] : 1.0;
             T(TC, j) = valid ? args.C[off] : 0.0;
             T(TD, j) = valid ? args.D[off] : 0.0;
         }
     }
+    (void)tmB;
+    // B of rows [c * SEG_BOXR, (c + 1) * SEG_BOXR) into registers (1 outside
+    // the batch or the segment)
+    const double* gB = args.B + (size_t)r0 * ns + sys;
+    auto load_b = [&](int c, double (&bb)[SEG_BOXR]) {
+#pragma unroll
+        for (int u = 0; u < SEG_BOXR; ++u) {
+            const int j = c * SEG_BOXR + u;
+            bb[u] = (valid && j < m) ? __ldg(gB + (size_t)j * ns) : 1.0;
+        }
+    };
     auto chunk_ready = [&](int j) {
         if (args.use_tma && ok && (j % SEG_BOXR) == 0)
             ok = mbar_wait_bounded(&bars[j / SEG_BOXR], 0, args.status);
@@ -165,12 +171,15 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     const int lo = (m - 2) - Jf;
 
     // ------------------------------------------------------- forward sweep
+    double bcur[SEG_BOXR], bnext[SEG_BOXR];
+    load_b(0, bcur);
+    if (nch > 1) load_b(1, bnext);
     chunk_ready(0);
-    double q0 = E::rcp(T(TB, 0));
+    double q0 = E::rcp(bcur[0]);
     double a0 = E::mul(T(TA, 0), q0);
     double c0 = E::mul(T(TC, 0), q0);
     double d0 = E::mul(T(TD, 0), q0);
-    double q1 = E::rcp(T(TB, 1));
+    double q1 = E::rcp(bcur[1]);
     double ap = E::mul(T(TA, 1), q1);
     double cp = E::mul(T(TC, 1), q1);
     double dp = E::mul(T(TD, 1), q1);
@@ -180,17 +189,27 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     T(TA, 1) = ap;
     T(TC, 1) = cp;
     T(TD, 1) = dp;
-    for (int j = 2; j < m; ++j) {
-        chunk_ready(j);
-        const double a = T(TA, j);
-        const double inv = E::rcp(E::sub(T(TB, j), E::mul(a, cp)));
-        dp = E::mul(inv, E::sub(T(TD, j), E::mul(a, dp)));
-        cp = E::mul(inv, T(TC, j));
-        T(TD, j) = dp;
-        T(TC, j) = cp;
-        if (METHOD != SEG_FILT_V2 || j <= Jf) {
-            ap = E::mul(E::mul(-inv, a), ap);
-            T(TA, j) = ap;
+    for (int c = 0; c < nch; ++c) {
+        if (c > 0) {
+#pragma unroll
+            for (int u = 0; u < SEG_BOXR; ++u) bcur[u] = bnext[u];
+            if (c + 1 < nch) load_b(c + 1, bnext);
+            chunk_ready(c * SEG_BOXR);
+        }
+#pragma unroll
+        for (int u = 0; u < SEG_BOXR; ++u) {
+            const int j = c * SEG_BOXR + u;
+            if (j < 2 || j >= m) continue;
+            const double a = T(TA, j);
+            const double inv = E::rcp(E::sub(bcur[u], E::mul(a, cp)));
+            dp = E::mul(inv, E::sub(T(TD, j), E::mul(a, dp)));
+            cp = E::mul(inv, T(TC, j));
+            T(TD, j) = dp;
+            T(TC, j) = cp;
+            if (METHOD != SEG_FILT_V2 || j <= Jf) {
+                ap = E::mul(E::mul(-inv, a), ap);
+                T(TA, j) = ap;
+            }
         }
     }
     const double aN = T(TA, m - 1), cN = T(TC, m - 1), dN = T(TD, m - 1);
