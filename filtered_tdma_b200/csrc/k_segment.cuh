@@ -7,13 +7,14 @@
 //
 //   * CTA k of the cluster owns rows [r0_k, r0_k + m_k) (para_range split) of
 //     systems [g*SEG_S, (g+1)*SEG_S); one thread per system.
-//   * The segment tile (A, C, D: 3 * m * SEG_S doubles) is staged once into
+//   * The segment tile (A, B, C, D: 4 * m * SEG_S doubles) is staged once into
 //     shared memory by TMA in chunks of SEG_BOXR rows, each chunk completing on
 //     its own mbarrier, so the forward sweep starts on the first chunk while the
-//     others are still in flight.  B is only read by the forward sweep: it comes
-//     straight from HBM, a chunk ahead into registers, which keeps the tile at
-//     three arrays (4 CTAs per SM at 64 rows instead of 3).  A, B, C, D are read
-//     from HBM exactly once.
+//     others are still in flight.  Filtered streams B instead (only the forward
+//     sweep reads it): straight from HBM, a chunk ahead into registers, which
+//     keeps its tile at three arrays (4 CTAs per SM at 64 rows instead of 3).
+//     PaScaL keeps B staged: the tile's B part holds its reduced-system scratch
+//     afterwards.  A, B, C, D are read from HBM exactly once.
 //   * The modified Thomas sweeps run in place on the tile (the reference's
 //     per-rank steps, pascal_tdma.cpp:131-183 / filtered_tdma_kernels.hpp:35-189,
 //     with the same operation order, IEEE round-to-nearest, no FMA).
@@ -66,16 +67,21 @@ struct SegArgs {
     unsigned* status;
 };
 
-// Dynamic shared memory layout of one CTA: the A, C, D tiles, the published
-// reduced rows, the reduced-solve scratch (PaScaL only) and the chunk barriers.
+// Dynamic shared memory layout of one CTA: the tiles (A, B, C, D for PaScaL;
+// A, C, D for Filtered), the published reduced rows, PaScaL's reduced-solve
+// scratch (in the B tile, dead after the forward sweep, whenever it fits there)
+// and the chunk barriers.
 __host__ __device__ __forceinline__ size_t seg_rsc_bytes(int P, bool cyclic) {
     return (cyclic ? 4ull : 3ull) * 2 * P * SEG_S * sizeof(double);
 }
+__host__ __device__ __forceinline__ bool seg_rsc_in_b(int mcap, int P, bool cyclic) {
+    return seg_rsc_bytes(P, cyclic) <= (size_t)mcap * SEG_S * sizeof(double);
+}
 __host__ __device__ __forceinline__ size_t seg_smem_bytes(int mcap, int P, bool cyclic,
                                                           bool pascal = true) {
-    size_t tiles = 3ull * mcap * SEG_S * sizeof(double);
+    size_t tiles = (pascal ? 4ull : 3ull) * mcap * SEG_S * sizeof(double);
     size_t red = 6ull * SEG_S * sizeof(double);
-    size_t rsc = pascal ? seg_rsc_bytes(P, cyclic) : 0;
+    size_t rsc = pascal && !seg_rsc_in_b(mcap, P, cyclic) ? seg_rsc_bytes(P, cyclic) : 0;
     size_t bars = (size_t)(mcap / SEG_BOXR) * sizeof(uint64_t);
     return tiles + red + rsc + bars + 128;  // +128: alignment slack
 }
@@ -96,14 +102,19 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     extern __shared__ unsigned char smem_raw[];
     double* base = reinterpret_cast<double*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    constexpr bool STREAM_B = METHOD != SEG_PASCAL;
     const int mcap = args.mcap;
     double* TA = base;
-    double* TC = TA + (size_t)mcap * SEG_S;
+    double* TB = TA + (size_t)mcap * SEG_S;  // PaScaL only
+    double* TC = TB + (STREAM_B ? 0 : (size_t)mcap * SEG_S);
     double* TD = TC + (size_t)mcap * SEG_S;
     double* red = TD + (size_t)mcap * SEG_S;  // [6][SEG_S]
-    double* rsc = red + 6 * SEG_S;            // reduced-solve scratch (PaScaL)
-    uint64_t* bars = reinterpret_cast<uint64_t*>(
-        rsc + (METHOD == SEG_PASCAL ? seg_rsc_bytes(args.P, CYCLIC) / sizeof(double) : 0));
+    double* after_red = red + 6 * SEG_S;
+    const bool rsc_in_b = !STREAM_B && seg_rsc_in_b(mcap, args.P, CYCLIC);
+    double* rsc = rsc_in_b ? TB : after_red;  // reduced-solve scratch (PaScaL)
+    const size_t rsc_extra =
+        (!STREAM_B && !rsc_in_b) ? seg_rsc_bytes(args.P, CYCLIC) / sizeof(double) : 0;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(after_red + rsc_extra);
 
     cg::cluster_group cluster = cg::this_cluster();
     const int P = args.P;
@@ -129,12 +140,13 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         }
         __syncwarp();
         if (s == 0) {
-            const uint32_t bytes = 3u * SEG_BOXR * SEG_S * sizeof(double);
+            const uint32_t bytes = (STREAM_B ? 3u : 4u) * SEG_BOXR * SEG_S * sizeof(double);
             for (int c = 0; c < nch; ++c) {
                 mbar_expect_tx(&bars[c], bytes);
                 const int y = r0 + c * SEG_BOXR;
                 const size_t o = (size_t)c * SEG_BOXR * SEG_S;
                 tma_load_2d(TA + o, &tmA, g * SEG_S, y, &bars[c]);
+                if (!STREAM_B) tma_load_2d(TB + o, &tmB, g * SEG_S, y, &bars[c]);
                 tma_load_2d(TC + o, &tmC, g * SEG_S, y, &bars[c]);
                 tma_load_2d(TD + o, &tmD, g * SEG_S, y, &bars[c]);
             }
@@ -143,11 +155,11 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         for (int j = 0; j < m; ++j) {
             size_t off = (size_t)(r0 + j) * ns + sys;
             T(TA, j) = valid ? args.A[off] : 0.0;
+            if (!STREAM_B) T(TB, j) = valid ? args.B[off] : 1.0;
             T(TC, j) = valid ? args.C[off] : 0.0;
             T(TD, j) = valid ? args.D[off] : 0.0;
         }
     }
-    (void)tmB;
     // B of rows [c * SEG_BOXR, (c + 1) * SEG_BOXR) into registers (1 outside
     // the batch or the segment)
     const double* gB = args.B + (size_t)r0 * ns + sys;
@@ -171,15 +183,24 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     const int lo = (m - 2) - Jf;
 
     // ------------------------------------------------------- forward sweep
+    // B of row j: the streamed registers (Filtered) or the staged tile (PaScaL)
     double bcur[SEG_BOXR], bnext[SEG_BOXR];
-    load_b(0, bcur);
-    if (nch > 1) load_b(1, bnext);
+    if constexpr (STREAM_B) {
+        load_b(0, bcur);
+        if (nch > 1) load_b(1, bnext);
+    }
     chunk_ready(0);
-    double q0 = E::rcp(bcur[0]);
+    auto bval = [&](int u, int j) {
+        if constexpr (STREAM_B)
+            return bcur[u];
+        else
+            return T(TB, j);
+    };
+    double q0 = E::rcp(bval(0, 0));
     double a0 = E::mul(T(TA, 0), q0);
     double c0 = E::mul(T(TC, 0), q0);
     double d0 = E::mul(T(TD, 0), q0);
-    double q1 = E::rcp(bcur[1]);
+    double q1 = E::rcp(bval(1, 1));
     double ap = E::mul(T(TA, 1), q1);
     double cp = E::mul(T(TC, 1), q1);
     double dp = E::mul(T(TD, 1), q1);
@@ -191,9 +212,11 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     T(TD, 1) = dp;
     for (int c = 0; c < nch; ++c) {
         if (c > 0) {
+            if constexpr (STREAM_B) {
 #pragma unroll
-            for (int u = 0; u < SEG_BOXR; ++u) bcur[u] = bnext[u];
-            if (c + 1 < nch) load_b(c + 1, bnext);
+                for (int u = 0; u < SEG_BOXR; ++u) bcur[u] = bnext[u];
+                if (c + 1 < nch) load_b(c + 1, bnext);
+            }
             chunk_ready(c * SEG_BOXR);
         }
 #pragma unroll
@@ -201,7 +224,7 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             const int j = c * SEG_BOXR + u;
             if (j < 2 || j >= m) continue;
             const double a = T(TA, j);
-            const double inv = E::rcp(E::sub(bcur[u], E::mul(a, cp)));
+            const double inv = E::rcp(E::sub(bval(u, j), E::mul(a, cp)));
             dp = E::mul(inv, E::sub(T(TD, j), E::mul(a, dp)));
             cp = E::mul(inv, T(TC, j));
             T(TD, j) = dp;
