@@ -60,7 +60,8 @@ int heat_enqueue(btdma_heat_t h, double* theta, cudaStream_t st, cudaEvent_t* ev
     const int tx = (g.ix + HEAT_TILE - 1) / HEAT_TILE, ty = (g.iy + HEAT_TILE - 1) / HEAT_TILE;
     int rc;
     mark(0);
-    heat_rhs_z_kernel<<<gr, b1, 0, st>>>(theta, h->buf0, g);
+    heat_rhs_z_kernel<<<dim3((g.ix + 127) / 128, g.iy, (g.iz + HEAT_KCH - 1) / HEAT_KCH), b1, 0,
+                        st>>>(theta, h->buf0, g);
     CK(cudaGetLastError());
     mark(1);
     // Z sweep: system jj * ix + ii, row kk; solution to [jj][kk][ii]

@@ -50,41 +50,64 @@ constexpr double HEAT_PI = 3.14159265358979323846;
 // Right-hand side of the step (all directions' explicit half) plus the Z wall
 // folds, written in the Z-sweep layout D[(kk * iy + jj) * ix + ii]
 // (solve_theta.cu:121-160 and build_lhs_z_kernel :168-202).
-__global__ void __launch_bounds__(256) heat_rhs_z_kernel(const double* __restrict__ theta,
+// 2.5-D: a thread owns column (ii, jj) and walks HEAT_KCH planes, keeping
+// theta at k - 1, k, k + 1 in registers; the x neighbours come from the
+// adjacent lanes (warp shuffles; the warp's edge lanes load theirs), the y
+// neighbours from the adjacent rows.  Block (128), grid (ix / 128, iy,
+// iz / HEAT_KCH).  Lanes past the row (ix % 32 == 16) take part in the
+// shuffles on the last column's values and store nothing; a live lane never
+// uses a dead neighbour (its x neighbour past the row is the wall ghost).
+constexpr int HEAT_KCH = 16;
+__global__ void __launch_bounds__(128) heat_rhs_z_kernel(const double* __restrict__ theta,
                                                          double* __restrict__ D,
                                                          const HeatGeom g) {
     const int ii = blockIdx.x * blockDim.x + threadIdx.x;
     const int jj = blockIdx.y;
-    const int kk = blockIdx.z;
-    if (ii >= g.ix) return;
-    const int i = ii + 1, j = jj + 1, k = kk + 1;
-    const int sy = g.ix + 2;               // j stride of the full grid
+    const int k0 = blockIdx.z * HEAT_KCH;  // first interior plane kk of this block
+    const int lane = threadIdx.x & 31;
+    if (ii - lane >= g.ix) return;         // the whole warp is past the row
+    const bool live = ii < g.ix;
+    const int i = (live ? ii : g.ix - 1) + 1, j = jj + 1;
+    const int sy = g.ix + 2;                 // j stride of the full grid
     const int sz = (g.iy + 2) * (g.ix + 2);  // k stride (< 2^31 for grids this library takes)
-    const double* c0 = theta + heat_full(g, i, j, k);
-    const double t = c0[0];
-    const double cxi = g.cx[i], cyj = g.cy[j], czk = g.cz[k];
-    double tip, tim, tjp, tjm, tkp, tkm;
-    {
-        const double ubc = -cyj * czk;  // x walls
-        tip = ii + 1 < g.ix ? c0[1] : 2.0 * ubc - t;
-        tim = ii > 0 ? c0[-1] : 2.0 * ubc - t;
+    const double cxi = g.cx[i], cyj = g.cy[j];
+    const double* col = theta + heat_full(g, i, j, 0);  // this column at k = 0
+    // theta at k - 1 and k for the first plane (k = k0 + 1)
+    double tm = col[(size_t)k0 * sz], t = col[(size_t)(k0 + 1) * sz];
+    for (int kk = k0; kk < k0 + HEAT_KCH; ++kk) {  // iz % HEAT_KCH == 0 (btdma_heat_create)
+        const int k = kk + 1;
+        const double* c0 = col + (size_t)k * sz;
+        const double tn = c0[sz];  // theta(k + 1): a ghost plane at the top wall, not read
+        const double czk = g.cz[k];
+        double tip, tim, tjp, tjm, tkp, tkm;
+        {
+            const double ubc = -cyj * czk;  // x walls
+            double right = __shfl_down_sync(0xffffffffu, t, 1);
+            double left = __shfl_up_sync(0xffffffffu, t, 1);
+            if (lane == 31) right = live && ii + 1 < g.ix ? c0[1] : 0.0;
+            if (lane == 0) left = ii > 0 ? c0[-1] : 0.0;
+            tip = ii + 1 < g.ix ? right : 2.0 * ubc - t;
+            tim = ii > 0 ? left : 2.0 * ubc - t;
+        }
+        {
+            const double ubc = -cxi * czk;  // y walls
+            tjp = jj + 1 < g.iy ? c0[sy] : 2.0 * ubc - t;
+            tjm = jj > 0 ? c0[-sy] : 2.0 * ubc - t;
+        }
+        const double ubz = -cxi * cyj;  // z walls
+        tkp = kk + 1 < g.iz ? tn : 2.0 * ubz - t;
+        tkm = kk > 0 ? tm : 2.0 * ubz - t;
+        const double src = g.dt * 3.0 * HEAT_PI * HEAT_PI * cxi * cyj * czk;
+        double rhs = (g.bx * tip + g.bx * tim) + (g.by * tjp + g.by * tjm) +
+                     (g.bz * tkp + g.bz * tkm) +
+                     (1.0 + (-2.0 * g.bx) + (-2.0 * g.by) + (-2.0 * g.bz)) * t + src;
+        // fully implicit Z walls: base * (ghost + boundary cell) to the right-hand side
+        if (kk == 0) rhs += g.bz * ((2.0 * ubz - t) + t);
+        if (kk == g.iz - 1) rhs += g.bz * ((2.0 * ubz - t) + t);
+        if (live) D[((size_t)kk * g.iy + jj) * g.ix + ii] = rhs;
+        tm = t;
+        t = tn;
     }
-    {
-        const double ubc = -cxi * czk;  // y walls
-        tjp = jj + 1 < g.iy ? c0[sy] : 2.0 * ubc - t;
-        tjm = jj > 0 ? c0[-sy] : 2.0 * ubc - t;
-    }
-    const double ubz = -cxi * cyj;  // z walls
-    tkp = kk + 1 < g.iz ? c0[sz] : 2.0 * ubz - t;
-    tkm = kk > 0 ? c0[-sz] : 2.0 * ubz - t;
-    const double src = g.dt * 3.0 * HEAT_PI * HEAT_PI * cxi * cyj * czk;
-    double rhs = (g.bx * tip + g.bx * tim) + (g.by * tjp + g.by * tjm) +
-                 (g.bz * tkp + g.bz * tkm) +
-                 (1.0 + (-2.0 * g.bx) + (-2.0 * g.by) + (-2.0 * g.bz)) * t + src;
-    // fully implicit Z walls: base * (ghost + boundary cell) to the right-hand side
-    if (kk == 0) rhs += g.bz * ((2.0 * ubz - t) + t);
-    if (kk == g.iz - 1) rhs += g.bz * ((2.0 * ubz - t) + t);
-    D[((size_t)kk * g.iy + jj) * g.ix + ii] = rhs;
 }
 
 // Y wall folds on the Z solution, already in the Y-sweep layout [jj][kk][ii]
