@@ -60,9 +60,12 @@ int rag_build_launches(btdma_t h) {
     if (wl.count) h->rag_launches.push_back(wl);
     for (int P = 512; P >= 64; P >>= 1)
         for (int stg = 0; stg < 2; ++stg) {
-            btdma_handle::RagLaunch cl{1, P, (int)tasks.size(), 0, 0, stg};
+            btdma_handle::RagLaunch cl{1, P, (int)tasks.size(), 0, 1, stg};
             for (const auto& b : h->rag_buckets)
-                if (b.cta && b.P == P && b.staged == stg) rag_bucket_tasks(b, 1, P, tasks);
+                if (b.cta && b.P == P && b.staged == stg) {
+                    rag_bucket_tasks(b, 1, P, tasks);
+                    cl.mcap = std::max(cl.mcap, rag_mcap(b.nmax, P));
+                }
             cl.count = (int)tasks.size() - cl.first;
             if (cl.count) h->rag_launches.push_back(cl);
         }
@@ -179,7 +182,7 @@ int rag_launch(btdma_t h, int cta, int P, int mcap, int staged, const int4* task
     a.mcap = mcap;
     a.status = h->status;
     if (cta) {
-        if (staged && rag_cta_smem_bytes(P, true) > (size_t)max_smem_optin()) staged = 0;
+        if (staged && rag_cta_smem_bytes(P, true, mcap) > (size_t)max_smem_optin()) staged = 0;
         auto kern = staged ? ragged_cta_kernel<TIN, true> : ragged_cta_kernel<TIN, false>;
         static bool attr_done[2] = {false, false};
         if (!attr_done[staged]) {
@@ -187,7 +190,7 @@ int rag_launch(btdma_t h, int cta, int P, int mcap, int staged, const int4* task
                                     max_smem_optin()));
             attr_done[staged] = true;
         }
-        kern<<<n_tasks, P, rag_cta_smem_bytes(P, staged), st>>>(a);
+        kern<<<n_tasks, P, rag_cta_smem_bytes(P, staged, mcap), st>>>(a);
     } else {
         auto kern = ragged_kernel<TIN>;
         static bool attr_done = false;
@@ -269,7 +272,8 @@ int rag_tune(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, 
         for (int P = 64; P <= 512 && b.nmin / P >= 3; P <<= 1)
             if (rag_mcap(b.nmax, P) <= RAG_MT) {
                 cands.push_back({1, P, 0});
-                if (rag_cta_smem_bytes(P, true) <= (size_t)max_smem_optin())
+                if (rag_cta_smem_bytes(P, true, rag_mcap(b.nmax, P)) <=
+                    (size_t)max_smem_optin())
                     cands.push_back({1, P, 1});
             }
         float best = 1e30f;
@@ -364,7 +368,8 @@ int btdma_ragged_set_plan(btdma_t h, const btdma_ragged_bucket* in, int n) {
             if (P < 64 || P > 512 || rag_mcap(b.nmax, P) > RAG_MT)
                 return fail(BTDMA_ERR_ARG, "bucket %d: CTA kind needs 64 <= P <= 512 and <= %d "
                             "rows per thread", i, RAG_MT);
-            if (kind == 2 && rag_cta_smem_bytes(P, true) > (size_t)max_smem_optin())
+            if (kind == 2 &&
+                rag_cta_smem_bytes(P, true, rag_mcap(b.nmax, P)) > (size_t)max_smem_optin())
                 return fail(BTDMA_ERR_ARG, "bucket %d: a staged system of %d threads does not "
                             "fit in shared memory", i, P);
         } else {

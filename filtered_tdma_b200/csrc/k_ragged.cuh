@@ -193,17 +193,20 @@ __global__ void __launch_bounds__(256) ragged_kernel(const RagArgs a) {
 constexpr int RAG_MT = 16;
 
 // STAGED: the whole system is first copied into shared memory with coalesced
-// loads, laid out [array][thread][row of segment] with an odd pitch of
-// RAG_MT + 1 doubles (A, B, C, D widened to FP64): consecutive rows of a
-// segment are consecutive words for the coalesced fill, and the threads reading
-// row k of their segments are 17 doubles apart (no bank conflicts either way).
+// loads, laid out [array][thread][row of segment] with an odd pitch of at least
+// the launch's rows per thread (A, B, C, D widened to FP64): consecutive rows
+// of a segment are consecutive words for the coalesced fill, and the threads
+// reading row k of their segments are an odd number of doubles apart (no bank
+// conflicts either way).
 // The elimination state then overwrites A, C, D in place and x goes through B
 // on its way out (coalesced stores).  Without staging each thread reads its
 // contiguous rows straight from global memory, which leaves L1 to hold four
 // lines per thread.
-constexpr int RAG_MP = RAG_MT + 1;  // staged pitch per thread
-__host__ __device__ __forceinline__ size_t rag_cta_smem_bytes(int P, bool staged) {
-    return (2ull * 3 * (P + 2) + (staged ? 4ull * RAG_MP * P : 3ull * RAG_MT * P)) *
+// mcap: rows per thread of the launch (<= RAG_MT); staged pitch mcap | 1 (odd).
+__host__ __device__ __forceinline__ int rag_pitch(int mcap) { return mcap | 1; }
+__host__ __device__ __forceinline__ size_t rag_cta_smem_bytes(int P, bool staged, int mcap) {
+    return (2ull * 3 * (P + 2) +
+            (staged ? 4ull * rag_pitch(mcap) * P : 3ull * (size_t)mcap * P)) *
            sizeof(double);
 }
 
@@ -266,11 +269,13 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
     const TIN* __restrict__ pD = static_cast<const TIN*>(a.D) + row0;
 
     double* const stg = rsm + 2 * 3 * gs;  // state / staging area
-    // this thread's slots: unstaged [field][row][thread] -> stt[(f * M + k) * P];
-    // staged [field][thread][row] -> stt[f * P * RAG_MP + k]
-    double* stt = STAGED ? stg + p * RAG_MP : stg + p;
-    const int fs = STAGED ? P * RAG_MP : M * P;  // field stride
-    const int ks = STAGED ? 1 : P;               // row stride
+    // this thread's slots (mcap = the launch's rows per thread, <= M):
+    // unstaged [field][row][thread] -> stt[(f * mcap + k) * P];
+    // staged [field][thread][row] -> stt[f * P * mp + k], mp = mcap | 1
+    const int mp = rag_pitch(a.mcap);
+    double* stt = STAGED ? stg + p * mp : stg + p;
+    const int fs = STAGED ? P * mp : a.mcap * P;  // field stride
+    const int ks = STAGED ? 1 : P;                // row stride
     const float inv0 = 1.0f / (float)(base > 0 ? base : 1), inv1 = 1.0f / (float)(base + 1);
     if constexpr (STAGED) {
         // fields 0..3 = A, B, C, D; coalesced over the system's rows
@@ -284,7 +289,7 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
         for (int r = p; r < n; r += P) {
             int q, k;
             rag_locate(r, base, rem, inv0, inv1, q, k);
-            double* dst = stg + q * RAG_MP + k;
+            double* dst = stg + q * mp + k;
             cp_async_elem(dst + 0 * fs, gA + r);
             cp_async_elem(dst + 1 * fs, gB + r);
             cp_async_elem(dst + 2 * fs, gC + r);
@@ -461,7 +466,7 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
         for (int r = p; r < n; r += P) {
             int q, k;
             rag_locate(r, base, rem, inv0, inv1, q, k);
-            gX[r] = stg[1 * fs + q * RAG_MP + k];
+            gX[r] = stg[1 * fs + q * mp + k];
         }
     } else {
         xp[0] = xf;

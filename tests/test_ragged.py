@@ -158,9 +158,10 @@ def _shapes(b):
         if b["n_row_min"] // P >= 3 and -(-b["n_row_max"] // P) <= 32:
             out.append((P, 0))
     for P in (64, 128, 256, 512):
-        if b["n_row_min"] // P >= 3 and -(-b["n_row_max"] // P) <= 16:
+        mcap = -(-b["n_row_max"] // P)  # rows per thread
+        if b["n_row_min"] // P >= 3 and mcap <= 16:
             out.append((P, 1))
-            if 4 * P * 17 * 8 + 6 * (P + 2) * 8 <= 227 * 1024:
+            if 4 * P * (mcap | 1) * 8 + 6 * (P + 2) * 8 <= 227 * 1024:  # staged tile fits
                 out.append((P, 2))
     return out
 
@@ -179,8 +180,8 @@ def test_ragged_every_launch_shape(cuda, orc, precision):
     X = torch.zeros(int(off[-1]), dtype=torch.float64, device=cuda)
     s.solve_ragged(dA, dB, dC, dD, X, off, per)
     plan = s.ragged_plan()
-    for bad in (dict(plan[0], lanes_per_system=3), dict(plan[-1], cta_per_system=2,
-                                                          lanes_per_system=512),
+    for bad in (dict(plan[0], lanes_per_system=3), dict(plan[-1], cta_per_system=1,
+                                                          lanes_per_system=32),
                 dict(plan[0], n_row_max=plan[0]["n_row_max"] + 1)):
         with pytest.raises(L.BtdmaError):
             s.ragged_set_plan([bad] + plan[1:] if bad["n_row_min"] == plan[0]["n_row_min"]
@@ -189,6 +190,7 @@ def test_ragged_every_launch_shape(cuda, orc, precision):
     opts = [_shapes(b) for b in plan]
     assert all(opts)
     assert any((P, 2) in o for o in opts for P in (64, 128, 256))
+    assert any((512, 2) in o for o in opts)  # staged 512-thread CTAs (<= 8 rows a thread)
     for j in range(max(len(o) for o in opts)):
         want = [o[j % len(o)] for o in opts]
         s.ragged_set_plan([dict(b, lanes_per_system=P, cta_per_system=k)
