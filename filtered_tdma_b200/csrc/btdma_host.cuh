@@ -139,9 +139,9 @@ inline int max_smem_optin() {
     return v;
 }
 
-template <int METHOD, bool CYCLIC>
-int launch_seg(const CUtensorMap* maps, const SegArgs& a, int groups, cudaStream_t st) {
-    auto kern = seg_f64_kernel<METHOD, CYCLIC>;
+template <int METHOD, bool CYCLIC, int RR>
+int launch_seg_rr(const CUtensorMap* maps, const SegArgs& a, int groups, cudaStream_t st) {
+    auto kern = seg_f64_kernel<METHOD, CYCLIC, RR>;
     static bool attr_done = false;
     if (!attr_done) {
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -152,7 +152,7 @@ int launch_seg(const CUtensorMap* maps, const SegArgs& a, int groups, cudaStream
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(a.P, groups, 1);
     cfg.blockDim = dim3(SEG_S, 1, 1);
-    cfg.dynamicSmemBytes = seg_smem_bytes(a.mcap, a.P, CYCLIC, METHOD == SEG_PASCAL);
+    cfg.dynamicSmemBytes = seg_smem_bytes(a.mcap, a.P, CYCLIC, METHOD == SEG_PASCAL, RR);
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -163,6 +163,17 @@ int launch_seg(const CUtensorMap* maps, const SegArgs& a, int groups, cudaStream
     cfg.numAttrs = 1;
     CK(cudaLaunchKernelEx(&cfg, kern, maps[0], maps[1], maps[2], maps[3], maps[4], a));
     return BTDMA_OK;
+}
+
+// Filtered keeps SEG_REG leading rows of each segment in registers when every
+// segment has room for them (seg_reg_rows).
+template <int METHOD, bool CYCLIC>
+int launch_seg(const CUtensorMap* maps, const SegArgs& a, int groups, cudaStream_t st) {
+    if constexpr (METHOD != SEG_PASCAL) {
+        if (seg_reg_rows(false, a.n_row, a.P) == SEG_REG)
+            return launch_seg_rr<METHOD, CYCLIC, SEG_REG>(maps, a, groups, st);
+    }
+    return launch_seg_rr<METHOD, CYCLIC, 0>(maps, a, groups, st);
 }
 
 // 3-D view [nseg][TILE_MT][n_sys] of an [n_row x n_sys] FP64 array; boxes of

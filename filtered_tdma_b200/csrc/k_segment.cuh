@@ -11,10 +11,12 @@
 //     shared memory by TMA in chunks of SEG_BOXR rows, each chunk completing on
 //     its own mbarrier, so the forward sweep starts on the first chunk while the
 //     others are still in flight.  Filtered streams B instead (only the forward
-//     sweep reads it): straight from HBM, a chunk ahead into registers, which
-//     keeps its tile at three arrays (4 CTAs per SM at 64 rows instead of 3).
-//     PaScaL keeps B staged: the tile's B part holds its reduced-system scratch
-//     afterwards.  A, B, C, D are read from HBM exactly once.
+//     sweep reads it): straight from HBM, a chunk ahead into registers, and
+//     holds the first SEG_REG rows of each segment (inputs, then state) in
+//     registers when every segment has SEG_REG + 2 rows or more, so its tile
+//     has three arrays of m - SEG_REG rows (5 CTAs per SM at 64 rows instead of
+//     3).  PaScaL keeps B staged: the tile's B part holds its reduced-system
+//     scratch afterwards.  A, B, C, D are read from HBM exactly once.
 //   * The modified Thomas sweeps run in place on the tile (the reference's
 //     per-rank steps, pascal_tdma.cpp:131-183 / filtered_tdma_kernels.hpp:35-189,
 //     with the same operation order, IEEE round-to-nearest, no FMA).
@@ -45,6 +47,7 @@ namespace cg = cooperative_groups;
 constexpr int SEG_S = 32;     // systems per CTA (one warp; a 256-byte TMA box row)
 constexpr int SEG_BOXR = 16;  // rows per TMA chunk
 constexpr int SEG_MAX_P = 16; // cluster size limit (non-portable above 8)
+constexpr int SEG_REG = 16;   // Filtered: leading rows of a segment held in registers
 
 enum SegMethod { SEG_PASCAL = 0, SEG_FILT_V1 = 1, SEG_FILT_V2 = 2 };
 
@@ -77,12 +80,21 @@ __host__ __device__ __forceinline__ size_t seg_rsc_bytes(int P, bool cyclic) {
 __host__ __device__ __forceinline__ bool seg_rsc_in_b(int mcap, int P, bool cyclic) {
     return seg_rsc_bytes(P, cyclic) <= (size_t)mcap * SEG_S * sizeof(double);
 }
+// Tile rows of a segment of mcap rows, rr of them held in registers.
+__host__ __device__ __forceinline__ int seg_tile_rows(int mcap, int rr) {
+    return mcap > rr ? mcap - rr : 0;
+}
+// rr = SEG_REG for Filtered when every segment has >= SEG_REG + 2 rows, else 0.
+__host__ __device__ __forceinline__ int seg_reg_rows(bool pascal, int n_row, int P) {
+    return (!pascal && n_row / P >= SEG_REG + 2) ? SEG_REG : 0;
+}
 __host__ __device__ __forceinline__ size_t seg_smem_bytes(int mcap, int P, bool cyclic,
-                                                          bool pascal = true) {
-    size_t tiles = (pascal ? 4ull : 3ull) * mcap * SEG_S * sizeof(double);
+                                                          bool pascal = true, int rr = 0) {
+    const int mt = seg_tile_rows(mcap, rr);
+    size_t tiles = (pascal ? 4ull : 3ull) * mt * SEG_S * sizeof(double);
     size_t red = 6ull * SEG_S * sizeof(double);
     size_t rsc = pascal && !seg_rsc_in_b(mcap, P, cyclic) ? seg_rsc_bytes(P, cyclic) : 0;
-    size_t bars = (size_t)(mcap / SEG_BOXR) * sizeof(uint64_t);
+    size_t bars = (size_t)(mt / SEG_BOXR + 1) * sizeof(uint64_t);
     return tiles + red + rsc + bars + 128;  // +128: alignment slack
 }
 
@@ -93,8 +105,10 @@ __device__ __forceinline__ void cluster_wait() {
     asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 
-template <int METHOD, bool CYCLIC>
-__global__ void __launch_bounds__(SEG_S, 4)
+// RR: leading rows of each segment held in registers (Filtered, when every
+// segment has at least RR + 2 rows, so rows m - 2 and m - 1 are tile rows).
+template <int METHOD, bool CYCLIC, int RR = 0>
+__global__ void __launch_bounds__(SEG_S, 5)
 seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                const __grid_constant__ CUtensorMap tmC, const __grid_constant__ CUtensorMap tmD,
                const __grid_constant__ CUtensorMap tmX, const SegArgs args) {
@@ -103,12 +117,15 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     double* base = reinterpret_cast<double*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     constexpr bool STREAM_B = METHOD != SEG_PASCAL;
+    static_assert(RR == 0 || (STREAM_B && RR >= 2), "register rows: Filtered only");
+    constexpr int RRA = RR > 0 ? RR : 1;
     const int mcap = args.mcap;
+    const int mt = seg_tile_rows(mcap, RR);  // tile rows
     double* TA = base;
-    double* TB = TA + (size_t)mcap * SEG_S;  // PaScaL only
-    double* TC = TB + (STREAM_B ? 0 : (size_t)mcap * SEG_S);
-    double* TD = TC + (size_t)mcap * SEG_S;
-    double* red = TD + (size_t)mcap * SEG_S;  // [6][SEG_S]
+    double* TB = TA + (size_t)mt * SEG_S;  // PaScaL only
+    double* TC = TB + (STREAM_B ? 0 : (size_t)mt * SEG_S);
+    double* TD = TC + (size_t)mt * SEG_S;
+    double* red = TD + (size_t)mt * SEG_S;  // [6][SEG_S]
     double* after_red = red + 6 * SEG_S;
     const bool rsc_in_b = !STREAM_B && seg_rsc_in_b(mcap, args.P, CYCLIC);
     double* rsc = rsc_in_b ? TB : after_red;  // reduced-solve scratch (PaScaL)
@@ -127,9 +144,26 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
 
     int r0, m;
     seg_range(args.n_row, P, k, r0, m);
-    const int nch = (m + SEG_BOXR - 1) / SEG_BOXR;
+    // rows [0, RR) of the segment live in registers (Filtered), rows [RR, m) in
+    // the shared-memory tile (tile row j - RR)
+    const int ms = m > RR ? m - RR : 0;
+    const int nch = (ms + SEG_BOXR - 1) / SEG_BOXR;
 
-#define T(Z, j) Z[(size_t)(j) * SEG_S + s]
+#define T(Z, j) Z[(size_t)((j) - RR) * SEG_S + s]
+
+    // register rows: A, B, C, D straight from HBM (the state then replaces A, C, D)
+    double rA[RRA], rB[RRA], rC[RRA], rD[RRA];
+    if constexpr (RR > 0) {
+#pragma unroll
+        for (int u = 0; u < RR; ++u) {
+            const bool in = valid && u < m;
+            const size_t off = (size_t)(r0 + u) * ns + sys;
+            rA[u] = in ? __ldg(args.A + off) : 0.0;
+            rB[u] = in ? __ldg(args.B + off) : 1.0;
+            rC[u] = in ? __ldg(args.C + off) : 0.0;
+            rD[u] = in ? __ldg(args.D + off) : 0.0;
+        }
+    }
 
     // ---------------------------------------------------------- stage the tile
     bool ok = true;
@@ -143,7 +177,7 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             const uint32_t bytes = (STREAM_B ? 3u : 4u) * SEG_BOXR * SEG_S * sizeof(double);
             for (int c = 0; c < nch; ++c) {
                 mbar_expect_tx(&bars[c], bytes);
-                const int y = r0 + c * SEG_BOXR;
+                const int y = r0 + RR + c * SEG_BOXR;
                 const size_t o = (size_t)c * SEG_BOXR * SEG_S;
                 tma_load_2d(TA + o, &tmA, g * SEG_S, y, &bars[c]);
                 if (!STREAM_B) tma_load_2d(TB + o, &tmB, g * SEG_S, y, &bars[c]);
@@ -152,7 +186,7 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             }
         }
     } else {
-        for (int j = 0; j < m; ++j) {
+        for (int j = RR; j < m; ++j) {
             size_t off = (size_t)(r0 + j) * ns + sys;
             T(TA, j) = valid ? args.A[off] : 0.0;
             if (!STREAM_B) T(TB, j) = valid ? args.B[off] : 1.0;
@@ -160,19 +194,18 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             T(TD, j) = valid ? args.D[off] : 0.0;
         }
     }
-    // B of rows [c * SEG_BOXR, (c + 1) * SEG_BOXR) into registers (1 outside
-    // the batch or the segment)
-    const double* gB = args.B + (size_t)r0 * ns + sys;
+    // B of tile rows [RR + c * SEG_BOXR, RR + (c + 1) * SEG_BOXR) into registers
+    // (1 outside the batch or the segment)
+    const double* gB = args.B + (size_t)(r0 + RR) * ns + sys;
     auto load_b = [&](int c, double (&bb)[SEG_BOXR]) {
 #pragma unroll
         for (int u = 0; u < SEG_BOXR; ++u) {
-            const int j = c * SEG_BOXR + u;
-            bb[u] = (valid && j < m) ? __ldg(gB + (size_t)j * ns) : 1.0;
+            const int j = c * SEG_BOXR + u;  // tile row
+            bb[u] = (valid && j < ms) ? __ldg(gB + (size_t)j * ns) : 1.0;
         }
     };
-    auto chunk_ready = [&](int j) {
-        if (args.use_tma && ok && (j % SEG_BOXR) == 0)
-            ok = mbar_wait_bounded(&bars[j / SEG_BOXR], 0, args.status);
+    auto chunk_wait = [&](int c) {
+        if (args.use_tma && ok) ok = mbar_wait_bounded(&bars[c], 0, args.status);
     };
 
     // J of this segment (Filtered); v1's interface pass runs the full sweeps.
@@ -183,48 +216,88 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     const int lo = (m - 2) - Jf;
 
     // ------------------------------------------------------- forward sweep
-    // B of row j: the streamed registers (Filtered) or the staged tile (PaScaL)
-    double bcur[SEG_BOXR], bnext[SEG_BOXR];
-    if constexpr (STREAM_B) {
-        load_b(0, bcur);
+    double q0, a0, c0, d0, q1, ap, cp, dp;
+    double bcur[SEG_BOXR], bnext[SEG_BOXR];  // B of tile chunks c, c + 1 (Filtered)
+    if constexpr (RR > 0) {
+        q0 = E::rcp(rB[0]);
+        a0 = E::mul(rA[0], q0);
+        c0 = E::mul(rC[0], q0);
+        d0 = E::mul(rD[0], q0);
+        q1 = E::rcp(rB[1]);
+        ap = E::mul(rA[1], q1);
+        cp = E::mul(rC[1], q1);
+        dp = E::mul(rD[1], q1);
+        rA[0] = a0;
+        rC[0] = c0;
+        rD[0] = d0;
+        rA[1] = ap;
+        rC[1] = cp;
+        rD[1] = dp;
+#pragma unroll
+        for (int u = 2; u < RR; ++u) {
+            if (u >= m) continue;
+            const double a = rA[u];
+            const double inv = E::rcp(E::sub(rB[u], E::mul(a, cp)));
+            dp = E::mul(inv, E::sub(rD[u], E::mul(a, dp)));
+            cp = E::mul(inv, rC[u]);
+            rD[u] = dp;
+            rC[u] = cp;
+            if (METHOD != SEG_FILT_V2 || u <= Jf) {
+                ap = E::mul(E::mul(-inv, a), ap);
+                rA[u] = ap;
+            }
+        }
+        if (nch > 0) load_b(0, bcur);
         if (nch > 1) load_b(1, bnext);
+    } else {
+        // rows 0 and 1 are tile rows; B streamed (Filtered) or staged (PaScaL)
+        double b0, b1;
+        if constexpr (STREAM_B) {
+            if (nch > 0) load_b(0, bcur);
+            if (nch > 1) load_b(1, bnext);
+            b0 = bcur[0];
+            b1 = bcur[1];
+        }
+        chunk_wait(0);
+        if constexpr (!STREAM_B) {
+            b0 = T(TB, 0);
+            b1 = T(TB, 1);
+        }
+        q0 = E::rcp(b0);
+        a0 = E::mul(T(TA, 0), q0);
+        c0 = E::mul(T(TC, 0), q0);
+        d0 = E::mul(T(TD, 0), q0);
+        q1 = E::rcp(b1);
+        ap = E::mul(T(TA, 1), q1);
+        cp = E::mul(T(TC, 1), q1);
+        dp = E::mul(T(TD, 1), q1);
+        T(TA, 0) = a0;
+        T(TC, 0) = c0;
+        T(TD, 0) = d0;
+        T(TA, 1) = ap;
+        T(TC, 1) = cp;
+        T(TD, 1) = dp;
     }
-    chunk_ready(0);
-    auto bval = [&](int u, int j) {
-        if constexpr (STREAM_B)
-            return bcur[u];
-        else
-            return T(TB, j);
-    };
-    double q0 = E::rcp(bval(0, 0));
-    double a0 = E::mul(T(TA, 0), q0);
-    double c0 = E::mul(T(TC, 0), q0);
-    double d0 = E::mul(T(TD, 0), q0);
-    double q1 = E::rcp(bval(1, 1));
-    double ap = E::mul(T(TA, 1), q1);
-    double cp = E::mul(T(TC, 1), q1);
-    double dp = E::mul(T(TD, 1), q1);
-    T(TA, 0) = a0;
-    T(TC, 0) = c0;
-    T(TD, 0) = d0;
-    T(TA, 1) = ap;
-    T(TC, 1) = cp;
-    T(TD, 1) = dp;
     for (int c = 0; c < nch; ++c) {
-        if (c > 0) {
-            if constexpr (STREAM_B) {
+        if constexpr (STREAM_B) {
+            if (c > 0) {
 #pragma unroll
                 for (int u = 0; u < SEG_BOXR; ++u) bcur[u] = bnext[u];
                 if (c + 1 < nch) load_b(c + 1, bnext);
             }
-            chunk_ready(c * SEG_BOXR);
         }
+        if (c > 0 || RR > 0) chunk_wait(c);  // RR == 0: chunk 0 was waited for above
 #pragma unroll
         for (int u = 0; u < SEG_BOXR; ++u) {
-            const int j = c * SEG_BOXR + u;
+            const int j = RR + c * SEG_BOXR + u;
             if (j < 2 || j >= m) continue;
             const double a = T(TA, j);
-            const double inv = E::rcp(E::sub(bval(u, j), E::mul(a, cp)));
+            double bj;
+            if constexpr (STREAM_B)
+                bj = bcur[u];
+            else
+                bj = T(TB, j);
+            const double inv = E::rcp(E::sub(bj, E::mul(a, cp)));
             dp = E::mul(inv, E::sub(T(TD, j), E::mul(a, dp)));
             cp = E::mul(inv, T(TC, j));
             T(TD, j) = dp;
@@ -235,24 +308,49 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             }
         }
     }
+    // rows m - 2 and m - 1 are tile rows (m >= RR + 2)
     const double aN = T(TA, m - 1), cN = T(TC, m - 1), dN = T(TD, m - 1);
 
     // ------------------------------------------------------ backward sweep
     {
         double dn = T(TD, m - 2), an = T(TA, m - 2), cn = T(TC, m - 2);
-        for (int j = m - 3; j >= 1; --j) {
-            const double c = T(TC, j);
-            dn = E::sub(T(TD, j), E::mul(c, dn));
-            T(TD, j) = dn;
+        // one row of the sweep on (A, C, D) of tile row j
+        auto bwd = [&](int j, double& A_, double& C_, double& D_) {
+            const double c = C_;
+            dn = E::sub(D_, E::mul(c, dn));
+            D_ = dn;
             if (METHOD != SEG_FILT_V2 || j < Jf) {
-                an = E::sub(T(TA, j), E::mul(c, an));
-                T(TA, j) = an;
+                an = E::sub(A_, E::mul(c, an));
+                A_ = an;
             } else {
-                an = T(TA, j);
+                an = A_;
             }
             if (METHOD != SEG_FILT_V2 || j > lo) {
                 cn = E::mul(c, -cn);
-                T(TC, j) = cn;
+                C_ = cn;
+            } else {
+                cn = c;
+            }
+        };
+        const int jlo = RR > 1 ? RR : 1;
+        for (int j = m - 3; j >= jlo; --j) bwd(j, T(TA, j), T(TC, j), T(TD, j));
+        // the register rows: the same steps, indexed directly (no references,
+        // which would move the arrays to local memory)
+#pragma unroll
+        for (int u = RR - 1; u >= 1; --u) {
+            if (u > m - 3) continue;
+            const double c = rC[u];
+            dn = E::sub(rD[u], E::mul(c, dn));
+            rD[u] = dn;
+            if (METHOD != SEG_FILT_V2 || u < Jf) {
+                an = E::sub(rA[u], E::mul(c, an));
+                rA[u] = an;
+            } else {
+                an = rA[u];
+            }
+            if (METHOD != SEG_FILT_V2 || u > lo) {
+                cn = E::mul(c, -cn);
+                rC[u] = cn;
             } else {
                 cn = c;
             }
@@ -261,10 +359,20 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     // Row-0 reduction: decouple row 0 from x_1 (pascal_tdma.cpp:173-178,
     // filtered_tdma_kernels.hpp:178-189; Filtered keeps C_0 unreduced).
     {
-        const double r = E::rcp(E::sub(1.0, E::mul(T(TA, 1), c0)));
-        d0 = E::mul(r, E::sub(d0, E::mul(c0, T(TD, 1))));
+        double a1, c1, d1;
+        if constexpr (RR > 0) {
+            a1 = rA[1];
+            c1 = rC[1];
+            d1 = rD[1];
+        } else {
+            a1 = T(TA, 1);
+            c1 = T(TC, 1);
+            d1 = T(TD, 1);
+        }
+        const double r = E::rcp(E::sub(1.0, E::mul(a1, c0)));
+        d0 = E::mul(r, E::sub(d0, E::mul(c0, d1)));
         a0 = E::mul(r, a0);
-        if (METHOD == SEG_PASCAL) c0 = E::mul(E::mul(-r, c0), T(TC, 1));
+        if (METHOD == SEG_PASCAL) c0 = E::mul(E::mul(-r, c0), c1);
     }
     red[0 * SEG_S + s] = a0;
     red[1 * SEG_S + s] = c0;
@@ -387,36 +495,56 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         }
     } else {
         // ------------------------------------------------ final update
-        T(TD, 0) = x0;
+        if constexpr (RR > 0) {
+            rD[0] = x0;
+        } else {
+            T(TD, 0) = x0;
+        }
         T(TD, m - 1) = xN;
-        if (METHOD == SEG_PASCAL) {
+        if constexpr (METHOD == SEG_PASCAL) {
             for (int j = 1; j < m - 1; ++j)
                 T(TD, j) = E::sub(T(TD, j), E::add(E::mul(T(TA, j), x0), E::mul(T(TC, j), xN)));
         } else {
             const int left_end = J < m - 2 ? J : m - 2;
             const int right_beg = (m - 1) - J < 1 ? 1 : (m - 1) - J;
-            for (int j = 1; j <= left_end; ++j) T(TD, j) = E::sub(T(TD, j), E::mul(T(TA, j), x0));
-            for (int j = right_beg; j < m - 1; ++j)
+#pragma unroll
+            for (int u = 1; u < RR; ++u)
+                if (u <= left_end) rD[u] = E::sub(rD[u], E::mul(rA[u], x0));
+            for (int j = RR > 1 ? RR : 1; j <= left_end; ++j)
+                T(TD, j) = E::sub(T(TD, j), E::mul(T(TA, j), x0));
+#pragma unroll
+            for (int u = 1; u < RR; ++u)
+                if (u >= right_beg && u < m - 1) rD[u] = E::sub(rD[u], E::mul(rC[u], xN));
+            for (int j = right_beg > RR ? right_beg : RR; j < m - 1; ++j)
                 T(TD, j) = E::sub(T(TD, j), E::mul(T(TC, j), xN));
         }
         bool finite = true;
-        for (int j = 0; j < m; ++j) finite &= isfinite(T(TD, j));
+#pragma unroll
+        for (int u = 0; u < RR; ++u)
+            if (u < m) finite &= isfinite(rD[u]);
+        for (int j = RR; j < m; ++j) finite &= isfinite(T(TD, j));
         if (valid && !finite) raise_status(args.status, ST_NONFINITE);
 
         // ------------------------------------------------ write x
-        const int full = args.use_tma ? m / SEG_BOXR : 0;  // whole chunks inside the segment
+        if (valid) {
+#pragma unroll
+            for (int u = 0; u < RR; ++u)
+                if (u < m) args.X[(size_t)(r0 + u) * ns + sys] = rD[u];
+        }
+        const int full = args.use_tma ? ms / SEG_BOXR : 0;  // whole chunks inside the tile
         if (full > 0) {
             fence_async_shared();
             __syncwarp();
             if (s == 0) {
                 for (int c = 0; c < full; ++c)
-                    tma_store_2d(&tmX, g * SEG_S, r0 + c * SEG_BOXR,
+                    tma_store_2d(&tmX, g * SEG_S, r0 + RR + c * SEG_BOXR,
                                  TD + (size_t)c * SEG_BOXR * SEG_S);
                 tma_store_commit();
             }
         }
         if (valid)
-            for (int j = full * SEG_BOXR; j < m; ++j) args.X[(size_t)(r0 + j) * ns + sys] = T(TD, j);
+            for (int j = RR + full * SEG_BOXR; j < m; ++j)
+                args.X[(size_t)(r0 + j) * ns + sys] = T(TD, j);
         if (full > 0 && s == 0) tma_store_wait_read();
     }
     if (!ok && args.use_tma) {
