@@ -105,8 +105,7 @@ int solve_impl(btdma_t h, const double* A, const double* B, const double* C, con
     a.status = h->status;
     a.mode = SEG_MODE_SOLVE;
     if (seg_smem_bytes(a.mcap, a.P, cyclic, h->method == BTDMA_PASCAL,
-                       seg_reg_rows(h->method == BTDMA_PASCAL, n_row, a.P)) >
-        (size_t)max_smem_optin())
+                       seg_reg_rows(n_row, a.P)) > (size_t)max_smem_optin())
         return fail(BTDMA_ERR_UNSUPPORTED,
                     "segment of %d rows does not fit in shared memory; use more segments",
                     a.mcap);

@@ -165,14 +165,12 @@ int launch_seg_rr(const CUtensorMap* maps, const SegArgs& a, int groups, cudaStr
     return BTDMA_OK;
 }
 
-// Filtered keeps SEG_REG leading rows of each segment in registers when every
-// segment has room for them (seg_reg_rows).
+// SEG_REG leading rows of each segment go to registers when every segment has
+// room for them (seg_reg_rows).
 template <int METHOD, bool CYCLIC>
 int launch_seg(const CUtensorMap* maps, const SegArgs& a, int groups, cudaStream_t st) {
-    if constexpr (METHOD != SEG_PASCAL) {
-        if (seg_reg_rows(false, a.n_row, a.P) == SEG_REG)
-            return launch_seg_rr<METHOD, CYCLIC, SEG_REG>(maps, a, groups, st);
-    }
+    if (seg_reg_rows(a.n_row, a.P) == SEG_REG)
+        return launch_seg_rr<METHOD, CYCLIC, SEG_REG>(maps, a, groups, st);
     return launch_seg_rr<METHOD, CYCLIC, 0>(maps, a, groups, st);
 }
 

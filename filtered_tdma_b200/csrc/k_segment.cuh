@@ -15,8 +15,9 @@
 //     holds the first SEG_REG rows of each segment (inputs, then state) in
 //     registers when every segment has SEG_REG + 2 rows or more, so its tile
 //     has three arrays of m - SEG_REG rows (5 CTAs per SM at 64 rows instead of
-//     3).  PaScaL keeps B staged: the tile's B part holds its reduced-system
-//     scratch afterwards.  A, B, C, D are read from HBM exactly once.
+//     3).  PaScaL keeps B staged (the tile's B part holds its reduced-system
+//     scratch afterwards) and the first SEG_REG rows in registers on the same
+//     condition (4 CTAs per SM).  A, B, C, D are read from HBM exactly once.
 //   * The modified Thomas sweeps run in place on the tile (the reference's
 //     per-rank steps, pascal_tdma.cpp:131-183 / filtered_tdma_kernels.hpp:35-189,
 //     with the same operation order, IEEE round-to-nearest, no FMA).
@@ -77,23 +78,24 @@ struct SegArgs {
 __host__ __device__ __forceinline__ size_t seg_rsc_bytes(int P, bool cyclic) {
     return (cyclic ? 4ull : 3ull) * 2 * P * SEG_S * sizeof(double);
 }
-__host__ __device__ __forceinline__ bool seg_rsc_in_b(int mcap, int P, bool cyclic) {
-    return seg_rsc_bytes(P, cyclic) <= (size_t)mcap * SEG_S * sizeof(double);
+// mt: tile rows (the B tile's capacity)
+__host__ __device__ __forceinline__ bool seg_rsc_in_b(int mt, int P, bool cyclic) {
+    return seg_rsc_bytes(P, cyclic) <= (size_t)mt * SEG_S * sizeof(double);
 }
 // Tile rows of a segment of mcap rows, rr of them held in registers.
 __host__ __device__ __forceinline__ int seg_tile_rows(int mcap, int rr) {
     return mcap > rr ? mcap - rr : 0;
 }
-// rr = SEG_REG for Filtered when every segment has >= SEG_REG + 2 rows, else 0.
-__host__ __device__ __forceinline__ int seg_reg_rows(bool pascal, int n_row, int P) {
-    return (!pascal && n_row / P >= SEG_REG + 2) ? SEG_REG : 0;
+// rr = SEG_REG when every segment has >= SEG_REG + 2 rows, else 0.
+__host__ __device__ __forceinline__ int seg_reg_rows(int n_row, int P) {
+    return n_row / P >= SEG_REG + 2 ? SEG_REG : 0;
 }
 __host__ __device__ __forceinline__ size_t seg_smem_bytes(int mcap, int P, bool cyclic,
                                                           bool pascal = true, int rr = 0) {
     const int mt = seg_tile_rows(mcap, rr);
     size_t tiles = (pascal ? 4ull : 3ull) * mt * SEG_S * sizeof(double);
     size_t red = 6ull * SEG_S * sizeof(double);
-    size_t rsc = pascal && !seg_rsc_in_b(mcap, P, cyclic) ? seg_rsc_bytes(P, cyclic) : 0;
+    size_t rsc = pascal && !seg_rsc_in_b(mt, P, cyclic) ? seg_rsc_bytes(P, cyclic) : 0;
     size_t bars = (size_t)(mt / SEG_BOXR + 1) * sizeof(uint64_t);
     return tiles + red + rsc + bars + 128;  // +128: alignment slack
 }
@@ -105,8 +107,8 @@ __device__ __forceinline__ void cluster_wait() {
     asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 
-// RR: leading rows of each segment held in registers (Filtered, when every
-// segment has at least RR + 2 rows, so rows m - 2 and m - 1 are tile rows).
+// RR: leading rows of each segment held in registers (when every segment has
+// at least RR + 2 rows, so rows m - 2 and m - 1 are tile rows).
 template <int METHOD, bool CYCLIC, int RR = 0>
 __global__ void __launch_bounds__(SEG_S, 5)
 seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -117,7 +119,7 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     double* base = reinterpret_cast<double*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     constexpr bool STREAM_B = METHOD != SEG_PASCAL;
-    static_assert(RR == 0 || (STREAM_B && RR >= 2), "register rows: Filtered only");
+    static_assert(RR == 0 || RR >= 2, "register rows hold rows 0 and 1");
     constexpr int RRA = RR > 0 ? RR : 1;
     const int mcap = args.mcap;
     const int mt = seg_tile_rows(mcap, RR);  // tile rows
@@ -127,7 +129,7 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     double* TD = TC + (size_t)mt * SEG_S;
     double* red = TD + (size_t)mt * SEG_S;  // [6][SEG_S]
     double* after_red = red + 6 * SEG_S;
-    const bool rsc_in_b = !STREAM_B && seg_rsc_in_b(mcap, args.P, CYCLIC);
+    const bool rsc_in_b = !STREAM_B && seg_rsc_in_b(mt, args.P, CYCLIC);
     double* rsc = rsc_in_b ? TB : after_red;  // reduced-solve scratch (PaScaL)
     const size_t rsc_extra =
         (!STREAM_B && !rsc_in_b) ? seg_rsc_bytes(args.P, CYCLIC) / sizeof(double) : 0;
@@ -502,7 +504,10 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         }
         T(TD, m - 1) = xN;
         if constexpr (METHOD == SEG_PASCAL) {
-            for (int j = 1; j < m - 1; ++j)
+#pragma unroll
+            for (int u = 1; u < RR; ++u)
+                if (u < m - 1) rD[u] = E::sub(rD[u], E::add(E::mul(rA[u], x0), E::mul(rC[u], xN)));
+            for (int j = RR > 1 ? RR : 1; j < m - 1; ++j)
                 T(TD, j) = E::sub(T(TD, j), E::add(E::mul(T(TA, j), x0), E::mul(T(TC, j), xN)));
         } else {
             const int left_end = J < m - 2 ? J : m - 2;
