@@ -48,7 +48,8 @@ namespace cg = cooperative_groups;
 constexpr int SEG_S = 32;     // systems per CTA (one warp; a 256-byte TMA box row)
 constexpr int SEG_BOXR = 16;  // rows per TMA chunk
 constexpr int SEG_MAX_P = 16; // cluster size limit (non-portable above 8)
-constexpr int SEG_REG = 16;   // Filtered: leading rows of a segment held in registers
+constexpr int SEG_REG = 16;   // leading rows of a segment held in registers
+static_assert(SEG_REG % SEG_BOXR == 0, "tile chunks start on a chunk boundary of the segment");
 
 enum SegMethod { SEG_PASCAL = 0, SEG_FILT_V1 = 1, SEG_FILT_V2 = 2 };
 
@@ -82,9 +83,11 @@ __host__ __device__ __forceinline__ size_t seg_rsc_bytes(int P, bool cyclic) {
 __host__ __device__ __forceinline__ bool seg_rsc_in_b(int mt, int P, bool cyclic) {
     return seg_rsc_bytes(P, cyclic) <= (size_t)mt * SEG_S * sizeof(double);
 }
-// Tile rows of a segment of mcap rows, rr of them held in registers.
+// Tile rows of a segment of mcap rows, rr of them held in registers: rounded up
+// to whole TMA chunks (every chunk lands as SEG_BOXR full rows).
 __host__ __device__ __forceinline__ int seg_tile_rows(int mcap, int rr) {
-    return mcap > rr ? mcap - rr : 0;
+    const int t = mcap > rr ? mcap - rr : 0;
+    return (t + SEG_BOXR - 1) / SEG_BOXR * SEG_BOXR;
 }
 // rr = SEG_REG when every segment has >= SEG_REG + 2 rows, else 0.
 __host__ __device__ __forceinline__ int seg_reg_rows(int n_row, int P) {
