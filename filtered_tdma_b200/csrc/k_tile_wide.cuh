@@ -16,13 +16,15 @@
 //       the per-row state in registers, as in k_tile.cuh.
 //   reduced system: one warp-shuffle solve per system (reduced_solve_shfl).
 //   B1  back substitution of A1's sub-segments from registers.
-//   B0  the rows of A0 are loaded again (they were read one group ago and are
+//   B0  the rows of A0 are loaded again (read earlier in the same group, mostly
 //       still in L2), the forward pass is repeated with its state in registers,
 //       and the back substitution follows.
 //
 // The ring (as in k_tile.cuh: full/empty mbarriers per stage, refills issued by
-// a rotating producer warp) carries 3 * SPG stages per group: A0, A1, B0.  HBM
-// reads stay 32 B/row (FP64) or 16 B/row (FP32); B0's reads come from L2.
+// a rotating producer warp; here with unhinted polls) carries 3 * SPG stages
+// per group: A0, A1, B0.  B0's reads come mostly from L2: DRAM traffic measured
+// 1.04x (FP32 storage) and 1.15x (FP64) the algorithmic 24 / 40 B/row at
+// 262144 x 512.
 // Every recurrence is the expression of k_tile.cuh; the two kernels agree to
 // rounding (bit for bit where the compiler contracts the same multiply-adds).
 // Needs NSEG = n_row / 16 even, 8 <= NSEG <= 32 (periodic: a power of two),
