@@ -439,7 +439,7 @@ int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, 
 // kernel; the coefficient fields of `gen` are used, the rest is filled here).
 // Returns 1 when launched, 0 when the shape is not tiled, < 0 on error.
 // GEN 1 and 3 (one matrix for every system): `tab` is device scratch of
-// n_row * 5 + (n_row / 16) * 6 doubles for the shared elimination factors.
+// gen_table_doubles(n_row) doubles for the shared elimination factors.
 template <int GEN, bool CYC = false>
 int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArgs& gen,
                  unsigned* status, cudaStream_t st, double* tab = nullptr) {
@@ -460,7 +460,7 @@ int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArg
     a.status = status;  // the layout map (xblk ...) comes with gen
     if constexpr (GEN == 1 || GEN == 3) {
         if (!tab) return fail(BTDMA_ERR_ARG, "shared-matrix sweep without a factor table");
-        tile_table_kernel<GEN><<<(pl.nseg + 127) / 128, 128, 0, st>>>(a, tab);
+        tile_table_kernel<GEN, CYC><<<(pl.nseg + 127) / 128, 128, 0, st>>>(a, tab);
         CK(cudaGetLastError());
         a.gtab = tab;
     }
@@ -472,10 +472,6 @@ int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArg
         default: rc = launch_tile_sys<16, CYC, double, double, GEN>(maps, a, st); break;
     }
     return rc == BTDMA_OK ? 1 : rc;
-}
-
-inline size_t gen_table_doubles(int n_row) {
-    return (size_t)n_row * 5 + (size_t)(n_row / 16 + 1) * 6;
 }
 
 template <bool CYCLIC>

@@ -59,6 +59,24 @@ constexpr int TILE_MAX_THREADS = 512;
 constexpr int TILE_MAX_NST = 8;       // ring stages (upper bound)
 constexpr int TILE_MAX_NST_CONST = 16;  // ring stages of D-only (constant-coefficient) rings
 
+// Shared-matrix reduced systems of up to 32 sub-segments: per lane p of the
+// shuffle group, the coefficients of every step of reduced_solve_shfl that do
+// not depend on the right-hand side (TILE_RED_LANE doubles, lane-major):
+//   [0] 1/pivot of the first cyclic-reduction step, [1] l1, [2] u1 (0 where
+//   the next sub-segment does not exist), [3] l0, [4] u0, then per PCR level v
+//   (distance 2^v, at most 5 levels) [5 + 3v] l, [6 + 3v] u (0 where that
+//   neighbour does not exist), [7 + 3v] 1/pivot.
+constexpr int TILE_RED_LEVELS = 5;
+constexpr int TILE_RED_LANE = 5 + 3 * TILE_RED_LEVELS;
+// Offset of the lane table in the factor table of an n_row-row matrix, and
+// the whole table's size (rows, sub-segments, lanes).
+__host__ __device__ constexpr size_t tile_red_offset(int n_row) {
+    return (size_t)n_row * 5 + (size_t)(n_row / 16 + 1) * 6;
+}
+__host__ __device__ constexpr size_t gen_table_doubles(int n_row) {
+    return tile_red_offset(n_row) + 32 * (size_t)TILE_RED_LANE;
+}
+
 struct TileArgs {
     double* X;
     int n_sys, n_row;
@@ -102,8 +120,9 @@ struct TileArgs {
     // GEN 1 and 3: every system of the batch has the same matrix, so the
     // elimination of each sub-segment is computed once (tile_table_kernel) into
     // gtab: per row [inv pivot, a * inv, pi, alpha, gamma] (n_row x 5), then
-    // per sub-segment [r, r c0, l0, u0, l1, u1] (nseg x 6); the solve runs the
-    // right-hand-side recurrences only
+    // per sub-segment [r, r c0, l0, u0, l1, u1] (nseg x 6), then (up to 32
+    // sub-segments) the reduced system's lane table at tile_red_offset(n_row);
+    // the solve runs the right-hand-side recurrences only
     const double* gtab;
     int gpin;
     unsigned* status;
@@ -127,11 +146,17 @@ __host__ __device__ __forceinline__ int tile_lanes(int nseg) {
 // Shared memory (doubles unless noted), T = SYS * NSC threads, SUB = SYS / CL,
 // RP = SYS + 1 (padded pitch of the exchange buffers):
 //   ring  NST * 4 * RPS * T       TMA stages (A, B, C, D; RPS rows per sub-segment)
-//   red   6 * NSC * RP            this CTA's reduced rows (l0,u0,r0 | l1,u1,r1)
+//   red   6 * NSC * RP            this CTA's reduced rows (l0,u0,r0 | l1,u1,r1);
+//                                 2 * NSC * RP (r0 | r1) for a shared matrix of
+//                                 NSEG <= 32, whose l, u come from the lane table
 //   xr    2 * NSC * RP            x_first / x_last of this CTA's sub-segments
 //   pcr   6 * (NSEG + 2) * SUB    PCR buffers, only when NSEG > 32
+//   tab   tile_tab_doubles(NSC)   shared matrix: this CTA's factor table
+//   lane  32 * TILE_RED_LANE      shared matrix, NSEG <= 32: the lane table
 //   bars  2 * NST mbarriers
-__host__ __device__ __forceinline__ size_t tile_fixed_doubles(int sys, int nsc, int nseg, int sub) {
+__host__ __device__ __forceinline__ size_t tile_fixed_doubles(int sys, int nsc, int nseg, int sub,
+                                                              bool shared_tab = false) {
+    if (shared_tab && nseg <= 32) return 4ull * nsc * (sys + 1) + 32ull * TILE_RED_LANE;
     size_t f = 8ull * nsc * (sys + 1);
     if (nseg > 32) f += 6ull * (nseg + 2) * sub;
     return f;
@@ -151,7 +176,7 @@ __host__ __device__ __forceinline__ size_t tile_smem_bytes(int sys, int nsc, int
                                                            bool shared_tab = false) {
     return tile_ring_bytes(sys, nsc, nst, elem, na) +
            (shared_tab ? tile_tab_doubles(nsc) * sizeof(double) : 0) +
-           tile_fixed_doubles(sys, nsc, nseg, sub) * sizeof(double) +
+           tile_fixed_doubles(sys, nsc, nseg, sub, shared_tab) * sizeof(double) +
            2ull * nst * sizeof(uint64_t) + 128;
 }
 
@@ -203,16 +228,19 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     const int sub = SYS / cl;    // systems whose reduced system this CTA solves
     const int W = tile_lanes(nseg);
     const bool shuffled = W <= 32;
+    const bool rhs_red = SH && shuffled;  // reduced matrix from the lane table
     const int fstride = nsc * RP;  // field stride of red / xr
 
     TIN* ring = reinterpret_cast<TIN*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     double* red = reinterpret_cast<double*>(ring + (size_t)nst * NA * RPS * T);
-    double* xr = red + 6 * fstride;
+    double* xr = red + (rhs_red ? 2 : 6) * fstride;
     double* pcr = xr + 2 * fstride;  // only when !shuffled
     const int gs = nseg + 2;
     double* tabs = pcr + (shuffled ? 0 : 6 * gs * sub);  // SH: this CTA's factor table
-    uint64_t* full = reinterpret_cast<uint64_t*>(tabs + (SH ? tile_tab_doubles(nsc) : 0));
+    double* lanes = tabs + (SH ? tile_tab_doubles(nsc) : 0);  // rhs_red: lane table [k][p]
+    uint64_t* full =
+        reinterpret_cast<uint64_t*>(lanes + (rhs_red ? 32 * TILE_RED_LANE : 0));
     uint64_t* empty = full + nst;
 
     const int tid = threadIdx.x;
@@ -240,6 +268,11 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         for (int i = threadIdx.x; i < nsc * M * 5; i += blockDim.x) tabs[i] = g0[i];
         const double* g1 = args.gtab + (size_t)args.n_row * 5 + (size_t)c0 * 6;
         for (int i = threadIdx.x; i < nsc * 6; i += blockDim.x) tabs[nsc * M * 5 + i] = g1[i];
+        if (rhs_red) {  // lane-major in global memory, field-major here (no bank conflicts)
+            const double* g2 = args.gtab + tile_red_offset(args.n_row);
+            for (int i = threadIdx.x; i < 32 * TILE_RED_LANE; i += blockDim.x)
+                lanes[(i % TILE_RED_LANE) * 32 + i / TILE_RED_LANE] = g2[i];
+        }
     }
     if (!shuffled && tid < sub) {  // zero guard rows of the PCR buffers
         for (int f = 0; f < 6; ++f) {
@@ -410,12 +443,17 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         if constexpr (SH) {
             const double* sb = tabs + nsc * M * 5 + ql * 6;
             double* w = red + ql * RP + s;
-            w[0 * fstride] = sb[2];
-            w[1 * fstride] = sb[3];
-            w[2 * fstride] = sb[0] * (double)db0 - sb[1] * (double)sd;
-            w[3 * fstride] = sb[4];
-            w[4 * fstride] = sb[5];
-            w[5 * fstride] = (double)de[M - 1];
+            if (rhs_red) {  // r0 | r1 only
+                w[0] = sb[0] * (double)db0 - sb[1] * (double)sd;
+                w[fstride] = (double)de[M - 1];
+            } else {
+                w[2 * fstride] = sb[0] * (double)db0 - sb[1] * (double)sd;
+                w[5 * fstride] = (double)de[M - 1];
+                w[0 * fstride] = sb[2];
+                w[1 * fstride] = sb[3];
+                w[3 * fstride] = sb[4];
+                w[4 * fstride] = sb[5];
+            }
         } else {
             const TC pi_last = -ga[M - 2] * pi;
             const TC r0 = rcp_tc(TC(1) - cb0 * sa);
@@ -445,15 +483,20 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                     const int owner = p / nsc;
                     const double* src = red + (p % nsc) * RP + c * sub + sp;
                     if (cl > 1 && owner != c) src = cg::this_cluster().map_shared_rank(src, owner);
-                    l0 = src[0 * fstride];
-                    u0 = src[1 * fstride];
-                    r0 = src[2 * fstride];
-                    l1 = src[3 * fstride];
-                    u1 = src[4 * fstride];
-                    r1 = src[5 * fstride];
+                    r0 = src[(SH ? 0 : 2) * fstride];
+                    r1 = src[(SH ? 1 : 5) * fstride];
+                    if constexpr (!SH) {
+                        l0 = src[0 * fstride];
+                        u0 = src[1 * fstride];
+                        l1 = src[3 * fstride];
+                        u1 = src[4 * fstride];
+                    }
                 }
                 double xf, xl;
-                reduced_solve_shfl<CYCLIC>(l0, u0, r0, l1, u1, r1, p, nseg, W, act, xf, xl);
+                if constexpr (SH)
+                    reduced_solve_rhs<CYCLIC>(r0, r1, p, nseg, W, lanes + p, 32, xf, xl);
+                else
+                    reduced_solve_shfl<CYCLIC>(l0, u0, r0, l1, u1, r1, p, nseg, W, act, xf, xl);
                 if (act) {
                     const int owner = p / nsc;
                     double* dst = xr + (p % nsc) * RP + c * sub + sp;
@@ -608,60 +651,76 @@ __device__ __forceinline__ void tile_gen_row(const TileArgs& args, int q, int k,
 
 // The elimination of every sub-segment of the shared matrix (the steps of the
 // tiled kernel's forward pass and reduced-row formation without the right-hand
-// side): one thread per sub-segment.
-template <int GEN>
+// side): one thread per sub-segment; then, for up to 32 sub-segments, warp 0
+// runs the matrix steps of the reduced system into the lane table.
+template <int GEN, bool CYCLIC>
 __global__ void tile_table_kernel(const TileArgs args, double* __restrict__ tab) {
     constexpr int M = TILE_MT;
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= args.nseg) return;
-    double* sub = tab + (size_t)args.n_row * 5 + (size_t)q * 6;
-    double ab0 = 0, cb0 = 0, sa = 0, pi = 1.0, alp = 0, gap = 0, gm2 = 0;
-    for (int k = 0; k < M; ++k) {
-        double a, b, c;
-        tile_gen_row<GEN>(args, q, k, a, b, c);
-        double* tr = tab + (size_t)(q * M + k) * 5;
-        if (k == 0) {
-            const double ib = rcp_nr(b);
-            ab0 = a * ib;
-            cb0 = c * ib;
-            tr[0] = ib;
-            tr[1] = tr[2] = tr[3] = tr[4] = 0.0;
-            continue;
-        }
-        double al, ga, inv;
-        if (k == 1) {
-            inv = rcp_nr(b);
-            al = a * inv;
-            ga = c * inv;
-            sa = al;
-            tr[1] = 0.0;
-            tr[2] = 1.0;
-        } else {
-            inv = rcp_nr(b - a * gap);
-            ga = c * inv;
-            al = -a * alp * inv;
-            tr[1] = a * inv;
-            if (k <= M - 2) {
-                pi = -gap * pi;
-                sa += pi * al;
+    if (q < args.nseg) {
+        double* sub = tab + (size_t)args.n_row * 5 + (size_t)q * 6;
+        double ab0 = 0, cb0 = 0, sa = 0, pi = 1.0, alp = 0, gap = 0, gm2 = 0;
+        for (int k = 0; k < M; ++k) {
+            double a, b, c;
+            tile_gen_row<GEN>(args, q, k, a, b, c);
+            double* tr = tab + (size_t)(q * M + k) * 5;
+            if (k == 0) {
+                const double ib = rcp_nr(b);
+                ab0 = a * ib;
+                cb0 = c * ib;
+                tr[0] = ib;
+                tr[1] = tr[2] = tr[3] = tr[4] = 0.0;
+                continue;
             }
-            tr[2] = pi;
+            double al, ga, inv;
+            if (k == 1) {
+                inv = rcp_nr(b);
+                al = a * inv;
+                ga = c * inv;
+                sa = al;
+                tr[1] = 0.0;
+                tr[2] = 1.0;
+            } else {
+                inv = rcp_nr(b - a * gap);
+                ga = c * inv;
+                al = -a * alp * inv;
+                tr[1] = a * inv;
+                if (k <= M - 2) {
+                    pi = -gap * pi;
+                    sa += pi * al;
+                }
+                tr[2] = pi;
+            }
+            tr[0] = inv;
+            tr[3] = al;
+            tr[4] = ga;
+            if (k == M - 2) gm2 = ga;
+            alp = al;
+            gap = ga;
         }
-        tr[0] = inv;
-        tr[3] = al;
-        tr[4] = ga;
-        if (k == M - 2) gm2 = ga;
-        alp = al;
-        gap = ga;
+        const double pi_last = -gm2 * pi;
+        const double rr = rcp_nr(1.0 - cb0 * sa);
+        sub[0] = rr;
+        sub[1] = rr * cb0;
+        sub[2] = rr * ab0;
+        sub[3] = rr * cb0 * pi_last;
+        sub[4] = alp;
+        sub[5] = gap;
     }
-    const double pi_last = -gm2 * pi;
-    const double rr = rcp_nr(1.0 - cb0 * sa);
-    sub[0] = rr;
-    sub[1] = rr * cb0;
-    sub[2] = rr * ab0;
-    sub[3] = rr * cb0 * pi_last;
-    sub[4] = alp;
-    sub[5] = gap;
+    const int nseg = args.nseg;
+    if (nseg > 32 || blockIdx.x != 0) return;
+    __syncthreads();  // one CTA holds every sub-segment when nseg <= 32
+    if (threadIdx.x >= 32) return;
+    const int W = tile_lanes(nseg);
+    const int p = threadIdx.x & (W - 1);
+    const bool act = p < nseg;
+    const double* sb = tab + (size_t)args.n_row * 5 + (size_t)p * 6;
+    const double l0 = act ? sb[2] : 0.0, u0 = act ? sb[3] : 0.0;
+    const double l1 = act ? sb[4] : 0.0, u1 = act ? sb[5] : 0.0;
+    double* lt = (int)threadIdx.x < W
+                     ? tab + tile_red_offset(args.n_row) + (size_t)p * TILE_RED_LANE
+                     : nullptr;
+    reduced_lane_table<CYCLIC>(l0, u0, l1, u1, p, nseg, W, act, lt);
 }
 
 }  // namespace btdma
