@@ -175,14 +175,15 @@ int launch_seg(const CUtensorMap* maps, const SegArgs& a, int groups, cudaStream
 }
 
 // 3-D view [nseg][TILE_MT][n_sys] of an [n_row x n_sys] FP64 array; boxes of
-// tile_rps(elem) rows of `nsc` consecutive sub-segments for `sys` systems.
+// tile_rps(elem, na) rows of `nsc` consecutive sub-segments for `sys` systems
+// (na: arrays of the ring the boxes go to).
 inline bool make_tile_map(CUtensorMap* map, const void* ptr, int n_sys, int nseg, int sys,
-                          int nsc, int elem = 8) {
+                          int nsc, int elem = 8, int na = 4) {
     auto fn = encode_fn();
     if (!fn) return false;
     cuuint64_t dims[3] = {(cuuint64_t)n_sys, (cuuint64_t)TILE_MT, (cuuint64_t)nseg};
     cuuint64_t strides[2] = {(cuuint64_t)n_sys * elem, (cuuint64_t)n_sys * TILE_MT * elem};
-    cuuint32_t box[3] = {(cuuint32_t)sys, (cuuint32_t)tile_rps(elem), (cuuint32_t)nsc};
+    cuuint32_t box[3] = {(cuuint32_t)sys, (cuuint32_t)tile_rps(elem, na), (cuuint32_t)nsc};
     cuuint32_t estr[3] = {1, 1, 1};
     const CUtensorMapDataType dt =
         elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
@@ -447,7 +448,7 @@ int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArg
     if (pl.sys == 0 || !tma_ok_elem(D, n_sys, 8)) return 0;
     const int nsc = pl.nseg / pl.cl;
     CUtensorMap maps[4];
-    if (!make_tile_map(&maps[3], D, n_sys, pl.nseg, pl.sys, nsc, 8)) return 0;
+    if (!make_tile_map(&maps[3], D, n_sys, pl.nseg, pl.sys, nsc, 8, 1)) return 0;
     maps[0] = maps[1] = maps[2] = maps[3];  // not read in this mode
     TileArgs a = gen;
     a.X = X;

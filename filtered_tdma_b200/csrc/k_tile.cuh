@@ -7,7 +7,8 @@
 // (CL = 1 for short systems), NSC = NSEG / CL sub-segments per CTA, SYS * NSC
 // <= 512 threads.  Persistent clusters walk over the groups:
 //
-//   1. Forward pass (RPS = 2 FP64 or 4 FP32 rows of every local sub-segment per step).
+//   1. Forward pass (RPS = 2 FP64 or 4 FP32 rows of every local sub-segment per
+//      step; 4 FP64 rows when only D is read).
 //      Rows k, k+1 of the CTA's NSC sub-segments of SYS systems arrive in one TMA
 //      box of a 3-D view [NSEG][TILE_MT][n_sys] (SYS * 8 bytes wide) through an
 //      NST-stage shared-memory ring.  Each stage has a "full" mbarrier (TMA
@@ -53,8 +54,13 @@ namespace btdma {
 
 constexpr int TILE_MT = 16;           // rows per sub-segment (per thread)
 // Rows per ring stage: 16 bytes of each array per sub-segment and system, i.e.
-// 2 FP64 rows or 4 FP32 rows, so a stage has the same size for both storages.
-__host__ __device__ constexpr int tile_rps(int elem) { return 16 / elem; }
+// 2 FP64 rows or 4 FP32 rows, so a stage has the same size for both storages;
+// 32 bytes (4 FP64 rows) for the D-only ring (na == 1) of the generated-
+// coefficient modes, whose per-stage bookkeeping would otherwise cost as much
+// as the rows' arithmetic.
+__host__ __device__ constexpr int tile_rps(int elem, int na = 4) {
+    return (na == 1 ? 32 : 16) / elem;
+}
 constexpr int TILE_MAX_THREADS = 512;
 constexpr int TILE_MAX_NST = 8;       // ring stages (upper bound)
 constexpr int TILE_MAX_NST_CONST = 16;  // ring stages of D-only (constant-coefficient) rings
@@ -145,7 +151,7 @@ __host__ __device__ __forceinline__ int tile_lanes(int nseg) {
 
 // Shared memory (doubles unless noted), T = SYS * NSC threads, SUB = SYS / CL,
 // RP = SYS + 1 (padded pitch of the exchange buffers):
-//   ring  NST * 4 * RPS * T       TMA stages (A, B, C, D; RPS rows per sub-segment)
+//   ring  NST * NA * RPS * T      TMA stages (A, B, C, D or D only; RPS rows per sub-segment)
 //   red   6 * NSC * RP            this CTA's reduced rows (l0,u0,r0 | l1,u1,r1);
 //                                 2 * NSC * RP (r0 | r1) for a shared matrix of
 //                                 NSEG <= 32, whose l, u come from the lane table
@@ -164,7 +170,7 @@ __host__ __device__ __forceinline__ size_t tile_fixed_doubles(int sys, int nsc, 
 // na: arrays per ring stage (4: A, B, C, D; 1: D only).
 __host__ __device__ __forceinline__ size_t tile_ring_bytes(int sys, int nsc, int nst, int elem,
                                                            int na = 4) {
-    return (size_t)nst * na * tile_rps(elem) * sys * nsc * elem;
+    return (size_t)nst * na * tile_rps(elem, na) * sys * nsc * elem;
 }
 // Shared-matrix table slice of one CTA (its nsc sub-segments): per row 5 and
 // per sub-segment 6 doubles.
@@ -215,11 +221,11 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                 const TileArgs args) {
     namespace cg = cooperative_groups;
     constexpr int M = TILE_MT;
-    constexpr int RPS = tile_rps((int)sizeof(TIN));  // rows per ring stage
-    constexpr int SPG = M / RPS;                      // stages per group
     constexpr bool CONSTC = GEN != 0;                 // coefficients generated, D only
     constexpr bool SH = GEN == 1 || GEN == 3;         // one matrix for all systems (gtab)
     constexpr int NA = CONSTC ? 1 : 4;                // arrays per ring stage
+    constexpr int RPS = tile_rps((int)sizeof(TIN), NA);  // rows per ring stage
+    constexpr int SPG = M / RPS;                         // stages per group
     constexpr int RP = SYS + 1;  // padded pitch of red / xr rows
     extern __shared__ unsigned char smem_raw[];
     const int nseg = args.nseg, cl = args.cl, nst = args.nst;
