@@ -221,7 +221,7 @@ inline int max_smem_per_sm() {
 }
 
 // na: arrays per ring stage (4, or 1 for the constant-coefficient D-only ring).
-// sh: shared-matrix sweep (factor table in shared memory, two CTAs per SM).
+// sh: shared-matrix sweep (factor table and lane table in shared memory).
 inline TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4, bool sh = false) {
     TilePlan pl;
     if (n_row % TILE_MT != 0) return pl;
@@ -250,10 +250,7 @@ inline TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4, bool
         if (cl == 0) return pl;
     }
     int nst = na == 4 ? TILE_MAX_NST : TILE_MAX_NST_CONST;
-    // two CTAs per SM for shared-matrix sweeps: half an SM's shared memory each
-    // (less 1 KB the runtime reserves per CTA)
-    const size_t cap =
-        sh && cl == 1 ? (size_t)max_smem_per_sm() / 2 - 1024 : (size_t)max_smem_optin();
+    const size_t cap = (size_t)max_smem_optin();
     while (nst >= 3 &&
            tile_smem_bytes(sys, nseg / cl, nseg, sys / cl, nst, elem, na, sh) > cap)
         --nst;
@@ -290,12 +287,6 @@ int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st)
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int clusters = num_sms();
-    if (SHT && a.cl == 1) {  // built for two CTAs per SM
-        int nb = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, threads,
-                                                         cfg.dynamicSmemBytes));
-        clusters = num_sms() * std::max(1, nb);
-    }
     if (a.cl > 1) {
         cfg.gridDim = dim3(a.cl * num_sms(), 1, 1);
         int nc = 0;

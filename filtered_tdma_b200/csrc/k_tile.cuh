@@ -212,10 +212,12 @@ __device__ __forceinline__ void tile_cluster_sync(int cl) {
 // the local sweeps — double (FP32 storage is widened exactly on load), or float
 // (the FP32 inner solve of iterative refinement).  The reduced system, the back
 // substitution and x are always FP64.
-// Shared-matrix instantiations (GEN 1, 3) hold no per-row matrix state, so they
-// are built for two CTAs per SM (64 registers a thread).
+// One CTA per SM in every mode.  (The shared-matrix instantiations, GEN 1 and
+// 3, were measured at two CTAs per SM as well: at 64 registers a thread they
+// spill and run 1.5x the instructions, which costs more than the second CTA
+// hides.)
 template <int SYS, bool CYCLIC, typename TIN = double, typename TC = double, int GEN = 0>
-__global__ void __launch_bounds__(TILE_MAX_THREADS, (GEN == 1 || GEN == 3) ? 2 : 1)
+__global__ void __launch_bounds__(TILE_MAX_THREADS, 1)
 tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 const __grid_constant__ CUtensorMap tmC, const __grid_constant__ CUtensorMap tmD,
                 const TileArgs args) {
