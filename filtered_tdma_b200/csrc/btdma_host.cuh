@@ -228,7 +228,15 @@ inline TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4, bool
     const int nseg = n_row / TILE_MT;
     if (cyclic && (nseg & (nseg - 1)) != 0) return pl;  // periodic PCR needs 2^k rows
     int sys, cl = 0;
-    if (nseg <= 4) {
+    if (sh && nseg <= 16) {
+        // Shared-matrix sweeps of up to 16 sub-segments: CTAs of at most
+        // TILE_SH_THREADS threads, two or more per SM, so that one CTA's reduced
+        // solve overlaps another's sweeps.  (Longer systems keep one CTA of up
+        // to 512 threads: splitting them over a 2-CTA cluster was measured
+        // slower, the cluster barriers waiting for the partner CTA.)
+        sys = std::min(128, TILE_SH_THREADS / tile_lanes(nseg));
+        cl = 1;
+    } else if (nseg <= 4) {
         sys = 128;
         cl = 1;
     } else if (nseg <= 8) {
@@ -250,7 +258,11 @@ inline TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4, bool
         if (cl == 0) return pl;
     }
     int nst = na == 4 ? TILE_MAX_NST : TILE_MAX_NST_CONST;
-    const size_t cap = (size_t)max_smem_optin();
+    size_t cap = (size_t)max_smem_optin();
+    if (sh) {  // an equal share of the SM per resident CTA (128 registers a thread)
+        const int per_sm = std::max(1, 65536 / (sys * (nseg / cl) * 128));
+        cap = std::min(cap, (size_t)max_smem_per_sm() / per_sm - 1024);
+    }
     while (nst >= 3 &&
            tile_smem_bytes(sys, nseg / cl, nseg, sys / cl, nst, elem, na, sh) > cap)
         --nst;
@@ -287,6 +299,12 @@ int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st)
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int clusters = num_sms();
+    if (a.cl == 1) {  // as many CTAs as fit on an SM (several for shared-matrix sweeps)
+        int nb = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, threads,
+                                                         cfg.dynamicSmemBytes));
+        clusters = num_sms() * std::max(1, nb);
+    }
     if (a.cl > 1) {
         cfg.gridDim = dim3(a.cl * num_sms(), 1, 1);
         int nc = 0;

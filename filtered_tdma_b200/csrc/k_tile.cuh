@@ -62,6 +62,7 @@ __host__ __device__ constexpr int tile_rps(int elem, int na = 4) {
     return (na == 1 ? 32 : 16) / elem;
 }
 constexpr int TILE_MAX_THREADS = 512;
+constexpr int TILE_SH_THREADS = 256;  // CTA size limit of the shared-matrix sweeps
 constexpr int TILE_MAX_NST = 8;       // ring stages (upper bound)
 constexpr int TILE_MAX_NST_CONST = 16;  // ring stages of D-only (constant-coefficient) rings
 
