@@ -23,6 +23,7 @@ TILE_AUTO, TILE_NARROW, TILE_WIDE = 0, 1, 2
 # every exported symbol of include/btdma.h
 EXPORTS = (
     "btdma_create", "btdma_destroy", "btdma_solve", "btdma_solve_cyclic", "btdma_solve_out",
+    "btdma_solve_host",
     "btdma_set_eps_constant", "btdma_set_rho", "btdma_set_rho_all", "btdma_last_J",
     "btdma_status", "btdma_set_method", "btdma_segments", "btdma_last_error",
     "btdma_solve_noalloc", "btdma_solve_f32", "btdma_set_refine", "btdma_last_stats",
@@ -82,6 +83,7 @@ def lib():
         L.btdma_solve.argtypes = [vp, vp, vp, vp, vp, i, i, vp]
         L.btdma_solve_cyclic.argtypes = [vp, vp, vp, vp, vp, i, i, vp]
         L.btdma_solve_out.argtypes = [vp, vp, vp, vp, vp, vp, i, i, i, vp]
+        L.btdma_solve_host.argtypes = [vp, vp, vp, vp, vp, vp, i, i, i, vp]
         L.btdma_set_eps_constant.argtypes = [vp, d]
         L.btdma_set_rho.argtypes = [vp, vp, vp, vp, i, i, vp]
         L.btdma_set_rho_all.argtypes = [vp, vp, vp, vp, i, i, vp]

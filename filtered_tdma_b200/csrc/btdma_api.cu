@@ -220,7 +220,92 @@ int btdma_destroy(btdma_t h) {
         if (h->rag_join[i]) cudaEventDestroy(h->rag_join[i]);
     }
     if (h->rag_fork) cudaEventDestroy(h->rag_fork);
+    if (auto* p = h->hp) {
+        cudaFree(p->buf);
+        for (auto s : p->s)
+            if (s) cudaStreamDestroy(s);
+        for (auto e : {p->start, p->done, p->in[0], p->in[1], p->solved[0], p->solved[1],
+                       p->out[0], p->out[1]})
+            if (e) cudaEventDestroy(e);
+        delete p;
+    }
     delete h;
+    return BTDMA_OK;
+}
+
+// Host-buffer solve: the batch passes through the GPU in chunks of systems,
+// each gathered from the [n_row][n_sys] host arrays by a 2-D copy into a
+// contiguous [n_row][chunk] device buffer; with two buffer sets, the copy-in
+// of chunk i + 1 (one copy engine), the solve of chunk i and the copy-out of
+// chunk i - 1 (the other copy engine) overlap.  Systems are independent, so a
+// PaScaL chunk solves exactly as in a whole-batch call; a Filtered batch goes
+// through as one chunk, its truncation depth depending on the whole batch's
+// right-hand sides.
+int btdma_solve_host(btdma_t h, const double* hA, const double* hB, const double* hC,
+                     const double* hD, double* hX, int n_sys, int n_row, int cyclic,
+                     cudaStream_t stream) {
+    int rc = check_sizes(h, n_sys, n_row);
+    if (rc) return rc;
+    if (!hA || !hB || !hC || !hD || !hX) return fail(BTDMA_ERR_ARG, "null array");
+    if (h->precision != BTDMA_FP64)
+        return fail(BTDMA_ERR_UNSUPPORTED, "host-buffer solves need an FP64 handle");
+    constexpr int CHUNKS = 8, MIN_CHUNK = 4096;
+    int chunk = n_sys;
+    if (h->method == BTDMA_PASCAL) {
+        chunk = ((n_sys + CHUNKS - 1) / CHUNKS + 31) / 32 * 32;
+        chunk = std::min(std::max(chunk, MIN_CHUNK), n_sys);
+    }
+    const size_t ce = ((size_t)chunk * n_row + 31) / 32 * 32;  // 256-byte aligned arrays
+    auto* p = h->hp;
+    if (!p) {
+        p = h->hp = new btdma_handle::HostPipe;
+        for (auto& s : p->s) CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        for (auto* e : {&p->start, &p->done, &p->in[0], &p->in[1], &p->solved[0],
+                        &p->solved[1], &p->out[0], &p->out[1]})
+            CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
+    if (p->chunk_elems < ce) {
+        CK(cudaStreamSynchronize(p->s[2]));  // the previous call's copies are done
+        CK(cudaFree(p->buf));
+        p->buf = nullptr;
+        p->chunk_elems = 0;
+        CK(cudaMalloc(&p->buf, sizeof(double) * 10 * ce));
+        p->chunk_elems = ce;
+    }
+    const size_t be = p->chunk_elems;  // elements per array of a buffer set
+    const double* hin[4] = {hA, hB, hC, hD};
+    const size_t pitch = sizeof(double) * (size_t)n_sys;
+    // after the caller's earlier work on `stream`, and after this handle's
+    // previous host-buffer solve (its buffers are reused)
+    CK(cudaEventRecord(p->start, stream));
+    for (auto s : p->s) {
+        CK(cudaStreamWaitEvent(s, p->start, 0));
+        CK(cudaStreamWaitEvent(s, p->done, 0));
+    }
+    const int nch = (n_sys + chunk - 1) / chunk;
+    for (int i = 0; i < nch; ++i) {
+        const int b = i & 1, s0 = i * chunk, c = std::min(chunk, n_sys - s0);
+        double* d = p->buf + (size_t)b * 5 * be;  // A, B, C, D, X of buffer set b
+        const size_t w = sizeof(double) * (size_t)c;
+        if (i >= 2) CK(cudaStreamWaitEvent(p->s[0], p->solved[b], 0));
+        for (int k = 0; k < 4; ++k)
+            CK(cudaMemcpy2DAsync(d + k * be, w, hin[k] + s0, pitch, w, n_row,
+                                 cudaMemcpyHostToDevice, p->s[0]));
+        CK(cudaEventRecord(p->in[b], p->s[0]));
+        CK(cudaStreamWaitEvent(p->s[1], p->in[b], 0));
+        if (i >= 2) CK(cudaStreamWaitEvent(p->s[1], p->out[b], 0));
+        if ((rc = solve_impl(h, d, d + be, d + 2 * be, d + 3 * be, d + 4 * be, c, n_row,
+                             cyclic != 0, p->s[1])))
+            return rc;
+        CK(cudaEventRecord(p->solved[b], p->s[1]));
+        CK(cudaStreamWaitEvent(p->s[2], p->solved[b], 0));
+        CK(cudaMemcpy2DAsync(hX + s0, pitch, d + 4 * be, w, w, n_row, cudaMemcpyDeviceToHost,
+                             p->s[2]));
+        CK(cudaEventRecord(p->out[b], p->s[2]));
+    }
+    CK(cudaEventRecord(p->done, p->s[2]));
+    CK(cudaStreamWaitEvent(stream, p->done, 0));
+    h->last_stream = stream;
     return BTDMA_OK;
 }
 

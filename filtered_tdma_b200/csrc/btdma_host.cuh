@@ -65,6 +65,16 @@ struct btdma_handle {
     static constexpr int RAG_STREAMS = 4;
     cudaStream_t rag_side[RAG_STREAMS] = {};
     cudaEvent_t rag_fork = nullptr, rag_join[RAG_STREAMS] = {};
+    // host-buffer solves (btdma_solve_host): streams for copy-in, solve and
+    // copy-out, and two device chunk buffers of A, B, C, D, X
+    struct HostPipe {
+        cudaStream_t s[3] = {};
+        cudaEvent_t start = nullptr, done = nullptr;
+        cudaEvent_t in[2] = {}, solved[2] = {}, out[2] = {};
+        double* buf = nullptr;  // [2][5][chunk_elems]
+        size_t chunk_elems = 0;
+    };
+    HostPipe* hp = nullptr;
 };
 namespace btdma_host {
 

@@ -133,6 +133,24 @@ class Solver:
                                         ns, nr, int(cyclic), _stream(stream)))
         return X
 
+    def solve_host(self, A, B, C, D, X, n_sys=None, n_row=None, stream=None, cyclic=False):
+        """X <- x for a batch in host memory (CPU float64 tensors [n_row, n_sys],
+        pinned for overlapping copies; btdma_solve_host).  D unchanged."""
+        if torch is None:
+            raise RuntimeError("solve_host takes torch CPU tensors")
+        _check_dtype(A, B, C, D, X)
+        for x in (A, B, C, D, X):
+            if not isinstance(x, torch.Tensor) or x.is_cuda or not x.is_contiguous():
+                raise ValueError("solve_host takes contiguous CPU tensors [n_row, n_sys]")
+        ns, nr = _shape(D, n_sys, n_row)
+        for x in (A, B, C, D, X):
+            if x.numel() < ns * nr:
+                raise ValueError("host array smaller than n_row * n_sys")
+        L.check(L.lib().btdma_solve_host(self._h, A.data_ptr(), B.data_ptr(), C.data_ptr(),
+                                         D.data_ptr(), X.data_ptr(), ns, nr, int(cyclic),
+                                         _stream(stream)))
+        return X
+
     def solve_f32(self, A, B, C, D, X, n_sys=None, n_row=None, stream=None, cyclic=False):
         """FP32-stored A, B, C, D (handle precision FP32_STORE or FP32_REFINE); X <- x in FP64."""
         if torch is not None:

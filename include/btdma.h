@@ -117,6 +117,23 @@ int btdma_solve_out(btdma_t h, const double* A, const double* B, const double* C
                     const double* D, double* X, int n_sys, int n_row, int cyclic,
                     cudaStream_t stream);
 
+/* Out-of-place solve of a batch in HOST memory: hA, hB, hC, hD, hX are host
+ * arrays [n_row x n_sys] (pinned for the copies to overlap; pageable memory
+ * works, without overlap).  No reference counterpart: the reference's callers
+ * copy to the device themselves (cudaMemcpy) and call solve.  The batch moves
+ * in chunks of systems through two device buffer sets that the handle
+ * allocates on first use (5 arrays of about n_sys / 8 systems each, kept until
+ * btdma_destroy or a larger call): the copy-in of one chunk, the solve of the
+ * previous one and the copy-out of the one before overlap on the GPU's two
+ * copy engines.  PaScaL chunks solve exactly as a whole-batch btdma_solve_out;
+ * Filtered batches go through as one chunk (their truncation depth depends on
+ * the whole batch).  Stream-ordered on `stream`: hX is complete once `stream`
+ * reaches this point; successive calls on one handle are serialised.  FP64
+ * handles only. */
+int btdma_solve_host(btdma_t h, const double* hA, const double* hB, const double* hC,
+                     const double* hD, double* hX, int n_sys, int n_row, int cyclic,
+                     cudaStream_t stream);
+
 /* FP32-stored batch (A, B, C, D float [n_row x n_sys]) solved into an FP64 x:
  * X <- x, 24 bytes of HBM traffic per row instead of 40.  The reference has no
  * FP32 path; the result is compared with the FP64 solve of the same values
