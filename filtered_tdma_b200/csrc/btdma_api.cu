@@ -295,8 +295,18 @@ int btdma_solve_host(btdma_t h, const double* hA, const double* hB, const double
         CK(cudaStreamWaitEvent(p->s[1], p->in[b], 0));
         if (i >= 2) CK(cudaStreamWaitEvent(p->s[1], p->out[b], 0));
         if ((rc = solve_impl(h, d, d + be, d + 2 * be, d + 3 * be, d + 4 * be, c, n_row,
-                             cyclic != 0, p->s[1])))
+                             cyclic != 0, p->s[1]))) {
+            // copies already queued still reference the host arrays: order the
+            // caller's stream after them before reporting the error
+            const std::string msg = g_err;
+            if (cudaEventRecord(p->done, p->s[2]) == cudaSuccess &&
+                cudaStreamWaitEvent(p->s[0], p->done, 0) == cudaSuccess &&
+                cudaEventRecord(p->done, p->s[0]) == cudaSuccess)
+                cudaStreamWaitEvent(stream, p->done, 0);
+            h->last_stream = stream;
+            g_err = msg;
             return rc;
+        }
         CK(cudaEventRecord(p->solved[b], p->s[1]));
         CK(cudaStreamWaitEvent(p->s[2], p->solved[b], 0));
         CK(cudaMemcpy2DAsync(hX + s0, pitch, d + 4 * be, w, w, n_row, cudaMemcpyDeviceToHost,

@@ -97,3 +97,18 @@ def test_rejects(cuda):
         s.solve_host(*[torch.zeros((64, 2048), dtype=torch.float64) for _ in range(5)])
     with pytest.raises(ValueError):
         s.solve_host(*[x.to(cuda) for x in h])
+
+
+def test_failed_chunk_leaves_the_handle_usable(cuda):
+    # periodic systems need 3 rows: the solve of the first chunk fails after its
+    # copy-in was queued; the call reports it and the handle keeps working
+    import torch
+    n_sys, n_row = 8192, 2
+    arrays = W.row_varying(n_sys, n_row, seed=9)
+    s = Solver("pascal", n_sys, n_row, 1)
+    hA, hB, hC, hD = host_arrays(arrays)
+    hX = torch.zeros_like(hD).pin_memory()
+    with pytest.raises(L.BtdmaError):
+        s.solve_host(hA, hB, hC, hD, hX, cyclic=True)
+    torch.cuda.synchronize()
+    assert np.array_equal(host_solve(s, arrays), device_solve(s, arrays, cuda))
