@@ -490,15 +490,16 @@ int btdma_momentum_sweep(btdma_momentum_t h, int dir, int comp, const double* q,
     t.xss = 1;
     int rc;
     if (dir == 2) {
-        mom_gather_kernel<2><<<dim3((g.nx + 127) / 128, g.ny, g.nz), b1, 0, stream>>>(
+        mom_gather_kernel<2><<<dim3((g.nx + 127) / 128, (g.ny + MOM_GR - 1) / MOM_GR, g.nz), b1,
+                                 0, stream>>>(
             q, h->buf, g, comp == 2 ? 1 : 0);
         CK(cudaGetLastError());
         t.xbs = g.nx + 2;
         t.xrs = sp;
         rc = try_tile_gen<3, false>(h->buf, dst_in, n_sys, g.nz, t, h->status, stream, h->gtab);
     } else if (dir == 1) {
-        mom_gather_kernel<1><<<dim3((g.nx + 127) / 128, g.nz, g.ny), b1, 0, stream>>>(q, h->buf,
-                                                                                   g, 0);
+        mom_gather_kernel<1><<<dim3((g.nx + 127) / 128, (g.nz + MOM_GR - 1) / MOM_GR, g.ny), b1,
+                                 0, stream>>>(q, h->buf, g, 0);
         CK(cudaGetLastError());
         t.xbs = sp;
         t.xrs = g.nx + 2;

@@ -28,18 +28,35 @@ __device__ __forceinline__ size_t mom_fld(const MomGeom& g, int i, int j, int k)
 }
 
 // z and y sweeps: i fastest on both sides, no transpose.  pin: row k = 1 of
-// the z sweep is the w wall (D = 0, k_build_z :150-152).
+// the z sweep is the w wall (D = 0, k_build_z :150-152).  A block copies
+// MOM_GR consecutive rows a (z: j, y: k) of one plane b, every load of a
+// thread issued before its stores.  Grid (ceil(nx / 128), ceil(na / MOM_GR),
+// nb), block 128.
+constexpr int MOM_GR = 4;
 template <int DIR>
-__global__ void __launch_bounds__(256) mom_gather_kernel(const double* __restrict__ q,
+__global__ void __launch_bounds__(128) mom_gather_kernel(const double* __restrict__ q,
                                                          double* __restrict__ D, const MomGeom g,
                                                          int pin) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int a = blockIdx.y + 1, b = blockIdx.z + 1;  // z: (j, k); y: (k, j)
+    const int a0 = blockIdx.y * MOM_GR + 1, b = blockIdx.z + 1;  // z: (j, k); y: (k, j)
+    const int na = DIR == 2 ? g.ny : g.nz;
     if (i > g.nx) return;
-    const int j = DIR == 2 ? a : b, k = DIR == 2 ? b : a;
-    const size_t o = DIR == 2 ? ((size_t)(k - 1) * g.ny + (j - 1)) * g.nx + (i - 1)
-                              : ((size_t)(j - 1) * g.nz + (k - 1)) * g.nx + (i - 1);
-    D[o] = (DIR == 2 && pin && k == 1) ? 0.0 : q[mom_fld(g, i, j, k)];
+    double v[MOM_GR];
+#pragma unroll
+    for (int r = 0; r < MOM_GR; ++r) {
+        const int a = a0 + r;
+        const int j = DIR == 2 ? a : b, k = DIR == 2 ? b : a;
+        v[r] = a <= na ? q[mom_fld(g, i, j, k)] : 0.0;
+    }
+#pragma unroll
+    for (int r = 0; r < MOM_GR; ++r) {
+        const int a = a0 + r;
+        if (a > na) break;
+        const int j = DIR == 2 ? a : b, k = DIR == 2 ? b : a;
+        const size_t o = DIR == 2 ? ((size_t)(k - 1) * g.ny + (j - 1)) * g.nx + (i - 1)
+                                  : ((size_t)(j - 1) * g.nz + (k - 1)) * g.nx + (i - 1);
+        D[o] = (DIR == 2 && pin && k == 1) ? 0.0 : v[r];
+    }
 }
 
 constexpr int MOM_TILE = 32;

@@ -669,9 +669,12 @@ __global__ void tile_table_kernel(const TileArgs args, double* __restrict__ tab)
     if (q < args.nseg) {
         double* sub = tab + (size_t)args.n_row * 5 + (size_t)q * 6;
         double ab0 = 0, cb0 = 0, sa = 0, pi = 1.0, alp = 0, gap = 0, gm2 = 0;
+        double ra[M], rb[M], rc[M];  // every row's coefficients before the recurrence
+#pragma unroll
+        for (int k = 0; k < M; ++k) tile_gen_row<GEN>(args, q, k, ra[k], rb[k], rc[k]);
+#pragma unroll
         for (int k = 0; k < M; ++k) {
-            double a, b, c;
-            tile_gen_row<GEN>(args, q, k, a, b, c);
+            const double a = ra[k], b = rb[k], c = rc[k];
             double* tr = tab + (size_t)(q * M + k) * 5;
             if (k == 0) {
                 const double ib = rcp_nr(b);
