@@ -138,12 +138,16 @@ __global__ void __launch_bounds__(256) heat_y_to_x_kernel(const double* __restri
                                                           const HeatGeom g) {
     __shared__ double tile[HEAT_TILE][HEAT_TILE + 1];
     const int ii0 = blockIdx.x * HEAT_TILE, jj0 = blockIdx.y * HEAT_TILE, kk = blockIdx.z;
-    for (int r = threadIdx.y; r < HEAT_TILE; r += blockDim.y) {
+#pragma unroll
+    for (int u = 0; u < HEAT_TILE / 8; ++u) {  // block (HEAT_TILE, 8)
+        const int r = threadIdx.y + 8 * u;
         const int ii = ii0 + threadIdx.x, jj = jj0 + r;
         if (ii < g.ix && jj < g.iy) tile[r][threadIdx.x] = Dy[((size_t)jj * g.iz + kk) * g.ix + ii];
     }
     __syncthreads();
-    for (int r = threadIdx.y; r < HEAT_TILE; r += blockDim.y) {
+#pragma unroll
+    for (int u = 0; u < HEAT_TILE / 8; ++u) {  // block (HEAT_TILE, 8)
+        const int r = threadIdx.y + 8 * u;
         const int jj = jj0 + threadIdx.x, ii = ii0 + r;
         if (ii < g.ix && jj < g.iy) {
             double v = tile[threadIdx.x][r];
@@ -166,12 +170,16 @@ __global__ void __launch_bounds__(256) heat_update_kernel(double* __restrict__ t
                                                           const HeatGeom g) {
     __shared__ double tile[HEAT_TILE][HEAT_TILE + 1];
     const int jj0 = blockIdx.x * HEAT_TILE, ii0 = blockIdx.y * HEAT_TILE, kk = blockIdx.z;
-    for (int r = threadIdx.y; r < HEAT_TILE; r += blockDim.y) {
+#pragma unroll
+    for (int u = 0; u < HEAT_TILE / 8; ++u) {  // block (HEAT_TILE, 8)
+        const int r = threadIdx.y + 8 * u;
         const int jj = jj0 + threadIdx.x, ii = ii0 + r;
         if (ii < g.ix && jj < g.iy) tile[r][threadIdx.x] = Dx[((size_t)ii * g.iz + kk) * g.iy + jj];
     }
     __syncthreads();
-    for (int r = threadIdx.y; r < HEAT_TILE; r += blockDim.y) {
+#pragma unroll
+    for (int u = 0; u < HEAT_TILE / 8; ++u) {  // block (HEAT_TILE, 8)
+        const int r = threadIdx.y + 8 * u;
         const int ii = ii0 + threadIdx.x, jj = jj0 + r;
         if (ii < g.ix && jj < g.iy) theta[heat_full(g, ii + 1, jj + 1, kk + 1)] = tile[threadIdx.x][r];
     }

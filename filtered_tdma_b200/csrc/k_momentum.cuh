@@ -67,12 +67,16 @@ __global__ void __launch_bounds__(256) mom_gather_x_kernel(const double* __restr
                                                            const MomGeom g) {
     __shared__ double tile[MOM_TILE][MOM_TILE + 1];
     const int i0 = blockIdx.x * MOM_TILE, j0 = blockIdx.y * MOM_TILE, k = blockIdx.z + 1;
-    for (int r = threadIdx.y; r < MOM_TILE; r += blockDim.y) {
+#pragma unroll
+    for (int u = 0; u < MOM_TILE / 8; ++u) {  // block (MOM_TILE, 8)
+        const int r = threadIdx.y + 8 * u;
         const int i = i0 + threadIdx.x + 1, j = j0 + r + 1;
         if (i <= g.nx && j <= g.ny) tile[r][threadIdx.x] = q[mom_fld(g, i, j, k)];
     }
     __syncthreads();
-    for (int r = threadIdx.y; r < MOM_TILE; r += blockDim.y) {
+#pragma unroll
+    for (int u = 0; u < MOM_TILE / 8; ++u) {  // block (MOM_TILE, 8)
+        const int r = threadIdx.y + 8 * u;
         const int j = j0 + threadIdx.x + 1, i = i0 + r + 1;
         if (i <= g.nx && j <= g.ny)
             D[((size_t)(i - 1) * g.nz + (k - 1)) * g.ny + (j - 1)] = tile[threadIdx.x][r];
@@ -84,13 +88,17 @@ __global__ void __launch_bounds__(256) mom_scatter_x_kernel(const double* __rest
                                                             const MomGeom g) {
     __shared__ double tile[MOM_TILE][MOM_TILE + 1];
     const int j0 = blockIdx.x * MOM_TILE, i0 = blockIdx.y * MOM_TILE, k = blockIdx.z + 1;
-    for (int r = threadIdx.y; r < MOM_TILE; r += blockDim.y) {
+#pragma unroll
+    for (int u = 0; u < MOM_TILE / 8; ++u) {  // block (MOM_TILE, 8)
+        const int r = threadIdx.y + 8 * u;
         const int j = j0 + threadIdx.x + 1, i = i0 + r + 1;
         if (i <= g.nx && j <= g.ny)
             tile[r][threadIdx.x] = D[((size_t)(i - 1) * g.nz + (k - 1)) * g.ny + (j - 1)];
     }
     __syncthreads();
-    for (int r = threadIdx.y; r < MOM_TILE; r += blockDim.y) {
+#pragma unroll
+    for (int u = 0; u < MOM_TILE / 8; ++u) {  // block (MOM_TILE, 8)
+        const int r = threadIdx.y + 8 * u;
         const int i = i0 + threadIdx.x + 1, j = j0 + r + 1;
         if (i <= g.nx && j <= g.ny) q[mom_fld(g, i, j, k)] = tile[threadIdx.x][r];
     }
