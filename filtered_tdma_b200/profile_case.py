@@ -28,10 +28,13 @@ def main():
     ap.add_argument("--cyclic", action="store_true")
     ap.add_argument("--storage", choices=["f64", "f32"], default="f64",
                     help="f32: A, B, C, D stored in FP32 (FP32_STORE handle)")
-    ap.add_argument("--case", choices=["batch", "ragged", "heat", "poisson"], default="batch",
+    ap.add_argument("--case", choices=["batch", "ragged", "heat", "poisson", "momentum"],
+                    default="batch",
                     help="batch: uniform [n_row x n_sys] solve; ragged: 10000 CSR systems "
                          "(n log-uniform 16..4096, autotuned); heat: fused ADI steps on "
-                         "--heat-grid; poisson: channel wall-normal solve 128 x 65 x 192")
+                         "--heat-grid; poisson: channel wall-normal solve 128 x 65 x 192; "
+                         "momentum: channel momentum ADI (z, y, x sweeps) of one velocity "
+                         "component on 256^3")
     ap.add_argument("--heat-grid", default="256,384,512")
     ap.add_argument("--no-tune", action="store_true", help="ragged: keep the default plan")
     ap.add_argument("--tile-shape", choices=["auto", "narrow", "wide"], default="auto",
@@ -116,6 +119,14 @@ def other_case(args):
         th = h.field(dev)
         ms = timed(lambda: h.step(th, 1), args.reps)
         print("heat step", ["%.4f ms" % t for t in ms], ix * iy * iz, "cells")
+    elif args.case == "momentum":
+        from filtered_tdma_b200.momentum import ChannelMomentum
+        mm = ChannelMomentum(256, 256, 256, gamma3=1.5)
+        rhs = torch.rand(mm.shape, dtype=torch.float64, device=dev)
+        q = torch.zeros_like(rhs)
+        c_visc = 0.5 * (1.0 / 180.0) * 1e-3  # as bench.py
+        ms = timed(lambda: mm.adi(0, rhs, q, c_visc), args.reps)
+        print("momentum component", ["%.4f ms" % t for t in ms], "status", mm.status())
     else:
         from filtered_tdma_b200.poisson import ChannelPoisson
         cp = ChannelPoisson(128, 128, 192, gamma=2.0)
