@@ -21,7 +21,8 @@ struct btdma_heat {
     double* buf1 = nullptr;  // Y sweep layout
     double* err = nullptr;   // L2 accumulator
     double* scratch = nullptr;  // full grid, the warm-up step before graph capture
-    double* tab = nullptr;      // shared elimination factors of one sweep
+    double* tab = nullptr;      // factor tables of the Z, Y, X sweeps, tab_stride apart
+    size_t tab_stride = 0;      // (built once at create: the matrices are fixed)
     unsigned* status = nullptr;
     cudaStream_t cap = nullptr;  // private stream the step graph is captured on
     cudaGraph_t graph = nullptr;
@@ -43,8 +44,8 @@ int heat_enqueue(btdma_heat_t h, double* theta, cudaStream_t st, cudaEvent_t* ev
     };
     // constant-coefficient sweep of D into X, stored through the layout map
     // (xblk, xbs, xss, xrs) of the tiled solve (xblk = 0: X in D's layout)
-    auto sweep = [&](const double* D, double* X, int n_sys, int n_row, double base, int xblk,
-                     int xbs, int xss, int xrs, const char* name) {
+    auto sweep = [&](int dir, const double* D, double* X, int n_sys, int n_row, double base,
+                     int xblk, int xbs, int xss, int xrs, const char* name) {
         TileArgs ga = {};
         ga.cs = base;
         ga.cbound = 1;
@@ -52,7 +53,8 @@ int heat_enqueue(btdma_heat_t h, double* theta, cudaStream_t st, cudaEvent_t* ev
         ga.xbs = xbs;
         ga.xss = xss;
         ga.xrs = xrs;
-        const int rc = try_tile_gen<1>(D, X, n_sys, n_row, ga, h->status, st, h->tab);
+        const int rc = try_tile_gen<1>(D, X, n_sys, n_row, ga, h->status, st,
+                                       h->tab + dir * h->tab_stride, true);
         return rc == 1 ? BTDMA_OK
                        : (rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "%s sweep not tileable", name));
     };
@@ -65,18 +67,19 @@ int heat_enqueue(btdma_heat_t h, double* theta, cudaStream_t st, cudaEvent_t* ev
     CK(cudaGetLastError());
     mark(1);
     // Z sweep: system jj * ix + ii, row kk; solution to [jj][kk][ii]
-    if ((rc = sweep(h->buf0, h->buf1, g.ix * g.iy, g.iz, g.bz, g.ix, g.iz * g.ix, 1, g.ix, "Z")))
+    if ((rc = sweep(0, h->buf0, h->buf1, g.ix * g.iy, g.iz, g.bz, g.ix, g.iz * g.ix, 1, g.ix,
+                    "Z")))
         return rc;
     mark(2);
     heat_y_fold_kernel<<<dim3((g.ix + 127) / 128, 2, g.iz), b1, 0, st>>>(theta, h->buf1, g);
     CK(cudaGetLastError());
     mark(3);
-    if ((rc = sweep(h->buf1, h->buf1, g.ix * g.iz, g.iy, g.by, 0, 0, 0, 0, "Y"))) return rc;
+    if ((rc = sweep(1, h->buf1, h->buf1, g.ix * g.iz, g.iy, g.by, 0, 0, 0, 0, "Y"))) return rc;
     mark(4);
     heat_y_to_x_kernel<<<dim3(tx, ty, g.iz), bt, 0, st>>>(theta, h->buf1, h->buf0, g);
     CK(cudaGetLastError());
     mark(5);
-    if ((rc = sweep(h->buf0, h->buf0, g.iy * g.iz, g.ix, g.bx, 0, 0, 0, 0, "X"))) return rc;
+    if ((rc = sweep(2, h->buf0, h->buf0, g.iy * g.iz, g.ix, g.bx, 0, 0, 0, 0, "X"))) return rc;
     mark(6);
     heat_update_kernel<<<dim3(ty, tx, g.iz), bt, 0, st>>>(theta, h->buf0, g);
     CK(cudaGetLastError());
@@ -142,7 +145,8 @@ int btdma_heat_create(int ix, int iy, int iz, double dt, btdma_heat_t* out) {
     CKH(cudaMalloc(&h->buf1, sizeof(double) * inner));
     CKH(cudaMalloc(&h->err, sizeof(double)));
     CKH(cudaMalloc(&h->scratch, sizeof(double) * (size_t)(ix + 2) * (iy + 2) * (iz + 2)));
-    CKH(cudaMalloc(&h->tab, sizeof(double) * gen_table_doubles(std::max(ix, std::max(iy, iz)))));
+    h->tab_stride = gen_table_doubles(std::max(ix, std::max(iy, iz)));
+    CKH(cudaMalloc(&h->tab, sizeof(double) * 3 * h->tab_stride));
     CKH(cudaMalloc(&h->status, sizeof(unsigned)));
     CKH(cudaMemset(h->status, 0, sizeof(unsigned)));
     CKH(cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking));
@@ -162,6 +166,20 @@ int btdma_heat_create(int ix, int iy, int iz, double dt, btdma_heat_t* out) {
     g.cx = h->cosx;
     g.cy = h->cosy;
     g.cz = h->cosz;
+    // the factor tables of the three sweeps, once: each direction's matrix is
+    // fixed by the grid and dt (fully implicit walls, cbound)
+    const int rows[3] = {iz, iy, ix};
+    const double base[3] = {g.bz, g.by, g.bx};
+    for (int d = 0; d < 3; ++d) {
+        TileArgs ga = {};
+        ga.cs = base[d];
+        ga.cbound = 1;
+        const int rc = build_gen_table<1>(rows[d], ga, h->tab + d * h->tab_stride, h->cap);
+        if (rc) return cleanup(rc);
+    }
+    const cudaError_t e = cudaStreamSynchronize(h->cap);
+    if (e != cudaSuccess)
+        return cleanup(fail(BTDMA_ERR_CUDA, "heat factor tables: %s", cudaGetErrorString(e)));
     *out = h;
     return BTDMA_OK;
 }
@@ -374,7 +392,15 @@ struct btdma_momentum {
     double* tab = nullptr;  // [dir][comp][ta, tb, tc][n_dir rows]
     size_t tab_off[3][3] = {};
     double* buf = nullptr;  // nx * ny * nz, the sweep layout
-    double* gtab = nullptr; // shared elimination factors of one sweep
+    // factor tables per (dir, comp), gstride apart, and what each was last
+    // built for: reused while the coefficient and the stream stay the same
+    double* gtab = nullptr;
+    size_t gstride = 0;
+    struct TabKey {
+        bool valid = false;
+        double c = 0.0;
+        cudaStream_t stream = nullptr;
+    } gkey[3][3];
     unsigned* status = nullptr;
 };
 
@@ -439,6 +465,7 @@ int btdma_momentum_create(int nx, int ny, int nz, const double* dx0, const doubl
     h->pbc[0] = pbc_x ? 1 : 0;
     h->pbc[1] = pbc_y ? 1 : 0;
     std::memcpy(h->tab_off, off, sizeof off);
+    h->gstride = gen_table_doubles(std::max(nx, std::max(ny, nz)));
     auto cleanup = [&](int code) {
         btdma_momentum_destroy(h);
         return code;
@@ -447,8 +474,7 @@ int btdma_momentum_create(int nx, int ny, int nz, const double* dx0, const doubl
         cudaMemcpy(h->tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice) !=
             cudaSuccess ||
         cudaMalloc(&h->buf, sizeof(double) * (size_t)nx * ny * nz) != cudaSuccess ||
-        cudaMalloc(&h->gtab, sizeof(double) * gen_table_doubles(std::max(nx, std::max(ny, nz)))) !=
-            cudaSuccess ||
+        cudaMalloc(&h->gtab, sizeof(double) * 9 * h->gstride) != cudaSuccess ||
         cudaMalloc(&h->status, sizeof(unsigned)) != cudaSuccess ||
         cudaMemset(h->status, 0, sizeof(unsigned)) != cudaSuccess)
         return cleanup(fail(BTDMA_ERR_CUDA, "momentum buffers: %s",
@@ -481,6 +507,16 @@ int btdma_momentum_sweep(btdma_momentum_t h, int dir, int comp, const double* q,
     t.gb = t.ga + n[dir];
     t.gc = t.gb + n[dir];
     const dim3 b1(128, 1, 1), bt(MOM_TILE, 8, 1);
+    // this (dir, comp)'s factor table: built in this call unless the last build
+    // was for the same coefficient on the same stream; always built inside a
+    // stream capture, so that a graph carries its own tables
+    auto& key = h->gkey[dir][comp];
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(stream, &cap));
+    const bool capturing = cap != cudaStreamCaptureStatusNone;
+    const bool ready = !capturing && key.valid && key.c == c && key.stream == stream;
+    double* const gt = h->gtab + (size_t)(dir * 3 + comp) * h->gstride;
+    if (!ready) key.valid = false;  // rebuilt below
     // z and y sweeps store straight into dst's interior through the tiled
     // solve's layout map (system s = (a, i) with i = s % nx fastest, row r):
     //   z: dst(i, j = s / nx + 1, k = r + 1);  y: dst(i, j = r + 1, k = s / nx + 1)
@@ -496,29 +532,34 @@ int btdma_momentum_sweep(btdma_momentum_t h, int dir, int comp, const double* q,
         CK(cudaGetLastError());
         t.xbs = g.nx + 2;
         t.xrs = sp;
-        rc = try_tile_gen<3, false>(h->buf, dst_in, n_sys, g.nz, t, h->status, stream, h->gtab);
+        rc = try_tile_gen<3, false>(h->buf, dst_in, n_sys, g.nz, t, h->status, stream, gt, ready);
     } else if (dir == 1) {
         mom_gather_kernel<1><<<dim3((g.nx + 127) / 128, (g.nz + MOM_GR - 1) / MOM_GR, g.ny), b1,
                                  0, stream>>>(q, h->buf, g, 0);
         CK(cudaGetLastError());
         t.xbs = sp;
         t.xrs = g.nx + 2;
-        rc = h->pbc[1]
-                 ? try_tile_gen<3, true>(h->buf, dst_in, n_sys, g.ny, t, h->status, stream, h->gtab)
-                 : try_tile_gen<3, false>(h->buf, dst_in, n_sys, g.ny, t, h->status, stream,
-                                          h->gtab);
+        rc = h->pbc[1] ? try_tile_gen<3, true>(h->buf, dst_in, n_sys, g.ny, t, h->status,
+                                               stream, gt, ready)
+                       : try_tile_gen<3, false>(h->buf, dst_in, n_sys, g.ny, t, h->status,
+                                                stream, gt, ready);
     } else {
         t.xblk = 0;  // x: the plain layout, transposed back below
         mom_gather_x_kernel<<<dim3((g.nx + MOM_TILE - 1) / MOM_TILE,
                                    (g.ny + MOM_TILE - 1) / MOM_TILE, g.nz), bt, 0, stream>>>(
             q, h->buf, g);
         CK(cudaGetLastError());
-        rc = h->pbc[0]
-                 ? try_tile_gen<3, true>(h->buf, h->buf, n_sys, g.nx, t, h->status, stream, h->gtab)
-                 : try_tile_gen<3, false>(h->buf, h->buf, n_sys, g.nx, t, h->status, stream,
-                                          h->gtab);
+        rc = h->pbc[0] ? try_tile_gen<3, true>(h->buf, h->buf, n_sys, g.nx, t, h->status,
+                                               stream, gt, ready)
+                       : try_tile_gen<3, false>(h->buf, h->buf, n_sys, g.nx, t, h->status,
+                                                stream, gt, ready);
     }
     if (rc != 1) return rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "sweep not tileable");
+    if (!capturing) {
+        key.valid = true;
+        key.c = c;
+        key.stream = stream;
+    }
     if (dir == 0) {
         mom_scatter_x_kernel<<<dim3((g.ny + MOM_TILE - 1) / MOM_TILE,
                                     (g.nx + MOM_TILE - 1) / MOM_TILE, g.nz), bt, 0, stream>>>(

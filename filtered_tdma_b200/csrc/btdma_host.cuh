@@ -455,14 +455,36 @@ int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, 
     return rc == BTDMA_OK ? 1 : rc;
 }
 
+// Factor table of a shared-matrix sweep (GEN 1 or 3) of n_row rows: the
+// elimination of every sub-segment and the reduced system's lane table, built
+// by one small launch.  It depends only on the matrix (gen's coefficient
+// fields), so a caller whose matrix does not change builds it once.
+template <int GEN, bool CYC = false>
+int build_gen_table(int n_row, const TileArgs& gen, double* tab, cudaStream_t st) {
+    static_assert(GEN == 1 || GEN == 3, "shared-matrix modes only");
+    const TilePlan pl = tile_plan(n_row, CYC, 8, 1, true);
+    if (pl.sys == 0) return fail(BTDMA_ERR_UNSUPPORTED, "%d rows are not tileable", n_row);
+    if (!tab) return fail(BTDMA_ERR_ARG, "shared-matrix sweep without a factor table");
+    TileArgs a = gen;
+    a.n_row = n_row;
+    a.nseg = pl.nseg;
+    a.cl = pl.cl;
+    a.nst = pl.nst;
+    tile_table_kernel<GEN, CYC><<<(pl.nseg + 127) / 128, 128, 0, st>>>(a, tab);
+    CK(cudaGetLastError());
+    return BTDMA_OK;
+}
+
 // Generated-coefficient batch, only D read (the GEN modes of the tiled
 // kernel; the coefficient fields of `gen` are used, the rest is filled here).
 // Returns 1 when launched, 0 when the shape is not tiled, < 0 on error.
 // GEN 1 and 3 (one matrix for every system): `tab` is device scratch of
-// gen_table_doubles(n_row) doubles for the shared elimination factors.
+// gen_table_doubles(n_row) doubles for the shared elimination factors, built
+// here unless `table_ready` (built earlier by build_gen_table for this matrix).
 template <int GEN, bool CYC = false>
 int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArgs& gen,
-                 unsigned* status, cudaStream_t st, double* tab = nullptr) {
+                 unsigned* status, cudaStream_t st, double* tab = nullptr,
+                 bool table_ready = false) {
     const TilePlan pl = tile_plan(n_row, CYC, 8, 1, GEN == 1 || GEN == 3);
     if (pl.sys == 0 || !tma_ok_elem(D, n_sys, 8)) return 0;
     const int nsc = pl.nseg / pl.cl;
@@ -480,8 +502,10 @@ int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArg
     a.status = status;  // the layout map (xblk ...) comes with gen
     if constexpr (GEN == 1 || GEN == 3) {
         if (!tab) return fail(BTDMA_ERR_ARG, "shared-matrix sweep without a factor table");
-        tile_table_kernel<GEN, CYC><<<(pl.nseg + 127) / 128, 128, 0, st>>>(a, tab);
-        CK(cudaGetLastError());
+        if (!table_ready) {
+            tile_table_kernel<GEN, CYC><<<(pl.nseg + 127) / 128, 128, 0, st>>>(a, tab);
+            CK(cudaGetLastError());
+        }
         a.gtab = tab;
     }
     int rc;

@@ -50,6 +50,29 @@ def test_adi_matches_oracle_walls_only(cuda, orc):
         assert _rel(d_q.cpu().numpy()[1:-1, 1:-1, 1:-1], ref[1:-1, 1:-1, 1:-1]) <= 1e-12
 
 
+@pytest.mark.gpu
+def test_factor_tables_follow_the_coefficient(cuda, orc):
+    # one handle, the coefficient changing between calls, repeated, and a call
+    # on another stream: each (dir, comp) factor table is reused only for the
+    # coefficient and stream it was built for
+    import torch
+    from filtered_tdma_b200.momentum import ChannelMomentum
+    m = ChannelMomentum(64, 32, 48, gamma3=1.5)
+    rng = np.random.default_rng(33)
+    q = rng.uniform(-1, 1, m.shape)
+    side = torch.cuda.Stream()
+    for c, stream in ((0.05, None), (0.2, None), (0.05, None), (0.05, None), (0.2, side)):
+        for direction in (0, 1, 2):
+            dq = torch.from_numpy(q).to(cuda)
+            out = torch.from_numpy(q).to(cuda)
+            torch.cuda.synchronize()
+            m.sweep(direction, 1, dq, out, c, stream=0 if stream is None else stream.cuda_stream)
+            torch.cuda.synchronize()
+            ref = MO.sweep(q, m.metrics, direction, 1, c, direction < 2)
+            assert _rel(out.cpu().numpy()[1:-1, 1:-1, 1:-1], ref[1:-1, 1:-1, 1:-1]) <= 1e-12
+    assert m.status() == 0
+
+
 def test_momentum_argument_checks():
     import ctypes
     from filtered_tdma_b200 import _lib as L
