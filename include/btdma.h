@@ -1,7 +1,8 @@
 /*
  * btdma — batched tridiagonal solves on one NVIDIA B200 (sm_100a).
  *
- * C ABI of the library.  Every array is a caller-owned DEVICE pointer in the
+ * C ABI of the library.  Every array is a caller-owned DEVICE pointer (except
+ * the host arrays of btdma_solve_host) in the
  * reference's row-interleaved layout [n_row x n_sys]: row j of system i at
  * j*n_sys + i (reference: libs/pascal_tdma/include/pascal_tdma.hpp:13,
  * libs/filtered_tdma/include/filtered_tdma_cuda.hpp:152-153).  A is the sub-,
@@ -28,7 +29,8 @@
  *   - Every segment needs >= 3 rows (the reference's PaScaL is wrong at 2,
  *     and indexes out of bounds at 1); btdma_create rejects such a P.
  *   - Calls are stream-ordered and never synchronise the host, except
- *     btdma_last_J and btdma_status, which read back device values.
+ *     btdma_last_J and btdma_status, which read back device values, and a
+ *     btdma_solve_host call that (re)allocates its staging buffers.
  *
  * Return value of every function: 0 on success, a negative BTDMA_ERR_* code
  * otherwise.  Kernels never trap: runtime faults of the data (NaN/Inf solution,
@@ -90,7 +92,8 @@ enum btdma_error {
  * (libs/pascal_tdma/include/pascal_tdma_cuda.hpp:20-21) and
  * FilteredTDMACUDA(n_sys, n_row, myrank, nprocs, comm, left, right, eps_constant)
  * (libs/filtered_tdma/include/filtered_tdma_cuda.hpp:163-166), with nprocs -> P.
- * Allocates the handle's device scratch; no allocation happens in a solve. */
+ * Allocates the handle's device scratch; no allocation happens in a solve
+ * (btdma_solve_host allocates its staging buffers on first use). */
 int btdma_create(int method, int n_sys, int n_row, int P, int precision, int flags,
                  btdma_t* out);
 
@@ -315,7 +318,10 @@ int btdma_poisson_status(btdma_poisson_t h, unsigned* status, cudaStream_t strea
  * the solve, never stored.  btdma_momentum_sweep reads q and writes dst (may
  * be q); btdma_momentum_adi runs z and y in place on rhs and x into q_out, as
  * MomentumSolverGPU::advance's diffuse step does after k_lap.  PaScaL (exact)
- * solves; n a multiple of 16, n / 16 a power of two for periodic sweeps. */
+ * solves; n a multiple of 16, n / 16 a power of two for periodic sweeps.  The
+ * handle keeps each (dir, comp) factor table until c or the stream changes
+ * (always rebuilt inside a stream capture); calls on one handle must be
+ * ordered (one stream, or synchronised). */
 typedef struct btdma_momentum* btdma_momentum_t;
 int btdma_momentum_create(int nx, int ny, int nz, const double* dx0, const double* dmx0,
                           const double* dx1, const double* dmx1, const double* dx2,
