@@ -23,7 +23,7 @@
  * number of MPI ranks a system is split over; here the P segments of a system
  * live in the P CTAs of one thread-block cluster on one GPU.
  *
- * Semantics that differ from the reference's (all documented in DESIGN.md):
+ * Semantics that differ from the reference's:
  *   - D <- x.  A, B and C are left unchanged (the reference leaves elimination
  *     scratch in A and C).
  *   - Every segment needs >= 3 rows (the reference's PaScaL is wrong at 2,
