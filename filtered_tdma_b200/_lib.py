@@ -42,11 +42,12 @@ class Stats(ctypes.Structure):
     """btdma_stats of include/btdma.h."""
     _fields_ = [("n_systems", ctypes.c_int), ("sweeps", ctypes.c_int),
                 ("converged_after", ctypes.c_int * (REFINE_MAX_SWEEPS + 1)),
-                ("n_fallback", ctypes.c_int)]
+                ("n_fallback", ctypes.c_int), ("filtered_exact", ctypes.c_int)]
 
     def as_dict(self) -> dict:
         return {"n_systems": self.n_systems, "sweeps": self.sweeps,
-                "converged_after": list(self.converged_after), "n_fallback": self.n_fallback}
+                "converged_after": list(self.converged_after), "n_fallback": self.n_fallback,
+                "filtered_exact": self.filtered_exact}
 
 
 class RaggedBucket(ctypes.Structure):

@@ -17,8 +17,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libbtdma.so")
 SOURCES = [os.path.join(PKG, "csrc", f) for f in ("btdma_api.cu", "btdma_ragged.cu", "btdma_apps.cu")]
-DEPS = SOURCES + [os.path.join(PKG, "csrc", f) for f in os.listdir(os.path.join(PKG, "csrc"))
-                  if f != "width_probe.cu"] + [
+DEPS = SOURCES + [os.path.join(PKG, "csrc", f) for f in os.listdir(os.path.join(PKG, "csrc"))] + [
     os.path.join(ROOT, "include", "btdma.h")]
 
 NVCC_FLAGS = [
@@ -29,10 +28,6 @@ NVCC_FLAGS = [
     "-Xlinker", "--exclude-libs=ALL",  # keep the static runtime's symbols private
     "-I" + os.path.join(ROOT, "include"),
 ]
-
-
-PROBE = os.path.join(PKG, "_width_probe")
-PROBE_SRC = os.path.join(PKG, "csrc", "width_probe.cu")
 
 
 def stale() -> bool:
@@ -68,14 +63,6 @@ def build(force: bool = False, verbose: bool = False) -> str:
                 "static", "-Xlinker", "--exclude-libs=ALL", "-o", LIB, *objs]
         subprocess.run(link, check=True)
     return LIB
-
-
-def build_probe(force: bool = False) -> str:
-    """The access-width bandwidth probe (a standalone executable)."""
-    if force or not os.path.exists(PROBE) or os.path.getmtime(PROBE_SRC) > os.path.getmtime(PROBE):
-        subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17",
-                        "-o", PROBE, PROBE_SRC], check=True)
-    return PROBE
 
 
 if __name__ == "__main__":

@@ -40,9 +40,11 @@ int jmax_launch(btdma_t h, const double* D, int n_sys, int n_row, cudaStream_t s
     return BTDMA_OK;
 }
 
-int jfinal_launch(btdma_t h, int n_row, int version, cudaStream_t st) {
+// exact: the device word jfinal sets when the batch needs the exact reduced
+// solve (null: the reference's behaviour, no fallback)
+int jfinal_launch(btdma_t h, int n_row, int version, unsigned* exact, cudaStream_t st) {
     jfinal_kernel<<<1, 32, 0, st>>>(h->work, h->J, h->rho_row, n_row, h->P, h->eps_constant,
-                                    version, (h->flags & BTDMA_FLAG_J_HOST) ? 1 : 0);
+                                    version, (h->flags & BTDMA_FLAG_J_HOST) ? 1 : 0, exact);
     CK(cudaGetLastError());
     return BTDMA_OK;
 }
@@ -67,6 +69,9 @@ int solve_impl(btdma_t h, const double* A, const double* B, const double* C, con
     if (h->precision != BTDMA_FP64)
         return fail(BTDMA_ERR_UNSUPPORTED, "FP64 arrays passed to an FP32-refine handle");
     h->last_stream = st;
+    h->last_n_sys = n_sys;
+    h->last_refined = false;
+    h->last_filtered = false;
 
     if (h->P == 1) {
         if (cyclic && n_row < 3) return fail(BTDMA_ERR_ARG, "periodic systems need n_row >= 3");
@@ -120,19 +125,47 @@ int solve_impl(btdma_t h, const double* A, const double* B, const double* C, con
     const int groups = (n_sys + SEG_S - 1) / SEG_S;
     if (groups > 65535) return fail(BTDMA_ERR_SIZE, "n_sys above %d", 65535 * SEG_S);
 
+    if (h->method == BTDMA_PASCAL)
+        return cyclic ? launch_seg_method<true>(h->method, maps, a, groups, st)
+                      : launch_seg_method<false>(h->method, maps, a, groups, st);
+
+    // Filtered.  Unless the reference's behaviour is asked for, a batch whose J
+    // reaches m - 2 (or whose rho is >= 0.5) in some segment takes the exact
+    // reduced solve instead: jfinal sets the device word h->exact, the
+    // Filtered kernel runs only while it is 0 and the exact solve only while it
+    // is 1 (both launched; no host round trip).
+    unsigned* exact = (h->flags & BTDMA_FLAG_REFERENCE_ORDER) ? nullptr : h->exact;
     if (h->method == BTDMA_FILTERED_V2) {
         if ((rc = jmax_launch(h, D, n_sys, n_row, st))) return rc;
-        if ((rc = jfinal_launch(h, n_row, 2, st))) return rc;
-    } else if (h->method == BTDMA_FILTERED_V1) {
+        if ((rc = jfinal_launch(h, n_row, 2, exact, st))) return rc;
+    } else {
         SegArgs ai = a;
         ai.mode = SEG_MODE_INTERFACE;
         rc = cyclic ? launch_seg_method<true>(h->method, maps, ai, groups, st)
                     : launch_seg_method<false>(h->method, maps, ai, groups, st);
         if (rc) return rc;
-        if ((rc = jfinal_launch(h, n_row, 1, st))) return rc;
+        if ((rc = jfinal_launch(h, n_row, 1, exact, st))) return rc;
     }
-    return cyclic ? launch_seg_method<true>(h->method, maps, a, groups, st)
-                  : launch_seg_method<false>(h->method, maps, a, groups, st);
+    h->last_filtered = true;
+    a.gate = exact;
+    a.gate_run = 0;
+    rc = cyclic ? launch_seg_method<true>(h->method, maps, a, groups, st)
+                : launch_seg_method<false>(h->method, maps, a, groups, st);
+    if (rc || !exact) return rc;
+    // the exact solve: the tiled PaScaL kernel, or the reference-order one
+    // where the shape is not tiled
+    rc = try_tile<double>(A, B, C, D, X, n_sys, n_row, cyclic, h->status, st, false, exact,
+                          h->tile_shape);
+    if (rc < 0) return rc;
+    if (rc == 1) return BTDMA_OK;
+    if (seg_smem_bytes(a.mcap, a.P, cyclic, true, seg_reg_rows(n_row, a.P)) >
+        (size_t)max_smem_optin())
+        return fail(BTDMA_ERR_UNSUPPORTED,
+                    "segment of %d rows does not fit in shared memory for the exact fallback",
+                    a.mcap);
+    a.gate_run = 1;
+    return cyclic ? launch_seg_method<true>(BTDMA_PASCAL, maps, a, groups, st)
+                  : launch_seg_method<false>(BTDMA_PASCAL, maps, a, groups, st);
 }
 
 }  // namespace
@@ -189,6 +222,8 @@ int btdma_create(int method, int n_sys, int n_row, int P, int precision, int fla
     CKC(cudaMemset(h->work, 0, sizeof(unsigned long long) * 2 * P));
     CKC(cudaMalloc(&h->status, sizeof(unsigned)));
     CKC(cudaMemset(h->status, 0, sizeof(unsigned)));
+    CKC(cudaMalloc(&h->exact, sizeof(unsigned)));
+    CKC(cudaMemset(h->exact, 0, sizeof(unsigned)));
     if (P == 1 && precision == BTDMA_FP64)
         CKC(cudaMalloc(&h->scratch, sizeof(double) * 2 * (size_t)n_row * n_sys));
     if (precision == BTDMA_FP32_REFINE) {
@@ -207,6 +242,7 @@ int btdma_destroy(btdma_t h) {
     cudaFree(h->J);
     cudaFree(h->work);
     cudaFree(h->status);
+    cudaFree(h->exact);
     cudaFree(h->scratch);
     cudaFree(h->resid);
     cudaFree(h->iters);
@@ -347,6 +383,7 @@ int btdma_solve_f32(btdma_t h, const float* A, const float* B, const float* C, c
     h->last_stream = stream;
     h->last_n_sys = n_sys;
     h->last_refined = false;
+    h->last_filtered = false;
     const bool cyc = cyclic != 0;
     const char* shape_msg =
         "FP32 storage needs n_row % 16 == 0, n_sys % 4 == 0, 16-byte alignment "
@@ -400,6 +437,18 @@ int btdma_last_stats(btdma_t h, btdma_stats* st) {
     if (!h || !st) return fail(BTDMA_ERR_ARG, "null argument");
     std::memset(st, 0, sizeof *st);
     st->n_systems = h->last_n_sys;
+    st->filtered_exact = -1;
+    if (h->last_filtered) {
+        if (h->flags & BTDMA_FLAG_REFERENCE_ORDER) {
+            st->filtered_exact = 0;
+        } else {
+            unsigned ex = 0;
+            CK(cudaMemcpyAsync(&ex, h->exact, sizeof ex, cudaMemcpyDeviceToHost,
+                               h->last_stream));
+            CK(cudaStreamSynchronize(h->last_stream));
+            st->filtered_exact = ex ? 1 : 0;
+        }
+    }
     if (!h->last_refined) return BTDMA_OK;
     std::vector<unsigned char> it((size_t)h->last_n_sys);
     unsigned open[BTDMA_REFINE_MAX_SWEEPS + 1];
@@ -499,8 +548,11 @@ int btdma_segments(btdma_t h, int* P) {
 // Allocation-free serial Thomas (btdma_solve_noalloc).  The forward sweep's c'
 // goes to this fixed device array instead of handle-owned scratch.  Host code
 // may not pass the array's name to a kernel (on the host it is only a
-// stand-in symbol), so its device address is looked up once per device with
-// that device current and cached here.
+// stand-in symbol), so its device address is looked up with the device
+// current and cached per device, keyed on the CUDA context it was looked up
+// in: a context that was destroyed and created again (cudaDeviceReset, a
+// primary context released and retained) has its module loaded anew, so the
+// address is looked up again there.
 // ---------------------------------------------------------------------------
 static __device__ __align__(256) double g_noalloc_scratch[BTDMA_NOALLOC_MAX_ELEMS];
 
@@ -508,19 +560,56 @@ namespace {
 
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
-double* g_noalloc_ptr[kMaxDevices] = {};
+struct NoallocEntry {
+    double* ptr = nullptr;
+    unsigned long long ctx = 0;  // id of the context the address belongs to
+    bool keyed = false;          // false: no context id available, look up every call
+};
+NoallocEntry g_noalloc[kMaxDevices];
+
+// Unique id of the calling thread's current context (cuCtxGetId, through the
+// runtime's driver entry points); false when there is none or the driver
+// lacks the call.
+bool current_ctx_id(unsigned long long* id) {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) ==
+                cudaSuccess && q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(p);
+    });
+    if (!get_current || !get_id) return false;
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+    return get_id(ctx, id) == CUDA_SUCCESS;
+}
 
 int noalloc_scratch(double** out) {
     int dev = 0;
     CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) return fail(BTDMA_ERR_UNSUPPORTED, "device %d", dev);
+    unsigned long long id = 0;
+    bool have_id = current_ctx_id(&id);
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
+    NoallocEntry& e = g_noalloc[dev];
+    if (!e.ptr || !e.keyed || !have_id || e.ctx != id) {
         void* p = nullptr;
-        CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-        g_noalloc_ptr[dev] = static_cast<double*>(p);
+        CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));  // creates the context if needed
+        if (!have_id) have_id = current_ctx_id(&id);
+        e.ptr = static_cast<double*>(p);
+        e.ctx = have_id ? id : 0;
+        e.keyed = have_id;
     }
-    *out = g_noalloc_ptr[dev];
+    *out = e.ptr;
     return BTDMA_OK;
 }
 

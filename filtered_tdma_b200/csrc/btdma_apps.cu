@@ -393,7 +393,10 @@ struct btdma_momentum {
     size_t tab_off[3][3] = {};
     double* buf = nullptr;  // nx * ny * nz, the sweep layout
     // factor tables per (dir, comp), gstride apart, and what each was last
-    // built for: reused while the coefficient and the stream stay the same
+    // built for: reused while the coefficient and the stream stay the same.
+    // A second set of 9 tables serves captured sweeps: a graph rebuilds its
+    // tables on every replay, and must not overwrite the cached ones (a later
+    // uncaptured call with the cached key would then use the graph's tables).
     double* gtab = nullptr;
     size_t gstride = 0;
     struct TabKey {
@@ -474,7 +477,7 @@ int btdma_momentum_create(int nx, int ny, int nz, const double* dx0, const doubl
         cudaMemcpy(h->tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice) !=
             cudaSuccess ||
         cudaMalloc(&h->buf, sizeof(double) * (size_t)nx * ny * nz) != cudaSuccess ||
-        cudaMalloc(&h->gtab, sizeof(double) * 9 * h->gstride) != cudaSuccess ||
+        cudaMalloc(&h->gtab, sizeof(double) * 18 * h->gstride) != cudaSuccess ||
         cudaMalloc(&h->status, sizeof(unsigned)) != cudaSuccess ||
         cudaMemset(h->status, 0, sizeof(unsigned)) != cudaSuccess)
         return cleanup(fail(BTDMA_ERR_CUDA, "momentum buffers: %s",
@@ -509,14 +512,16 @@ int btdma_momentum_sweep(btdma_momentum_t h, int dir, int comp, const double* q,
     const dim3 b1(128, 1, 1), bt(MOM_TILE, 8, 1);
     // this (dir, comp)'s factor table: built in this call unless the last build
     // was for the same coefficient on the same stream; always built inside a
-    // stream capture, so that a graph carries its own tables
+    // stream capture, into the capture set of tables, so that a graph carries
+    // its own tables and its replays leave the cached ones intact
     auto& key = h->gkey[dir][comp];
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     CK(cudaStreamIsCapturing(stream, &cap));
     const bool capturing = cap != cudaStreamCaptureStatusNone;
     const bool ready = !capturing && key.valid && key.c == c && key.stream == stream;
-    double* const gt = h->gtab + (size_t)(dir * 3 + comp) * h->gstride;
-    if (!ready) key.valid = false;  // rebuilt below
+    double* const gt =
+        h->gtab + (size_t)((capturing ? 9 : 0) + dir * 3 + comp) * h->gstride;
+    if (!ready && !capturing) key.valid = false;  // rebuilt below
     // z and y sweeps store straight into dst's interior through the tiled
     // solve's layout map (system s = (a, i) with i = s % nx fastest, row r):
     //   z: dst(i, j = s / nx + 1, k = r + 1);  y: dst(i, j = r + 1, k = s / nx + 1)

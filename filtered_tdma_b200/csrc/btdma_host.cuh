@@ -30,6 +30,10 @@ struct btdma_handle {
     int* J = nullptr;                        // [P]
     unsigned long long* work = nullptr;      // [2P] J accumulators (kept zero between solves)
     unsigned* status = nullptr;              // device status word
+    // Filtered: 1 when the latest solve took the exact reduced system (rho >= 0.5
+    // or J >= m - 2 in a segment), set on the device by jfinal_kernel
+    unsigned* exact = nullptr;
+    bool last_filtered = false;              // the latest solve was a Filtered one (P > 1)
     double* scratch = nullptr;               // P == 1: c' and e' [2][n_row_cap * n_sys_cap]
     cudaStream_t last_stream = nullptr;
     // FP32_REFINE: residual [n_row_cap * n_sys_cap] (FP32), per-system sweep
@@ -414,7 +418,8 @@ inline bool tma_ok_elem(const void* p, int n_sys, int elem) {
 // cluster-per-segment kernel, < 0 on error.
 // TC: arithmetic of the local sweeps; accumulate: X += solution; gate: the
 // kernel does nothing while *gate == 0.
-// shape: BTDMA_TILE_* (the wide-box kernel serves FP64-arithmetic plain solves).
+// shape: BTDMA_TILE_* (the wide-box kernel serves FP64-arithmetic solves that
+// do not accumulate).
 template <typename TIN, typename TC = double>
 int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, int n_sys,
              int n_row, bool cyclic, unsigned* status, cudaStream_t st, bool accumulate = false,
@@ -422,7 +427,7 @@ int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, 
     const int elem = (int)sizeof(TIN);
     bool wide = false;
     TilePlan pl;
-    if (shape != BTDMA_TILE_NARROW && sizeof(TC) == 8 && !accumulate && gate == nullptr) {
+    if (shape != BTDMA_TILE_NARROW && sizeof(TC) == 8 && !accumulate) {
         pl = tile_wide_plan(n_row, cyclic, elem);
         wide = pl.sys != 0 && (shape == BTDMA_TILE_WIDE || wide_by_default(n_row, elem));
     }

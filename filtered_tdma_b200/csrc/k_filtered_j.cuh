@@ -73,9 +73,15 @@ jmax_kernel(const double* __restrict__ D, int n_sys, int n_row, int P, int all_r
 //   v2 / device v1: B = q(2+q)/((1-q)(1-2rho)) * max_b (filtered_tdma_kernels.cuh:249-257),
 //   host v1:        B = (max|x0| + max|xN|) q/(1-q)    (filtered_tdma.cpp:110-114),
 //   J = int(log(eps/B)/log q) + 1 clamped to [0, m-1]; rho in {0} u [0.5, inf) -> m-1.
+// exact (optional): set to 1 when some segment has rho >= 0.5 (the bound does
+// not hold) or J >= m - 2 (the truncation keeps every row, so only the 2x2
+// interface approximation would remain), else 0: the solve then takes the exact
+// reduced system instead of the Filtered interface.  One warp.
 __global__ void jfinal_kernel(unsigned long long* __restrict__ work, int* __restrict__ J,
                               const double* __restrict__ rho_row, int n_row, int P,
-                              double eps_constant, int version, int host_semantics) {
+                              double eps_constant, int version, int host_semantics,
+                              unsigned* __restrict__ exact) {
+    bool need_exact = false;
     for (int k = threadIdx.x; k < P; k += blockDim.x) {
         int r0, m;
         seg_range(n_row, P, k, r0, m);
@@ -106,9 +112,12 @@ __global__ void jfinal_kernel(unsigned long long* __restrict__ work, int* __rest
             Jk = (int)Jl;
         }
         J[k] = Jk;
+        need_exact |= rho >= 0.5 || Jk >= m - 2;
         work[2 * k] = 0ull;
         work[2 * k + 1] = 0ull;
     }
+    const bool any = __any_sync(0xffffffffu, need_exact);
+    if (exact != nullptr && threadIdx.x == 0) *exact = any ? 1u : 0u;
 }
 
 }  // namespace btdma

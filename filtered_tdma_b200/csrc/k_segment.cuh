@@ -70,6 +70,11 @@ struct SegArgs {
     const int* J;  // Filtered: J per segment (device)
     unsigned long long* bnd;  // v1 interface pass: per segment max |x0|, max |xN| (bits)
     unsigned* status;
+    // gate (optional): the launch runs only when (*gate != 0) == gate_run; a
+    // Filtered solve and its exact fallback are launched back to back and one
+    // of them does nothing (the device decides, no host round trip)
+    const unsigned* gate;
+    int gate_run;
 };
 
 // Dynamic shared memory layout of one CTA: the tiles (A, B, C, D for PaScaL;
@@ -118,6 +123,11 @@ seg_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                const __grid_constant__ CUtensorMap tmC, const __grid_constant__ CUtensorMap tmD,
                const __grid_constant__ CUtensorMap tmX, const SegArgs args) {
     using E = Exact64;
+    // every CTA of the cluster reads the same word: all leave together, before
+    // any barrier
+    if (args.gate != nullptr &&
+        ((*static_cast<const volatile unsigned*>(args.gate) != 0u) != (args.gate_run != 0)))
+        return;
     extern __shared__ unsigned char smem_raw[];
     double* base = reinterpret_cast<double*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));

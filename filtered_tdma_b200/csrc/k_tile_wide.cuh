@@ -152,7 +152,10 @@ tile_wide_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
     }
     __syncthreads();
 
-    const int n_my = args.n_groups > (int)blockIdx.x
+    // a closed gate (*gate == 0) leaves the CTA without groups
+    const bool gated_off =
+        args.gate != nullptr && *static_cast<const volatile unsigned*>(args.gate) == 0u;
+    const int n_my = (!gated_off && args.n_groups > (int)blockIdx.x)
                          ? (args.n_groups - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x
                          : 0;
     const int total = n_my * SPT;

@@ -12,6 +12,12 @@ These generators stand in for them:
 * ``diag_dominant``   per-system r drawn log-uniform in [r_lo, r_hi]
                       (A = C = -r, B = 1+2r), D uniform in [-1, 1].
 * ``weak_dominance``  per-system rho uniform in [rho_lo, rho_hi], r = rho/(1-2rho).
+* ``rho_band``        per-system rho = max(|A/B|, |C/B|) uniform in
+                      [rho_lo, rho_hi], reaching past 0.5 while the rows stay
+                      strictly dominant: B = 1, A = -rho, C = -(0.9 - rho)
+                      (|A| + |C| = 0.9), D uniform in [-1, 1].  The Filtered
+                      J bound does not hold at rho >= 0.5 (the reference then
+                      sets J = m - 1).
 * ``row_varying``     every coefficient drawn on its own (|A|, |C| log-uniform in
                       [0.05, 5] with random signs, B = (|A| + |C|) / rho with rho
                       uniform in [0.3, 0.9] per row), so a kernel that takes a
@@ -74,6 +80,17 @@ def weak_dominance(n_sys: int, n_row: int, rho_lo: float = 0.45, rho_hi: float =
     r = rho / (1.0 - 2.0 * rho)
     D = rng.uniform(-1.0, 1.0, size=(n_row, n_sys))
     return _np_batch(r, n_row, D, dtype)
+
+
+def rho_band(n_sys: int, n_row: int, rho_lo: float = 0.45, rho_hi: float = 0.55,
+             seed: int = 8, dtype=np.float64):
+    rng = np.random.default_rng(seed)
+    rho = rng.uniform(rho_lo, rho_hi, size=n_sys)
+    A = np.broadcast_to(-rho[None, :], (n_row, n_sys))
+    C = np.broadcast_to(-(0.9 - rho)[None, :], (n_row, n_sys))
+    B = np.ones((n_row, n_sys))
+    D = rng.uniform(-1.0, 1.0, size=(n_row, n_sys))
+    return tuple(np.ascontiguousarray(v, dtype=dtype) for v in (A, B, C, D))
 
 
 def row_varying(n_sys: int, n_row: int, seed: int = 7, dtype=np.float64):

@@ -17,6 +17,14 @@
  *                      the interface solve (FilteredTDMACUDA::solve_filtered_v1)
  *   BTDMA_FILTERED_V2  "filtered_v2"  J taken before the sweeps
  *                      (FilteredTDMACUDA::solve_filtered_v2)
+ *   Filtered full-solve fallback: where the reference's truncation gives no
+ *   saving or no bound — J >= m - 2 in some segment of m rows (J = m - 1 is
+ *   also what the reference sets for rho = 0 or rho >= 0.5,
+ *   libs/filtered_tdma/gpu/filtered_tdma_kernels.cuh:245-250) — the reference
+ *   still solves the interfaces by the 2x2 approximation; here the batch is
+ *   solved with the exact reduced system instead (PaScaL), decided on the
+ *   device, and btdma_last_stats reports it (filtered_exact).  With
+ *   BTDMA_FLAG_REFERENCE_ORDER the reference's behaviour is kept, bit for bit.
  * With P = 1 every method is the serial Thomas algorithm, bit-identical to the
  * reference's tdma_many / tdma_cyclic_many (libs/pascal_tdma/cpu/tdma_local.cpp),
  * exactly as the reference falls back at nprocs == 1.  In the reference P is the
@@ -72,7 +80,9 @@ enum btdma_flags {
      * bit-identical to PaScaLTDMA::solve with nprocs = P
      * (libs/pascal_tdma/cpu/pascal_tdma.cpp:113-227).  Without the flag PaScaL
      * uses the register-tiled kernel, exact to rounding (<= 1e-12 relative to
-     * the serial Thomas) and faster. */
+     * the serial Thomas) and faster.  For Filtered handles the flag keeps the
+     * reference's 2x2 interface where J >= m - 2 (no exact fallback), so every
+     * Filtered result is bit-identical to the reference's. */
     BTDMA_FLAG_REFERENCE_ORDER = 1 << 1
 };
 
@@ -196,6 +206,10 @@ typedef struct btdma_stats {
     int sweeps;
     int converged_after[BTDMA_REFINE_MAX_SWEEPS + 1];
     int n_fallback;
+    /* Filtered solves (P > 1): 1 when the batch was solved with the exact
+     * reduced system instead of the Filtered interface (see BTDMA_FILTERED_V1),
+     * 0 when the J-truncated Filtered scheme ran; -1 for other solves. */
+    int filtered_exact;
 } btdma_stats;
 int btdma_last_stats(btdma_t h, btdma_stats* stats);
 
@@ -319,8 +333,10 @@ int btdma_poisson_status(btdma_poisson_t h, unsigned* status, cudaStream_t strea
  * be q); btdma_momentum_adi runs z and y in place on rhs and x into q_out, as
  * MomentumSolverGPU::advance's diffuse step does after k_lap.  PaScaL (exact)
  * solves; n a multiple of 16, n / 16 a power of two for periodic sweeps.  The
- * handle keeps each (dir, comp) factor table until c or the stream changes
- * (always rebuilt inside a stream capture); calls on one handle must be
+ * handle keeps each (dir, comp) factor table until c or the stream changes;
+ * a sweep captured into a CUDA graph builds its table on every replay, into a
+ * second set of tables kept for captured sweeps, so replays never change what
+ * uncaptured calls reuse.  Calls and graph replays on one handle must be
  * ordered (one stream, or synchronised). */
 typedef struct btdma_momentum* btdma_momentum_t;
 int btdma_momentum_create(int nx, int ny, int nz, const double* dx0, const double* dmx0,
@@ -374,8 +390,10 @@ int btdma_set_tile_shape(btdma_t h, int shape);
  * doubles (8 MiB) that every GPU loading the library keeps until the process
  * exits.  Batches with n_sys * n_row above that return BTDMA_ERR_SIZE.
  *
- * The first call on a device looks up the array's device address (make it
- * before any stream capture).  All calls share the one array and leave their
+ * The first call on a device (and the first after that device's context was
+ * destroyed and created again) looks up the array's device address in the
+ * current context; make that first call before any stream capture.  All
+ * calls share the one array and leave their
  * scratch in it, so calls that overlap on the GPU (other streams, other host
  * threads) race with each other: order them on one stream.  A, B, C are
  * unchanged; no device status word is kept. */

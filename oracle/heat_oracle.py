@@ -53,10 +53,13 @@ def coords(n: int) -> np.ndarray:
 
 
 def initial(ix: int, iy: int, iz: int) -> np.ndarray:
+    """sin(pi x) sin(pi y) sin(pi z) + cos(pi x) cos(pi y) cos(pi z) on the full
+    grid (products of the 1-D factors, evaluated left to right per cell)."""
     x, y, z = coords(ix), coords(iy), coords(iz)
-    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
-    return (np.sin(PI * X) * np.sin(PI * Y) * np.sin(PI * Z)
-            + np.cos(PI * X) * np.cos(PI * Y) * np.cos(PI * Z))
+    sx, sy, sz = np.sin(PI * x), np.sin(PI * y), np.sin(PI * z)
+    cx, cy, cz = np.cos(PI * x), np.cos(PI * y), np.cos(PI * z)
+    return ((sx[None, None, :] * sy[None, :, None]) * sz[:, None, None]
+            + (cx[None, None, :] * cy[None, :, None]) * cz[:, None, None])
 
 
 def _ghosts(th, x, y, z):

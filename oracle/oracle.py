@@ -34,13 +34,25 @@ _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
 
 
+def reference_dir() -> str | None:
+    """Root of the reference sources, from the environment variable
+    BTDMA_REFERENCE_DIR (no default: the build recipe sets it where the sources
+    exist)."""
+    d = os.environ.get("BTDMA_REFERENCE_DIR")
+    return d if d and os.path.isdir(os.path.join(d, "libs")) else None
+
+
 def build(with_ref: bool | None = None) -> None:
     """Compile the restatement (and the reference build when its sources exist)."""
     subprocess.run(["make", "-s", "-C", _HERE, "all"], check=True)
+    ref_dir = reference_dir()
     if with_ref is None:
-        with_ref = os.path.isdir("/root/reference/libs")
+        with_ref = ref_dir is not None
     if with_ref:
-        subprocess.run(["make", "-s", "-C", _HERE, "ref"], check=True)
+        if ref_dir is None:
+            raise RuntimeError("BTDMA_REFERENCE_DIR does not name the reference sources")
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", "ref_gpu", f"REF={ref_dir}"],
+                       check=True)
 
 
 _lib = None

@@ -36,55 +36,80 @@ void orc_split(int n, int nparts, int part, int* first, int* count) {
  * ------------------------------------------------------------------------- */
 void orc_thomas(const double* A, const double* B, double* C, double* D,
                 int n_sys, int n_row) {
+    /* Row sweeps over all systems, as tdma_many's loops (rows outer, systems
+     * inner); every system sees exactly the operations of the serial
+     * recurrence. */
     for (int i = 0; i < n_sys; ++i) {
         double inv_b = 1.0 / AT(B, 0, i);
         AT(D, 0, i) = AT(D, 0, i) * inv_b;
         AT(C, 0, i) = AT(C, 0, i) * inv_b;
-        for (int j = 1; j < n_row; ++j) {
+    }
+    for (int j = 1; j < n_row; ++j)
+        for (int i = 0; i < n_sys; ++i) {
             double a = AT(A, j, i);
             double r = 1.0 / (AT(B, j, i) - a * AT(C, j - 1, i));
             AT(D, j, i) = r * (AT(D, j, i) - a * AT(D, j - 1, i));
             AT(C, j, i) = r * AT(C, j, i);
         }
-        for (int j = n_row - 2; j >= 0; --j)
+    for (int j = n_row - 2; j >= 0; --j)
+        for (int i = 0; i < n_sys; ++i)
             AT(D, j, i) = AT(D, j, i) - AT(C, j, i) * AT(D, j + 1, i);
-    }
 }
 
 /* ---------------------------------------------------------------------------
  * Periodic Thomas with the correction vector E,
  * libs/pascal_tdma/cpu/tdma_local.cpp:108-208 (tdma_cyclic_many).
  * Row 0 couples to row n_row-1 through A[0] and C[n_row-1].  Needs n_row >= 3.
+ * Systems go in blocks of ORC_BLK, rows outer within a block (E is the
+ * block's [n_row x ORC_BLK] workspace).
  * ------------------------------------------------------------------------- */
+#define ORC_BLK 256
 void orc_thomas_cyclic(const double* A, const double* B, double* C, double* D,
                        int n_sys, int n_row) {
-    double* E = (double*)malloc(sizeof(double) * (size_t)n_row);
-    for (int i = 0; i < n_sys; ++i) {
-        for (int j = 0; j < n_row; ++j) E[j] = 0.0;
-        E[1] = -AT(A, 1, i);
-        E[n_row - 1] = -AT(C, n_row - 1, i);
-        double inv_b = 1.0 / AT(B, 1, i);
-        AT(D, 1, i) = AT(D, 1, i) * inv_b;
-        E[1] = E[1] * inv_b;
-        AT(C, 1, i) = AT(C, 1, i) * inv_b;
-        for (int j = 2; j < n_row; ++j) {
-            double a = AT(A, j, i);
-            double r = 1.0 / (AT(B, j, i) - a * AT(C, j - 1, i));
-            AT(D, j, i) = r * (AT(D, j, i) - a * AT(D, j - 1, i));
-            E[j] = r * (E[j] - a * E[j - 1]);
-            AT(C, j, i) = r * AT(C, j, i);
+    double* E = (double*)malloc(sizeof(double) * (size_t)n_row * ORC_BLK);
+#define EB(j, b) E[(size_t)(j) * ORC_BLK + (b)]
+    for (int i0 = 0; i0 < n_sys; i0 += ORC_BLK) {
+        const int nb = n_sys - i0 < ORC_BLK ? n_sys - i0 : ORC_BLK;
+        for (int b = 0; b < nb; ++b) {
+            const int i = i0 + b;
+            for (int j = 0; j < n_row; ++j) EB(j, b) = 0.0;
+            EB(1, b) = -AT(A, 1, i);
+            EB(n_row - 1, b) = -AT(C, n_row - 1, i);
+            double inv_b = 1.0 / AT(B, 1, i);
+            AT(D, 1, i) = AT(D, 1, i) * inv_b;
+            EB(1, b) = EB(1, b) * inv_b;
+            AT(C, 1, i) = AT(C, 1, i) * inv_b;
         }
-        for (int j = n_row - 2; j >= 1; --j) {
-            double c = AT(C, j, i);
-            AT(D, j, i) = AT(D, j, i) - c * AT(D, j + 1, i);
-            E[j] = E[j] - c * E[j + 1];
+        for (int j = 2; j < n_row; ++j)
+            for (int b = 0; b < nb; ++b) {
+                const int i = i0 + b;
+                double a = AT(A, j, i);
+                double r = 1.0 / (AT(B, j, i) - a * AT(C, j - 1, i));
+                AT(D, j, i) = r * (AT(D, j, i) - a * AT(D, j - 1, i));
+                EB(j, b) = r * (EB(j, b) - a * EB(j - 1, b));
+                AT(C, j, i) = r * AT(C, j, i);
+            }
+        for (int j = n_row - 2; j >= 1; --j)
+            for (int b = 0; b < nb; ++b) {
+                const int i = i0 + b;
+                double c = AT(C, j, i);
+                AT(D, j, i) = AT(D, j, i) - c * AT(D, j + 1, i);
+                EB(j, b) = EB(j, b) - c * EB(j + 1, b);
+            }
+        for (int b = 0; b < nb; ++b) {
+            const int i = i0 + b;
+            double a0 = AT(A, 0, i), c0 = AT(C, 0, i);
+            double x0 = (AT(D, 0, i) - a0 * AT(D, n_row - 1, i) - c0 * AT(D, 1, i)) /
+                        (AT(B, 0, i) + a0 * EB(n_row - 1, b) + c0 * EB(1, b));
+            AT(D, 0, i) = x0;
         }
-        double a0 = AT(A, 0, i), c0 = AT(C, 0, i);
-        double x0 = (AT(D, 0, i) - a0 * AT(D, n_row - 1, i) - c0 * AT(D, 1, i)) /
-                    (AT(B, 0, i) + a0 * E[n_row - 1] + c0 * E[1]);
-        AT(D, 0, i) = x0;
-        for (int j = 1; j < n_row; ++j) AT(D, j, i) = AT(D, j, i) + x0 * E[j];
+        for (int j = 1; j < n_row; ++j)
+            for (int b = 0; b < nb; ++b) {
+                const int i = i0 + b;
+                AT(D, j, i) = AT(D, j, i) + AT(D, 0, i) * EB(j, b);
+            }
     }
+#undef EB
     free(E);
 }
 

@@ -81,6 +81,12 @@ int main(int argc, char** argv) {
         f.solve_cycl_filtered_v2(dA, dB, dC, dD);
         report("filtered_v2_cyclic");
         std::printf("J %d\n", f.last_J());
+        // the reference's interface also where J >= m - 2 (no exact fallback)
+        upload();
+        FilteredTDMACUDA fr(n_sys, n_row, 0, 4, 0, -2, -2, 1.0e-3, BTDMA_FLAG_REFERENCE_ORDER);
+        fr.set_rho_device(dA, dB, dC);
+        fr.solve_filtered_v2(dA, dB, dC, dD);
+        report("filtered_v2_reference");
         // the same values read as 512 systems of 512 rows, through both tiled
         // kernel shapes
         for (int shape : {BTDMA_TILE_NARROW, BTDMA_TILE_WIDE}) {

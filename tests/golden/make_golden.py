@@ -1,9 +1,9 @@
 """Generate tests/golden/ref_vectors.npz from the reference's own CPU library.
 
-Run here, where the reference sources exist (``make -C oracle ref`` builds
-oracle/_ref/libref.so from them):
+Run where the reference sources exist, with BTDMA_REFERENCE_DIR naming their
+root (``make -C oracle ref REF=<dir>`` builds oracle/_ref/libref.so from them):
 
-    python tests/golden/make_golden.py
+    BTDMA_REFERENCE_DIR=<reference root> python tests/golden/make_golden.py
 
 Every output in the file was produced by the reference's code (tdma_many,
 tdma_cyclic_many, PaScaLTDMA::solve[_cyclic], FilteredTDMA::solve_[cycl_]

@@ -51,14 +51,18 @@ def test_argument_checks(lib):
 
 
 def test_stats_struct_layout():
-    # btdma_stats: n_systems, sweeps, converged_after[BTDMA_REFINE_MAX_SWEEPS + 1], n_fallback
+    # btdma_stats: n_systems, sweeps, converged_after[BTDMA_REFINE_MAX_SWEEPS + 1],
+    # n_fallback, filtered_exact
     import os
     import re
     from filtered_tdma_b200 import _lib as L
     hdr = open(os.path.join(os.path.dirname(__file__), "..", "include", "btdma.h")).read()
     m = re.search(r"#define BTDMA_REFINE_MAX_SWEEPS (\d+)", hdr)
     assert m and int(m.group(1)) == L.REFINE_MAX_SWEEPS
-    assert ctypes.sizeof(L.Stats) == 4 * (3 + L.REFINE_MAX_SWEEPS + 1)
+    assert ctypes.sizeof(L.Stats) == 4 * (4 + L.REFINE_MAX_SWEEPS + 1)
+    fields = re.search(r"typedef struct btdma_stats \{(.*?)\} btdma_stats;", hdr, re.S).group(1)
+    names = re.findall(r"int (\w+)", re.sub(r"/\*.*?\*/", "", fields, flags=re.S))
+    assert names == [f[0] for f in L.Stats._fields_]
 
 
 def test_backend_strings():

@@ -143,17 +143,24 @@ def test_pascal_default_weak_dominance(cuda, orc):
     assert rel_err(x, orc.thomas(A, B, C, D)) <= 1e-12
 
 
+FILTERED_SHAPES = [(64, 128, 2), (100, 96, 8), (33, 200, 5), (2048, 512, 8)]
+
+
 @pytest.mark.parametrize("version", [1, 2])
 @pytest.mark.parametrize("cyclic", [False, True])
-@pytest.mark.parametrize("n_sys,n_row,P", [(64, 128, 2), (100, 96, 8), (33, 200, 5),
-                                           (2048, 512, 8)])
+@pytest.mark.parametrize("n_sys,n_row,P", FILTERED_SHAPES)
 def test_filtered_bit_exact(cuda, orc, version, cyclic, n_sys, n_row, P):
+    # BTDMA_FLAG_REFERENCE_ORDER: the reference's Filtered everywhere, also
+    # where J reaches m - 2 (no exact fallback)
+    from filtered_tdma_b200 import _lib as L
     A, B, C, D = W.diag_dominant(n_sys, n_row, 0.1, 1.0, seed=version + n_row)
     rho = orc.rho_rows_all(A, B, C)
-    x, s = run(cuda, f"filtered_v{version}", A, B, C, D, P, cyclic=cyclic, rho=rho)
+    x, s = run(cuda, f"filtered_v{version}", A, B, C, D, P, cyclic=cyclic, rho=rho,
+               flags=L.FLAG_REFERENCE_ORDER)
     xo, Jo = orc.filtered(A, B, C, D, P, version, cyclic, 1e-3, rho, orc.J_DEVICE)
     assert s.last_J() == list(Jo)
     assert np.array_equal(x, xo)
+    assert s.last_stats()["filtered_exact"] == 0
     # The eps bound holds when the truncation is active in every segment
     # (J < m-2); the dropped interface couplings then decay below it too.
     segs = orc.split(n_row, P)
@@ -164,11 +171,88 @@ def test_filtered_bit_exact(cuda, orc, version, cyclic, n_sys, n_row, P):
 
 
 @pytest.mark.parametrize("version", [1, 2])
+@pytest.mark.parametrize("cyclic", [False, True])
+@pytest.mark.parametrize("n_sys,n_row,P", FILTERED_SHAPES)
+def test_filtered_default_exact_fallback(cuda, orc, version, cyclic, n_sys, n_row, P):
+    # default Filtered: the reference's scheme bit for bit while every segment
+    # truncates (J < m - 2); the exact reduced solve (within 1e-12 of the serial
+    # Thomas) as soon as one segment does not, reported by last_stats
+    A, B, C, D = W.diag_dominant(n_sys, n_row, 0.1, 1.0, seed=version + n_row)
+    rho = orc.rho_rows_all(A, B, C)
+    x, s = run(cuda, f"filtered_v{version}", A, B, C, D, P, cyclic=cyclic, rho=rho)
+    xo, Jo = orc.filtered(A, B, C, D, P, version, cyclic, 1e-3, rho, orc.J_DEVICE)
+    assert s.last_J() == list(Jo)
+    segs = orc.split(n_row, P)
+    exact = any(J >= c - 2 for J, (_, c) in zip(Jo, segs))
+    assert s.last_stats()["filtered_exact"] == int(exact)
+    if exact:
+        xt = orc.thomas_cyclic(A, B, C, D) if cyclic else orc.thomas(A, B, C, D)
+        assert rel_err(x, xt) <= 1e-12
+    else:
+        assert np.array_equal(x, xo)
+
+
+@pytest.mark.parametrize("version", [1, 2])
+def test_filtered_config2_coefficients(cuda, orc, version):
+    # the Filtered-vs-PaScaL shape's coefficients, r log-uniform in [0.1, 10]
+    # (rho up to 0.476), 32768 x 512, P = 8 (m = 64): J clamps to m - 1 = 63 in
+    # every segment.  Reference order: bit-identical to the oracle, J = 63.
+    # Default: the exact fallback, within 1e-12 of the serial Thomas; the
+    # reference's result is within its eps of it.
+    from filtered_tdma_b200 import _lib as L
+    A, B, C, D = W.diag_dominant(32768, 512, seed=2)
+    rho = orc.rho_rows_all(A, B, C)
+    xo, Jo = orc.filtered(A, B, C, D, 8, version, False, 1e-3, rho, orc.J_DEVICE)
+    assert list(Jo) == [63] * 8
+    x, s = run(cuda, f"filtered_v{version}", A, B, C, D, 8, rho=rho,
+               flags=L.FLAG_REFERENCE_ORDER)
+    assert s.last_J() == list(Jo)
+    assert np.array_equal(x, xo)
+    x, s = run(cuda, f"filtered_v{version}", A, B, C, D, 8, rho=rho)
+    assert s.last_stats()["filtered_exact"] == 1
+    xt = orc.thomas(A, B, C, D)
+    assert rel_err(x, xt) <= 1e-12
+    assert np.max(np.abs(xo - xt)) <= 1e-3 / 512.0 ** 2
+
+
+@pytest.mark.parametrize("cyclic", [False, True])
+def test_filtered_rho_at_one_half(cuda, orc, cyclic):
+    # rho = max(|A/B|, |C/B|) uniform in [0.45, 0.55] (rows still dominant): the
+    # bound does not hold past 0.5; the default Filtered solve takes the exact
+    # reduced system and says so, the reference order keeps the 2x2 interface
+    from filtered_tdma_b200 import _lib as L
+    A, B, C, D = W.rho_band(4096, 512, 0.45, 0.55, seed=8)
+    rho = orc.rho_rows_all(A, B, C)
+    assert rho.max() >= 0.5
+    xt = orc.thomas_cyclic(A, B, C, D) if cyclic else orc.thomas(A, B, C, D)
+    for version in (1, 2):
+        x, s = run(cuda, f"filtered_v{version}", A, B, C, D, 8, cyclic=cyclic, rho=rho)
+        assert s.last_stats()["filtered_exact"] == 1
+        assert rel_err(x, xt) <= 1e-12
+        x, s = run(cuda, f"filtered_v{version}", A, B, C, D, 8, cyclic=cyclic, rho=rho,
+                   flags=L.FLAG_REFERENCE_ORDER)
+        xo, Jo = orc.filtered(A, B, C, D, 8, version, cyclic, 1e-3, rho, orc.J_DEVICE)
+        assert list(Jo) == [63] * 8
+        assert np.array_equal(x, xo)
+
+
+def test_filtered_untileable_shape_falls_back_to_reference_order_pascal(cuda, orc):
+    # odd n_sys (no TMA) and 100 rows (not a multiple of 16): the exact fallback
+    # runs the reference-order PaScaL kernel, bit-identical to the oracle's
+    A, B, C, D = W.diag_dominant(101, 100, 1.0, 10.0, seed=12)
+    rho = orc.rho_rows_all(A, B, C)
+    x, s = run(cuda, "filtered_v2", A, B, C, D, 4, rho=rho)
+    assert s.last_stats()["filtered_exact"] == 1
+    assert np.array_equal(x, orc.pascal(A, B, C, D, 4))
+
+
+@pytest.mark.parametrize("version", [1, 2])
 def test_filtered_host_j_semantics(cuda, orc, version):
     A, B, C, D = W.diag_dominant(80, 160, 0.1, 1.0, seed=42)
     rho = orc.rho_rows_all(A, B, C)
     from filtered_tdma_b200 import _lib as L
-    x, s = run(cuda, f"filtered_v{version}", A, B, C, D, 4, rho=rho, flags=L.FLAG_J_HOST)
+    x, s = run(cuda, f"filtered_v{version}", A, B, C, D, 4, rho=rho,
+               flags=L.FLAG_J_HOST | L.FLAG_REFERENCE_ORDER)
     xo, Jo = orc.filtered(A, B, C, D, 4, version, False, 1e-3, rho, orc.J_HOST)
     assert np.array_equal(x, xo)
 
@@ -177,7 +261,8 @@ def test_filtered_set_rho_system0(cuda, orc):
     # set_rho reads system 0's column, like the reference's k_set_rho.
     A, B, C, D = W.diag_dominant(64, 96, seed=3)
     n_row, n_sys = D.shape
-    s = Solver("filtered_v2", n_sys, n_row, 4)
+    from filtered_tdma_b200 import _lib as L
+    s = Solver("filtered_v2", n_sys, n_row, 4, flags=L.FLAG_REFERENCE_ORDER)
     s.set_eps_constant(1e-3)
     dA, dB, dC, dD = dev(cuda, A, B, C, D)
     s.set_rho(dA, dB, dC)
@@ -215,12 +300,21 @@ def test_dropin_classes(cuda, orc):
         b.solve(dA, dB, dC, dD)
         assert np.array_equal(host(dD), xt)  # nprocs = 1: serial Thomas
         assert b.last_comm_ms() == 0.0 and b.last_gpu_ms() > 0.0
-    f = FilteredTDMACUDA(n_sys, n_row, 0, 4, None, -2, -2, 1e-3)
-    dA, dB, dC, dD = dev(cuda, A, B, C, D)
-    f.set_rho_device(dA, dB, dC)
-    f.solve_filtered_v2(dA, dB, dC, dD)
+    # m = 16 rows per segment, J = 22 >= m - 2: the exact fallback by default,
+    # the reference's Filtered bit for bit with the reference-order flag
+    from filtered_tdma_b200 import _lib as L
     xo, Jo = orc.filtered(A, B, C, D, 4, 2, False, 1e-3, orc.rho_rows(A, B, C, 0), orc.J_DEVICE)
-    assert np.array_equal(host(dD), xo) and f.last_J() == Jo[0]
+    assert min(Jo) >= 16 - 2
+    for flags, want, exact in ((0, None, True), (L.FLAG_REFERENCE_ORDER, xo, False)):
+        f = FilteredTDMACUDA(n_sys, n_row, 0, 4, None, -2, -2, 1e-3, flags=flags)
+        dA, dB, dC, dD = dev(cuda, A, B, C, D)
+        f.set_rho_device(dA, dB, dC)
+        f.solve_filtered_v2(dA, dB, dC, dD)
+        if exact:
+            assert rel_err(host(dD), xt) <= 1e-12
+        else:
+            assert np.array_equal(host(dD), want)
+        assert f.last_J() == Jo[0]
 
 
 def test_full_size_properties(cuda):

@@ -59,6 +59,42 @@ def test_gpu_steps_graph_and_eager_agree_non_cubic(cuda, orc):
     assert _rel(a.cpu().numpy()[1:-1, 1:-1, 1:-1], ref[1:-1, 1:-1, 1:-1]) <= 1e-12
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("grid", [(16, 384, 16), (16, 16, 512), (256, 16, 16), (16, 16, 256),
+                                  (128, 16, 16)])
+def test_gpu_step_long_sweeps_match_oracle(cuda, orc, grid):
+    # the shared-matrix sweeps at the sub-segment counts of the 256 x 384 x 512
+    # step: Y 384 rows (24 sub-segments, a 384-thread CTA), Z 512 rows (32, one
+    # 512-thread CTA), X 256 rows (16, two 256-thread CTAs per SM); also 16 and
+    # 8 sub-segments along Z and X
+    from filtered_tdma_b200.heat import HeatADI, dt_from_rho
+    ix, iy, iz = grid
+    dt = dt_from_rho(1.0 / 3.0, iz, option="strong")
+    h = HeatADI(ix, iy, iz, dt=dt)
+    th = h.field(cuda)
+    h.step(th, 2)
+    ref = H.initial(ix, iy, iz)
+    for _ in range(2):
+        ref = H.step(ref, dt)
+    assert _rel(th.cpu().numpy()[1:-1, 1:-1, 1:-1], ref[1:-1, 1:-1, 1:-1]) <= 1e-12
+
+
+@pytest.mark.gpu
+def test_gpu_step_benched_grid_matches_oracle(cuda, orc):
+    # one step of the benched 256 x 384 x 512 grid (Z 512, Y 384, X 256 rows)
+    from filtered_tdma_b200.heat import HeatADI, dt_from_rho
+    ix, iy, iz = 256, 384, 512
+    dt = dt_from_rho(1.0 / 3.0, iz, option="strong")
+    h = HeatADI(ix, iy, iz, dt=dt)
+    th = h.field(cuda)
+    h.step(th, 1)
+    got = th.cpu().numpy()[1:-1, 1:-1, 1:-1]
+    del th
+    h.close()
+    ref = H.step(H.initial(ix, iy, iz), dt)[1:-1, 1:-1, 1:-1]
+    assert _rel(got, ref) <= 1e-12
+
+
 def test_heat_argument_checks():
     import ctypes
     from filtered_tdma_b200 import _lib as L

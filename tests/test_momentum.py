@@ -34,6 +34,29 @@ def test_sweep_matches_oracle(cuda, orc, direction, comp):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("comp", [0, 2])
+def test_adi_benched_256_axes_matches_oracle(cuda, orc, comp):
+    # the benched channel grid's sweep length, 256 rows (16 sub-segments) along
+    # every axis: periodic x and y, stretched walls in z; the z sweep's systems
+    # span the full 256 x 256 plane, x and y are thinner to keep the oracle short
+    import torch
+    from filtered_tdma_b200.momentum import ChannelMomentum
+    c = 0.5 * (1.0 / 180.0) * 1e-3 * 50
+    for nx, ny, nz in ((256, 256, 32), (32, 256, 256), (256, 32, 256)):
+        m = ChannelMomentum(nx, ny, nz, gamma3=1.5)
+        rng = np.random.default_rng(50 + nx + 2 * ny + 3 * nz + comp)
+        rhs = rng.uniform(-1, 1, m.shape)
+        d_rhs = torch.from_numpy(rhs).to(cuda)
+        d_q = torch.zeros_like(d_rhs)
+        m.adi(comp, d_rhs, d_q, c)
+        torch.cuda.synchronize()
+        assert m.status() == 0
+        ref = MO.adi(rhs, m.metrics, comp, c, (True, True))
+        assert _rel(d_q.cpu().numpy()[1:-1, 1:-1, 1:-1], ref[1:-1, 1:-1, 1:-1]) <= 1e-12
+        m.close()
+
+
+@pytest.mark.gpu
 def test_adi_matches_oracle_walls_only(cuda, orc):
     import torch
     from filtered_tdma_b200.momentum import ChannelMomentum
@@ -70,6 +93,46 @@ def test_factor_tables_follow_the_coefficient(cuda, orc):
             torch.cuda.synchronize()
             ref = MO.sweep(q, m.metrics, direction, 1, c, direction < 2)
             assert _rel(out.cpu().numpy()[1:-1, 1:-1, 1:-1], ref[1:-1, 1:-1, 1:-1]) <= 1e-12
+    assert m.status() == 0
+
+
+@pytest.mark.gpu
+def test_graph_replays_leave_the_cached_tables_alone(cuda, orc):
+    # normal call with c1 (caches its tables), capture with c2, normal call with
+    # c1, replay the c2 graph, normal call with c1 again: the last call must
+    # still use c1's tables (bit-identical to a fresh handle), and the replay
+    # must give c2's solution
+    import torch
+    from filtered_tdma_b200.momentum import ChannelMomentum
+    m = ChannelMomentum(64, 32, 48, gamma3=1.5)
+    fresh = ChannelMomentum(64, 32, 48, gamma3=1.5)
+    rng = np.random.default_rng(44)
+    q = rng.uniform(-1, 1, m.shape)
+    c1, c2 = 0.05, 0.2
+    stream = torch.cuda.Stream()
+    s = stream.cuda_stream
+    for direction in (2, 1, 0):
+        dq = torch.from_numpy(q).to(cuda)
+        out = torch.zeros_like(dq)
+        gout = torch.zeros_like(dq)
+        with torch.cuda.stream(stream):
+            m.sweep(direction, 1, dq, out, c1, stream=s)
+        stream.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            m.sweep(direction, 1, dq, gout, c2, stream=s)
+        with torch.cuda.stream(stream):
+            m.sweep(direction, 1, dq, out, c1, stream=s)
+            g.replay()
+            m.sweep(direction, 1, dq, out, c1, stream=s)
+        stream.synchronize()
+        want = torch.zeros_like(dq)
+        fresh.sweep(direction, 1, dq, want, c1)
+        torch.cuda.synchronize()
+        assert torch.equal(out, want)
+        ref2 = MO.sweep(q, m.metrics, direction, 1, c2, direction < 2)
+        assert _rel(gout.cpu().numpy()[1:-1, 1:-1, 1:-1], ref2[1:-1, 1:-1, 1:-1]) <= 1e-12
+        del g
     assert m.status() == 0
 
 

@@ -3,9 +3,11 @@
 It serves callers that may not allocate device memory (a framework that owns
 the memory pool, latency-critical loops, contexts where allocation calls are
 forbidden): its scratch is a fixed array inside the library.  Here it must give
-exactly what the handle-based serial Thomas (btdma_solve with P = 1) gives —
-bit-identical, the tolerance every P = 1 test uses — on two calls in a row (the
-array keeps the first call's contents), and refuse batches above its limit.
+exactly what the oracle's serial Thomas (the reference's tdma_many restated)
+gives — bit-identical, the bar of every P = 1 test — and exactly what the
+handle-based entry point (btdma_solve with P = 1) gives, on two calls in a row
+(the array keeps the first call's contents), and refuse batches above its
+limit.
 
 This file is collected last so that a failure here cannot hide another test;
 it also passes on its own in a fresh process.
@@ -41,12 +43,13 @@ def _solve_handle(cuda, A, B, C, D):
     return dD.cpu().numpy()
 
 
-def test_noalloc_matches_handle_solve_twice(cuda):
+def test_noalloc_matches_oracle_and_handle_solve_twice(cuda, orc):
     # Two different batches back to back: the second call reuses the scratch
     # array the first one left behind.
     batches = [W.diag_dominant(4096, 64, seed=21), W.heat_sweep(2048, 512, r=1.0, seed=22)]
     for A, B, C, D in batches:
         x_na = _solve_noalloc(cuda, A, B, C, D)
+        assert np.array_equal(x_na, orc.thomas(A, B, C, D))
         x_h = _solve_handle(cuda, A, B, C, D)
         assert np.array_equal(x_na, x_h)
 
