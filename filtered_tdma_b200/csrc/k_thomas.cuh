@@ -7,8 +7,9 @@
 // divides row 0 by B instead of multiplying by 1/B
 // (libs/pascal_tdma/gpu/tdma_local_cuda.cu:43-44), so it is not the bit oracle.
 //
-// The forward sweep keeps the running (c', d') in registers and spills c' to the
-// handle's scratch and d' to X; the backward sweep reads them back.  Loads are
+// thomas_f64_kernel: the forward sweep keeps the running (c', d') in registers
+// and spills c' to the handle's scratch and d' to X; the backward sweep reads
+// them back.  thomas_staged_kernel (short systems) keeps both on chip.  Loads are
 // issued a block of UNR rows ahead of the arithmetic (X may alias D, so the
 // compiler cannot hoist them itself).
 #pragma once
@@ -92,6 +93,132 @@ thomas_f64_kernel(const double* __restrict__ A, const double* __restrict__ B,
         finite &= isfinite(x);
     }
     if (!finite) raise_status(status, ST_NONFINITE);
+}
+
+// Staged serial Thomas for short systems (n_row <= THOMAS_STAGED_MAX_ROWS),
+// bit-identical to thomas_f64_kernel and to tdma_many, at the algorithmic
+// 40 B/row: one warp per CTA owns 32 consecutive systems; their C and D rows
+// come into shared memory by TMA in chunks of 16 rows (one mbarrier per chunk,
+// so the sweep starts on the first chunk), and the sweep overwrites them with
+// c' and d' and then x in place — the scratch never leaves the chip
+// (thomas_f64_kernel writes c' and d' to HBM and reads them back: 72 B/row).
+// A and B go straight from HBM into registers, a chunk ahead of the sweep.
+// x leaves by TMA stores of the D tile.  Rows past n_row and systems past
+// n_sys in the last chunk / CTA are zero-filled by the loads and clipped by
+// the stores.  Needs 16-byte aligned C, D, X and an even n_sys (TMA).
+constexpr int THOMAS_STAGED_MAX_ROWS = 128;
+constexpr int THOMAS_STAGED_SYS = 32;
+constexpr int THOMAS_STAGED_CHUNK = 16;
+
+__host__ __device__ __forceinline__ size_t thomas_staged_smem_bytes(int n_row) {
+    const int nch = (n_row + THOMAS_STAGED_CHUNK - 1) / THOMAS_STAGED_CHUNK;
+    return 2ull * nch * THOMAS_STAGED_CHUNK * THOMAS_STAGED_SYS * sizeof(double) +
+           (size_t)nch * sizeof(uint64_t) + 128;
+}
+
+__global__ void __launch_bounds__(THOMAS_STAGED_SYS)
+thomas_staged_kernel(const __grid_constant__ CUtensorMap tmC,
+                     const __grid_constant__ CUtensorMap tmD,
+                     const __grid_constant__ CUtensorMap tmX, const double* __restrict__ A,
+                     const double* __restrict__ B, int n_sys, int n_row, unsigned* status) {
+    using E = Exact64;
+    constexpr int S = THOMAS_STAGED_SYS, CH = THOMAS_STAGED_CHUNK;
+    extern __shared__ unsigned char smem_raw[];
+    double* TC = reinterpret_cast<double*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    const int nch = (n_row + CH - 1) / CH;
+    double* TD = TC + (size_t)nch * CH * S;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(TD + (size_t)nch * CH * S);
+    const int s = threadIdx.x;
+    const int g = blockIdx.x;
+    const int sys = g * S + s;
+    const bool valid = sys < n_sys;
+    const size_t ns = (size_t)n_sys;
+
+    if (s == 0) {
+        for (int c = 0; c < nch; ++c) mbar_init(&bars[c], 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    if (s == 0) {
+        for (int c = 0; c < nch; ++c) {
+            mbar_expect_tx(&bars[c], 2u * CH * S * sizeof(double));
+            tma_load_2d(TC + (size_t)c * CH * S, &tmC, g * S, c * CH, &bars[c]);
+            tma_load_2d(TD + (size_t)c * CH * S, &tmD, g * S, c * CH, &bars[c]);
+        }
+    }
+    // A and B of chunk c into registers (0 and 1 outside the batch)
+    auto load_ab = [&](int c, double (&a)[CH], double (&b)[CH]) {
+#pragma unroll
+        for (int u = 0; u < CH; ++u) {
+            const int j = c * CH + u;
+            const bool in = valid && j < n_row;
+            a[u] = in ? __ldg(A + (size_t)j * ns + sys) : 0.0;
+            b[u] = in ? __ldg(B + (size_t)j * ns + sys) : 1.0;
+        }
+    };
+    double ac[CH], bc[CH], an[CH], bn[CH];
+    load_ab(0, ac, bc);
+    if (nch > 1) load_ab(1, an, bn);
+    bool ok = mbar_wait_bounded(&bars[0], 0, status);
+#define TS(Z, j) Z[(size_t)(j) * S + s]
+    // row 0: inv = 1/B, d = D inv, c = C inv (tdma_local.cpp:17-22)
+    double c, d;
+    {
+        const double inv_b = E::rcp(bc[0]);
+        d = E::mul(TS(TD, 0), inv_b);
+        c = E::mul(TS(TC, 0), inv_b);
+        TS(TD, 0) = d;
+        TS(TC, 0) = c;
+    }
+    for (int ch = 0; ch < nch; ++ch) {
+        if (ch > 0) {
+#pragma unroll
+            for (int u = 0; u < CH; ++u) {
+                ac[u] = an[u];
+                bc[u] = bn[u];
+            }
+            if (ch + 1 < nch) load_ab(ch + 1, an, bn);
+            if (ok) ok = mbar_wait_bounded(&bars[ch], 0, status);
+        }
+#pragma unroll
+        for (int u = 0; u < CH; ++u) {
+            const int j = ch * CH + u;
+            if (j == 0 || j >= n_row) continue;
+            const double a = ac[u];
+            const double r = E::rcp(E::sub(bc[u], E::mul(a, c)));
+            d = E::mul(r, E::sub(TS(TD, j), E::mul(a, d)));
+            c = E::mul(r, TS(TC, j));
+            TS(TD, j) = d;
+            TS(TC, j) = c;
+        }
+    }
+    // backward substitution: x_j = d'_j - c'_j x_{j+1}; x_{n-1} = d'_{n-1}
+    double x = d;
+    bool finite = isfinite(x);
+#pragma unroll 8
+    for (int j = n_row - 2; j >= 0; --j) {
+        x = E::sub(TS(TD, j), E::mul(TS(TC, j), x));
+        TS(TD, j) = x;
+        finite &= isfinite(x);
+    }
+#undef TS
+    if (valid && !finite) raise_status(status, ST_NONFINITE);
+    fence_async_shared();
+    __syncwarp();
+    if (s == 0) {
+        for (int c2 = 0; c2 < nch; ++c2)
+            tma_store_2d(&tmX, g * S, c2 * CH, TD + (size_t)c2 * CH * S);
+        tma_store_commit();
+        tma_store_wait_read();
+    }
+    if (!ok) {
+        // a chunk wait gave up: one more bounded chance for the copies to land
+        // before this CTA's shared memory is released
+        if (s == 0)
+            for (int c2 = 0; c2 < nch; ++c2) mbar_wait_bounded(&bars[c2], 0, nullptr, 1u << 16);
+    }
+    __syncwarp();
 }
 
 // Periodic Thomas with the correction vector e (tdma_local.cpp:108-208).

@@ -57,11 +57,24 @@ def run(cuda, method, A, B, C, D, P, cyclic=False, out=False, rho=None, eps_c=1e
 
 
 SHAPES_P1 = [(1, 1), (3, 2), (5, 3), (31, 17), (64, 64), (4096, 64), (1000, 129), (257, 512)]
+# even n_sys and at most 128 rows: the staged kernel (c', d' in shared memory),
+# including ragged last chunks and a last CTA of fewer than 32 systems
+SHAPES_P1_STAGED = [(2, 1), (2, 2), (34, 3), (100, 16), (66, 17), (4096, 64), (1000, 100),
+                    (262, 128), (16384, 128), (65536, 64)]
 
 
 @pytest.mark.parametrize("n_sys,n_row", SHAPES_P1)
 def test_thomas_bit_exact(cuda, orc, n_sys, n_row):
     A, B, C, D = W.diag_dominant(n_sys, n_row, seed=n_sys + n_row)
+    x, _ = run(cuda, "pascal", A, B, C, D, 1)
+    assert np.array_equal(x, orc.thomas(A, B, C, D))
+    x2, _ = run(cuda, "pascal", A, B, C, D, 1, out=True)
+    assert np.array_equal(x2, x)
+
+
+@pytest.mark.parametrize("n_sys,n_row", SHAPES_P1_STAGED)
+def test_thomas_staged_bit_exact(cuda, orc, n_sys, n_row):
+    A, B, C, D = W.row_varying(n_sys, n_row, seed=n_sys + 3 * n_row)
     x, _ = run(cuda, "pascal", A, B, C, D, 1)
     assert np.array_equal(x, orc.thomas(A, B, C, D))
     x2, _ = run(cuda, "pascal", A, B, C, D, 1, out=True)

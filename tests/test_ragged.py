@@ -63,6 +63,25 @@ def test_ragged_config_shape_fp64(cuda, orc):
 
 
 @pytest.mark.gpu
+def test_ragged_full_config_10000(cuda, orc):
+    # the whole ragged configuration: 10000 systems, n log-uniform in
+    # [16, 4096] (7.3 M rows), 25 % periodic, r log-uniform in [0.05, 20],
+    # autotuned; FP64 and FP32 storage (on the widened values), every system
+    # within 1e-12 of the oracle's serial (periodic) Thomas
+    A, B, C, D, off, per = W.ragged_batch(10000, seed=5)
+    assert int(off[-1]) > 7_000_000 and per.sum() > 2000
+    ref = ragged_oracle(orc, A, B, C, D, off, per)
+    x, plan = solve_on_device(cuda, (A, B, C, D), off, per, tune=True)
+    assert per_system_err(x, ref, off) <= 1e-12
+    assert sum(b["n_systems"] for b in plan) == 10000
+    A32, B32, C32, D32 = (v.astype(np.float32) for v in (A, B, C, D))
+    ref32 = ragged_oracle(orc, *(v.astype(np.float64) for v in (A32, B32, C32, D32)), off, per)
+    x32, _ = solve_on_device(cuda, (A32, B32, C32, D32), off, per, precision=L.FP32_STORE,
+                             tune=True)
+    assert per_system_err(x32, ref32, off) <= 1e-12
+
+
+@pytest.mark.gpu
 def test_ragged_autotuned_and_inplace(cuda, orc):
     A, B, C, D, off, per = W.ragged_batch(300, seed=51)
     ref = ragged_oracle(orc, A, B, C, D, off, per)
