@@ -33,6 +33,7 @@ EXPORTS = (
     "btdma_poisson_solve", "btdma_poisson_status", "btdma_momentum_create",
     "btdma_momentum_destroy", "btdma_momentum_sweep", "btdma_momentum_adi", "btdma_momentum_status",
     "btdma_selftest_wait_timeout", "btdma_set_tile_shape", "btdma_ragged_set_plan",
+    "btdma_momentum_set_backend",
 )
 NOALLOC_MAX_ELEMS = 1 << 20
 REFINE_MAX_SWEEPS = 4
@@ -119,6 +120,7 @@ def lib():
         L.btdma_momentum_sweep.argtypes = [vp, i, i, vp, vp, d, vp]
         L.btdma_momentum_adi.argtypes = [vp, i, vp, vp, d, vp]
         L.btdma_momentum_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint), vp]
+        L.btdma_momentum_set_backend.argtypes = [vp, i, i, i, d]
         L.btdma_selftest_wait_timeout.argtypes = [i, ctypes.POINTER(ctypes.c_uint), vp]
         L.btdma_last_error.restype = ctypes.c_char_p
         for name in EXPORTS:

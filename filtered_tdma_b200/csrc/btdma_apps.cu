@@ -405,6 +405,15 @@ struct btdma_momentum {
         cudaStream_t stream = nullptr;
     } gkey[3][3];
     unsigned* status = nullptr;
+    // Array-based backend (btdma_momentum_set_backend): the method and
+    // segments of the per-direction library handles, the raw axis factors
+    // [dir][comp][ar, cr][n] and the explicit A, B, C, X of a sweep.
+    int backend = BTDMA_PASCAL;
+    double eps_constant = 1.0e-12;
+    double* raw = nullptr;
+    size_t raw_off[3][3] = {};
+    double* coef = nullptr;  // A, B, C, X, each nx * ny * nz
+    btdma_t hd[3] = {};
 };
 
 int btdma_momentum_create(int nx, int ny, int nz, const double* dx0, const double* dmx0,
@@ -428,18 +437,21 @@ int btdma_momentum_create(int nx, int ny, int nz, const double* dx0, const doubl
     // r = 1..n, staggered when comp == dir;  a = -c ta, c = -c tc, b = 1 + c tb
     const double* dxs[3] = {dx0, dx1, dx2};
     const double* dms[3] = {dmx0, dmx1, dmx2};
-    std::vector<double> tab;
-    size_t off[3][3];
+    std::vector<double> tab, raw;
+    size_t off[3][3], roff[3][3];
     for (int d = 0; d < 3; ++d)
         for (int comp = 0; comp < 3; ++comp) {
             off[d][comp] = tab.size();
+            roff[d][comp] = raw.size();
             const int m = n[d];
-            std::vector<double> ta(m), tb(m), tc(m);
+            std::vector<double> ta(m), tb(m), tc(m), ra(m), rc(m);
             const double* dx = dxs[d];
             const double* dm = dms[d];
             for (int r = 1; r <= m; ++r) {
                 const double ar = comp == d ? 1.0 / (dm[r] * dx[r - 1]) : 1.0 / (dx[r] * dm[r]);
                 const double cr = comp == d ? 1.0 / (dm[r] * dx[r]) : 1.0 / (dx[r] * dm[r + 1]);
+                ra[r - 1] = ar;
+                rc[r - 1] = cr;
                 double a_ = ar, b_ = ar + cr, c_ = cr;
                 if (d == 2) {  // no-slip walls at both ends (one rank holds all of z)
                     const bool is_w = comp == 2;
@@ -460,6 +472,8 @@ int btdma_momentum_create(int nx, int ny, int nz, const double* dx0, const doubl
             tab.insert(tab.end(), ta.begin(), ta.end());
             tab.insert(tab.end(), tb.begin(), tb.end());
             tab.insert(tab.end(), tc.begin(), tc.end());
+            raw.insert(raw.end(), ra.begin(), ra.end());
+            raw.insert(raw.end(), rc.begin(), rc.end());
         }
     btdma_momentum* h = new btdma_momentum();
     h->g.nx = nx;
@@ -468,6 +482,7 @@ int btdma_momentum_create(int nx, int ny, int nz, const double* dx0, const doubl
     h->pbc[0] = pbc_x ? 1 : 0;
     h->pbc[1] = pbc_y ? 1 : 0;
     std::memcpy(h->tab_off, off, sizeof off);
+    std::memcpy(h->raw_off, roff, sizeof roff);
     h->gstride = gen_table_doubles(std::max(nx, std::max(ny, nz)));
     auto cleanup = [&](int code) {
         btdma_momentum_destroy(h);
@@ -478,6 +493,9 @@ int btdma_momentum_create(int nx, int ny, int nz, const double* dx0, const doubl
             cudaSuccess ||
         cudaMalloc(&h->buf, sizeof(double) * (size_t)nx * ny * nz) != cudaSuccess ||
         cudaMalloc(&h->gtab, sizeof(double) * 18 * h->gstride) != cudaSuccess ||
+        cudaMalloc(&h->raw, sizeof(double) * raw.size()) != cudaSuccess ||
+        cudaMemcpy(h->raw, raw.data(), sizeof(double) * raw.size(), cudaMemcpyHostToDevice) !=
+            cudaSuccess ||
         cudaMalloc(&h->status, sizeof(unsigned)) != cudaSuccess ||
         cudaMemset(h->status, 0, sizeof(unsigned)) != cudaSuccess)
         return cleanup(fail(BTDMA_ERR_CUDA, "momentum buffers: %s",
@@ -492,7 +510,46 @@ int btdma_momentum_destroy(btdma_momentum_t h) {
     cudaFree(h->buf);
     cudaFree(h->gtab);
     cudaFree(h->status);
+    cudaFree(h->raw);
+    cudaFree(h->coef);
+    for (auto& d : h->hd) btdma_destroy(d);
     delete h;
+    return BTDMA_OK;
+}
+
+int btdma_momentum_set_backend(btdma_momentum_t h, int method, int P, int flags,
+                               double eps_constant) {
+    if (!h) return fail(BTDMA_ERR_ARG, "null handle");
+    if (method < BTDMA_PASCAL || method > BTDMA_FILTERED_V2)
+        return fail(BTDMA_ERR_ARG, "unknown method %d", method);
+    if (method != BTDMA_PASCAL && P < 1) return fail(BTDMA_ERR_ARG, "P must be >= 1");
+    if (!(eps_constant > 0.0)) return fail(BTDMA_ERR_ARG, "eps_constant must be positive");
+    for (auto& d : h->hd) {
+        btdma_destroy(d);
+        d = nullptr;
+    }
+    h->backend = BTDMA_PASCAL;
+    if (method == BTDMA_PASCAL) return BTDMA_OK;
+    const MomGeom& g = h->g;
+    const int n[3] = {g.nx, g.ny, g.nz};
+    const size_t cells = (size_t)g.nx * g.ny * g.nz;
+    if (!h->coef && cudaMalloc(&h->coef, sizeof(double) * 4 * cells) != cudaSuccess)
+        return fail(BTDMA_ERR_CUDA, "momentum coefficient arrays: %s",
+                    cudaGetErrorString(cudaGetLastError()));
+    for (int d = 0; d < 3; ++d) {
+        const int rc = btdma_create(method, (int)(cells / n[d]), n[d], P, BTDMA_FP64, flags,
+                                    &h->hd[d]);
+        if (rc) {
+            for (auto& x : h->hd) {
+                btdma_destroy(x);
+                x = nullptr;
+            }
+            return rc;
+        }
+        btdma_set_eps_constant(h->hd[d], eps_constant);
+    }
+    h->backend = method;
+    h->eps_constant = eps_constant;
     return BTDMA_OK;
 }
 
@@ -504,6 +561,48 @@ int btdma_momentum_sweep(btdma_momentum_t h, int dir, int comp, const double* q,
     const MomGeom& g = h->g;
     const int n[3] = {g.nx, g.ny, g.nz};
     const int n_sys = g.nx * g.ny * g.nz / n[dir];
+    if (h->backend != BTDMA_PASCAL) {
+        // the reference's sequence (adi_{z,y,x}_): build A, B, C, D, set rho
+        // from system 0's column, solve with the handle's method, scatter
+        const size_t cells = (size_t)g.nx * g.ny * g.nz;
+        double* A = h->coef;
+        double* B = A + cells;
+        double* C = B + cells;
+        double* X = C + cells;
+        const dim3 b1(128, 1, 1), bt(MOM_TILE, 8, 1);
+        if (dir == 2)
+            mom_gather_kernel<2><<<dim3((g.nx + 127) / 128, (g.ny + MOM_GR - 1) / MOM_GR, g.nz),
+                                   b1, 0, stream>>>(q, h->buf, g, comp == 2 ? 1 : 0);
+        else if (dir == 1)
+            mom_gather_kernel<1><<<dim3((g.nx + 127) / 128, (g.nz + MOM_GR - 1) / MOM_GR, g.ny),
+                                   b1, 0, stream>>>(q, h->buf, g, 0);
+        else
+            mom_gather_x_kernel<<<dim3((g.nx + MOM_TILE - 1) / MOM_TILE,
+                                       (g.ny + MOM_TILE - 1) / MOM_TILE, g.nz), bt, 0, stream>>>(
+                q, h->buf, g);
+        CK(cudaGetLastError());
+        const double* ra = h->raw + h->raw_off[dir][comp];
+        mom_coef_kernel<<<std::min<size_t>((cells + 255) / 256, 148 * 16), 256, 0, stream>>>(
+            A, B, C, ra, ra + n[dir], n[dir], n_sys, c, dir == 2 ? 1 : 0, comp == 2 ? 1 : 0);
+        CK(cudaGetLastError());
+        const bool cyc = dir < 2 && h->pbc[dir] != 0;
+        btdma_t hd = h->hd[dir];
+        int rc = btdma_set_rho(hd, A, B, C, n_sys, n[dir], stream);
+        if (!rc) rc = btdma_solve_out(hd, A, B, C, h->buf, X, n_sys, n[dir], cyc ? 1 : 0, stream);
+        if (rc) return rc;
+        if (dir == 2)
+            mom_scatter_kernel<2><<<dim3((g.nx + 127) / 128, (g.ny + MOM_GR - 1) / MOM_GR, g.nz),
+                                    b1, 0, stream>>>(X, dst, g);
+        else if (dir == 1)
+            mom_scatter_kernel<1><<<dim3((g.nx + 127) / 128, (g.nz + MOM_GR - 1) / MOM_GR, g.ny),
+                                    b1, 0, stream>>>(X, dst, g);
+        else
+            mom_scatter_x_kernel<<<dim3((g.ny + MOM_TILE - 1) / MOM_TILE,
+                                        (g.nx + MOM_TILE - 1) / MOM_TILE, g.nz), bt, 0, stream>>>(
+                X, dst, g);
+        CK(cudaGetLastError());
+        return BTDMA_OK;
+    }
     TileArgs t = {};
     t.cs = c;
     t.ga = h->tab + h->tab_off[dir][comp];
@@ -588,5 +687,12 @@ int btdma_momentum_status(btdma_momentum_t h, unsigned* status, cudaStream_t str
     CK(cudaStreamSynchronize(stream));
     CK(cudaMemsetAsync(h->status, 0, sizeof(unsigned), stream));
     CK(cudaStreamSynchronize(stream));
+    for (btdma_t hd : h->hd) {  // the array-based backend's handles
+        if (!hd) continue;
+        unsigned s = 0;
+        const int rc = btdma_status(hd, &s);
+        if (rc) return rc;
+        *status |= s;
+    }
     return BTDMA_OK;
 }

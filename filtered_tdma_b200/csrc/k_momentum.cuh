@@ -59,6 +59,72 @@ __global__ void __launch_bounds__(128) mom_gather_kernel(const double* __restric
     }
 }
 
+// Inverse of mom_gather_kernel (z and y sweeps): the solution X in the sweep
+// layout back into the field's interior.  Same grid and block.
+template <int DIR>
+__global__ void __launch_bounds__(128) mom_scatter_kernel(const double* __restrict__ X,
+                                                          double* __restrict__ q,
+                                                          const MomGeom g) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int a0 = blockIdx.y * MOM_GR + 1, b = blockIdx.z + 1;  // z: (j, k); y: (k, j)
+    const int na = DIR == 2 ? g.ny : g.nz;
+    if (i > g.nx) return;
+    double v[MOM_GR];
+#pragma unroll
+    for (int r = 0; r < MOM_GR; ++r) {
+        const int a = a0 + r;
+        const int j = DIR == 2 ? a : b, k = DIR == 2 ? b : a;
+        const size_t o = DIR == 2 ? ((size_t)(k - 1) * g.ny + (j - 1)) * g.nx + (i - 1)
+                                  : ((size_t)(j - 1) * g.nz + (k - 1)) * g.nx + (i - 1);
+        v[r] = a <= na ? X[o] : 0.0;
+    }
+#pragma unroll
+    for (int r = 0; r < MOM_GR; ++r) {
+        const int a = a0 + r;
+        if (a > na) break;
+        const int j = DIR == 2 ? a : b, k = DIR == 2 ? b : a;
+        q[mom_fld(g, i, j, k)] = v[r];
+    }
+}
+
+// Explicit coefficients of one sweep for the array-based solvers (the
+// Filtered backend), in the arithmetic and order of k_build_{x,y,z}
+// (apps/channel_gpu/MomentumSolverGPU.cu:135-210): for row r with the axis
+// factors ar, cr,  a = -c ar, cc = -c cr, b = 1 - a - cc; the z walls (one
+// rank holds all of z): row 0 a = 0 and b += c ar, the last row cc = 0 and
+// b += c cr (velocity components along the wall), or the w row 0 pinned to
+// (0, 1, 0).  Every system of the sweep has the same rows.  Grid-stride over
+// n_row x n_sys; round-to-nearest operations, no contraction.
+__global__ void mom_coef_kernel(double* __restrict__ A, double* __restrict__ B,
+                                double* __restrict__ C, const double* __restrict__ ar_,
+                                const double* __restrict__ cr_, int n_row, int n_sys, double c,
+                                int walls, int is_w) {
+    const size_t n = (size_t)n_row * n_sys;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+         e += (size_t)gridDim.x * blockDim.x) {
+        const int r = (int)(e / (size_t)n_sys);
+        const double ar = ar_[r], cr = cr_[r];
+        double a = -__dmul_rn(c, ar), cc = -__dmul_rn(c, cr);
+        double b = __dsub_rn(__dsub_rn(1.0, a), cc);
+        if (walls && r == 0) {
+            a = 0.0;
+            if (!is_w) b = __dadd_rn(b, __dmul_rn(c, ar));
+        }
+        if (walls && r == n_row - 1) {
+            cc = 0.0;
+            if (!is_w) b = __dadd_rn(b, __dmul_rn(c, cr));
+        }
+        if (walls && is_w && r == 0) {
+            a = 0.0;
+            b = 1.0;
+            cc = 0.0;
+        }
+        A[e] = a;
+        B[e] = b;
+        C[e] = cc;
+    }
+}
+
 constexpr int MOM_TILE = 32;
 
 // x sweep: (i, j) transposed through a shared 32 x 32 tile per k; block (32, 8).

@@ -54,6 +54,18 @@ class ChannelMomentum:
                                            float(c), stream))
         return q_out
 
+    def set_backend(self, method="pascal", P=1, flags=0, eps_constant=1.0e-12):
+        """Solver of the sweeps: "pascal" (default, tiled exact solve with
+        generated coefficients), or a Filtered method ("filtered", "filtered_v2"
+        or the integer method) with P segments: the reference channel's
+        build / set_rho / solve / scatter sequence on explicit arrays."""
+        if isinstance(method, str):
+            t = method.lower()
+            method = (L.PASCAL if t in ("pascal", "pascal_tdma") else
+                      L.FILTERED_V1 if t in ("filtered_v1",) else L.FILTERED_V2)
+        L.check(L.lib().btdma_momentum_set_backend(self._h, int(method), int(P), int(flags),
+                                                   float(eps_constant)))
+
     def status(self, stream=0) -> int:
         st = ctypes.c_uint()
         L.check(L.lib().btdma_momentum_status(self._h, ctypes.byref(st), stream))

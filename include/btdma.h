@@ -349,6 +349,23 @@ int btdma_momentum_adi(btdma_momentum_t h, int comp, double* rhs, double* q_out,
                        cudaStream_t stream);
 int btdma_momentum_status(btdma_momentum_t h, unsigned* status, cudaStream_t stream);
 
+/* Solver of the momentum sweeps: BTDMA_PASCAL (the default: the tiled exact
+ * solve with generated coefficients above), or BTDMA_FILTERED_V1 / _V2 with P
+ * segments per system, the backend string of the reference's channel solver
+ * (TdmaSolverGPU::parse_backend: anything but "pascal" selects
+ * FilteredTDMACUDA::solve_[cycl_]filtered_v2; apps/channel_gpu/
+ * TdmaSolverGPU.cpp:10-17, 37-51).  With a Filtered method every sweep runs the
+ * reference's sequence (MomentumSolverGPU::adi_{z,y,x}_, :261-313): A, B, C, D
+ * built into arrays in k_build_{x,y,z}'s arithmetic, rho from system 0's
+ * column (set_rho_device), the solve of a library handle of that method, P and
+ * flags (btdma_create; eps_constant as set_eps_constant, the reference passes
+ * dt), periodic x / y sweeps by the cyclic solve, then the scatter.  P = 1 is
+ * the serial Thomas algorithm, bit-identical to the reference's one-rank
+ * channel run with either backend.  Allocates four field-sized arrays on
+ * first use.  No counterpart of its own in the reference. */
+int btdma_momentum_set_backend(btdma_momentum_t h, int method, int P, int flags,
+                               double eps_constant);
+
 /* Self test of the failure path of every pipeline wait: a one-thread kernel
  * waits with each of the library's bounded waits (at most `limit` polls; a
  * hinted poll lasts up to 20 us, an unhinted one far less) on an mbarrier

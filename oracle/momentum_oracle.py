@@ -41,8 +41,9 @@ def _coeffs(dx, dm, n, comp, d, c):
     return a, b, cc
 
 
-def sweep(q, metrics, direction, comp, c, periodic):
-    """The solution of one sweep, scattered into a copy of q's interior."""
+def sweep(q, metrics, direction, comp, c, periodic, solver=None):
+    """The solution of one sweep, scattered into a copy of q's interior.
+    solver(A, B, C, D, periodic) -> x replaces the serial (periodic) Thomas."""
     nz, ny, nx = q.shape[0] - 2, q.shape[1] - 2, q.shape[2] - 2
     n = (nx, ny, nz)[direction]
     dx, dm = metrics[direction]
@@ -56,7 +57,10 @@ def sweep(q, metrics, direction, comp, c, periodic):
     A = np.repeat(a[:, None], n_sys, axis=1)
     B = np.repeat(b[:, None], n_sys, axis=1)
     C = np.repeat(cc[:, None], n_sys, axis=1)
-    x = O.thomas_cyclic(A, B, C, D) if periodic else O.thomas(A, B, C, D)
+    if solver is not None:
+        x = solver(A, B, C, D, periodic)
+    else:
+        x = O.thomas_cyclic(A, B, C, D) if periodic else O.thomas(A, B, C, D)
     out = q.copy()
     shape = list(np.moveaxis(inner, axis, 0).shape)
     out[1:-1, 1:-1, 1:-1] = np.moveaxis(x.reshape(shape), 0, axis)

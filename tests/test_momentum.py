@@ -136,6 +136,68 @@ def test_graph_replays_leave_the_cached_tables_alone(cuda, orc):
     assert m.status() == 0
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("direction", [0, 1, 2])
+def test_filtered_backend_one_segment_is_serial_thomas(cuda, orc, direction):
+    # the reference's channel on one rank: FilteredTDMACUDA with nprocs = 1
+    # falls back to the serial Thomas; P = 1 here is bit-identical to it
+    import torch
+    from filtered_tdma_b200.momentum import ChannelMomentum
+    m = ChannelMomentum(64, 32, 48, gamma3=1.5)
+    m.set_backend("filtered", P=1, eps_constant=1e-3)
+    rng = np.random.default_rng(70 + direction)
+    q = rng.uniform(-1, 1, m.shape)
+    c = 0.5 * (1.0 / 180.0) * 2e-3 * 50
+    for comp in (0, 2):
+        dq = torch.from_numpy(q).to(cuda)
+        out = torch.from_numpy(q).to(cuda)
+        m.sweep(direction, comp, dq, out, c)
+        torch.cuda.synchronize()
+        ref = MO.sweep(q, m.metrics, direction, comp, c, direction < 2)
+        assert np.array_equal(out.cpu().numpy(), ref)
+    assert m.status() == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("direction", [0, 1, 2])
+def test_filtered_backend_segments(cuda, orc, direction):
+    # Filtered v2 over 4 segments: with the reference-order flag bit-identical
+    # to the oracle's Filtered v2 on the same A, B, C, D (rho from system 0's
+    # column, the device J estimator, eps_constant as given); by default the
+    # same where every segment truncates, the exact solve where one does not
+    import torch
+    from filtered_tdma_b200 import _lib as L
+    from filtered_tdma_b200.momentum import ChannelMomentum
+    rng = np.random.default_rng(80 + direction)
+    for c, eps_c in ((0.5 * (1.0 / 180.0) * 2e-3 * 50, 1e-3), (0.5, 1e-3)):
+        for flags in (L.FLAG_REFERENCE_ORDER, 0):
+            m = ChannelMomentum(64, 64, 64, gamma3=1.5)
+            m.set_backend("filtered_v2", P=4, flags=flags, eps_constant=eps_c)
+            q = rng.uniform(-1, 1, m.shape)
+            dq = torch.from_numpy(q).to(cuda)
+            out = torch.from_numpy(q).to(cuda)
+            m.sweep(direction, 1, dq, out, c)
+            torch.cuda.synchronize()
+            assert m.status() == 0
+            got = out.cpu().numpy()
+            Js = []
+
+            def filt(A, B, C, D, periodic):
+                x, J = orc.filtered(A, B, C, D, 4, 2, periodic, eps_c,
+                                    orc.rho_rows(A, B, C, 0), orc.J_DEVICE)
+                Js.append(list(J))
+                return x
+
+            ref = MO.sweep(q, m.metrics, direction, 1, c, direction < 2, solver=filt)
+            exact = flags == 0 and max(Js[0]) >= 64 // 4 - 2
+            if exact:
+                ref = MO.sweep(q, m.metrics, direction, 1, c, direction < 2)
+                assert _rel(got[1:-1, 1:-1, 1:-1], ref[1:-1, 1:-1, 1:-1]) <= 1e-12
+            else:
+                assert np.array_equal(got, ref)
+            m.close()
+
+
 def test_momentum_argument_checks():
     import ctypes
     from filtered_tdma_b200 import _lib as L
@@ -147,3 +209,4 @@ def test_momentum_argument_checks():
     assert L.lib().btdma_momentum_create(48, 32, 32, p, p, p, p, p, p, 1, 1,
                                          ctypes.byref(h)) == L.ERR_UNSUPPORTED  # 48/16 not 2^k
     assert L.lib().btdma_momentum_sweep(None, 0, 0, None, None, 0.1, None) == L.ERR_ARG
+    assert L.lib().btdma_momentum_set_backend(None, 2, 4, 0, 1e-3) == L.ERR_ARG
