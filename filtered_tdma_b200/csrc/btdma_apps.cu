@@ -20,6 +20,7 @@ struct btdma_heat {
     double* buf0 = nullptr;  // Z and X sweep layouts
     double* buf1 = nullptr;  // Y sweep layout
     double* err = nullptr;   // L2 accumulator
+    double* hpar = nullptr;  // {bx, by, dt 3 pi^2, iy, iz} for the fused Z sweep
     double* scratch = nullptr;  // full grid, the warm-up step before graph capture
     double* tab = nullptr;      // factor tables of the Z, Y, X sweeps, tab_stride apart
     size_t tab_stride = 0;      // (built once at create: the matrices are fixed)
@@ -62,14 +63,34 @@ int heat_enqueue(btdma_heat_t h, double* theta, cudaStream_t st, cudaEvent_t* ev
     const int tx = (g.ix + HEAT_TILE - 1) / HEAT_TILE, ty = (g.iy + HEAT_TILE - 1) / HEAT_TILE;
     int rc;
     mark(0);
-    heat_rhs_z_kernel<<<dim3((g.ix + 127) / 128, g.iy, (g.iz + HEAT_KCH - 1) / HEAT_KCH), b1, 0,
-                        st>>>(theta, h->buf0, g);
-    CK(cudaGetLastError());
-    mark(1);
-    // Z sweep: system jj * ix + ii, row kk; solution to [jj][kk][ii]
-    if ((rc = sweep(0, h->buf0, h->buf1, g.ix * g.iy, g.iz, g.bz, g.ix, g.iz * g.ix, 1, g.ix,
-                    "Z")))
-        return rc;
+    if (tile_plan_heat_z(g.iz).sys != 0) {
+        // Z sweep with the right-hand side computed inside the solve from
+        // theta (no right-hand-side pass); system jj * ix + ii, row kk;
+        // solution to [jj][kk][ii]
+        mark(1);
+        TileArgs za = {};
+        za.cs = g.bz;
+        za.cbound = 1;
+        za.xblk = g.ix;
+        za.xbs = g.iz * g.ix;
+        za.xss = 1;
+        za.xrs = g.ix;
+        za.ga = h->cosx;
+        za.gb = h->cosy;
+        za.gc = h->cosz;
+        za.glam = h->hpar;
+        rc = try_heat_z(theta, h->buf1, g.ix, g.iy, g.iz, za, h->status, st, h->tab);
+        if (rc != 1) return rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "Z sweep not tileable");
+    } else {
+        heat_rhs_z_kernel<<<dim3((g.ix + 127) / 128, g.iy, (g.iz + HEAT_KCH - 1) / HEAT_KCH), b1,
+                            0, st>>>(theta, h->buf0, g);
+        CK(cudaGetLastError());
+        mark(1);
+        // Z sweep: system jj * ix + ii, row kk; solution to [jj][kk][ii]
+        if ((rc = sweep(0, h->buf0, h->buf1, g.ix * g.iy, g.iz, g.bz, g.ix, g.iz * g.ix, 1, g.ix,
+                        "Z")))
+            return rc;
+    }
     mark(2);
     heat_y_fold_kernel<<<dim3((g.ix + 127) / 128, 2, g.iz), b1, 0, st>>>(theta, h->buf1, g);
     CK(cudaGetLastError());
@@ -140,6 +161,11 @@ int btdma_heat_create(int ix, int iy, int iz, double dt, btdma_heat_t* out) {
     CKH(upload(&h->cosx, kx));
     CKH(upload(&h->cosy, ky));
     CKH(upload(&h->cosz, kz));
+    {
+        const double bx = dt / (2.0 * (2.0 / ix) * (2.0 / ix));
+        const double by = dt / (2.0 * (2.0 / iy) * (2.0 / iy));
+        CKH(upload(&h->hpar, {bx, by, dt * 3.0 * HEAT_PI * HEAT_PI, (double)iy, (double)iz}));
+    }
     const size_t inner = (size_t)ix * iy * iz;
     CKH(cudaMalloc(&h->buf0, sizeof(double) * inner));
     CKH(cudaMalloc(&h->buf1, sizeof(double) * inner));
@@ -198,6 +224,7 @@ int btdma_heat_destroy(btdma_heat_t h) {
     cudaFree(h->buf0);
     cudaFree(h->buf1);
     cudaFree(h->err);
+    cudaFree(h->hpar);
     cudaFree(h->scratch);
     cudaFree(h->tab);
     cudaFree(h->status);

@@ -301,9 +301,9 @@ int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st)
     const int threads = SYS * a.nseg / a.cl;
     cudaLaunchConfig_t cfg = {};
     cfg.blockDim = dim3(threads, 1, 1);
-    constexpr bool SHT = GEN == 1 || GEN == 3;
+    constexpr bool SHT = GEN == 1 || GEN == 3 || GEN == 4;
     cfg.dynamicSmemBytes = tile_smem_bytes(SYS, a.nseg / a.cl, a.nseg, SYS / a.cl, a.nst,
-                                           (int)sizeof(TIN), GEN ? 1 : 4, SHT);
+                                           (int)sizeof(TIN), GEN ? 1 : 4, SHT, GEN);
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -520,6 +520,80 @@ int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArg
         case 32: rc = launch_tile_sys<32, CYC, double, double, GEN>(maps, a, st); break;
         default: rc = launch_tile_sys<16, CYC, double, double, GEN>(maps, a, st); break;
     }
+    return rc == BTDMA_OK ? 1 : rc;
+}
+
+// Heat Z sweep with the right-hand side fused (GEN 4 of the tiled kernel):
+// the plan (16 systems per group, one CTA of 16 x n_row / 16 threads, 2 to 32
+// sub-segments), or sys == 0 when the shape does not take it.
+inline TilePlan tile_plan_heat_z(int n_row) {
+    TilePlan pl;
+    if (n_row % TILE_MT != 0) return pl;
+    const int nseg = n_row / TILE_MT;
+    if (nseg < 2 || nseg > 32) return pl;
+    const int T = TILE_HEAT_SYS * nseg;
+    const int per_sm = std::max(1, 65536 / (T * 128));
+    const size_t cap = std::min((size_t)max_smem_optin(), (size_t)max_smem_per_sm() / per_sm - 1024);
+    int nst = TILE_MAX_NST_CONST;
+    while (nst >= 2 &&
+           tile_smem_bytes(TILE_HEAT_SYS, nseg, nseg, TILE_HEAT_SYS, nst, 8, 1, true, 4) > cap)
+        --nst;
+    if (nst < 2) return pl;
+    pl.sys = TILE_HEAT_SYS;
+    pl.cl = 1;
+    pl.nst = nst;
+    pl.nseg = nseg;
+    return pl;
+}
+
+// 4-D view of the heat field theta [(iz + 2) x (iy + 2) x (ix + 2)] for the
+// fused Z sweep: (x = i, y = j, row within the sub-segment, sub-segment) from
+// plane k = 1; boxes of TILE_HEAT_BOX_I x 3 x 4 rows x nsc sub-segments.
+inline bool make_heat_theta_map(CUtensorMap* map, const double* theta, int ix, int iy, int nseg,
+                                int nsc) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    const size_t nx = (size_t)ix + 2, plane = nx * ((size_t)iy + 2);
+    cuuint64_t dims[4] = {(cuuint64_t)nx, (cuuint64_t)iy + 2, (cuuint64_t)TILE_MT,
+                          (cuuint64_t)nseg};
+    cuuint64_t strides[3] = {nx * sizeof(double), plane * sizeof(double),
+                             (cuuint64_t)TILE_MT * plane * sizeof(double)};
+    cuuint32_t box[4] = {(cuuint32_t)TILE_HEAT_BOX_I, 3u, (cuuint32_t)tile_rps(8, 1),
+                         (cuuint32_t)nsc};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(theta + plane),
+                    dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+// The heat Z sweep with its right-hand side computed inside the solve from
+// theta (GEN 4).  gen carries the sweep's fields: cs = bz, cbound = 1, ga / gb
+// / gc = cos(pi x), cos(pi y), cos(pi z) tables (ghosts included), glam = the
+// device array {bx, by, dt 3 pi^2, iy, iz}, xblk = ix and the output layout map.
+// tab: the Z matrix's factor table (build_gen_table<1>).  Returns 1 when
+// launched, 0 when the shape is not taken, < 0 on error.
+inline int try_heat_z(const double* theta, double* X, int ix, int iy, int iz, const TileArgs& gen,
+                      unsigned* status, cudaStream_t st, const double* tab) {
+    const TilePlan pl = tile_plan_heat_z(iz);
+    if (pl.sys == 0 || ix % TILE_HEAT_SYS != 0 ||
+        (reinterpret_cast<uintptr_t>(theta) & 15) != 0 || ((size_t)(ix + 2) * 8) % 16 != 0)
+        return 0;
+    CUtensorMap maps[4];
+    if (!make_heat_theta_map(&maps[3], theta, ix, iy, pl.nseg, pl.nseg)) return 0;
+    maps[0] = maps[1] = maps[2] = maps[3];  // not read in this mode
+    TileArgs a = gen;
+    a.X = X;
+    a.n_sys = ix * iy;
+    a.n_row = iz;
+    a.nseg = pl.nseg;
+    a.cl = pl.cl;
+    a.nst = pl.nst;
+    a.n_groups = a.n_sys / TILE_HEAT_SYS;
+    a.status = status;
+    a.gtab = tab;
+    const int rc = launch_tile_sys<TILE_HEAT_SYS, false, double, double, 4>(maps, a, st);
     return rc == BTDMA_OK ? 1 : rc;
 }
 

@@ -17,6 +17,11 @@
 //     computed as 2 u_BC - theta(cell), exactly the value the reference's ghost
 //     kernels write there;
 //   * A, B, C are never materialised (the solve generates them);
+//   * the right-hand side of the step (all directions' explicit half and the
+//     Z wall folds) is computed inside the Z sweep from theta (the tiled
+//     solve's GEN 4 mode, k_tile.cuh), so it is never stored; heat_rhs_z_kernel
+//     below remains for Z sweeps that mode does not take (fewer than 2 or
+//     more than 32 sub-segments);
 //   * the Z sweep stores its solution straight into the Y sweep's layout
 //     ([kk][jj][ii] -> [jj][kk][ii], the tiled solve's mapped store; the Y wall
 //     folds then touch the two wall planes only), so the only copies left are

@@ -168,10 +168,21 @@ __host__ __device__ __forceinline__ size_t tile_fixed_doubles(int sys, int nsc, 
     if (nseg > 32) f += 6ull * (nseg + 2) * sub;
     return f;
 }
+// Elements of one ring stage: na arrays of RPS rows of sys systems of nsc
+// sub-segments; GEN == 4 (heat Z sweep with the right-hand side fused): a box of
+// theta of TILE_HEAT_BOX_I x 3 cells (the 16 systems' columns with their x
+// and y neighbours) per row instead of one D value per system.
+constexpr int TILE_HEAT_SYS = 16;
+constexpr int TILE_HEAT_BOX_I = TILE_HEAT_SYS + 2;
+__host__ __device__ __forceinline__ int tile_stage_elems(int sys, int nsc, int elem, int na,
+                                                         int gen = 0) {
+    return gen == 4 ? TILE_HEAT_BOX_I * 3 * tile_rps(elem, na) * nsc
+                    : na * tile_rps(elem, na) * sys * nsc;
+}
 // na: arrays per ring stage (4: A, B, C, D; 1: D only).
 __host__ __device__ __forceinline__ size_t tile_ring_bytes(int sys, int nsc, int nst, int elem,
-                                                           int na = 4) {
-    return (size_t)nst * na * tile_rps(elem, na) * sys * nsc * elem;
+                                                           int na = 4, int gen = 0) {
+    return (size_t)nst * tile_stage_elems(sys, nsc, elem, na, gen) * elem;
 }
 // Shared-matrix table slice of one CTA (its nsc sub-segments): per row 5 and
 // per sub-segment 6 doubles.
@@ -180,8 +191,8 @@ __host__ __device__ __forceinline__ size_t tile_tab_doubles(int nsc) {
 }
 __host__ __device__ __forceinline__ size_t tile_smem_bytes(int sys, int nsc, int nseg, int sub,
                                                            int nst, int elem = 8, int na = 4,
-                                                           bool shared_tab = false) {
-    return tile_ring_bytes(sys, nsc, nst, elem, na) +
+                                                           bool shared_tab = false, int gen = 0) {
+    return tile_ring_bytes(sys, nsc, nst, elem, na, gen) +
            (shared_tab ? tile_tab_doubles(nsc) * sizeof(double) : 0) +
            tile_fixed_doubles(sys, nsc, nseg, sub, shared_tab) * sizeof(double) +
            2ull * nst * sizeof(uint64_t) + 128;
@@ -193,6 +204,16 @@ __device__ __forceinline__ void tma_load_3d(void* smem_dst, const CUtensorMap* m
         "cp.async.bulk.tensor.3d.shared::cta.global.tile.mbarrier::complete_tx::bytes"
         " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(smem_dst)),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_4d(void* smem_dst, const CUtensorMap* map, int x, int y,
+                                            int z, int w, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cta.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(smem_dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(w),
+        "r"(smem_u32(bar))
         : "memory");
 }
 
@@ -225,7 +246,8 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     namespace cg = cooperative_groups;
     constexpr int M = TILE_MT;
     constexpr bool CONSTC = GEN != 0;                 // coefficients generated, D only
-    constexpr bool SH = GEN == 1 || GEN == 3;         // one matrix for all systems (gtab)
+    constexpr bool SH = GEN == 1 || GEN == 3 || GEN == 4;  // one matrix for all systems (gtab)
+    static_assert(GEN != 4 || (SYS == TILE_HEAT_SYS && !CYCLIC), "heat Z sweep: 16 systems");
     constexpr int NA = CONSTC ? 1 : 4;                // arrays per ring stage
     constexpr int RPS = tile_rps((int)sizeof(TIN), NA);  // rows per ring stage
     constexpr int SPG = M / RPS;                         // stages per group
@@ -242,7 +264,8 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 
     TIN* ring = reinterpret_cast<TIN*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-    double* red = reinterpret_cast<double*>(ring + (size_t)nst * NA * RPS * T);
+    const int sstride = tile_stage_elems(SYS, nsc, (int)sizeof(TIN), NA, GEN);  // per stage
+    double* red = reinterpret_cast<double*>(ring + (size_t)nst * sstride);
     double* xr = red + (rhs_red ? 2 : 6) * fstride;
     double* pcr = xr + 2 * fstride;  // only when !shuffled
     const int gs = nseg + 2;
@@ -300,7 +323,6 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                          ? (args.n_groups - cluster_id + n_clusters - 1) / n_clusters
                          : 0;
     const int total = n_my * SPG;  // ring stages this CTA consumes
-    const int sstride = NA * RPS * T;  // elements per stage
     const uint32_t stage_bytes = (uint32_t)sstride * sizeof(TIN);
 
     auto issue = [&](int t) {  // one thread
@@ -309,6 +331,14 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         const int k0 = (t % SPG) * RPS;
         TIN* dst = ring + (size_t)slot * sstride;
         mbar_expect_tx(&full[slot], stage_bytes);
+        if constexpr (GEN == 4) {
+            // theta box: x from the system's left neighbour (ghosted index ii0),
+            // y = jj - 1 .. jj + 1 (ghosted jj .. jj + 2), RPS rows of every
+            // sub-segment (the map's base is plane k = 1)
+            const int s0 = g * SYS;
+            tma_load_4d(dst, &tmD, s0 % args.xblk, s0 / args.xblk, k0, c * nsc, &full[slot]);
+            return;
+        }
         if constexpr (!CONSTC) {
             tma_load_3d(dst + 0 * RPS * T, &tmA, g * SYS, k0, c * nsc, &full[slot]);
             tma_load_3d(dst + 1 * RPS * T, &tmB, g * SYS, k0, c * nsc, &full[slot]);
@@ -342,108 +372,207 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         if constexpr (GEN == 2) lam = valid ? args.glam[sys >> 1] : 0.0;
         TC ab0 = 0, cb0 = 0, db0 = 0;
         TC pi = 1, sa = 0, sd = 0;
-#pragma unroll
-        for (int j = 0; j < SPG; ++j) {
-            if (ok) ok = mbar_wait_bounded(&full[slot], phase, args.status);
-            TIN a2[RPS], b2[RPS], c2[RPS], d2[RPS];  // widened where used
-#pragma unroll
-            for (int r = 0; r < RPS; ++r) {
-                if constexpr (!CONSTC) {
-                    a2[r] = st[0 * RPS * T + r * SYS];
-                    b2[r] = st[1 * RPS * T + r * SYS];
-                    c2[r] = st[2 * RPS * T + r * SYS];
-                }
-                d2[r] = st[(NA - 1) * RPS * T + r * SYS];
-            }
-            __syncwarp();
-            if (lane == 0) {
-                mbar_arrive(&empty[slot]);
-                // Rotating producer: one stage later, warp (t % nwarps) refills
-                // the slot of stage t - 1 with stage t - 1 + nst once every warp
-                // has released it.
-                if (t >= 1 && warp == tw && t - 1 + nst < total && ok) {
-                    ok = mbar_wait_bounded(&empty[pslot], pphase, args.status);
-                    if (ok) issue(t - 1 + nst);
-                }
-            }
-            pslot = slot;
-            pphase = phase;
-            ++t;
-            if (++tw == nwarps) tw = 0;
-            st += sstride;
-            if (++slot == nst) {
-                slot = 0;
-                phase ^= 1u;
-                st = ring + toff;
-            }
-#pragma unroll
-            for (int r = 0; r < RPS; ++r) {
-                const int k = j * RPS + r;
-                if constexpr (SH) {  // right-hand side only, factors from gtab
-                    const double* tr = tabs + (ql * M + k) * 5;
-                    const double d = (double)d2[r];
-                    if (k == 0) {
-                        db0 = d * tr[0];
-                    } else if (k == 1) {
-                        de[1] = d * tr[0];
-                        sd = de[1];
-                    } else {
-                        de[k] = d * tr[0] - tr[1] * de[k - 1];
-                        if (k <= M - 2) sd += tr[2] * de[k];
-                    }
-                    continue;
-                }
-                TC a, b, cc, d = (TC)d2[r];
-                if constexpr (GEN == 1) {
-                    const int q = c * nsc + ql;  // sub-segment of this thread
-                    const bool wall = args.cbound != 0 && ((q == 0 && k == 0) ||
-                                                           (q == nseg - 1 && k == M - 1));
-                    a = (TC)-args.cs;
-                    cc = (TC)-args.cs;
-                    b = (TC)(1.0 + 2.0 * args.cs + (wall ? args.cs : 0.0));
-                } else if constexpr (GEN == 3) {
-                    const int kg = (c * nsc + ql) * M + k;  // row of the system
-                    a = (TC)(-args.cs * args.ga[kg]);
-                    cc = (TC)(-args.cs * args.gc[kg]);
-                    b = (TC)(1.0 + args.cs * args.gb[kg]);
-                } else if constexpr (GEN == 2) {
-                    const int kg = (c * nsc + ql) * M + k;  // row of the system
-                    const double ta = args.ga[kg], tc = args.gc[kg];
-                    a = (TC)ta;
-                    cc = (TC)tc;
-                    b = (TC)(-(ta + tc) - lam);
-                    if (args.gpin != 0 && kg == 0 && (sys >> 1) == 0) {
-                        a = 0;
-                        b = 1;
-                        cc = 0;
-                        d = 0;
-                    }
-                } else {
-                    a = (TC)a2[r];
-                    b = (TC)b2[r];
-                    cc = (TC)c2[r];
-                }
-                if (k == 0) {
-                    const TC ib = rcp_tc(b);
-                    ab0 = a * ib;
-                    cb0 = cc * ib;
-                    db0 = d * ib;
-                } else if (k == 1) {
-                    const TC ib = rcp_tc(b);
-                    al[1] = a * ib;
-                    ga[1] = cc * ib;
-                    de[1] = d * ib;
-                    sa = al[1];
+        if constexpr (GEN == 4) {
+            // Heat Z sweep: the right-hand side of every row is computed here
+            // from the theta box of the stage (the reference's rhs_kernel and
+            // build_lhs_z wall folds, apps/heat_gpu/solve_theta.cu:121-202),
+            // with the ghosts computed where read (2 u_BC - theta).  Row k's z
+            // neighbours are rows k - 1 and k + 1, so a row is finished one row
+            // later; row 0 of the sub-segment takes its lower neighbour from the
+            // previous sub-segment's last row in the last stage, row M - 1 its
+            // upper one from the next sub-segment's first row in the first.
+            const double* hp = args.glam;  // bx, by, dt 3 pi^2, iy, iz
+            const int ixg = args.xblk, s0 = g * SYS;
+            const int jj = s0 / ixg, ii = s0 % ixg + s;
+            const int q = c * nsc + ql;
+            const int kk0 = q * M;
+            const int iy = (int)__ldg(hp + 3), iz = (int)__ldg(hp + 4);
+            const double bx = __ldg(hp + 0), by = __ldg(hp + 1), bz = args.cs,
+                         srcs = __ldg(hp + 2);
+            const double cxi = __ldg(args.ga + ii + 1), cyj = __ldg(args.gb + jj + 1);
+            const double diag = 1.0 + (-2.0 * bx) + (-2.0 * by) + (-2.0 * bz);
+            const double ubz = -cxi * cyj;
+            double pp0 = 0.0, pp = 0.0, pc = 0.0, tnext = 0.0, tkm0 = 0.0;
+            // the recurrence of the shared-matrix modes on a finished row
+            auto feed = [&](int k, double d) {
+                const double* tr = tabs + (ql * M + k) * 5;
+                if (k == 1) {
+                    de[1] = d * tr[0];
                     sd = de[1];
                 } else {
-                    const TC inv = rcp_tc(b - a * ga[k - 1]);
-                    ga[k] = cc * inv;
-                    de[k] = (d - a * de[k - 1]) * inv;
-                    al[k] = -a * al[k - 1] * inv;
-                    if (k <= M - 2) {
-                        pi = -ga[k - 1] * pi;
-                        sa += pi * al[k];
-                        sd += pi * de[k];
+                    de[k] = d * tr[0] - tr[1] * de[k - 1];
+                    if (k <= M - 2) sd += tr[2] * de[k];
+                }
+            };
+#pragma unroll
+            for (int j = 0; j < SPG; ++j) {
+                if (ok) ok = mbar_wait_bounded(&full[slot], phase, args.status);
+                // box [sub-segment][row][y][x], x = system + 1 (+-1: x neighbours)
+                const double* sb = ring + (size_t)slot * sstride;
+                auto at = [&](int qq, int r, int y, int dx) {
+                    return sb[((qq * RPS + r) * 3 + y) * TILE_HEAT_BOX_I + s + 1 + dx];
+                };
+                if (j == 0 && q + 1 < nseg) tnext = at(ql + 1, 0, 1, 0);
+                if (j == SPG - 1 && q > 0) tkm0 = at(ql - 1, RPS - 1, 1, 0);
+                double tc[RPS], tl[RPS], tr_[RPS], ym[RPS], yp[RPS];
+#pragma unroll
+                for (int r = 0; r < RPS; ++r) {
+                    tc[r] = at(ql, r, 1, 0);
+                    tl[r] = at(ql, r, 1, -1);
+                    tr_[r] = at(ql, r, 1, 1);
+                    ym[r] = at(ql, r, 0, 0);
+                    yp[r] = at(ql, r, 2, 0);
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&empty[slot]);
+                    if (t >= 1 && warp == tw && t - 1 + nst < total && ok) {
+                        ok = mbar_wait_bounded(&empty[pslot], pphase, args.status);
+                        if (ok) issue(t - 1 + nst);
+                    }
+                }
+                pslot = slot;
+                pphase = phase;
+                ++t;
+                if (++tw == nwarps) tw = 0;
+                if (++slot == nst) {
+                    slot = 0;
+                    phase ^= 1u;
+                }
+#pragma unroll
+                for (int r = 0; r < RPS; ++r) {
+                    const int k = j * RPS + r;
+                    const int kk = kk0 + k;
+                    const double tt = tc[r];
+                    const double czk = __ldg(args.gc + kk + 1);
+                    const double ux = -cyj * czk, uy = -cxi * czk;  // x, y wall values
+                    const double tip = ii + 1 < ixg ? tr_[r] : 2.0 * ux - tt;
+                    const double tim = ii > 0 ? tl[r] : 2.0 * ux - tt;
+                    const double tjp = jj + 1 < iy ? yp[r] : 2.0 * uy - tt;
+                    const double tjm = jj > 0 ? ym[r] : 2.0 * uy - tt;
+                    const double src = srcs * cxi * cyj * czk;
+                    double p = (bx * tip + bx * tim) + (by * tjp + by * tjm) + diag * tt + src;
+                    if (kk == 0) p += bz * (2.0 * ubz - tt) + bz * ((2.0 * ubz - tt) + tt);
+                    if (kk == iz - 1) p += bz * (2.0 * ubz - tt) + bz * ((2.0 * ubz - tt) + tt);
+                    if (k >= 1) p += bz * pc;  // lower neighbour: the previous row
+                    if (k == 1) pp0 += bz * tt;  // row 0's upper neighbour
+                    if (k >= 2) feed(k - 1, pp + bz * tt);
+                    if (k == 0)
+                        pp0 = p;
+                    else
+                        pp = p;
+                    pc = tt;
+                }
+            }
+            // row M - 1: the next sub-segment's first row above it (the top wall's
+            // ghost is already in); row 0: the previous sub-segment's last row
+            // below it (or the bottom wall's ghost, already in)
+            feed(M - 1, kk0 + M - 1 == iz - 1 ? pp : pp + bz * tnext);
+            db0 = (kk0 == 0 ? pp0 : pp0 + bz * tkm0) * tabs[(ql * M) * 5];
+        } else {
+#pragma unroll
+            for (int j = 0; j < SPG; ++j) {
+                if (ok) ok = mbar_wait_bounded(&full[slot], phase, args.status);
+                TIN a2[RPS], b2[RPS], c2[RPS], d2[RPS];  // widened where used
+#pragma unroll
+                for (int r = 0; r < RPS; ++r) {
+                    if constexpr (!CONSTC) {
+                        a2[r] = st[0 * RPS * T + r * SYS];
+                        b2[r] = st[1 * RPS * T + r * SYS];
+                        c2[r] = st[2 * RPS * T + r * SYS];
+                    }
+                    d2[r] = st[(NA - 1) * RPS * T + r * SYS];
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&empty[slot]);
+                    // Rotating producer: one stage later, warp (t % nwarps) refills
+                    // the slot of stage t - 1 with stage t - 1 + nst once every warp
+                    // has released it.
+                    if (t >= 1 && warp == tw && t - 1 + nst < total && ok) {
+                        ok = mbar_wait_bounded(&empty[pslot], pphase, args.status);
+                        if (ok) issue(t - 1 + nst);
+                    }
+                }
+                pslot = slot;
+                pphase = phase;
+                ++t;
+                if (++tw == nwarps) tw = 0;
+                st += sstride;
+                if (++slot == nst) {
+                    slot = 0;
+                    phase ^= 1u;
+                    st = ring + toff;
+                }
+#pragma unroll
+                for (int r = 0; r < RPS; ++r) {
+                    const int k = j * RPS + r;
+                    if constexpr (SH) {  // right-hand side only, factors from gtab
+                        const double* tr = tabs + (ql * M + k) * 5;
+                        const double d = (double)d2[r];
+                        if (k == 0) {
+                            db0 = d * tr[0];
+                        } else if (k == 1) {
+                            de[1] = d * tr[0];
+                            sd = de[1];
+                        } else {
+                            de[k] = d * tr[0] - tr[1] * de[k - 1];
+                            if (k <= M - 2) sd += tr[2] * de[k];
+                        }
+                        continue;
+                    }
+                    TC a, b, cc, d = (TC)d2[r];
+                    if constexpr (GEN == 1) {
+                        const int q = c * nsc + ql;  // sub-segment of this thread
+                        const bool wall = args.cbound != 0 && ((q == 0 && k == 0) ||
+                                                               (q == nseg - 1 && k == M - 1));
+                        a = (TC)-args.cs;
+                        cc = (TC)-args.cs;
+                        b = (TC)(1.0 + 2.0 * args.cs + (wall ? args.cs : 0.0));
+                    } else if constexpr (GEN == 3) {
+                        const int kg = (c * nsc + ql) * M + k;  // row of the system
+                        a = (TC)(-args.cs * args.ga[kg]);
+                        cc = (TC)(-args.cs * args.gc[kg]);
+                        b = (TC)(1.0 + args.cs * args.gb[kg]);
+                    } else if constexpr (GEN == 2) {
+                        const int kg = (c * nsc + ql) * M + k;  // row of the system
+                        const double ta = args.ga[kg], tc = args.gc[kg];
+                        a = (TC)ta;
+                        cc = (TC)tc;
+                        b = (TC)(-(ta + tc) - lam);
+                        if (args.gpin != 0 && kg == 0 && (sys >> 1) == 0) {
+                            a = 0;
+                            b = 1;
+                            cc = 0;
+                            d = 0;
+                        }
+                    } else {
+                        a = (TC)a2[r];
+                        b = (TC)b2[r];
+                        cc = (TC)c2[r];
+                    }
+                    if (k == 0) {
+                        const TC ib = rcp_tc(b);
+                        ab0 = a * ib;
+                        cb0 = cc * ib;
+                        db0 = d * ib;
+                    } else if (k == 1) {
+                        const TC ib = rcp_tc(b);
+                        al[1] = a * ib;
+                        ga[1] = cc * ib;
+                        de[1] = d * ib;
+                        sa = al[1];
+                        sd = de[1];
+                    } else {
+                        const TC inv = rcp_tc(b - a * ga[k - 1]);
+                        ga[k] = cc * inv;
+                        de[k] = (d - a * de[k - 1]) * inv;
+                        al[k] = -a * al[k - 1] * inv;
+                        if (k <= M - 2) {
+                            pi = -ga[k - 1] * pi;
+                            sa += pi * al[k];
+                            sd += pi * de[k];
+                        }
                     }
                 }
             }
