@@ -56,7 +56,8 @@ class RaggedBucket(ctypes.Structure):
     _fields_ = [("periodic", ctypes.c_int), ("n_systems", ctypes.c_int),
                 ("n_row_min", ctypes.c_int), ("n_row_max", ctypes.c_int),
                 ("lanes_per_system", ctypes.c_int), ("warps_per_cta", ctypes.c_int),
-                ("cta_per_system", ctypes.c_int), ("tuned_ms", ctypes.c_float)]
+                ("cta_per_system", ctypes.c_int), ("tuned_ms", ctypes.c_float),
+                ("persistent", ctypes.c_int)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -277,6 +277,7 @@ int btdma_destroy(btdma_t h) {
     cudaFree(h->rag_d_list);
     cudaFree(h->rag_d_tasks);
     cudaFree(h->rag_d_probe);
+    cudaFree(h->rag_d_next);
     for (int i = 0; i < btdma_handle::RAG_STREAMS; ++i) {
         if (h->rag_side[i]) cudaStreamDestroy(h->rag_side[i]);
         if (h->rag_join[i]) cudaEventDestroy(h->rag_join[i]);

@@ -61,7 +61,12 @@ struct btdma_handle {
     int* rag_d_list = nullptr;             // device copy of rag_order
     int4* rag_d_tasks = nullptr;           // task tables [2 * n_sys]
     int4* rag_d_probe = nullptr;           // task table of one bucket being tuned [n_sys]
-    // launches of a solve: warp-kind tasks (one launch), CTA-kind tasks per P
+    int* rag_d_next = nullptr;             // task counters of the persistent launch [3]
+    int rag_cls_first[3] = {}, rag_cls_count[3] = {};  // its classes (P = 256, 128, 64)
+    bool rag_persist = false;              // CTA-kind buckets in the persistent launch
+    // launches of a solve: warp-kind tasks (one launch), the long systems of
+    // at most RAG_PERSIST_THREADS threads in one persistent launch (cta == 2),
+    // longer ones per P (cta == 1)
     struct RagLaunch {
         int cta, P, first, count, mcap, staged;
     };

@@ -44,8 +44,11 @@ void rag_bucket_tasks(const btdma_handle::RagBucket& b, int cta, int P, std::vec
         out.push_back(make_int4(b.first + i, std::min(G, b.count - i), P, b.cyc));
 }
 
-// Task tables of the whole plan: one warp-kind launch (buckets longest first)
-// and one CTA-kind launch per P.
+// Task tables of the whole plan: one warp-kind launch (buckets longest first),
+// one persistent launch for every CTA-kind bucket of at most
+// RAG_PERSIST_THREADS threads (tasks {list index, cyclic, P, staged}, the
+// longest systems first, so the tail of the launch is short work), and one
+// CTA-kind launch per longer P.
 int rag_build_launches(btdma_t h) {
     std::vector<int4> tasks;
     h->rag_launches.clear();
@@ -58,7 +61,30 @@ int rag_build_launches(btdma_t h) {
     }
     wl.count = (int)tasks.size();
     if (wl.count) h->rag_launches.push_back(wl);
-    for (int P = 512; P >= 64; P >>= 1)
+    if (h->rag_persist) {
+        // one class per P (256, 128, 64), each longest first
+        btdma_handle::RagLaunch pl{2, RAG_PERSIST_THREADS, (int)tasks.size(), 0, RAG_MT, 0};
+        for (int c = 0; c < RAG_PERSIST_CLASSES; ++c) {
+            const int Pc = RAG_PERSIST_THREADS >> c;
+            std::vector<int> ids;
+            for (int i = 0; i < (int)h->rag_buckets.size(); ++i)
+                if (h->rag_buckets[i].cta && h->rag_buckets[i].P == Pc) ids.push_back(i);
+            std::stable_sort(ids.begin(), ids.end(), [&](int x, int y) {
+                return h->rag_buckets[x].nmax > h->rag_buckets[y].nmax;
+            });
+            h->rag_cls_first[c] = (int)tasks.size() - pl.first;
+            for (int i : ids) {
+                const auto& b = h->rag_buckets[i];
+                for (int k = 0; k < b.count; ++k)
+                    tasks.push_back(make_int4(b.first + k, b.cyc, b.P, b.staged));
+            }
+            h->rag_cls_count[c] = (int)tasks.size() - pl.first - h->rag_cls_first[c];
+        }
+        pl.count = (int)tasks.size() - pl.first;
+        if (pl.count) h->rag_launches.push_back(pl);
+    }
+    for (int P = 512; P >= 64; P >>= 1) {
+        if (h->rag_persist && P <= RAG_PERSIST_THREADS) break;
         for (int stg = 0; stg < 2; ++stg) {
             btdma_handle::RagLaunch cl{1, P, (int)tasks.size(), 0, 1, stg};
             for (const auto& b : h->rag_buckets)
@@ -69,6 +95,7 @@ int rag_build_launches(btdma_t h) {
             cl.count = (int)tasks.size() - cl.first;
             if (cl.count) h->rag_launches.push_back(cl);
         }
+    }
     CK(cudaMemcpy(h->rag_d_tasks, tasks.data(), sizeof(int4) * tasks.size(),
                   cudaMemcpyHostToDevice));
     return BTDMA_OK;
@@ -144,6 +171,7 @@ int rag_plan(btdma_t h, const long long* off, const unsigned char* per, int n_sy
     CK(cudaMalloc(&h->rag_d_list, sizeof(int) * n_sys));
     CK(cudaMalloc(&h->rag_d_tasks, sizeof(int4) * 2 * n_sys));
     CK(cudaMalloc(&h->rag_d_probe, sizeof(int4) * n_sys));
+    if (!h->rag_d_next) CK(cudaMalloc(&h->rag_d_next, sizeof(int) * RAG_PERSIST_CLASSES));
     CK(cudaMemcpy(h->rag_d_off, off, sizeof(long long) * (n_sys + 1), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->rag_d_list, order.data(), sizeof(int) * n_sys, cudaMemcpyHostToDevice));
     if (!h->rag_fork) {
@@ -181,7 +209,28 @@ int rag_launch(btdma_t h, int cta, int P, int mcap, int staged, const int4* task
     a.n_tasks = n_tasks;
     a.mcap = mcap;
     a.status = h->status;
-    if (cta) {
+    a.next = h->rag_d_next;
+    if (cta == 2) {
+        auto kern = ragged_persist_kernel<TIN>;
+        const size_t smem = rag_persist_slice(RAG_PERSIST_THREADS);
+        for (int c = 0; c < RAG_PERSIST_CLASSES; ++c) {
+            a.cls_first[c] = h->rag_cls_first[c];
+            a.cls_count[c] = h->rag_cls_count[c];
+        }
+        static bool attr_done = false;
+        static int per_sm = 1;
+        if (!attr_done) {
+            CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, RAG_PERSIST_THREADS,
+                                                             smem));
+            per_sm = std::max(1, per_sm);
+            attr_done = true;
+        }
+        a.mcap = RAG_MT;
+        CK(cudaMemsetAsync(h->rag_d_next, 0, sizeof(int) * RAG_PERSIST_CLASSES, st));
+        kern<<<std::min(n_tasks, per_sm * num_sms()), RAG_PERSIST_THREADS, smem, st>>>(a);
+    } else if (cta) {
         if (staged && rag_cta_smem_bytes(P, true, mcap) > (size_t)max_smem_optin()) staged = 0;
         auto kern = staged ? ragged_cta_kernel<TIN, true> : ragged_cta_kernel<TIN, false>;
         static bool attr_done[2] = {false, false};
@@ -313,9 +362,27 @@ int rag_tune(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, 
         b.mcap = rag_mcap(b.nmax, pick.P);
         b.best_ms = best;
     }
+    // the launch structure: a launch per CTA-kind shape, or the persistent
+    // launch; the whole solve timed both ways (best of 3)
+    float whole[2] = {1e30f, 1e30f};
+    for (int pers = 0; pers < 2 && !rc; ++pers) {
+        h->rag_persist = pers != 0;
+        if ((rc = rag_build_launches(h))) break;
+        for (int rep = 0; rep < 4 && !rc; ++rep) {
+            CK(cudaEventRecord(e0, st));
+            rc = rag_run<TIN>(h, A, B, C, D, X, st);
+            if (rc) break;
+            CK(cudaEventRecord(e1, st));
+            CK(cudaEventSynchronize(e1));
+            float t = 0.f;
+            CK(cudaEventElapsedTime(&t, e0, e1));
+            if (rep > 0) whole[pers] = std::min(whole[pers], t);  // rep 0 warms up
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc) return rc;
+    h->rag_persist = whole[1] < whole[0];
     return rag_build_launches(h);
 }
 
@@ -385,6 +452,9 @@ int btdma_ragged_set_plan(btdma_t h, const btdma_ragged_bucket* in, int n) {
         b.mcap = rag_mcap(b.nmax, b.P);
         b.best_ms = in[i].tuned_ms;
     }
+    // the persistent launch when any bucket is marked for it
+    h->rag_persist = false;
+    for (int i = 0; i < n; ++i) h->rag_persist |= in[i].persistent != 0;
     return rag_build_launches(h);
 }
 
@@ -401,6 +471,7 @@ int btdma_ragged_plan_info(btdma_t h, btdma_ragged_bucket* out, int cap, int* n_
         out[i].warps_per_cta = b.warps;
         out[i].cta_per_system = b.cta + b.staged;
         out[i].tuned_ms = b.best_ms;
+        out[i].persistent = h->rag_persist && b.cta && b.P <= RAG_PERSIST_THREADS ? 1 : 0;
     }
     return BTDMA_OK;
 }

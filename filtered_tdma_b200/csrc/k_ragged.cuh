@@ -40,6 +40,10 @@ struct RagArgs {
     int n_tasks;
     int mcap;              // ragged_kernel: state slots per lane (>= every task's rows per lane)
     unsigned* status;
+    // ragged_persist_kernel: task counters per class (zero at launch), and each
+    // class's first task and task count in the table
+    int* next;
+    int cls_first[3], cls_count[3];
 };
 
 constexpr int RAG_LOOKAHEAD = 4;  // rows loaded ahead of the elimination
@@ -192,21 +196,24 @@ __global__ void __launch_bounds__(256) ragged_kernel(const RagArgs a) {
 // per level (the same steps as reduced_solve_shfl).
 constexpr int RAG_MT = 16;
 
-// STAGED: the whole system is first copied into shared memory with coalesced
-// loads, laid out [array][thread][row of segment] with an odd pitch of at least
-// the launch's rows per thread (A, B, C, D widened to FP64): consecutive rows
-// of a segment are consecutive words for the coalesced fill, and the threads
-// reading row k of their segments are an odd number of doubles apart (no bank
-// conflicts either way).
-// The elimination state then overwrites A, C, D in place and x goes through B
-// on its way out (coalesced stores).  Without staging each thread reads its
+// STAGED: A, C and D of the whole system are first copied into shared memory
+// with coalesced loads (B, read by the forward sweep only, comes straight from
+// global memory a few rows ahead), laid out [array][thread][row of segment]
+// with RAG_MT slots per thread and the row index XOR-swizzled by the thread's
+// low four bits (slot k ^ (p & 15)): consecutive rows of a segment land in
+// distinct banks for the coalesced fill, and the threads reading row k of
+// their segments hit distinct banks too, with no padding.  The elimination
+// state then overwrites A, C, D in place, x overwrites D during the back
+// substitution and leaves with coalesced stores.  At 4096 rows (256 threads of
+// 16 rows) a staged CTA takes 110 KB, so two fit on an SM and one's fill
+// overlaps the other's sweeps.  Without staging each thread reads its
 // contiguous rows straight from global memory, which leaves L1 to hold four
 // lines per thread.
-// mcap: rows per thread of the launch (<= RAG_MT); staged pitch mcap | 1 (odd).
-__host__ __device__ __forceinline__ int rag_pitch(int mcap) { return mcap | 1; }
+// mcap: rows per thread of the launch (<= RAG_MT).
+__host__ __device__ __forceinline__ int rag_slot(int p, int k) { return k ^ (p & 15); }
 __host__ __device__ __forceinline__ size_t rag_cta_smem_bytes(int P, bool staged, int mcap) {
     return (2ull * 3 * (P + 2) +
-            (staged ? 4ull * rag_pitch(mcap) * P : 3ull * (size_t)mcap * P)) *
+            (staged ? 3ull * RAG_MT * P : 3ull * (size_t)mcap * P)) *
            sizeof(double);
 }
 
@@ -242,12 +249,16 @@ __device__ __forceinline__ void rag_locate(int r, int base, int rem, float inv0,
     }
 }
 
+// One system (task {list index, cyclic, ...}) solved by a group of P threads
+// (thread p of the group), whose barrier is bar.sync bid, P (bid 0 with the
+// whole CTA: __syncthreads) and whose shared memory starts at rsm.
 template <typename TIN, bool STAGED>
-__global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
-    extern __shared__ double rsm[];
+__device__ __forceinline__ void rag_cta_body(const RagArgs& a, const int4 task, const int P,
+                                             double* rsm, const int p, const int bid) {
     constexpr int M = RAG_MT;
-    const int P = blockDim.x;
-    const int p = threadIdx.x;
+    const int NT = P;
+    const bool act = p < P;
+    auto gsync = [&]() { asm volatile("bar.sync %0, %1;" ::"r"(bid), "r"(P) : "memory"); };
     const int gs = P + 2;  // guard rows at 0 and P + 1 stay zero (non-periodic ends)
     auto F = [&](int b, int f, int row) -> double& { return rsm[(b * 3 + f) * gs + row + 1]; };
     if (p < 6) {
@@ -255,13 +266,12 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
         rsm[p * gs + P + 1] = 0.0;
     }
 
-    const int4 task = a.tasks[blockIdx.x];
     const bool cyclic = task.y != 0;  // uniform over the CTA
     const int sys = a.list[task.x];
     const long long o = a.off[sys];
     const int n = (int)(a.off[sys + 1] - o);
     const int base = n / P, rem = n % P;
-    const int m = base + (p < rem ? 1 : 0);  // 3 <= m <= M (host's choice of P)
+    const int m = act ? base + (p < rem ? 1 : 0) : 0;  // 3 <= m <= M (host's choice of P)
     const long long row0 = o + (long long)p * base + (p < rem ? p : rem);
     const TIN* __restrict__ pA = static_cast<const TIN*>(a.A) + row0;
     const TIN* __restrict__ pB = static_cast<const TIN*>(a.B) + row0;
@@ -271,47 +281,47 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
     double* const stg = rsm + 2 * 3 * gs;  // state / staging area
     // this thread's slots (mcap = the launch's rows per thread, <= M):
     // unstaged [field][row][thread] -> stt[(f * mcap + k) * P];
-    // staged [field][thread][row] -> stt[f * P * mp + k], mp = mcap | 1
-    const int mp = rag_pitch(a.mcap);
-    double* stt = STAGED ? stg + p * mp : stg + p;
-    const int fs = STAGED ? P * mp : a.mcap * P;  // field stride
-    const int ks = STAGED ? 1 : P;                // row stride
+    // staged [field][thread][slot] -> stt[f * P * M + rag_slot(p, k)]
+    double* stt = STAGED ? stg + p * M : stg + p;
+    const int fs = STAGED ? P * M : a.mcap * P;  // field stride
+    const int ks = STAGED ? 1 : P;               // row stride (unstaged)
     const float inv0 = 1.0f / (float)(base > 0 ? base : 1), inv1 = 1.0f / (float)(base + 1);
     if constexpr (STAGED) {
-        // fields 0..3 = A, B, C, D; coalesced over the system's rows
+        // fields 0..2 = A, C, D; coalesced over the system's rows
         const TIN* __restrict__ gA = static_cast<const TIN*>(a.A) + o;
-        const TIN* __restrict__ gB = static_cast<const TIN*>(a.B) + o;
         const TIN* __restrict__ gC = static_cast<const TIN*>(a.C) + o;
         const TIN* __restrict__ gD = static_cast<const TIN*>(a.D) + o;
         // asynchronous copies straight into the staged layout, every row of the
         // thread in flight at once; FP32 values land in the low word of their
         // 8-byte slot and each thread widens its own rows once they are in
-        for (int r = p; r < n; r += P) {
+        for (int r = p; r < n; r += NT) {
             int q, k;
             rag_locate(r, base, rem, inv0, inv1, q, k);
-            double* dst = stg + q * mp + k;
+            double* dst = stg + q * M + rag_slot(q, k);
             cp_async_elem(dst + 0 * fs, gA + r);
-            cp_async_elem(dst + 1 * fs, gB + r);
-            cp_async_elem(dst + 2 * fs, gC + r);
-            cp_async_elem(dst + 3 * fs, gD + r);
+            cp_async_elem(dst + 1 * fs, gC + r);
+            cp_async_elem(dst + 2 * fs, gD + r);
         }
         asm volatile("cp.async.wait_all;" ::: "memory");
-        __syncthreads();
+        gsync();
         if constexpr (sizeof(TIN) == 4) {
             for (int k = 0; k < m; ++k)
 #pragma unroll
-                for (int f = 0; f < 4; ++f) {
-                    double* sl = stt + f * fs + k;
+                for (int f = 0; f < 3; ++f) {
+                    double* sl = stt + f * fs + rag_slot(p, k);
                     *sl = (double)*reinterpret_cast<const float*>(sl);
                 }
         }
     }
+    // slot of row k: staged swizzled, unstaged [row][thread]
+    auto SL = [&](int k) { return STAGED ? rag_slot(p, k) : k * ks; };
     // state: alpha, gamma, delta (in place of A, C, D when staged)
-    auto AL = [&](int k) -> double& { return stt[0 * fs + k * ks]; };
-    auto GA = [&](int k) -> double& { return stt[(STAGED ? 2 : 1) * fs + k * ks]; };
-    auto DE = [&](int k) -> double& { return stt[(STAGED ? 3 : 2) * fs + k * ks]; };
+    auto AL = [&](int k) -> double& { return stt[0 * fs + SL(k)]; };
+    auto GA = [&](int k) -> double& { return stt[1 * fs + SL(k)]; };
+    auto DE = [&](int k) -> double& { return stt[2 * fs + SL(k)]; };
     double ab0 = 0, cb0 = 0, db0 = 0, pi = 1.0, sa = 0.0, sd = 0.0, pi_last = 0.0;
     double alp = 0, gap = 0, dep = 0;  // row k-1
+    if (act) {
     // rows of batch k0 .. k0 + RAG_LOOKAHEAD - 1 (clamped in bounds); the next
     // batch is requested before the current one is eliminated
     double ra[RAG_LOOKAHEAD], rb[RAG_LOOKAHEAD], rc[RAG_LOOKAHEAD], rd[RAG_LOOKAHEAD];
@@ -320,10 +330,11 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
         for (int j = 0; j < RAG_LOOKAHEAD; ++j) {
             const int kk = k0 + j < m ? k0 + j : m - 1;
             if constexpr (STAGED) {
-                fa[j] = stt[0 * fs + kk];
-                fb[j] = stt[1 * fs + kk];
-                fc[j] = stt[2 * fs + kk];
-                fd[j] = stt[3 * fs + kk];
+                const int sl = rag_slot(p, kk);
+                fa[j] = stt[0 * fs + sl];
+                fb[j] = (double)__ldg(pB + kk);
+                fc[j] = stt[1 * fs + sl];
+                fd[j] = stt[2 * fs + sl];
             } else {
                 fa[j] = (double)__ldg(pA + kk);
                 fb[j] = (double)__ldg(pB + kk);
@@ -385,16 +396,19 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
             }
         }
     }
+    }  // act
     const double l1 = alp, u1 = gap, r1 = dep;  // row m - 1
     const double rr = rcp_nr(1.0 - cb0 * sa);
     const double l0 = rr * ab0, u0 = rr * cb0 * pi_last, r0 = rr * (db0 - cb0 * sd);
 
     // ---------------------------------------------- reduced system (shared memory)
-    F(1, 0, p) = l0;
-    F(1, 1, p) = u0;
-    F(1, 2, p) = r0;
-    __syncthreads();
-    {
+    if (act) {
+        F(1, 0, p) = l0;
+        F(1, 1, p) = u0;
+        F(1, 2, p) = r0;
+    }
+    gsync();
+    if (act) {
         const int pn = (cyclic && p == P - 1) ? 0 : p + 1;  // p + 1 == P: the zero guard
         const double l0n = F(1, 0, pn), u0n = F(1, 1, pn), r0n = F(1, 2, pn);
         const double ib = rcp_nr(1.0 - l1 * u0 - u1 * l0n);
@@ -402,51 +416,59 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
         F(0, 1, p) = -u1 * u0n * ib;
         F(0, 2, p) = (r1 - l1 * r0 - u1 * r0n) * ib;
     }
-    __syncthreads();
+    gsync();
     int cur = 0;
     double xl = 0.0;
     bool solved = false;
     for (int dl = 1; dl < P; dl <<= 1) {
-        int im = p - dl, ip = p + dl;
-        if (cyclic) {
-            im = im < 0 ? im + P : im;
-            ip = ip >= P ? ip - P : ip;
-        } else {
-            im = im < -1 ? -1 : im;
-            ip = ip > P ? P : ip;
+        if (act) {
+            int im = p - dl, ip = p + dl;
+            if (cyclic) {
+                im = im < 0 ? im + P : im;
+                ip = ip >= P ? ip - P : ip;
+            } else {
+                im = im < -1 ? -1 : im;
+                ip = ip > P ? P : ip;
+            }
+            double li = F(cur, 0, p), ui = F(cur, 1, p), ri = F(cur, 2, p);
+            const double lm = F(cur, 0, im), um = F(cur, 1, im), rm = F(cur, 2, im);
+            const double lp = F(cur, 0, ip), up = F(cur, 1, ip), rp = F(cur, 2, ip);
+            if (cyclic && 2 * dl == P) {
+                const double si = li + ui, sj = lm + um;
+                xl = (ri - si * rm) * rcp_nr(1.0 - si * sj);
+                solved = true;
+            } else {
+                pcr_step(li, ui, ri, lm, um, rm, lp, up, rp);
+                F(cur ^ 1, 0, p) = li;
+                F(cur ^ 1, 1, p) = ui;
+                F(cur ^ 1, 2, p) = ri;
+            }
         }
-        double li = F(cur, 0, p), ui = F(cur, 1, p), ri = F(cur, 2, p);
-        const double lm = F(cur, 0, im), um = F(cur, 1, im), rm = F(cur, 2, im);
-        const double lp = F(cur, 0, ip), up = F(cur, 1, ip), rp = F(cur, 2, ip);
-        if (cyclic && 2 * dl == P) {
-            const double si = li + ui, sj = lm + um;
-            xl = (ri - si * rm) * rcp_nr(1.0 - si * sj);
-            solved = true;
-        } else {
-            pcr_step(li, ui, ri, lm, um, rm, lp, up, rp);
-            F(cur ^ 1, 0, p) = li;
-            F(cur ^ 1, 1, p) = ui;
-            F(cur ^ 1, 2, p) = ri;
-        }
-        __syncthreads();
+        gsync();
         cur ^= 1;
     }
-    if (!solved) xl = F(cur, 2, p);
-    F(cur ^ 1, 2, p) = xl;
-    __syncthreads();
-    double xlm;
-    if (cyclic)
-        xlm = F(cur ^ 1, 2, p == 0 ? P - 1 : p - 1);
-    else
-        xlm = p == 0 ? 0.0 : F(cur ^ 1, 2, p - 1);
-    const double xf = r0 - l0 * xlm - u0 * xl;
+    if (act) {
+        if (!solved) xl = F(cur, 2, p);
+        F(cur ^ 1, 2, p) = xl;
+    }
+    gsync();
+    double xlm = 0.0;
+    if (act) {
+        if (cyclic)
+            xlm = F(cur ^ 1, 2, p == 0 ? P - 1 : p - 1);
+        else
+            xlm = p == 0 ? 0.0 : F(cur ^ 1, 2, p - 1);
+    }
+    const double xf = act ? r0 - l0 * xlm - u0 * xl : 0.0;
+    if (!act) xl = 0.0;
 
     // ------------------------------------------------ back substitution
     double* xp = a.X + row0;
     double nonfinite = fma(xf, 0.0, fma(xl, 0.0, 0.0));
     double xn = xl;
-    // staged: x goes into the B field (no longer read) and leaves coalesced
-    auto XO = [&](int k) -> double& { return stt[1 * fs + k * ks]; };
+    // staged: x overwrites delta in the D field (each row's delta is read just
+    // before) and leaves coalesced
+    auto XO = [&](int k) -> double& { return stt[2 * fs + SL(k)]; };
 #pragma unroll
     for (int k = M - 2; k >= 1; --k) {
         if (k <= m - 2) {
@@ -459,20 +481,71 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
         }
     }
     if constexpr (STAGED) {
-        XO(0) = xf;
-        XO(m - 1) = xl;
-        __syncthreads();
+        if (act) {
+            XO(0) = xf;
+            XO(m - 1) = xl;
+        }
+        gsync();
         double* gX = a.X + o;
-        for (int r = p; r < n; r += P) {
+        for (int r = p; r < n; r += NT) {
             int q, k;
             rag_locate(r, base, rem, inv0, inv1, q, k);
-            gX[r] = stg[1 * fs + q * mp + k];
+            gX[r] = stg[2 * fs + q * M + rag_slot(q, k)];
         }
-    } else {
+    } else if (act) {
         xp[0] = xf;
         xp[m - 1] = xl;
     }
     if (nonfinite != 0.0) raise_status(a.status, ST_NONFINITE);  // NaN != 0
+}
+
+// One launch per bucket shape: one system per CTA of P = blockDim.x threads.
+template <typename TIN, bool STAGED>
+__global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
+    extern __shared__ double rsm[];
+    rag_cta_body<TIN, STAGED>(a, a.tasks[blockIdx.x], (int)blockDim.x, rsm, (int)threadIdx.x, 0);
+}
+
+// Persistent form: every long system of the plan in one launch.  CTAs of
+// RAG_PERSIST_THREADS threads (two per SM) work through three classes of
+// tasks {list index, cyclic, P, staged} (P = 256, 128, 64: the shape each
+// bucket was tuned to), each class's tasks in the table's order (longest
+// first) from its own counter a.next[c] (zeroed before the launch).  In class
+// c the CTA splits into 2^c groups of P threads, each with its own named
+// barrier and shared-memory slice, taking tasks independently; a group moves
+// on to the next class when its class is drained (the next class's groups lie
+// inside it, with barriers of their own).  a.mcap must be RAG_MT.
+constexpr int RAG_PERSIST_THREADS = 256;
+constexpr int RAG_PERSIST_CLASSES = 3;
+// shared-memory slice of a group of P threads (nested: two slices of P / 2
+// fit in one of P)
+__host__ __device__ __forceinline__ size_t rag_persist_slice(int P) {
+    return rag_cta_smem_bytes(64, true, RAG_MT) * (size_t)(P / 64);
+}
+template <typename TIN>
+__global__ void __launch_bounds__(RAG_PERSIST_THREADS, 2) ragged_persist_kernel(const RagArgs a) {
+    extern __shared__ double rsm[];
+    __shared__ int next_task[1 << RAG_PERSIST_CLASSES];  // by barrier id (unique per group)
+    const int tid = threadIdx.x;
+    for (int c = 0; c < RAG_PERSIST_CLASSES; ++c) {
+        const int P = RAG_PERSIST_THREADS >> c;
+        const int g = tid / P, p = tid % P;
+        const int bid = (1 << c) + g;  // 1; 2, 3; 4 .. 7
+        double* sm = rsm + rag_persist_slice(P) / sizeof(double) * g;
+        for (;;) {
+            if (p == 0) next_task[bid] = atomicAdd(&a.next[c], 1);
+            asm volatile("bar.sync %0, %1;" ::"r"(bid), "r"(P) : "memory");
+            const int t = next_task[bid];
+            if (t >= a.cls_count[c]) break;
+            const int4 task = a.tasks[a.cls_first[c] + t];
+            if (task.w)
+                rag_cta_body<TIN, true>(a, task, P, sm, p, bid);
+            else
+                rag_cta_body<TIN, false>(a, task, P, sm, p, bid);
+            // the group's shared memory and next_task are rewritten by its next task
+            asm volatile("bar.sync %0, %1;" ::"r"(bid), "r"(P) : "memory");
+        }
+    }
 }
 
 }  // namespace btdma

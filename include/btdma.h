@@ -237,7 +237,11 @@ int btdma_solve_ragged_f32(btdma_t h, const float* A, const float* B, const floa
  * shape — P lanes of a warp per system (P = 1..32) with 1..8 warps per CTA, or
  * one CTA of P = 64..512 threads per system (<= 16 rows per thread) — with at
  * least 3 rows per thread, on this batch, and keeps the fastest for later
- * solves of the same layout.
+ * solves of the same layout.  Then it times the whole solve two ways — every
+ * CTA-kind shape as a launch of its own, or the CTA-kind buckets of at most
+ * 256 threads in one persistent launch (CTAs split into groups of their
+ * buckets' thread counts, taking systems longest first from a counter) — and
+ * keeps the faster.
  * A..D are double or float as the handle's precision says; X is overwritten.
  * Blocking (it synchronises the stream). */
 int btdma_ragged_autotune(btdma_t h, const void* A, const void* B, const void* C, const void* D,
@@ -255,12 +259,17 @@ typedef struct btdma_ragged_bucket {
                              (long systems); 2: one CTA per system staged through
                              shared memory */
     float tuned_ms;       /* fastest time measured by the autotuner (0 before tuning) */
+    int persistent;       /* 1: the bucket's systems run in the plan's one persistent
+                             launch (CTA-kind buckets of at most 256 threads, when the
+                             autotuner measured that faster than a launch per
+                             shape); 0: a launch of its own shape */
 } btdma_ragged_bucket;
 int btdma_ragged_plan_info(btdma_t h, btdma_ragged_bucket* out, int cap, int* n_out);
 
 /* Replace the launch shapes of the current ragged plan (lanes_per_system and
- * cta_per_system of every bucket; the other fields must match the plan, in
- * plan_info's order): restores a plan tuned earlier, e.g. by another process,
+ * cta_per_system of every bucket, and the persistent launch when any bucket's
+ * persistent is set; the other fields must match the plan, in plan_info's
+ * order): restores a plan tuned earlier, e.g. by another process,
  * without timing again.  Every shape is checked against the limits the
  * autotuner uses (P a power of two, >= 3 rows per thread, per-thread row and
  * shared-memory caps); a rejected plan leaves the current one in place.  No

@@ -210,13 +210,19 @@ def test_ragged_every_launch_shape(cuda, orc, precision):
     assert all(opts)
     assert any((P, 2) in o for o in opts for P in (64, 128, 256))
     assert any((512, 2) in o for o in opts)  # staged 512-thread CTAs (<= 8 rows a thread)
-    for j in range(max(len(o) for o in opts)):
-        want = [o[j % len(o)] for o in opts]
-        s.ragged_set_plan([dict(b, lanes_per_system=P, cta_per_system=k)
-                           for b, (P, k) in zip(plan, want)])
-        assert [(b["lanes_per_system"], b["cta_per_system"]) for b in s.ragged_plan()] == want
-        X.zero_()
-        s.solve_ragged(dA, dB, dC, dD, X, off, per)
-        torch.cuda.synchronize()
-        assert s.status() == 0
-        assert per_system_err(X.cpu().numpy(), ref, off) <= 1e-12, want
+    # each shape as a launch of its own, then in the persistent launch (CTA
+    # kinds of at most 256 threads, split into groups of their thread counts)
+    for pers in (0, 1):
+        for j in range(max(len(o) for o in opts)):
+            want = [o[j % len(o)] for o in opts]
+            s.ragged_set_plan([dict(b, lanes_per_system=P, cta_per_system=k, persistent=pers)
+                               for b, (P, k) in zip(plan, want)])
+            got = s.ragged_plan()
+            assert [(b["lanes_per_system"], b["cta_per_system"]) for b in got] == want
+            assert [b["persistent"] for b in got] == [
+                int(pers and k > 0 and P <= 256) for P, k in want]
+            X.zero_()
+            s.solve_ragged(dA, dB, dC, dD, X, off, per)
+            torch.cuda.synchronize()
+            assert s.status() == 0
+            assert per_system_err(X.cpu().numpy(), ref, off) <= 1e-12, (pers, want)
