@@ -14,6 +14,13 @@
  * in the same order, so this cannot deadlock); point-to-point messages are
  * matched by (source, destination, tag) at wait time.
  *
+ * The reference's channel-flow GPU sources (apps/channel_gpu/
+ * MomentumSolverGPU.cu, PressureSolverGPU.cu) are also compiled against this
+ * header, for their coefficient-build kernels only (oracle/_ref/
+ * libref_channel.so).  The further calls those files name -- MPI_Allreduce,
+ * MPI_Alltoall, MPI_Alltoallv, MPI_Bcast -- are declared so that they compile
+ * and throw if ever called: nothing that drives those kernels calls them.
+ *
  * The product library never includes this file.  It is used by oracle/_ref
  * (the reference built from its own sources) and the CPU baseline only.
  */
@@ -40,6 +47,11 @@ extern struct shim_type shim_type_int;
 #define MPI_SUCCESS 0
 #define MPI_STATUS_IGNORE ((MPI_Status*)0)
 #define MPI_STATUSES_IGNORE ((MPI_Status*)0)
+#define MPI_COMM_NULL ((MPI_Comm)0)
+
+typedef int MPI_Op;
+#define MPI_MAX 1
+#define MPI_SUM 2
 
 int MPI_Allgather(const void* sendbuf, int sendcount, MPI_Datatype sendtype,
                   void* recvbuf, int recvcount, MPI_Datatype recvtype,
@@ -62,6 +74,16 @@ int MPI_Wait(MPI_Request* request, MPI_Status* status);
 int MPI_Waitall(int count, MPI_Request requests[], MPI_Status statuses[]);
 int MPI_Barrier(MPI_Comm comm);
 double MPI_Wtime(void);
+
+/* Declared for the channel sources; they throw (see above). */
+int MPI_Allreduce(const void* sendbuf, void* recvbuf, int count, MPI_Datatype datatype,
+                  MPI_Op op, MPI_Comm comm);
+int MPI_Alltoall(const void* sendbuf, int sendcount, MPI_Datatype sendtype, void* recvbuf,
+                 int recvcount, MPI_Datatype recvtype, MPI_Comm comm);
+int MPI_Alltoallv(const void* sendbuf, const int sendcounts[], const int sdispls[],
+                  MPI_Datatype sendtype, void* recvbuf, const int recvcounts[],
+                  const int rdispls[], MPI_Datatype recvtype, MPI_Comm comm);
+int MPI_Bcast(void* buffer, int count, MPI_Datatype datatype, int root, MPI_Comm comm);
 
 /* Shim control (not MPI): create a communicator of `size` thread ranks and
  * bind the calling thread to `rank` of it. */

@@ -277,5 +277,22 @@ double MPI_Wtime(void) {
     return duration<double>(steady_clock::now().time_since_epoch()).count();
 }
 
+int MPI_Allreduce(const void*, void*, int, MPI_Datatype, MPI_Op, MPI_Comm) {
+    throw std::runtime_error("mpi shim: MPI_Allreduce is not provided");
+}
+
+int MPI_Alltoall(const void*, int, MPI_Datatype, void*, int, MPI_Datatype, MPI_Comm) {
+    throw std::runtime_error("mpi shim: MPI_Alltoall is not provided");
+}
+
+int MPI_Alltoallv(const void*, const int[], const int[], MPI_Datatype, void*, const int[],
+                  const int[], MPI_Datatype, MPI_Comm) {
+    throw std::runtime_error("mpi shim: MPI_Alltoallv is not provided");
+}
+
+int MPI_Bcast(void*, int, MPI_Datatype, int, MPI_Comm) {
+    throw std::runtime_error("mpi shim: MPI_Bcast is not provided");
+}
+
 }  // extern "C"
 

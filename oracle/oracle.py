@@ -51,8 +51,8 @@ def build(with_ref: bool | None = None) -> None:
     if with_ref:
         if ref_dir is None:
             raise RuntimeError("BTDMA_REFERENCE_DIR does not name the reference sources")
-        subprocess.run(["make", "-s", "-C", _HERE, "ref", "ref_gpu", f"REF={ref_dir}"],
-                       check=True)
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", "ref_gpu", "ref_channel",
+                        f"REF={ref_dir}"], check=True)
 
 
 _lib = None
