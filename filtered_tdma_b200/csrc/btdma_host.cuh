@@ -225,6 +225,7 @@ inline int num_sms() {
 // Shape plan of the tiled kernel: systems per group, CTAs per cluster, ring stages.
 struct TilePlan {
     int sys = 0, cl = 0, nst = 0, nseg = 0;
+    int pr = 1;  // sub-segments per thread (2: shared-matrix sweeps of 18..32 sub-segments)
 };
 
 inline int max_smem_per_sm() {
@@ -246,8 +247,15 @@ inline TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4, bool
     if (n_row % TILE_MT != 0) return pl;
     const int nseg = n_row / TILE_MT;
     if (cyclic && (nseg & (nseg - 1)) != 0) return pl;  // periodic PCR needs 2^k rows
-    int sys, cl = 0;
-    if (sh && nseg <= 16) {
+    int sys, cl = 0, pr = 1;
+    if (sh && nseg > 16 && nseg <= 32 && nseg % 2 == 0) {
+        // Longer shared-matrix sweeps: two sub-segments per thread, so a CTA of
+        // 16 systems has at most 256 threads and two share an SM, as for the
+        // shorter sweeps below.
+        sys = 16;
+        cl = 1;
+        pr = 2;
+    } else if (sh && nseg <= 16) {
         // Shared-matrix sweeps of up to 16 sub-segments: CTAs of at most
         // TILE_SH_THREADS threads, two or more per SM, so that one CTA's reduced
         // solve overlaps another's sweeps.  (Longer systems keep one CTA of up
@@ -279,7 +287,7 @@ inline TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4, bool
     int nst = na == 4 ? TILE_MAX_NST : TILE_MAX_NST_CONST;
     size_t cap = (size_t)max_smem_optin();
     if (sh) {  // an equal share of the SM per resident CTA (128 registers a thread)
-        const int per_sm = std::max(1, 65536 / (sys * (nseg / cl) * 128));
+        const int per_sm = std::max(1, 65536 / (sys * (nseg / cl / pr) * 128));
         cap = std::min(cap, (size_t)max_smem_per_sm() / per_sm - 1024);
     }
     while (nst >= 3 &&
@@ -290,12 +298,14 @@ inline TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4, bool
     pl.cl = cl;
     pl.nst = nst;
     pl.nseg = nseg;
+    pl.pr = pr;
     return pl;
 }
 
-template <int SYS, bool CYCLIC, typename TIN = double, typename TC = double, int GEN = 0>
+template <int SYS, bool CYCLIC, typename TIN = double, typename TC = double, int GEN = 0,
+          int PR = 1>
 int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st) {
-    auto kern = tile_f64_kernel<SYS, CYCLIC, TIN, TC, GEN>;
+    auto kern = tile_f64_kernel<SYS, CYCLIC, TIN, TC, GEN, PR>;
     static bool attr_done = false;
     if (!attr_done) {
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -303,7 +313,10 @@ int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st)
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         attr_done = true;
     }
-    const int threads = SYS * a.nseg / a.cl;
+    const int threads = SYS * a.nseg / a.cl / PR;
+    if (PR > 1 && (a.nseg > 32 || a.cl != 1 || (a.nseg / a.cl) % PR != 0))
+        return fail(BTDMA_ERR_UNSUPPORTED, "%d sub-segments per thread need one CTA of <= 32",
+                    PR);
     cudaLaunchConfig_t cfg = {};
     cfg.blockDim = dim3(threads, 1, 1);
     constexpr bool SHT = GEN == 1 || GEN == 3 || GEN == 4;
@@ -519,6 +532,12 @@ int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArg
         a.gtab = tab;
     }
     int rc;
+    if constexpr (GEN == 1 || GEN == 3) {
+        if (pl.pr == 2) {
+            rc = launch_tile_sys<16, CYC, double, double, GEN, 2>(maps, a, st);
+            return rc == BTDMA_OK ? 1 : rc;
+        }
+    }
     switch (pl.sys) {
         case 128: rc = launch_tile_sys<128, CYC, double, double, GEN>(maps, a, st); break;
         case 64: rc = launch_tile_sys<64, CYC, double, double, GEN>(maps, a, st); break;
@@ -536,7 +555,10 @@ inline TilePlan tile_plan_heat_z(int n_row) {
     if (n_row % TILE_MT != 0) return pl;
     const int nseg = n_row / TILE_MT;
     if (nseg < 2 || nseg > 32) return pl;
-    const int T = TILE_HEAT_SYS * nseg;
+    // one sub-segment per thread: with two, the stencil's stage values and the
+    // two recurrences exceed 128 registers and spill
+    const int pr = 1;
+    const int T = TILE_HEAT_SYS * nseg / pr;
     const int per_sm = std::max(1, 65536 / (T * 128));
     const size_t cap = std::min((size_t)max_smem_optin(), (size_t)max_smem_per_sm() / per_sm - 1024);
     int nst = TILE_MAX_NST_CONST;
@@ -548,6 +570,7 @@ inline TilePlan tile_plan_heat_z(int n_row) {
     pl.cl = 1;
     pl.nst = nst;
     pl.nseg = nseg;
+    pl.pr = pr;
     return pl;
 }
 

@@ -238,7 +238,13 @@ __device__ __forceinline__ void tile_cluster_sync(int cl) {
 // 3, were measured at two CTAs per SM as well: at 64 registers a thread they
 // spill and run 1.5x the instructions, which costs more than the second CTA
 // hides.)
-template <int SYS, bool CYCLIC, typename TIN = double, typename TC = double, int GEN = 0>
+// PR: sub-segments per thread.  The shared-matrix sweeps keep only delta per
+// row, so a thread can own two sub-segments (ql and ql + nsc / 2): half the
+// threads per system, two independent recurrences per thread, and CTAs small
+// enough that two share an SM and one's reduced solve overlaps the other's
+// streaming.
+template <int SYS, bool CYCLIC, typename TIN = double, typename TC = double, int GEN = 0,
+          int PR = 1>
 __global__ void __launch_bounds__(TILE_MAX_THREADS, 1)
 tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 const __grid_constant__ CUtensorMap tmC, const __grid_constant__ CUtensorMap tmD,
@@ -248,6 +254,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     constexpr bool CONSTC = GEN != 0;                 // coefficients generated, D only
     constexpr bool SH = GEN == 1 || GEN == 3 || GEN == 4;  // one matrix for all systems (gtab)
     static_assert(GEN != 4 || (SYS == TILE_HEAT_SYS && !CYCLIC), "heat Z sweep: 16 systems");
+    static_assert(PR == 1 || (PR == 2 && SH), "two sub-segments per thread: shared matrix only");
     constexpr int NA = CONSTC ? 1 : 4;                // arrays per ring stage
     constexpr int RPS = tile_rps((int)sizeof(TIN), NA);  // rows per ring stage
     constexpr int SPG = M / RPS;                         // stages per group
@@ -255,7 +262,9 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     extern __shared__ unsigned char smem_raw[];
     const int nseg = args.nseg, cl = args.cl, nst = args.nst;
     const int nsc = nseg / cl;   // sub-segments per CTA
-    const int T = SYS * nsc;     // == blockDim.x
+    const int hsc = nsc / PR;    // thread rows: a thread owns sub-segments ql + h * hsc
+    const int TS = SYS * nsc;    // columns of a ring stage
+    const int T = SYS * hsc;     // == blockDim.x
     const int sub = SYS / cl;    // systems whose reduced system this CTA solves
     const int W = tile_lanes(nseg);
     const bool shuffled = W <= 32;
@@ -367,11 +376,18 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         const bool valid = sys < args.n_sys;
 
         // ------------------------------------------------------ forward pass
-        TC al[M], ga[M], de[M];  // rows 1..M-1 used (register resident)
-        double lam = 0.0;        // GEN == 2: this system's diagonal shift
+        // rows 1..M-1 used (register resident); deP[h]: sub-segment ql + h * hsc
+        TC al[M], ga[M], deP[PR][M];
+        TC db0P[PR], sdP[PR];
+#pragma unroll
+        for (int h = 0; h < PR; ++h) db0P[h] = sdP[h] = 0;
+        TC(&de)[M] = deP[0];  // the one sub-segment of the PR == 1 modes
+        TC& db0 = db0P[0];
+        TC& sd = sdP[0];
+        double lam = 0.0;  // GEN == 2: this system's diagonal shift
         if constexpr (GEN == 2) lam = valid ? args.glam[sys >> 1] : 0.0;
-        TC ab0 = 0, cb0 = 0, db0 = 0;
-        TC pi = 1, sa = 0, sd = 0;
+        TC ab0 = 0, cb0 = 0;
+        TC pi = 1, sa = 0;
         if constexpr (GEN == 4) {
             // Heat Z sweep: the right-hand side of every row is computed here
             // from the theta box of the stage (the reference's rhs_kernel and
@@ -384,24 +400,26 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             const double* hp = args.glam;  // bx, by, dt 3 pi^2, iy, iz
             const int ixg = args.xblk, s0 = g * SYS;
             const int jj = s0 / ixg, ii = s0 % ixg + s;
-            const int q = c * nsc + ql;
-            const int kk0 = q * M;
             const int iy = (int)__ldg(hp + 3), iz = (int)__ldg(hp + 4);
             const double bx = __ldg(hp + 0), by = __ldg(hp + 1), bz = args.cs,
                          srcs = __ldg(hp + 2);
             const double cxi = __ldg(args.ga + ii + 1), cyj = __ldg(args.gb + jj + 1);
             const double diag = 1.0 + (-2.0 * bx) + (-2.0 * by) + (-2.0 * bz);
             const double ubz = -cxi * cyj;
-            double pp0 = 0.0, pp = 0.0, pc = 0.0, tnext = 0.0, tkm0 = 0.0;
+            // per owned sub-segment: row 0's partial sum, the pending row's
+            // partial sum, the previous row's theta, the neighbours' edge rows
+            double pp0[PR], pp[PR], pc[PR], tnext[PR], tkm0[PR];
+#pragma unroll
+            for (int h = 0; h < PR; ++h) pp0[h] = pp[h] = pc[h] = tnext[h] = tkm0[h] = 0.0;
             // the recurrence of the shared-matrix modes on a finished row
-            auto feed = [&](int k, double d) {
-                const double* tr = tabs + (ql * M + k) * 5;
+            auto feed = [&](int h, int k, double d) {
+                const double* tr = tabs + ((ql + h * hsc) * M + k) * 5;
                 if (k == 1) {
-                    de[1] = d * tr[0];
-                    sd = de[1];
+                    deP[h][1] = d * tr[0];
+                    sdP[h] = deP[h][1];
                 } else {
-                    de[k] = d * tr[0] - tr[1] * de[k - 1];
-                    if (k <= M - 2) sd += tr[2] * de[k];
+                    deP[h][k] = d * tr[0] - tr[1] * deP[h][k - 1];
+                    if (k <= M - 2) sdP[h] += tr[2] * deP[h][k];
                 }
             };
 #pragma unroll
@@ -412,76 +430,95 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                 auto at = [&](int qq, int r, int y, int dx) {
                     return sb[((qq * RPS + r) * 3 + y) * TILE_HEAT_BOX_I + s + 1 + dx];
                 };
-                if (j == 0 && q + 1 < nseg) tnext = at(ql + 1, 0, 1, 0);
-                if (j == SPG - 1 && q > 0) tkm0 = at(ql - 1, RPS - 1, 1, 0);
-                double tc[RPS], tl[RPS], tr_[RPS], ym[RPS], yp[RPS];
 #pragma unroll
-                for (int r = 0; r < RPS; ++r) {
-                    tc[r] = at(ql, r, 1, 0);
-                    tl[r] = at(ql, r, 1, -1);
-                    tr_[r] = at(ql, r, 1, 1);
-                    ym[r] = at(ql, r, 0, 0);
-                    yp[r] = at(ql, r, 2, 0);
+                for (int h = 0; h < PR; ++h) {
+                    const int qq = ql + h * hsc;  // sub-segment in the CTA
+                    const int q = c * nsc + qq;
+                    const int kk0 = q * M;
+                    if (j == 0 && q + 1 < nseg) tnext[h] = at(qq + 1, 0, 1, 0);
+                    if (j == SPG - 1 && q > 0) tkm0[h] = at(qq - 1, RPS - 1, 1, 0);
+                    double tc[RPS], tl[RPS], tr_[RPS], ym[RPS], yp[RPS];
+#pragma unroll
+                    for (int r = 0; r < RPS; ++r) {
+                        tc[r] = at(qq, r, 1, 0);
+                        tl[r] = at(qq, r, 1, -1);
+                        tr_[r] = at(qq, r, 1, 1);
+                        ym[r] = at(qq, r, 0, 0);
+                        yp[r] = at(qq, r, 2, 0);
+                    }
+#pragma unroll
+                    for (int r = 0; r < RPS; ++r) {
+                        const int k = j * RPS + r;
+                        const int kk = kk0 + k;
+                        const double tt = tc[r];
+                        const double czk = __ldg(args.gc + kk + 1);
+                        const double ux = -cyj * czk, uy = -cxi * czk;  // x, y wall values
+                        const double tip = ii + 1 < ixg ? tr_[r] : 2.0 * ux - tt;
+                        const double tim = ii > 0 ? tl[r] : 2.0 * ux - tt;
+                        const double tjp = jj + 1 < iy ? yp[r] : 2.0 * uy - tt;
+                        const double tjm = jj > 0 ? ym[r] : 2.0 * uy - tt;
+                        const double src = srcs * cxi * cyj * czk;
+                        double p =
+                            (bx * tip + bx * tim) + (by * tjp + by * tjm) + diag * tt + src;
+                        if (kk == 0) p += bz * (2.0 * ubz - tt) + bz * ((2.0 * ubz - tt) + tt);
+                        if (kk == iz - 1)
+                            p += bz * (2.0 * ubz - tt) + bz * ((2.0 * ubz - tt) + tt);
+                        if (k >= 1) p += bz * pc[h];  // lower neighbour: the previous row
+                        if (k == 1) pp0[h] += bz * tt;  // row 0's upper neighbour
+                        if (k >= 2) feed(h, k - 1, pp[h] + bz * tt);
+                        if (k == 0)
+                            pp0[h] = p;
+                        else
+                            pp[h] = p;
+                        pc[h] = tt;
+                    }
+                    // PR == 2: one sub-segment's stage values live at a time
+                    if constexpr (PR == 2) __syncwarp();
                 }
-                __syncwarp();
-                if (lane == 0) {
-                    mbar_arrive(&empty[slot]);
-                    if (t >= 1 && warp == tw && t - 1 + nst < total && ok) {
-                        ok = mbar_wait_bounded(&empty[pslot], pphase, args.status);
-                        if (ok) issue(t - 1 + nst);
+                {  // release the slot (after the arithmetic: measured spill-free)
+                    __syncwarp();
+                    if (lane == 0) {
+                        mbar_arrive(&empty[slot]);
+                        if (t >= 1 && warp == tw && t - 1 + nst < total && ok) {
+                            ok = mbar_wait_bounded(&empty[pslot], pphase, args.status);
+                            if (ok) issue(t - 1 + nst);
+                        }
+                    }
+                    pslot = slot;
+                    pphase = phase;
+                    ++t;
+                    if (++tw == nwarps) tw = 0;
+                    if (++slot == nst) {
+                        slot = 0;
+                        phase ^= 1u;
                     }
                 }
-                pslot = slot;
-                pphase = phase;
-                ++t;
-                if (++tw == nwarps) tw = 0;
-                if (++slot == nst) {
-                    slot = 0;
-                    phase ^= 1u;
-                }
-#pragma unroll
-                for (int r = 0; r < RPS; ++r) {
-                    const int k = j * RPS + r;
-                    const int kk = kk0 + k;
-                    const double tt = tc[r];
-                    const double czk = __ldg(args.gc + kk + 1);
-                    const double ux = -cyj * czk, uy = -cxi * czk;  // x, y wall values
-                    const double tip = ii + 1 < ixg ? tr_[r] : 2.0 * ux - tt;
-                    const double tim = ii > 0 ? tl[r] : 2.0 * ux - tt;
-                    const double tjp = jj + 1 < iy ? yp[r] : 2.0 * uy - tt;
-                    const double tjm = jj > 0 ? ym[r] : 2.0 * uy - tt;
-                    const double src = srcs * cxi * cyj * czk;
-                    double p = (bx * tip + bx * tim) + (by * tjp + by * tjm) + diag * tt + src;
-                    if (kk == 0) p += bz * (2.0 * ubz - tt) + bz * ((2.0 * ubz - tt) + tt);
-                    if (kk == iz - 1) p += bz * (2.0 * ubz - tt) + bz * ((2.0 * ubz - tt) + tt);
-                    if (k >= 1) p += bz * pc;  // lower neighbour: the previous row
-                    if (k == 1) pp0 += bz * tt;  // row 0's upper neighbour
-                    if (k >= 2) feed(k - 1, pp + bz * tt);
-                    if (k == 0)
-                        pp0 = p;
-                    else
-                        pp = p;
-                    pc = tt;
-                }
             }
-            // row M - 1: the next sub-segment's first row above it (the top wall's
+            // row M - 1: the next sub-segment's first row above it            // row M - 1: the next sub-segment's first row above it (the top wall's
             // ghost is already in); row 0: the previous sub-segment's last row
             // below it (or the bottom wall's ghost, already in)
-            feed(M - 1, kk0 + M - 1 == iz - 1 ? pp : pp + bz * tnext);
-            db0 = (kk0 == 0 ? pp0 : pp0 + bz * tkm0) * tabs[(ql * M) * 5];
+#pragma unroll
+            for (int h = 0; h < PR; ++h) {
+                const int qq = ql + h * hsc;
+                const int kk0 = (c * nsc + qq) * M;
+                feed(h, M - 1, kk0 + M - 1 == iz - 1 ? pp[h] : pp[h] + bz * tnext[h]);
+                db0P[h] = (kk0 == 0 ? pp0[h] : pp0[h] + bz * tkm0[h]) * tabs[(qq * M) * 5];
+            }
         } else {
 #pragma unroll
             for (int j = 0; j < SPG; ++j) {
                 if (ok) ok = mbar_wait_bounded(&full[slot], phase, args.status);
-                TIN a2[RPS], b2[RPS], c2[RPS], d2[RPS];  // widened where used
+                TIN a2[RPS], b2[RPS], c2[RPS], d2[PR][RPS];  // widened where used
 #pragma unroll
                 for (int r = 0; r < RPS; ++r) {
                     if constexpr (!CONSTC) {
-                        a2[r] = st[0 * RPS * T + r * SYS];
-                        b2[r] = st[1 * RPS * T + r * SYS];
-                        c2[r] = st[2 * RPS * T + r * SYS];
+                        a2[r] = st[0 * RPS * TS + r * SYS];
+                        b2[r] = st[1 * RPS * TS + r * SYS];
+                        c2[r] = st[2 * RPS * TS + r * SYS];
                     }
-                    d2[r] = st[(NA - 1) * RPS * T + r * SYS];
+#pragma unroll
+                    for (int h = 0; h < PR; ++h)
+                        d2[h][r] = st[(NA - 1) * RPS * TS + h * hsc * RPS * SYS + r * SYS];
                 }
                 __syncwarp();
                 if (lane == 0) {
@@ -504,74 +541,68 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                     phase ^= 1u;
                     st = ring + toff;
                 }
+                if constexpr (SH) {  // right-hand side only, factors from gtab
 #pragma unroll
-                for (int r = 0; r < RPS; ++r) {
-                    const int k = j * RPS + r;
-                    if constexpr (SH) {  // right-hand side only, factors from gtab
-                        const double* tr = tabs + (ql * M + k) * 5;
-                        const double d = (double)d2[r];
+                    for (int h = 0; h < PR; ++h)
+#pragma unroll
+                        for (int r = 0; r < RPS; ++r) {
+                            const int k = j * RPS + r;
+                            const double* tr = tabs + ((ql + h * hsc) * M + k) * 5;
+                            const double d = (double)d2[h][r];
+                            if (k == 0) {
+                                db0P[h] = d * tr[0];
+                            } else if (k == 1) {
+                                deP[h][1] = d * tr[0];
+                                sdP[h] = deP[h][1];
+                            } else {
+                                deP[h][k] = d * tr[0] - tr[1] * deP[h][k - 1];
+                                if (k <= M - 2) sdP[h] += tr[2] * deP[h][k];
+                            }
+                        }
+                } else {
+#pragma unroll
+                    for (int r = 0; r < RPS; ++r) {
+                        const int k = j * RPS + r;
+                        TC a, b, cc, d = (TC)d2[0][r];
+                        if constexpr (GEN == 2) {
+                            const int kg = (c * nsc + ql) * M + k;  // row of the system
+                            const double ta = args.ga[kg], tc = args.gc[kg];
+                            a = (TC)ta;
+                            cc = (TC)tc;
+                            b = (TC)(-(ta + tc) - lam);
+                            if (args.gpin != 0 && kg == 0 && (sys >> 1) == 0) {
+                                a = 0;
+                                b = 1;
+                                cc = 0;
+                                d = 0;
+                            }
+                        } else {
+                            a = (TC)a2[r];
+                            b = (TC)b2[r];
+                            cc = (TC)c2[r];
+                        }
                         if (k == 0) {
-                            db0 = d * tr[0];
+                            const TC ib = rcp_tc(b);
+                            ab0 = a * ib;
+                            cb0 = cc * ib;
+                            db0 = d * ib;
                         } else if (k == 1) {
-                            de[1] = d * tr[0];
+                            const TC ib = rcp_tc(b);
+                            al[1] = a * ib;
+                            ga[1] = cc * ib;
+                            de[1] = d * ib;
+                            sa = al[1];
                             sd = de[1];
                         } else {
-                            de[k] = d * tr[0] - tr[1] * de[k - 1];
-                            if (k <= M - 2) sd += tr[2] * de[k];
-                        }
-                        continue;
-                    }
-                    TC a, b, cc, d = (TC)d2[r];
-                    if constexpr (GEN == 1) {
-                        const int q = c * nsc + ql;  // sub-segment of this thread
-                        const bool wall = args.cbound != 0 && ((q == 0 && k == 0) ||
-                                                               (q == nseg - 1 && k == M - 1));
-                        a = (TC)-args.cs;
-                        cc = (TC)-args.cs;
-                        b = (TC)(1.0 + 2.0 * args.cs + (wall ? args.cs : 0.0));
-                    } else if constexpr (GEN == 3) {
-                        const int kg = (c * nsc + ql) * M + k;  // row of the system
-                        a = (TC)(-args.cs * args.ga[kg]);
-                        cc = (TC)(-args.cs * args.gc[kg]);
-                        b = (TC)(1.0 + args.cs * args.gb[kg]);
-                    } else if constexpr (GEN == 2) {
-                        const int kg = (c * nsc + ql) * M + k;  // row of the system
-                        const double ta = args.ga[kg], tc = args.gc[kg];
-                        a = (TC)ta;
-                        cc = (TC)tc;
-                        b = (TC)(-(ta + tc) - lam);
-                        if (args.gpin != 0 && kg == 0 && (sys >> 1) == 0) {
-                            a = 0;
-                            b = 1;
-                            cc = 0;
-                            d = 0;
-                        }
-                    } else {
-                        a = (TC)a2[r];
-                        b = (TC)b2[r];
-                        cc = (TC)c2[r];
-                    }
-                    if (k == 0) {
-                        const TC ib = rcp_tc(b);
-                        ab0 = a * ib;
-                        cb0 = cc * ib;
-                        db0 = d * ib;
-                    } else if (k == 1) {
-                        const TC ib = rcp_tc(b);
-                        al[1] = a * ib;
-                        ga[1] = cc * ib;
-                        de[1] = d * ib;
-                        sa = al[1];
-                        sd = de[1];
-                    } else {
-                        const TC inv = rcp_tc(b - a * ga[k - 1]);
-                        ga[k] = cc * inv;
-                        de[k] = (d - a * de[k - 1]) * inv;
-                        al[k] = -a * al[k - 1] * inv;
-                        if (k <= M - 2) {
-                            pi = -ga[k - 1] * pi;
-                            sa += pi * al[k];
-                            sd += pi * de[k];
+                            const TC inv = rcp_tc(b - a * ga[k - 1]);
+                            ga[k] = cc * inv;
+                            de[k] = (d - a * de[k - 1]) * inv;
+                            al[k] = -a * al[k - 1] * inv;
+                            if (k <= M - 2) {
+                                pi = -ga[k - 1] * pi;
+                                sa += pi * al[k];
+                                sd += pi * de[k];
+                            }
                         }
                     }
                 }
@@ -579,18 +610,22 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         }
         // reduced rows of this sub-segment -> red[f][ql][s]
         if constexpr (SH) {
-            const double* sb = tabs + nsc * M * 5 + ql * 6;
-            double* w = red + ql * RP + s;
-            if (rhs_red) {  // r0 | r1 only
-                w[0] = sb[0] * (double)db0 - sb[1] * (double)sd;
-                w[fstride] = (double)de[M - 1];
-            } else {
-                w[2 * fstride] = sb[0] * (double)db0 - sb[1] * (double)sd;
-                w[5 * fstride] = (double)de[M - 1];
-                w[0 * fstride] = sb[2];
-                w[1 * fstride] = sb[3];
-                w[3 * fstride] = sb[4];
-                w[4 * fstride] = sb[5];
+#pragma unroll
+            for (int h = 0; h < PR; ++h) {
+                const int qq = ql + h * hsc;
+                const double* sb = tabs + nsc * M * 5 + qq * 6;
+                double* w = red + qq * RP + s;
+                if (rhs_red) {  // r0 | r1 only
+                    w[0] = sb[0] * (double)db0P[h] - sb[1] * (double)sdP[h];
+                    w[fstride] = (double)deP[h][M - 1];
+                } else {
+                    w[2 * fstride] = sb[0] * (double)db0P[h] - sb[1] * (double)sdP[h];
+                    w[5 * fstride] = (double)deP[h][M - 1];
+                    w[0 * fstride] = sb[2];
+                    w[1 * fstride] = sb[3];
+                    w[3 * fstride] = sb[4];
+                    w[4 * fstride] = sb[5];
+                }
             }
         } else {
             const TC pi_last = -ga[M - 2] * pi;
@@ -717,10 +752,13 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         tile_cluster_sync(cl);
 
         // --------------------------------------------------- back substitution
-        const double x_first = xr[ql * RP + s];
-        const double x_last = xr[fstride + ql * RP + s];
-        if (valid) {
-            const int q = c * nsc + ql;
+#pragma unroll
+        for (int h = 0; h < PR; ++h) {
+            const int qq = ql + h * hsc;  // sub-segment in the CTA
+            const double x_first = xr[qq * RP + s];
+            const double x_last = xr[fstride + qq * RP + s];
+            if (!valid) continue;
+            const int q = c * nsc + qq;
             double* xp = args.X + (size_t)(q * M + M - 1) * ns + sys;  // row M-1
             if constexpr (CONSTC) {
                 if (args.xblk > 0)
@@ -746,8 +784,8 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             for (int k = M - 2; k >= 1; --k) {
                 xp -= ns;
                 if constexpr (SH) {
-                    const double* tr = tabs + (ql * M + k) * 5;
-                    xn = (double)de[k] - tr[3] * x_first - tr[4] * xn;
+                    const double* tr = tabs + (qq * M + k) * 5;
+                    xn = (double)deP[h][k] - tr[3] * x_first - tr[4] * xn;
                 } else {
                     xn = (double)de[k] - (double)al[k] * x_first - (double)ga[k] * xn;
                 }
