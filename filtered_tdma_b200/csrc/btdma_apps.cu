@@ -95,15 +95,32 @@ int heat_enqueue(btdma_heat_t h, double* theta, cudaStream_t st, cudaEvent_t* ev
     heat_y_fold_kernel<<<dim3((g.ix + 127) / 128, 2, g.iz), b1, 0, st>>>(theta, h->buf1, g);
     CK(cudaGetLastError());
     mark(3);
-    if ((rc = sweep(1, h->buf1, h->buf1, g.ix * g.iz, g.iy, g.by, 0, 0, 0, 0, "Y"))) return rc;
-    mark(4);
-    heat_y_to_x_kernel<<<dim3(tx, ty, g.iz), bt, 0, st>>>(theta, h->buf1, h->buf0, g);
+    if (tile_plan(g.iy, false, 8, 1, true, true).sys != 0) {
+        // Y sweep: system kk * ix + ii, row jj; the solution goes straight into
+        // the X sweep's layout [ii][kk][jj] (rows contiguous: staged and stored
+        // coalesced), then the X wall folds on its two wall planes
+        if ((rc = sweep(1, h->buf1, h->buf0, g.ix * g.iz, g.iy, g.by, g.ix, g.iy, g.iz * g.iy, 1,
+                        "Y")))
+            return rc;
+        mark(4);
+        heat_x_fold_kernel<<<dim3((g.iy + 127) / 128, 2, g.iz), b1, 0, st>>>(theta, h->buf0, g);
+    } else {
+        if ((rc = sweep(1, h->buf1, h->buf1, g.ix * g.iz, g.iy, g.by, 0, 0, 0, 0, "Y")))
+            return rc;
+        mark(4);
+        heat_y_to_x_kernel<<<dim3(tx, ty, g.iz), bt, 0, st>>>(theta, h->buf1, h->buf0, g);
+    }
     CK(cudaGetLastError());
     mark(5);
-    if ((rc = sweep(2, h->buf0, h->buf0, g.iy * g.iz, g.ix, g.bx, 0, 0, 0, 0, "X"))) return rc;
+    // X sweep: system kk * iy + jj, row ii; the solution goes straight into
+    // theta's interior (update_theta_kernel's copy, solve_theta.cu:335-347):
+    // a system's rows are contiguous there, so the sweep stages them in shared
+    // memory and stores them coalesced
+    const int plane = (g.ix + 2) * (g.iy + 2);
+    if ((rc = sweep(2, h->buf0, theta + plane + (g.ix + 2) + 1, g.iy * g.iz, g.ix, g.bx, g.iy,
+                    plane, g.ix + 2, 1, "X")))
+        return rc;
     mark(6);
-    heat_update_kernel<<<dim3(ty, tx, g.iz), bt, 0, st>>>(theta, h->buf0, g);
-    CK(cudaGetLastError());
     mark(7);
     return BTDMA_OK;
 }

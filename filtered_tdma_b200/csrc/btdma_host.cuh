@@ -242,7 +242,9 @@ inline int max_smem_per_sm() {
 
 // na: arrays per ring stage (4, or 1 for the constant-coefficient D-only ring).
 // sh: shared-matrix sweep (factor table and lane table in shared memory).
-inline TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4, bool sh = false) {
+// tstore: the sweep stores rows contiguously through a shared tile (xrs == 1).
+inline TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4, bool sh = false,
+                          bool tstore = false) {
     TilePlan pl;
     if (n_row % TILE_MT != 0) return pl;
     const int nseg = n_row / TILE_MT;
@@ -290,8 +292,8 @@ inline TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4, bool
         const int per_sm = std::max(1, 65536 / (sys * (nseg / cl / pr) * 128));
         cap = std::min(cap, (size_t)max_smem_per_sm() / per_sm - 1024);
     }
-    while (nst >= 3 &&
-           tile_smem_bytes(sys, nseg / cl, nseg, sys / cl, nst, elem, na, sh) > cap)
+    while (nst >= 3 && tile_smem_bytes(sys, nseg / cl, nseg, sys / cl, nst, elem, na, sh, 0,
+                                       tstore && cl == 1 ? n_row / pr : 0) > cap)
         --nst;
     if (nst < 3) return pl;
     pl.sys = sys;
@@ -320,8 +322,11 @@ int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st)
     cudaLaunchConfig_t cfg = {};
     cfg.blockDim = dim3(threads, 1, 1);
     constexpr bool SHT = GEN == 1 || GEN == 3 || GEN == 4;
+    // the kernel stages row-contiguous stores (xrs == 1) in a tile after the mbarriers
+    const bool tstore = SHT && a.xblk > 0 && a.xrs == 1 && a.cl == 1;
     cfg.dynamicSmemBytes = tile_smem_bytes(SYS, a.nseg / a.cl, a.nseg, SYS / a.cl, a.nst,
-                                           (int)sizeof(TIN), GEN ? 1 : 4, SHT, GEN);
+                                           (int)sizeof(TIN), GEN ? 1 : 4, SHT, GEN,
+                                           tstore ? a.n_row / PR : 0);
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -508,7 +513,8 @@ template <int GEN, bool CYC = false>
 int try_tile_gen(const double* D, double* X, int n_sys, int n_row, const TileArgs& gen,
                  unsigned* status, cudaStream_t st, double* tab = nullptr,
                  bool table_ready = false) {
-    const TilePlan pl = tile_plan(n_row, CYC, 8, 1, GEN == 1 || GEN == 3);
+    const bool tstore = (GEN == 1 || GEN == 3) && gen.xblk > 0 && gen.xrs == 1;
+    const TilePlan pl = tile_plan(n_row, CYC, 8, 1, GEN == 1 || GEN == 3, tstore);
     if (pl.sys == 0 || !tma_ok_elem(D, n_sys, 8)) return 0;
     const int nsc = pl.nseg / pl.cl;
     CUtensorMap maps[4];

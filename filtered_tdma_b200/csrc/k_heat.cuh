@@ -24,10 +24,14 @@
 //     more than 32 sub-segments);
 //   * the Z sweep stores its solution straight into the Y sweep's layout
 //     ([kk][jj][ii] -> [jj][kk][ii], the tiled solve's mapped store; the Y wall
-//     folds then touch the two wall planes only), so the only copies left are
-//     the two transposes, Y -> X and X -> theta, through shared-memory tiles.
-//     (Storing the X sweep straight into theta was measured slower than the
-//     transpose it saves: its lanes write rows 2 KB apart.)
+//     folds then touch the two wall planes only), and the X sweep straight
+//     into theta (its rows are contiguous there: the tiled solve stages each
+//     group's solution in shared memory and stores it coalesced; storing it
+//     row by row from the lanes, rows 2 KB apart, was slower than a separate
+//     transpose); the Y sweep stores into the X sweep's layout the same way,
+//     and the X wall folds touch the two wall planes.  heat_y_to_x_kernel
+//     (a transpose through shared-memory tiles) remains for Y sweeps whose
+//     staged store does not fit.
 #pragma once
 
 #include "btdma_common.cuh"
@@ -132,6 +136,23 @@ __global__ void __launch_bounds__(128) heat_y_fold_kernel(const double* __restri
     Dy[((size_t)jj * g.iz + kk) * g.ix + ii] += g.by * ((2.0 * ubc - t) + t);
 }
 
+// X wall folds on the Y solution, already in the X-sweep layout [ii][kk][jj]
+// (build_lhs_x_kernel's right-hand-side terms, solve_theta.cu:256-332): planes
+// ii = 0 and ii = ix - 1 get base * (ghost + boundary cell), added to the
+// value as heat_y_to_x_kernel adds it.  Grid (iy / 128, 2, iz).
+__global__ void __launch_bounds__(128) heat_x_fold_kernel(const double* __restrict__ theta,
+                                                          double* __restrict__ Dx,
+                                                          const HeatGeom g) {
+    const int jj = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ii = blockIdx.y == 0 ? 0 : g.ix - 1;
+    const int kk = blockIdx.z;
+    if (jj >= g.iy) return;
+    const int i = ii + 1, j = jj + 1, k = kk + 1;
+    const double t = theta[heat_full(g, i, j, k)];
+    const double ubc = -g.cy[j] * g.cz[k];
+    Dx[((size_t)ii * g.iz + kk) * g.iy + jj] += g.bx * ((2.0 * ubc - t) + t);
+}
+
 constexpr int HEAT_TILE = 32;
 
 // Y solution [jj][kk][ii] -> X-sweep layout [ii][kk][jj] plus the X wall folds
@@ -165,28 +186,6 @@ __global__ void __launch_bounds__(256) heat_y_to_x_kernel(const double* __restri
             }
             Dx[((size_t)ii * g.iz + kk) * g.iy + jj] = v;
         }
-    }
-}
-
-// theta(i, j, k) = X solution [ii][kk][jj] (update_theta_kernel,
-// solve_theta.cu:335-347), transposed back through a shared tile.
-__global__ void __launch_bounds__(256) heat_update_kernel(double* __restrict__ theta,
-                                                          const double* __restrict__ Dx,
-                                                          const HeatGeom g) {
-    __shared__ double tile[HEAT_TILE][HEAT_TILE + 1];
-    const int jj0 = blockIdx.x * HEAT_TILE, ii0 = blockIdx.y * HEAT_TILE, kk = blockIdx.z;
-#pragma unroll
-    for (int u = 0; u < HEAT_TILE / 8; ++u) {  // block (HEAT_TILE, 8)
-        const int r = threadIdx.y + 8 * u;
-        const int jj = jj0 + threadIdx.x, ii = ii0 + r;
-        if (ii < g.ix && jj < g.iy) tile[r][threadIdx.x] = Dx[((size_t)ii * g.iz + kk) * g.iy + jj];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < HEAT_TILE / 8; ++u) {  // block (HEAT_TILE, 8)
-        const int r = threadIdx.y + 8 * u;
-        const int ii = ii0 + threadIdx.x, jj = jj0 + r;
-        if (ii < g.ix && jj < g.iy) theta[heat_full(g, ii + 1, jj + 1, kk + 1)] = tile[threadIdx.x][r];
     }
 }
 

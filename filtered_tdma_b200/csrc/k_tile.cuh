@@ -100,9 +100,12 @@ struct TileArgs {
         // map instead of the plain [n_row][n_sys]: with xblk > 0, row j of
         // system s goes to  X + (s / xblk) * xbs + (s % xblk) * xss + j * xrs
         // (xrs > 0).  The heat step writes its Z sweep in the Y sweep's layout
-        // and its X sweep into the ghosted field, without a copy pass.  (A union
-        // with the refinement fields: a larger argument struct made ptxas spill
-        // more in every instantiation.)
+        // and its X sweep into the ghosted field, without a copy pass.  xrs == 1
+        // (a system's rows contiguous) in a shared-matrix sweep of one CTA per
+        // group stages the group's x in shared memory and stores every
+        // system's rows with coalesced warp stores (the launch adds the tile,
+        // tile_tstore_bytes).  (A union with the refinement fields: a larger
+        // argument struct made ptxas spill more in every instantiation.)
         struct {
             int xblk, xbs, xss, xrs;
         };
@@ -189,13 +192,23 @@ __host__ __device__ __forceinline__ size_t tile_ring_bytes(int sys, int nsc, int
 __host__ __device__ __forceinline__ size_t tile_tab_doubles(int nsc) {
     return (size_t)nsc * TILE_MT * 5 + (size_t)nsc * 6;
 }
+// Row-contiguous stores (xrs == 1): a [sys][rows + 1] tile of x after the
+// mbarriers, rows = n_row / PR (a thread owning two sub-segments stages and
+// stores the group's two halves in turn); the odd pitch keeps the back
+// substitution's writes, 16 systems a warp, on distinct banks.
+__host__ __device__ __forceinline__ size_t tile_tstore_bytes(int sys, int rows) {
+    return (size_t)sys * (rows + 1) * sizeof(double);
+}
 __host__ __device__ __forceinline__ size_t tile_smem_bytes(int sys, int nsc, int nseg, int sub,
                                                            int nst, int elem = 8, int na = 4,
-                                                           bool shared_tab = false, int gen = 0) {
+                                                           bool shared_tab = false, int gen = 0,
+                                                           int tstore_rows = 0) {
     return tile_ring_bytes(sys, nsc, nst, elem, na, gen) +
            (shared_tab ? tile_tab_doubles(nsc) * sizeof(double) : 0) +
            tile_fixed_doubles(sys, nsc, nseg, sub, shared_tab) * sizeof(double) +
-           2ull * nst * sizeof(uint64_t) + 128;
+           (gen == 4 ? ((size_t)nseg * TILE_MT + 2) * sizeof(double) : 0) +
+           2ull * nst * sizeof(uint64_t) + 128 +
+           (tstore_rows > 0 ? tile_tstore_bytes(sys, tstore_rows) : 0);
 }
 
 __device__ __forceinline__ void tma_load_3d(void* smem_dst, const CUtensorMap* map, int x, int y,
@@ -280,9 +293,14 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     const int gs = nseg + 2;
     double* tabs = pcr + (shuffled ? 0 : 6 * gs * sub);  // SH: this CTA's factor table
     double* lanes = tabs + (SH ? tile_tab_doubles(nsc) : 0);  // rhs_red: lane table [k][p]
-    uint64_t* full =
-        reinterpret_cast<uint64_t*>(lanes + (rhs_red ? 32 * TILE_RED_LANE : 0));
+    // GEN == 4: the cos(pi z) table of the rows (ghosts included), read every row
+    double* czt = lanes + (rhs_red ? 32 * TILE_RED_LANE : 0);
+    uint64_t* full = reinterpret_cast<uint64_t*>(czt + (GEN == 4 ? args.n_row + 2 : 0));
     uint64_t* empty = full + nst;
+    // row-contiguous stores through a shared tile (shared-matrix modes, one CTA)
+    const bool tstore = SH && args.xblk > 0 && args.xrs == 1 && cl == 1;
+    double* xt = reinterpret_cast<double*>(empty + nst);  // [SYS][n_row / PR + 1] when tstore
+    const int xtp = args.n_row / PR + 1;
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
@@ -314,6 +332,8 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             for (int i = threadIdx.x; i < 32 * TILE_RED_LANE; i += blockDim.x)
                 lanes[(i % TILE_RED_LANE) * 32 + i / TILE_RED_LANE] = g2[i];
         }
+        if constexpr (GEN == 4)
+            for (int i = threadIdx.x; i < args.n_row + 2; i += blockDim.x) czt[i] = args.gc[i];
     }
     if (!shuffled && tid < sub) {  // zero guard rows of the PCR buffers
         for (int f = 0; f < 6; ++f) {
@@ -406,6 +426,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             const double cxi = __ldg(args.ga + ii + 1), cyj = __ldg(args.gb + jj + 1);
             const double diag = 1.0 + (-2.0 * bx) + (-2.0 * by) + (-2.0 * bz);
             const double ubz = -cxi * cyj;
+            const double sxy = srcs * cxi * cyj;  // the source term's x, y factor
             // per owned sub-segment: row 0's partial sum, the pending row's
             // partial sum, the previous row's theta, the neighbours' edge rows
             double pp0[PR], pp[PR], pc[PR], tnext[PR], tkm0[PR];
@@ -451,13 +472,13 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                         const int k = j * RPS + r;
                         const int kk = kk0 + k;
                         const double tt = tc[r];
-                        const double czk = __ldg(args.gc + kk + 1);
+                        const double czk = czt[kk + 1];
                         const double ux = -cyj * czk, uy = -cxi * czk;  // x, y wall values
                         const double tip = ii + 1 < ixg ? tr_[r] : 2.0 * ux - tt;
                         const double tim = ii > 0 ? tl[r] : 2.0 * ux - tt;
                         const double tjp = jj + 1 < iy ? yp[r] : 2.0 * uy - tt;
                         const double tjm = jj > 0 ? ym[r] : 2.0 * uy - tt;
-                        const double src = srcs * cxi * cyj * czk;
+                        const double src = sxy * czk;
                         double p =
                             (bx * tip + bx * tim) + (by * tjp + by * tjm) + diag * tt + src;
                         if (kk == 0) p += bz * (2.0 * ubz - tt) + bz * ((2.0 * ubz - tt) + tt);
@@ -757,44 +778,63 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             const int qq = ql + h * hsc;  // sub-segment in the CTA
             const double x_first = xr[qq * RP + s];
             const double x_last = xr[fstride + qq * RP + s];
-            if (!valid) continue;
-            const int q = c * nsc + qq;
-            double* xp = args.X + (size_t)(q * M + M - 1) * ns + sys;  // row M-1
-            if constexpr (CONSTC) {
-                if (args.xblk > 0)
-                    xp = args.X + (ptrdiff_t)(sys / args.xblk) * (ptrdiff_t)args.xbs +
-                         (ptrdiff_t)(sys % args.xblk) * (ptrdiff_t)args.xss +
-                         (size_t)(q * M + M - 1) * ns;
-            }
-            // corrections are accumulated only by the FP32 inner solve of
-            // refinement (the FP64-arithmetic instantiations keep the plain
-            // store); the old x of all M rows is loaded before any store
-            double xo[M] = {};
-            bool acc = false;
-            if constexpr (sizeof(TC) == 4) {
-                acc = args.accumulate != 0;
-                if (acc) {
-#pragma unroll
-                    for (int k = 0; k < M; ++k) xo[k] = xp[-(ptrdiff_t)(M - 1 - k) * (ptrdiff_t)ns];
+            if (valid) {
+                const int q = c * nsc + qq;
+                double* xp = args.X + (size_t)(q * M + M - 1) * ns + sys;  // row M-1
+                if constexpr (CONSTC) {
+                    if (tstore)  // staged, rows contiguous (relative to this half's first row)
+                        xp = xt + (size_t)s * xtp + ql * M + M - 1;
+                    else if (args.xblk > 0)
+                        xp = args.X + (ptrdiff_t)(sys / args.xblk) * (ptrdiff_t)args.xbs +
+                             (ptrdiff_t)(sys % args.xblk) * (ptrdiff_t)args.xss +
+                             (size_t)(q * M + M - 1) * ns;
                 }
-            }
-            *xp = acc ? xo[M - 1] + x_last : x_last;
-            double xn = x_last;
+                // corrections are accumulated only by the FP32 inner solve of
+                // refinement (the FP64-arithmetic instantiations keep the plain
+                // store); the old x of all M rows is loaded before any store
+                double xo[M] = {};
+                bool acc = false;
+                if constexpr (sizeof(TC) == 4) {
+                    acc = args.accumulate != 0;
+                    if (acc) {
 #pragma unroll
-            for (int k = M - 2; k >= 1; --k) {
+                        for (int k = 0; k < M; ++k) xo[k] = xp[-(ptrdiff_t)(M - 1 - k) * (ptrdiff_t)ns];
+                    }
+                }
+                *xp = acc ? xo[M - 1] + x_last : x_last;
+                double xn = x_last;
+#pragma unroll
+                for (int k = M - 2; k >= 1; --k) {
+                    xp -= ns;
+                    if constexpr (SH) {
+                        const double* tr = tabs + (qq * M + k) * 5;
+                        xn = (double)deP[h][k] - tr[3] * x_first - tr[4] * xn;
+                    } else {
+                        xn = (double)de[k] - (double)al[k] * x_first - (double)ga[k] * xn;
+                    }
+                    nonfinite = fma(xn, 0.0, nonfinite);
+                    *xp = acc ? xo[k] + xn : xn;
+                }
                 xp -= ns;
-                if constexpr (SH) {
-                    const double* tr = tabs + (qq * M + k) * 5;
-                    xn = (double)deP[h][k] - tr[3] * x_first - tr[4] * xn;
-                } else {
-                    xn = (double)de[k] - (double)al[k] * x_first - (double)ga[k] * xn;
-                }
-                nonfinite = fma(xn, 0.0, nonfinite);
-                *xp = acc ? xo[k] + xn : xn;
+                *xp = acc ? xo[0] + x_first : x_first;
+                nonfinite = fma(x_first, 0.0, fma(x_last, 0.0, nonfinite));
             }
-            xp -= ns;
-            *xp = acc ? xo[0] + x_first : x_first;
-            nonfinite = fma(x_first, 0.0, fma(x_last, 0.0, nonfinite));
+            if (tstore) {
+                // this half's x from the tile, each system's rows by one warp
+                // with coalesced stores; the tile is written again after the
+                // barrier below, or after the next group's two barriers
+                const int r0 = h * hsc * M, nr = hsc * M;
+                __syncthreads();
+                for (int ss = warp; ss < SYS; ss += nwarps) {
+                    const int sg = g * SYS + ss;
+                    if (sg >= args.n_sys) break;
+                    double* dst = args.X + (ptrdiff_t)(sg / args.xblk) * (ptrdiff_t)args.xbs +
+                                  (ptrdiff_t)(sg % args.xblk) * (ptrdiff_t)args.xss + r0;
+                    const double* src = xt + (size_t)ss * xtp;
+                    for (int r = lane; r < nr; r += 32) dst[r] = src[r];
+                }
+                if (h + 1 < PR) __syncthreads();
+            }
         }
     }
     if (nonfinite != 0.0) raise_status(args.status, ST_NONFINITE);  // NaN != 0
