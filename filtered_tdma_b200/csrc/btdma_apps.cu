@@ -435,7 +435,8 @@ struct btdma_momentum {
     int pbc[2] = {0, 0};
     double* tab = nullptr;  // [dir][comp][ta, tb, tc][n_dir rows]
     size_t tab_off[3][3] = {};
-    double* buf = nullptr;  // nx * ny * nz, the sweep layout
+    double* buf = nullptr;   // nx * ny * nz, the sweep layout
+    double* buf2 = nullptr;  // a second one: the fused step's y-sweep input
     // factor tables per (dir, comp), gstride apart, and what each was last
     // built for: reused while the coefficient and the stream stay the same.
     // A second set of 9 tables serves captured sweeps: a graph rebuilds its
@@ -536,6 +537,7 @@ int btdma_momentum_create(int nx, int ny, int nz, const double* dx0, const doubl
         cudaMemcpy(h->tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice) !=
             cudaSuccess ||
         cudaMalloc(&h->buf, sizeof(double) * (size_t)nx * ny * nz) != cudaSuccess ||
+        cudaMalloc(&h->buf2, sizeof(double) * (size_t)nx * ny * nz) != cudaSuccess ||
         cudaMalloc(&h->gtab, sizeof(double) * 18 * h->gstride) != cudaSuccess ||
         cudaMalloc(&h->raw, sizeof(double) * raw.size()) != cudaSuccess ||
         cudaMemcpy(h->raw, raw.data(), sizeof(double) * raw.size(), cudaMemcpyHostToDevice) !=
@@ -552,6 +554,7 @@ int btdma_momentum_destroy(btdma_momentum_t h) {
     if (!h) return BTDMA_OK;
     cudaFree(h->tab);
     cudaFree(h->buf);
+    cudaFree(h->buf2);
     cudaFree(h->gtab);
     cudaFree(h->status);
     cudaFree(h->raw);
@@ -596,6 +599,53 @@ int btdma_momentum_set_backend(btdma_momentum_t h, int method, int P, int flags,
     h->eps_constant = eps_constant;
     return BTDMA_OK;
 }
+
+namespace {
+
+// One momentum sweep of the tiled solve with generated coefficients: D in the
+// sweep's layout (system index fastest), x stored through the layout map
+// (system s, row r -> X + (s / xblk) xbs + (s % xblk) xss + r xrs).  This
+// (dir, comp)'s factor table is built here unless the last build was for the
+// same coefficient on the same stream; inside a stream capture it is always
+// built, into the capture set of tables, so that a graph carries its own
+// tables and its replays leave the cached ones intact.
+int mom_tile_sweep(btdma_momentum_t h, int dir, int comp, const double* D, double* X, int xblk,
+                   int xbs, int xss, int xrs, double c, cudaStream_t stream) {
+    const MomGeom& g = h->g;
+    const int n[3] = {g.nx, g.ny, g.nz};
+    const int n_sys = g.nx * g.ny * g.nz / n[dir];
+    TileArgs t = {};
+    t.cs = c;
+    t.ga = h->tab + h->tab_off[dir][comp];
+    t.gb = t.ga + n[dir];
+    t.gc = t.gb + n[dir];
+    t.xblk = xblk;
+    t.xbs = xbs;
+    t.xss = xss;
+    t.xrs = xrs;
+    auto& key = h->gkey[dir][comp];
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(stream, &cap));
+    const bool capturing = cap != cudaStreamCaptureStatusNone;
+    const bool ready = !capturing && key.valid && key.c == c && key.stream == stream;
+    double* const gt =
+        h->gtab + (size_t)((capturing ? 9 : 0) + dir * 3 + comp) * h->gstride;
+    if (!ready && !capturing) key.valid = false;  // rebuilt below
+    const bool cyc = dir < 2 && h->pbc[dir] != 0;
+    const int rc = cyc ? try_tile_gen<3, true>(D, X, n_sys, n[dir], t, h->status, stream, gt,
+                                               ready)
+                       : try_tile_gen<3, false>(D, X, n_sys, n[dir], t, h->status, stream, gt,
+                                                ready);
+    if (rc != 1) return rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "sweep not tileable");
+    if (!capturing) {
+        key.valid = true;
+        key.c = c;
+        key.stream = stream;
+    }
+    return BTDMA_OK;
+}
+
+}  // namespace
 
 int btdma_momentum_sweep(btdma_momentum_t h, int dir, int comp, const double* q, double* dst,
                          double c, cudaStream_t stream) {
@@ -647,81 +697,58 @@ int btdma_momentum_sweep(btdma_momentum_t h, int dir, int comp, const double* q,
         CK(cudaGetLastError());
         return BTDMA_OK;
     }
-    TileArgs t = {};
-    t.cs = c;
-    t.ga = h->tab + h->tab_off[dir][comp];
-    t.gb = t.ga + n[dir];
-    t.gc = t.gb + n[dir];
     const dim3 b1(128, 1, 1), bt(MOM_TILE, 8, 1);
-    // this (dir, comp)'s factor table: built in this call unless the last build
-    // was for the same coefficient on the same stream; always built inside a
-    // stream capture, into the capture set of tables, so that a graph carries
-    // its own tables and its replays leave the cached ones intact
-    auto& key = h->gkey[dir][comp];
-    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-    CK(cudaStreamIsCapturing(stream, &cap));
-    const bool capturing = cap != cudaStreamCaptureStatusNone;
-    const bool ready = !capturing && key.valid && key.c == c && key.stream == stream;
-    double* const gt =
-        h->gtab + (size_t)((capturing ? 9 : 0) + dir * 3 + comp) * h->gstride;
-    if (!ready && !capturing) key.valid = false;  // rebuilt below
-    // z and y sweeps store straight into dst's interior through the tiled
-    // solve's layout map (system s = (a, i) with i = s % nx fastest, row r):
-    //   z: dst(i, j = s / nx + 1, k = r + 1);  y: dst(i, j = r + 1, k = s / nx + 1)
     const int sp = (g.nx + 2) * (g.ny + 2);  // plane stride (< 2^31, checked at create)
     double* const dst_in = dst + sp + (g.nx + 2) + 1;  // dst(1, 1, 1)
-    t.xblk = g.nx;
-    t.xss = 1;
-    int rc;
     if (dir == 2) {
+        // z: system s = (j, i), i = s % nx fastest, row r -> dst(i, j, k = r + 1)
         mom_gather_kernel<2><<<dim3((g.nx + 127) / 128, (g.ny + MOM_GR - 1) / MOM_GR, g.nz), b1,
-                                 0, stream>>>(
-            q, h->buf, g, comp == 2 ? 1 : 0);
+                                 0, stream>>>(q, h->buf, g, comp == 2 ? 1 : 0);
         CK(cudaGetLastError());
-        t.xbs = g.nx + 2;
-        t.xrs = sp;
-        rc = try_tile_gen<3, false>(h->buf, dst_in, n_sys, g.nz, t, h->status, stream, gt, ready);
-    } else if (dir == 1) {
+        return mom_tile_sweep(h, 2, comp, h->buf, dst_in, g.nx, g.nx + 2, 1, sp, c, stream);
+    }
+    if (dir == 1) {
+        // y: system s = (k, i), row r -> dst(i, j = r + 1, k)
         mom_gather_kernel<1><<<dim3((g.nx + 127) / 128, (g.nz + MOM_GR - 1) / MOM_GR, g.ny), b1,
                                  0, stream>>>(q, h->buf, g, 0);
         CK(cudaGetLastError());
-        t.xbs = sp;
-        t.xrs = g.nx + 2;
-        rc = h->pbc[1] ? try_tile_gen<3, true>(h->buf, dst_in, n_sys, g.ny, t, h->status,
-                                               stream, gt, ready)
-                       : try_tile_gen<3, false>(h->buf, dst_in, n_sys, g.ny, t, h->status,
-                                                stream, gt, ready);
-    } else {
-        t.xblk = 0;  // x: the plain layout, transposed back below
-        mom_gather_x_kernel<<<dim3((g.nx + MOM_TILE - 1) / MOM_TILE,
-                                   (g.ny + MOM_TILE - 1) / MOM_TILE, g.nz), bt, 0, stream>>>(
-            q, h->buf, g);
-        CK(cudaGetLastError());
-        rc = h->pbc[0] ? try_tile_gen<3, true>(h->buf, h->buf, n_sys, g.nx, t, h->status,
-                                               stream, gt, ready)
-                       : try_tile_gen<3, false>(h->buf, h->buf, n_sys, g.nx, t, h->status,
-                                                stream, gt, ready);
+        return mom_tile_sweep(h, 1, comp, h->buf, dst_in, g.nx, sp, 1, g.nx + 2, c, stream);
     }
-    if (rc != 1) return rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "sweep not tileable");
-    if (!capturing) {
-        key.valid = true;
-        key.c = c;
-        key.stream = stream;
-    }
-    if (dir == 0) {
-        mom_scatter_x_kernel<<<dim3((g.ny + MOM_TILE - 1) / MOM_TILE,
-                                    (g.nx + MOM_TILE - 1) / MOM_TILE, g.nz), bt, 0, stream>>>(
-            h->buf, dst, g);
-        CK(cudaGetLastError());
-    }
-    return BTDMA_OK;
+    // x: system s = (k, j), j = s % ny fastest, row r -> dst(i = r + 1, j, k): a
+    // system's rows are contiguous in the field, so the sweep stages them and
+    // stores them coalesced (no transposing scatter)
+    mom_gather_x_kernel<<<dim3((g.nx + MOM_TILE - 1) / MOM_TILE, (g.ny + MOM_TILE - 1) / MOM_TILE,
+                               g.nz), bt, 0, stream>>>(q, h->buf, g);
+    CK(cudaGetLastError());
+    return mom_tile_sweep(h, 0, comp, h->buf, dst_in, g.ny, sp, g.nx + 2, 1, c, stream);
 }
 
 int btdma_momentum_adi(btdma_momentum_t h, int comp, double* rhs, double* q_out, double c,
                        cudaStream_t stream) {
-    int rc = btdma_momentum_sweep(h, 2, comp, rhs, rhs, c, stream);
-    if (!rc) rc = btdma_momentum_sweep(h, 1, comp, rhs, rhs, c, stream);
-    if (!rc) rc = btdma_momentum_sweep(h, 0, comp, rhs, q_out, c, stream);
+    if (!h || !rhs || !q_out) return fail(BTDMA_ERR_ARG, "null argument");
+    if (comp < 0 || comp > 2) return fail(BTDMA_ERR_ARG, "comp must be 0, 1 or 2");
+    if (h->backend != BTDMA_PASCAL) {  // the reference's sequence, z and y in place on rhs
+        int rc = btdma_momentum_sweep(h, 2, comp, rhs, rhs, c, stream);
+        if (!rc) rc = btdma_momentum_sweep(h, 1, comp, rhs, rhs, c, stream);
+        if (!rc) rc = btdma_momentum_sweep(h, 0, comp, rhs, q_out, c, stream);
+        return rc;
+    }
+    // Each sweep stores its solution straight into the next sweep's layout:
+    // z [k][j][i] -> y layout [j][k][i] (mapped rows), y -> x layout [i][k][j]
+    // (contiguous rows: staged, coalesced), x -> q_out's interior (staged);
+    // rhs is only read.
+    const MomGeom& g = h->g;
+    const dim3 b1(128, 1, 1);
+    const int sp = (g.nx + 2) * (g.ny + 2);
+    mom_gather_kernel<2><<<dim3((g.nx + 127) / 128, (g.ny + MOM_GR - 1) / MOM_GR, g.nz), b1, 0,
+                           stream>>>(rhs, h->buf, g, comp == 2 ? 1 : 0);
+    CK(cudaGetLastError());
+    int rc = mom_tile_sweep(h, 2, comp, h->buf, h->buf2, g.nx, g.nx * g.nz, 1, g.nx, c, stream);
+    if (!rc)
+        rc = mom_tile_sweep(h, 1, comp, h->buf2, h->buf, g.nx, g.ny, g.nz * g.ny, 1, c, stream);
+    if (!rc)
+        rc = mom_tile_sweep(h, 0, comp, h->buf, q_out + sp + (g.nx + 2) + 1, g.ny, sp, g.nx + 2,
+                            1, c, stream);
     return rc;
 }
 
