@@ -3,7 +3,8 @@ viscous half-step of apps/channel_gpu/MomentumSolverGPU.cu (adi_z_, adi_y_,
 adi_x_ with k_build_* / k_scatter_*).
 
     m = ChannelMomentum(256, 256, 256)            # x, y periodic; z stretched walls
-    m.adi(comp, rhs, q, nu_dt_half)               # z, y in place on rhs; x into q
+    m.adi(comp, rhs, q, nu_dt_half)               # z, y, x sweeps of rhs into q
+                                                  # (a Filtered backend: z, y in place on rhs)
 """
 from __future__ import annotations
 

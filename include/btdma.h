@@ -339,8 +339,12 @@ int btdma_poisson_status(btdma_poisson_t h, unsigned* status, cudaStream_t strea
  * / y sweeps when pbc_x / pbc_y.  dx*, dmx* are HOST arrays of n + 2 entries
  * (ghosts included), read at create time.  Coefficients are generated inside
  * the solve, never stored.  btdma_momentum_sweep reads q and writes dst (may
- * be q); btdma_momentum_adi runs z and y in place on rhs and x into q_out, as
- * MomentumSolverGPU::advance's diffuse step does after k_lap.  PaScaL (exact)
+ * be q); btdma_momentum_adi runs the z, y and x sweeps of
+ * MomentumSolverGPU::advance's diffuse step after k_lap and writes the result
+ * into q_out's interior.  With the default (PaScaL) backend it only reads
+ * rhs: each sweep stores its solution straight into the next sweep's layout
+ * (four kernels); with a Filtered backend it runs the reference's sequence, z
+ * and y in place on rhs.  PaScaL (exact)
  * solves; n a multiple of 16, n / 16 a power of two for periodic sweeps.  The
  * handle keeps each (dir, comp) factor table until c or the stream changes;
  * a sweep captured into a CUDA graph builds its table on every replay, into a
