@@ -603,14 +603,18 @@ int btdma_momentum_set_backend(btdma_momentum_t h, int method, int P, int flags,
 namespace {
 
 // One momentum sweep of the tiled solve with generated coefficients: D in the
-// sweep's layout (system index fastest), x stored through the layout map
-// (system s, row r -> X + (s / xblk) xbs + (s % xblk) xss + r xrs).  This
+// sweep's layout (system index fastest), or for the z sweep (zfield non-null)
+// the ghosted field itself, read by the sweep without a gather (pin: the w
+// component's row 0 is x = 0); x stored through the layout map (system s, row
+// r -> X + (s / xblk) xbs + (s % xblk) xss + r xrs).  Returns 0 with `taken`
+// false when a zfield sweep's shape is not tiled that way.  This
 // (dir, comp)'s factor table is built here unless the last build was for the
 // same coefficient on the same stream; inside a stream capture it is always
 // built, into the capture set of tables, so that a graph carries its own
 // tables and its replays leave the cached ones intact.
 int mom_tile_sweep(btdma_momentum_t h, int dir, int comp, const double* D, double* X, int xblk,
-                   int xbs, int xss, int xrs, double c, cudaStream_t stream) {
+                   int xbs, int xss, int xrs, double c, cudaStream_t stream,
+                   const double* zfield = nullptr, bool* taken = nullptr) {
     const MomGeom& g = h->g;
     const int n[3] = {g.nx, g.ny, g.nz};
     const int n_sys = g.nx * g.ny * g.nz / n[dir];
@@ -632,10 +636,16 @@ int mom_tile_sweep(btdma_momentum_t h, int dir, int comp, const double* D, doubl
         h->gtab + (size_t)((capturing ? 9 : 0) + dir * 3 + comp) * h->gstride;
     if (!ready && !capturing) key.valid = false;  // rebuilt below
     const bool cyc = dir < 2 && h->pbc[dir] != 0;
-    const int rc = cyc ? try_tile_gen<3, true>(D, X, n_sys, n[dir], t, h->status, stream, gt,
-                                               ready)
-                       : try_tile_gen<3, false>(D, X, n_sys, n[dir], t, h->status, stream, gt,
-                                                ready);
+    int rc;
+    if (zfield) {
+        rc = try_mom_z(zfield, X, g.nx, g.ny, g.nz, t, comp == 2 ? 1 : 0, h->status, stream, gt,
+                       ready);
+        if (taken) *taken = rc == 1;
+        if (rc == 0) return BTDMA_OK;  // the caller gathers instead
+    } else {
+        rc = cyc ? try_tile_gen<3, true>(D, X, n_sys, n[dir], t, h->status, stream, gt, ready)
+                 : try_tile_gen<3, false>(D, X, n_sys, n[dir], t, h->status, stream, gt, ready);
+    }
     if (rc != 1) return rc < 0 ? rc : fail(BTDMA_ERR_UNSUPPORTED, "sweep not tileable");
     if (!capturing) {
         key.valid = true;
@@ -701,7 +711,15 @@ int btdma_momentum_sweep(btdma_momentum_t h, int dir, int comp, const double* q,
     const int sp = (g.nx + 2) * (g.ny + 2);  // plane stride (< 2^31, checked at create)
     double* const dst_in = dst + sp + (g.nx + 2) + 1;  // dst(1, 1, 1)
     if (dir == 2) {
-        // z: system s = (j, i), i = s % nx fastest, row r -> dst(i, j, k = r + 1)
+        // z: system s = (j, i), i = s % nx fastest, row r -> dst(i, j, k = r + 1);
+        // read from q directly unless q is dst (in place: other CTAs' stores
+        // would land in rows still to be read) or the shape is not tiled so
+        bool taken = false;
+        if (q != dst) {
+            const int rc = mom_tile_sweep(h, 2, comp, nullptr, dst_in, g.nx, g.nx + 2, 1, sp, c,
+                                          stream, q, &taken);
+            if (rc || taken) return rc;
+        }
         mom_gather_kernel<2><<<dim3((g.nx + 127) / 128, (g.ny + MOM_GR - 1) / MOM_GR, g.nz), b1,
                                  0, stream>>>(q, h->buf, g, comp == 2 ? 1 : 0);
         CK(cudaGetLastError());
@@ -734,16 +752,21 @@ int btdma_momentum_adi(btdma_momentum_t h, int comp, double* rhs, double* q_out,
         return rc;
     }
     // Each sweep stores its solution straight into the next sweep's layout:
-    // z [k][j][i] -> y layout [j][k][i] (mapped rows), y -> x layout [i][k][j]
-    // (contiguous rows: staged, coalesced), x -> q_out's interior (staged);
-    // rhs is only read.
+    // z (read from rhs itself) -> y layout [j][k][i] (mapped rows), y -> x
+    // layout [i][k][j] (contiguous rows: staged, coalesced), x -> q_out's
+    // interior (staged); rhs is only read.
     const MomGeom& g = h->g;
     const dim3 b1(128, 1, 1);
     const int sp = (g.nx + 2) * (g.ny + 2);
-    mom_gather_kernel<2><<<dim3((g.nx + 127) / 128, (g.ny + MOM_GR - 1) / MOM_GR, g.nz), b1, 0,
-                           stream>>>(rhs, h->buf, g, comp == 2 ? 1 : 0);
-    CK(cudaGetLastError());
-    int rc = mom_tile_sweep(h, 2, comp, h->buf, h->buf2, g.nx, g.nx * g.nz, 1, g.nx, c, stream);
+    bool taken = false;  // the z sweep reads rhs directly when its shape allows
+    int rc = mom_tile_sweep(h, 2, comp, nullptr, h->buf2, g.nx, g.nx * g.nz, 1, g.nx, c, stream,
+                            rhs, &taken);
+    if (!rc && !taken) {
+        mom_gather_kernel<2><<<dim3((g.nx + 127) / 128, (g.ny + MOM_GR - 1) / MOM_GR, g.nz), b1,
+                               0, stream>>>(rhs, h->buf, g, comp == 2 ? 1 : 0);
+        CK(cudaGetLastError());
+        rc = mom_tile_sweep(h, 2, comp, h->buf, h->buf2, g.nx, g.nx * g.nz, 1, g.nx, c, stream);
+    }
     if (!rc)
         rc = mom_tile_sweep(h, 1, comp, h->buf2, h->buf, g.nx, g.ny, g.nz * g.ny, 1, c, stream);
     if (!rc)

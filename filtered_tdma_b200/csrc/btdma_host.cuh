@@ -321,7 +321,7 @@ int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st)
                     PR);
     cudaLaunchConfig_t cfg = {};
     cfg.blockDim = dim3(threads, 1, 1);
-    constexpr bool SHT = GEN == 1 || GEN == 3 || GEN == 4;
+    constexpr bool SHT = GEN == 1 || GEN == 3 || GEN == 4 || GEN == 5;
     // the kernel stages row-contiguous stores (xrs == 1) in a tile after the mbarriers
     const bool tstore = SHT && a.xblk > 0 && a.xrs == 1 && a.cl == 1;
     cfg.dynamicSmemBytes = tile_smem_bytes(SYS, a.nseg / a.cl, a.nseg, SYS / a.cl, a.nst,
@@ -628,6 +628,88 @@ inline int try_heat_z(const double* theta, double* X, int ix, int iy, int iz, co
     a.status = status;
     a.gtab = tab;
     const int rc = launch_tile_sys<TILE_HEAT_SYS, false, double, double, 4>(maps, a, st);
+    return rc == BTDMA_OK ? 1 : rc;
+}
+
+// Momentum z sweep reading the ghosted field directly (GEN 5 of the tiled
+// kernel): 16 systems per group, two sub-segments per thread above 16
+// sub-segments (as tile_plan's shared-matrix sweeps), or sys == 0.
+inline TilePlan tile_plan_field_z(int n_row) {
+    TilePlan pl;
+    if (n_row % TILE_MT != 0) return pl;
+    const int nseg = n_row / TILE_MT;
+    if (nseg < 2 || nseg > 32) return pl;
+    const int pr = nseg > 16 && nseg % 2 == 0 ? 2 : 1;
+    const int T = TILE_HEAT_SYS * nseg / pr;
+    const int per_sm = std::max(1, 65536 / (T * 128));
+    const size_t cap = std::min((size_t)max_smem_optin(), (size_t)max_smem_per_sm() / per_sm - 1024);
+    int nst = TILE_MAX_NST_CONST;
+    while (nst >= 3 &&
+           tile_smem_bytes(TILE_HEAT_SYS, nseg, nseg, TILE_HEAT_SYS, nst, 8, 1, true, 5) > cap)
+        --nst;
+    if (nst < 3) return pl;
+    pl.sys = TILE_HEAT_SYS;
+    pl.cl = 1;
+    pl.nst = nst;
+    pl.nseg = nseg;
+    pl.pr = pr;
+    return pl;
+}
+
+// 4-D view of a ghosted field q [(nz + 2) x (ny + 2) x (nx + 2)] for the z
+// sweep: (x = i, y = j, row within the sub-segment, sub-segment) from plane
+// k = 1; boxes of TILE_HEAT_BOX_I x 1 x 4 rows x nsc sub-segments.
+inline bool make_field_row_map(CUtensorMap* map, const double* q, int nx, int ny, int nseg,
+                               int nsc) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    const size_t rx = (size_t)nx + 2, plane = rx * ((size_t)ny + 2);
+    cuuint64_t dims[4] = {(cuuint64_t)rx, (cuuint64_t)ny + 2, (cuuint64_t)TILE_MT,
+                          (cuuint64_t)nseg};
+    cuuint64_t strides[3] = {rx * sizeof(double), plane * sizeof(double),
+                             (cuuint64_t)TILE_MT * plane * sizeof(double)};
+    cuuint32_t box[4] = {(cuuint32_t)TILE_HEAT_BOX_I, 1u, (cuuint32_t)tile_rps(8, 1),
+                         (cuuint32_t)nsc};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(q + plane), dims,
+                    strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+// The momentum z sweep straight from the ghosted field q (no gather): system
+// s = (j - 1) nx + (i - 1), row k - 1; x through gen's layout map (xblk = nx).
+// gen carries the GEN 3 row tables (ga, gb, gc), cs and the map; pin: row 0 is
+// x = 0 (the w component).  tab: the (z, comp) factor table, built here unless
+// table_ready.  Returns 1 when launched, 0 when the shape is not taken, < 0 on
+// error.
+inline int try_mom_z(const double* q, double* X, int nx, int ny, int nz, const TileArgs& gen,
+                     int pin, unsigned* status, cudaStream_t st, double* tab, bool table_ready) {
+    const TilePlan pl = tile_plan_field_z(nz);
+    if (pl.sys == 0 || nx % TILE_HEAT_SYS != 0 || (reinterpret_cast<uintptr_t>(q) & 15) != 0 ||
+        ((size_t)(nx + 2) * 8) % 16 != 0 || gen.xblk != nx)
+        return 0;
+    CUtensorMap maps[4];
+    if (!make_field_row_map(&maps[3], q, nx, ny, pl.nseg, pl.nseg)) return 0;
+    maps[0] = maps[1] = maps[2] = maps[3];  // not read in this mode
+    TileArgs a = gen;
+    a.X = X;
+    a.n_sys = nx * ny;
+    a.n_row = nz;
+    a.nseg = pl.nseg;
+    a.cl = pl.cl;
+    a.nst = pl.nst;
+    a.n_groups = a.n_sys / TILE_HEAT_SYS;
+    a.status = status;
+    a.gpin = pin;
+    if (!table_ready) {
+        tile_table_kernel<3, false><<<(pl.nseg + 127) / 128, 128, 0, st>>>(a, tab);
+        CK(cudaGetLastError());
+    }
+    a.gtab = tab;
+    const int rc = pl.pr == 2
+                       ? launch_tile_sys<TILE_HEAT_SYS, false, double, double, 5, 2>(maps, a, st)
+                       : launch_tile_sys<TILE_HEAT_SYS, false, double, double, 5>(maps, a, st);
     return rc == BTDMA_OK ? 1 : rc;
 }
 

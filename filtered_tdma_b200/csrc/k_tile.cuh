@@ -177,10 +177,21 @@ __host__ __device__ __forceinline__ size_t tile_fixed_doubles(int sys, int nsc, 
 // and y neighbours) per row instead of one D value per system.
 constexpr int TILE_HEAT_SYS = 16;
 constexpr int TILE_HEAT_BOX_I = TILE_HEAT_SYS + 2;
+// GEN == 5 (momentum z sweep reading the ghosted field): one row of 18 cells.
+// tile_stage_box_elems: what a stage's TMA boxes deliver (its transaction
+// count); tile_stage_elems: the distance between stages, rounded up to 128
+// bytes, since a tensor copy's shared-memory destination must be 128-byte
+// aligned (the 18-cell boxes of GEN 4 / 5 are not, for an odd nsc).
+__host__ __device__ __forceinline__ int tile_stage_box_elems(int sys, int nsc, int elem, int na,
+                                                             int gen = 0) {
+    return gen == 4   ? TILE_HEAT_BOX_I * 3 * tile_rps(elem, na) * nsc
+           : gen == 5 ? TILE_HEAT_BOX_I * tile_rps(elem, na) * nsc
+                      : na * tile_rps(elem, na) * sys * nsc;
+}
 __host__ __device__ __forceinline__ int tile_stage_elems(int sys, int nsc, int elem, int na,
                                                          int gen = 0) {
-    return gen == 4 ? TILE_HEAT_BOX_I * 3 * tile_rps(elem, na) * nsc
-                    : na * tile_rps(elem, na) * sys * nsc;
+    const int q = 128 / elem;
+    return (tile_stage_box_elems(sys, nsc, elem, na, gen) + q - 1) / q * q;
 }
 // na: arrays per ring stage (4: A, B, C, D; 1: D only).
 __host__ __device__ __forceinline__ size_t tile_ring_bytes(int sys, int nsc, int nst, int elem,
@@ -265,8 +276,10 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     namespace cg = cooperative_groups;
     constexpr int M = TILE_MT;
     constexpr bool CONSTC = GEN != 0;                 // coefficients generated, D only
-    constexpr bool SH = GEN == 1 || GEN == 3 || GEN == 4;  // one matrix for all systems (gtab)
+    // one matrix for all systems (gtab)
+    constexpr bool SH = GEN == 1 || GEN == 3 || GEN == 4 || GEN == 5;
     static_assert(GEN != 4 || (SYS == TILE_HEAT_SYS && !CYCLIC), "heat Z sweep: 16 systems");
+    static_assert(GEN != 5 || (SYS == TILE_HEAT_SYS && !CYCLIC), "field-box sweep: 16 systems");
     static_assert(PR == 1 || (PR == 2 && SH), "two sub-segments per thread: shared matrix only");
     constexpr int NA = CONSTC ? 1 : 4;                // arrays per ring stage
     constexpr int RPS = tile_rps((int)sizeof(TIN), NA);  // rows per ring stage
@@ -352,7 +365,9 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                          ? (args.n_groups - cluster_id + n_clusters - 1) / n_clusters
                          : 0;
     const int total = n_my * SPG;  // ring stages this CTA consumes
-    const uint32_t stage_bytes = (uint32_t)sstride * sizeof(TIN);
+    // bytes the TMA boxes of a stage deliver (the stage stride may be padded)
+    const uint32_t stage_bytes =
+        (uint32_t)tile_stage_box_elems(SYS, nsc, (int)sizeof(TIN), NA, GEN) * sizeof(TIN);
 
     auto issue = [&](int t) {  // one thread
         const int slot = t % nst;
@@ -366,6 +381,13 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             // sub-segment (the map's base is plane k = 1)
             const int s0 = g * SYS;
             tma_load_4d(dst, &tmD, s0 % args.xblk, s0 / args.xblk, k0, c * nsc, &full[slot]);
+            return;
+        }
+        if constexpr (GEN == 5) {
+            // the field's row (x from the system's left neighbour, ghosted
+            // index ii0; y = jj + 1), RPS rows of every sub-segment
+            const int s0 = g * SYS;
+            tma_load_4d(dst, &tmD, s0 % args.xblk, s0 / args.xblk + 1, k0, c * nsc, &full[slot]);
             return;
         }
         if constexpr (!CONSTC) {
@@ -538,8 +560,13 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                         c2[r] = st[2 * RPS * TS + r * SYS];
                     }
 #pragma unroll
-                    for (int h = 0; h < PR; ++h)
-                        d2[h][r] = st[(NA - 1) * RPS * TS + h * hsc * RPS * SYS + r * SYS];
+                    for (int h = 0; h < PR; ++h) {
+                        if constexpr (GEN == 5)  // box [sub-segment][row][x], x = system + 1
+                            d2[h][r] = ring[(size_t)slot * sstride +
+                                            ((ql + h * hsc) * RPS + r) * TILE_HEAT_BOX_I + s + 1];
+                        else
+                            d2[h][r] = st[(NA - 1) * RPS * TS + h * hsc * RPS * SYS + r * SYS];
+                    }
                 }
                 __syncwarp();
                 if (lane == 0) {
@@ -569,7 +596,12 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                         for (int r = 0; r < RPS; ++r) {
                             const int k = j * RPS + r;
                             const double* tr = tabs + ((ql + h * hsc) * M + k) * 5;
-                            const double d = (double)d2[h][r];
+                            double d = (double)d2[h][r];
+                            // GEN == 5 with gpin: row 0 of the system is x = 0
+                            // (the w component's first face, k_build_z)
+                            if (GEN == 5 && args.gpin != 0 && c * nsc + ql + h * hsc == 0 &&
+                                k == 0)
+                                d = 0.0;
                             if (k == 0) {
                                 db0P[h] = d * tr[0];
                             } else if (k == 1) {

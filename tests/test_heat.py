@@ -61,12 +61,13 @@ def test_gpu_steps_graph_and_eager_agree_non_cubic(cuda, orc):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("grid", [(16, 384, 16), (16, 16, 512), (256, 16, 16), (16, 16, 256),
-                                  (128, 16, 16)])
+                                  (128, 16, 16), (32, 48, 48), (16, 16, 80)])
 def test_gpu_step_long_sweeps_match_oracle(cuda, orc, grid):
     # the shared-matrix sweeps at the sub-segment counts of the 256 x 384 x 512
-    # step: Y 384 rows (24 sub-segments, a 384-thread CTA), Z 512 rows (32, one
-    # 512-thread CTA), X 256 rows (16, two 256-thread CTAs per SM); also 16 and
-    # 8 sub-segments along Z and X
+    # step: Y 384 rows (24 sub-segments, two per thread), Z 512 rows (32, the
+    # fused right-hand side), X 256 rows (16, two 256-thread CTAs per SM); also
+    # 16 and 8 sub-segments along Z and X, and odd sub-segment counts (3, 5)
+    # along Z, whose theta boxes need the ring's 128-byte stage padding
     from filtered_tdma_b200.heat import HeatADI, dt_from_rho
     ix, iy, iz = grid
     dt = dt_from_rho(1.0 / 3.0, iz, option="strong")
