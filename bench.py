@@ -693,13 +693,13 @@ def main():
             "frac_of_peak": 48 * cells / (ms * 1e-3) / 1e9 / peak,
             # the design's field passes of 16 B: Z sweep reading theta (its
             # right-hand side computed inside the solve) into the Y layout, Y
-            # sweep, Y -> X, X sweep, X -> theta
-            "design_bytes_per_cell": 80,
+            # sweep into the X layout, X sweep into theta (plus the wall planes)
+            "design_bytes_per_cell": 48,
             "parity": "tests/test_heat.py::test_gpu_step_benched_grid_matches_oracle",
-            # 6 kernels a step (the sweeps' factor tables are built at
+            # 5 kernels a step (the sweeps' factor tables are built at
             # create): Z sweep with the right-hand side, Y wall folds, Y sweep,
-            # Y -> X, X sweep, X -> theta
-            "launches_per_step": 6, "graph": True,
+            # X wall folds, X sweep
+            "launches_per_step": 5, "graph": True,
             "finite": bool(torch.isfinite(th).all().item())}
         heat.close()
         del th
@@ -737,8 +737,9 @@ def main():
 
         # Channel momentum ADI (implicit viscous half-step of one velocity
         # component: z, y, x sweeps) on the reference's 256^3 channel grid (x, y
-        # periodic, z tanh-stretched walls); per sweep a gather, a generated-
-        # coefficient solve and a scatter: 6 passes of 16 B per cell.
+        # periodic, z tanh-stretched walls): three generated-coefficient
+        # sweeps, the z sweep reading the field, each storing into the next
+        # sweep's layout, the x sweep into the field: 3 passes of 16 B per cell.
         from filtered_tdma_b200.momentum import ChannelMomentum
         mm = ChannelMomentum(256, 256, 256, gamma3=1.5)
         mrhs = torch.rand(mm.shape, dtype=torch.float64, device=dev)
@@ -762,11 +763,9 @@ def main():
             "algorithmic_bytes_per_cell": 48,
             "hbm_gbs_algorithmic": 48 * mcells / (ms * 1e-3) / 1e9,
             "frac_of_peak": 48 * mcells / (ms * 1e-3) / 1e9 / peak,
-            # the design's 7 field passes of 16 B: gather + sweep (z, y: stored
-            # straight into the field), gather + sweep + transposing scatter (x);
-            # 7 kernels a component once the factor tables exist (the first
+            # 3 kernels a component once the factor tables exist (the first
             # call for a coefficient builds them: 3 more)
-            "design_bytes_per_cell": 112, "launches": 7,
+            "design_bytes_per_cell": 48, "launches": 3,
             "status": mm.status()}
         mm.close()
         del mrhs, mq
