@@ -548,6 +548,40 @@ def main():
                 variants[name]["filtered_exact"] = s.last_stats()["filtered_exact"]
             s.close()
 
+        # Filtered v2 where the truncation holds: the same shape with r
+        # log-uniform in [0.1, 1] (rho <= 1/3, J = 9 < m - 2).  By default the
+        # tiled kernels with Filtered's 2 x 2 interfaces (4 launches: J, the
+        # Filtered solve, the gated exact one); with FLAG_REFERENCE_ORDER the
+        # reference's scheme bit for bit (3 launches).  Their distance to the
+        # tiled PaScaL solve of the same batch is reported beside eps.
+        tA, tB, tC, tD = W.diag_dominant(N_SYS, N_ROW, 0.1, 1.0, seed=3, device=dev)
+        tX = torch.empty_like(tD)
+        sp_ = Solver("pascal", N_SYS, N_ROW, 8)
+        sp_.solve_out(tA, tB, tC, tD, tX)
+        torch.cuda.synchronize()
+        xpas = tX.clone()
+        sp_.close()
+        trunc = {"workload": "262144 x 512, r log-uniform [0.1, 1] (rho <= 1/3), eps_c = 1e-3, "
+                             "rho over all systems", "eps": 1e-3 / N_ROW ** 2}
+        for key, fl, lps in (("tiled", 0, 4), ("reference_order", L.FLAG_REFERENCE_ORDER, 3)):
+            s = Solver("filtered_v2", N_SYS, N_ROW, 8, flags=fl)
+            s.set_eps_constant(1e-3)
+            s.set_rho(tA, tB, tC, all_systems=True)
+            tot, _, _ = time_variant(torch, s, tA, tB, tC, tD, tX, max(3, args.steps // 2), 3,
+                                     lps)
+            ms = tot / max(3, args.steps // 2)
+            torch.cuda.synchronize()
+            trunc[key] = {"ms_per_step": ms, "rows_per_s": rows / (ms * 1e-3),
+                          "frac_of_peak": gbps(ms, BYTES_PER_ROW_F64) / peak,
+                          "launches_per_step": lps, "J": s.last_J(),
+                          "filtered_exact": s.last_stats()["filtered_exact"],
+                          "max_abs_diff_vs_pascal": float((tX - xpas).abs().max().item())}
+            s.close()
+        trunc["speedup_tiled_vs_reference_order"] = (trunc["reference_order"]["ms_per_step"] /
+                                                     trunc["tiled"]["ms_per_step"])
+        variants["filtered_v2_truncating_P8"] = trunc
+        del tA, tB, tC, tD, tX, xpas
+
         # The reference's own GPU kernels on this GPU (oracle/_ref/libref_gpu.so:
         # the reference's sources compiled for sm_100a, its P ranks run as row
         # blocks of one array with the MPI transport replaced by pointers), on

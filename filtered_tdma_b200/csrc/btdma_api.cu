@@ -49,6 +49,19 @@ int jfinal_launch(btdma_t h, int n_row, int version, unsigned* exact, cudaStream
     return BTDMA_OK;
 }
 
+// Sub-segments per Filtered segment when the tiled kernels take a Filtered
+// batch of P segments: R = n_row / (16 P), a power of two, with at most 32
+// sub-segments a system (a power of two when periodic); 0 when they do not.
+int filtered_tile_lanes(int n_row, int P, bool cyclic) {
+    if (P < 2 || n_row % TILE_MT != 0) return 0;
+    const int nseg = n_row / TILE_MT;
+    if (nseg > 32 || nseg % P != 0) return 0;
+    const int R = nseg / P;
+    if ((R & (R - 1)) != 0) return 0;
+    if (cyclic && (nseg & (nseg - 1)) != 0) return 0;
+    return R;
+}
+
 int check_sizes(btdma_t h, int n_sys, int n_row) {
     if (!h) return fail(BTDMA_ERR_ARG, "null handle");
     if (n_sys <= 0 || n_row <= 0) return fail(BTDMA_ERR_ARG, "n_sys and n_row must be positive");
@@ -119,6 +132,32 @@ int solve_impl(btdma_t h, const double* A, const double* B, const double* C, con
                               nullptr, h->tile_shape);
         if (rc < 0) return rc;
         if (rc == 1) return BTDMA_OK;
+    }
+
+    // Filtered v2 on the tiled kernels: the reference's P segments are groups
+    // of R = n_row / (16 P) sub-segments of the tiled solve, whose reduced
+    // system takes Filtered's 2 x 2 interfaces (reduced_solve_filtered).  J
+    // and the exact-fallback word come from the reference's device estimator
+    // as below; the Filtered launch runs while the word is 0, the exact tiled
+    // PaScaL while it is set.  Shapes the tiled kernels do not take go to the
+    // segment kernels below (the J accumulators reset themselves).
+    if (h->method == BTDMA_FILTERED_V2 && !(h->flags & BTDMA_FLAG_REFERENCE_ORDER)) {
+        const int R = filtered_tile_lanes(n_row, h->P, cyclic);
+        if (R > 0) {
+            if ((rc = jmax_launch(h, D, n_sys, n_row, st))) return rc;
+            if ((rc = jfinal_launch(h, n_row, 2, h->exact, st))) return rc;
+            rc = try_tile<double>(A, B, C, D, X, n_sys, n_row, cyclic, h->status, st, false,
+                                  h->exact, h->tile_shape, R, true);
+            if (rc < 0) return rc;
+            if (rc == 1) {
+                h->last_filtered = true;
+                rc = try_tile<double>(A, B, C, D, X, n_sys, n_row, cyclic, h->status, st, false,
+                                      h->exact, h->tile_shape);
+                if (rc < 0) return rc;
+                if (rc == 1) return BTDMA_OK;
+                return fail(BTDMA_ERR_UNSUPPORTED, "exact fallback not tileable");
+            }
+        }
     }
 
     SegArgs a = {};

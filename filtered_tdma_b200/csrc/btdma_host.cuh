@@ -440,13 +440,15 @@ inline bool tma_ok_elem(const void* p, int n_sys, int elem) {
 // Returns 1 when the tiled kernel was launched, 0 when the shape needs the
 // cluster-per-segment kernel, < 0 on error.
 // TC: arithmetic of the local sweeps; accumulate: X += solution; gate: the
-// kernel does nothing while *gate == 0.
+// kernel does nothing while *gate == 0 (gate_zero: while *gate != 0); filt_r >
+// 0: Filtered's reduced system with segments of filt_r sub-segments.
 // shape: BTDMA_TILE_* (the wide-box kernel serves FP64-arithmetic solves that
 // do not accumulate).
 template <typename TIN, typename TC = double>
 int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, int n_sys,
              int n_row, bool cyclic, unsigned* status, cudaStream_t st, bool accumulate = false,
-             const unsigned* gate = nullptr, int shape = BTDMA_TILE_NARROW) {
+             const unsigned* gate = nullptr, int shape = BTDMA_TILE_NARROW, int filt_r = 0,
+             bool gate_zero = false) {
     const int elem = (int)sizeof(TIN);
     bool wide = false;
     TilePlan pl;
@@ -475,7 +477,8 @@ int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, 
     a.cl = pl.cl;
     a.nst = pl.nst;
     a.n_groups = (n_sys + pl.sys - 1) / pl.sys;
-    a.accumulate = accumulate ? 1 : 0;
+    a.mode = (accumulate ? TILE_MODE_ACCUMULATE : 0) | (gate_zero ? TILE_MODE_GATE_ZERO : 0) |
+             (filt_r << TILE_MODE_FILT_SHIFT);
     a.gate = gate;
     a.status = status;
     const int rc = wide ? launch_tile_wide_plan<TIN>(pl, maps, a, cyclic, st)

@@ -89,6 +89,95 @@ __device__ __forceinline__ void reduced_solve_shfl(double l0, double u0, double 
     xf = r0 - l0 * xlm - u0 * xl;
 }
 
+// Filtered's reduced system (FilteredTDMA v2, libs/filtered_tdma/cpu/
+// filtered_tdma.cpp:217-238 with filtered_tdma_kernels.hpp's steps) in the
+// lanes of reduced_solve_shfl: the sub-segments are grouped into segments of R
+// consecutive lanes (R a power of two; the reference's ranks of m = 16 R rows).
+// Inside a segment the system is solved exactly, with the two couplings to
+// the neighbouring segments as parameters: three right-hand sides, y0 (the
+// rows' own), yl (the left neighbour's last unknown = 1) and yr (the right
+// neighbour's first unknown = 1), so every unknown is y0 + lam yl + rho yr.
+// Across segments Filtered's approximation: the far couplings (a segment's
+// first unknown's response to its right neighbour, its last unknown's to its
+// left neighbour, of order rho^m) are dropped, which leaves one 2 x 2 system
+// per interface (solve_interfaces, filtered_tdma_kernels.hpp:172-196):
+//   f_k = y0F_k + yl F_k l_{k-1},  l_{k-1} = y0L_{k-1} + yr L_{k-1} f_k.
+// lam and rho of each segment then come from its interfaces (0 outside the
+// batch unless CYCLIC).  The J-row truncation of the correction is not
+// applied: every row is back-substituted with the full correction, which costs
+// nothing extra here; the result stays within Filtered's eps of the exact one.
+template <bool CYCLIC>
+__device__ __forceinline__ void reduced_solve_filtered(double l0, double u0, double r0, double l1,
+                                                       double u1, double r1, int p, int nseg,
+                                                       int W, int R, bool act, double& xf,
+                                                       double& xl) {
+    const unsigned FULL = 0xffffffffu;
+    const int t = p & (R - 1);     // lane in the segment
+    const int k0 = p - t;          // first lane of the segment
+    const double l0s = t == 0 ? 0.0 : l0;  // couplings inside the segment only
+    const double u1s = t == R - 1 ? 0.0 : u1;
+    // the three right-hand sides of the first / last rows
+    double a0 = r0, a1 = r1;
+    double b0 = t == 0 ? -l0 : 0.0, b1 = 0.0;
+    double c0 = 0.0, c1 = t == R - 1 ? -u1 : 0.0;
+    // cyclic reduction: the next sub-segment's first row (inside the segment)
+    const int pn = (p + 1) & (W - 1);
+    const double l0n = __shfl_sync(FULL, l0, pn, W), u0n = __shfl_sync(FULL, u0, pn, W);
+    const double a0n = __shfl_sync(FULL, a0, pn, W), b0n = __shfl_sync(FULL, b0, pn, W);
+    const double c0n = __shfl_sync(FULL, c0, pn, W);
+    const double ib = rcp_nr(1.0 - l1 * u0 - u1s * l0n);
+    double al = -l1 * l0s * ib, cl = -u1s * u0n * ib;
+    double da = (a1 - l1 * a0 - u1s * a0n) * ib;
+    double db = (b1 - l1 * b0 - u1s * b0n) * ib;
+    double dc = (c1 - l1 * c0 - u1s * c0n) * ib;
+    if (!act) al = cl = da = db = dc = 0.0;
+    // parallel cyclic reduction inside the segment
+    for (int dl = 1; dl < R; dl <<= 1) {
+        const bool vm = t - dl >= 0, vp = t + dl < R;
+        const int im = (p - dl) & (W - 1), ip = (p + dl) & (W - 1);
+        double lm = __shfl_sync(FULL, al, im, W), um = __shfl_sync(FULL, cl, im, W);
+        double lp = __shfl_sync(FULL, al, ip, W), up = __shfl_sync(FULL, cl, ip, W);
+        double am = __shfl_sync(FULL, da, im, W), ap = __shfl_sync(FULL, da, ip, W);
+        double bm = __shfl_sync(FULL, db, im, W), bp = __shfl_sync(FULL, db, ip, W);
+        double cm = __shfl_sync(FULL, dc, im, W), cp = __shfl_sync(FULL, dc, ip, W);
+        if (!vm) lm = um = am = bm = cm = 0.0;
+        if (!vp) lp = up = ap = bp = cp = 0.0;
+        const double ibl = rcp_nr(1.0 - al * um - cl * lp);
+        da = (da - al * am - cl * ap) * ibl;
+        db = (db - al * bm - cl * bp) * ibl;
+        dc = (dc - al * cm - cl * cp) * ibl;
+        const double nl = -al * lm * ibl;
+        cl = -cl * up * ibl;
+        al = nl;
+    }
+    // last unknowns (da, db, dc); first unknowns from the first rows
+    const int pm = (p - 1) & (W - 1);
+    double xam = __shfl_sync(FULL, da, pm, W), xbm = __shfl_sync(FULL, db, pm, W);
+    double xcm = __shfl_sync(FULL, dc, pm, W);
+    if (t == 0) xam = xbm = xcm = 0.0;
+    const double fa = a0 - l0s * xam - u0 * da;
+    const double fb = b0 - l0s * xbm - u0 * db;
+    const double fc = c0 - l0s * xcm - u0 * dc;
+    // interface 2 x 2 at each segment's first lane: f_k and l_{k-1}, with
+    // the previous segment's last lane's y0 and yr
+    const int pl = (k0 - 1) & (W - 1);
+    const double yl0 = __shfl_sync(FULL, da, pl, W), ylr = __shfl_sync(FULL, dc, pl, W);
+    const bool left = CYCLIC || k0 > 0;
+    double f = fa, lam = 0.0;
+    if (left) {
+        f = (fa + fb * yl0) * rcp_nr(1.0 - fb * ylr);
+        lam = yl0 + ylr * f;
+    }
+    // every lane: lam of its segment (from its first lane) and rho (the next
+    // segment's first lane's f)
+    const int kn = (k0 + R) & (W - 1);
+    const double lk = __shfl_sync(FULL, lam, k0, W);
+    double rk = __shfl_sync(FULL, f, kn, W);
+    if (!CYCLIC && k0 + R >= nseg) rk = 0.0;
+    xf = fa + lk * fb + rk * fc;
+    xl = da + lk * db + rk * dc;
+}
+
 // The matrix steps of reduced_solve_shfl for one lane, written to lt[0 .. 5 +
 // 3 * levels) (the lane table of a matrix shared by every system, see
 // reduced_solve_rhs).  Every lane of the warp calls it with the same nseg

@@ -84,6 +84,15 @@ __host__ __device__ constexpr size_t gen_table_doubles(int n_row) {
     return tile_red_offset(n_row) + 32 * (size_t)TILE_RED_LANE;
 }
 
+// TileArgs::mode of the modes that read A, B, C (GEN == 0): bit 0 X +=
+// solution (refinement corrections), bit 1 the gate's polarity (run while
+// *gate == 0 instead of while *gate != 0), bits 8..15 R > 0: Filtered's
+// reduced system with segments of R sub-segments (reduced_solve_filtered)
+// instead of the exact one.
+constexpr int TILE_MODE_ACCUMULATE = 1;
+constexpr int TILE_MODE_GATE_ZERO = 2;
+constexpr int TILE_MODE_FILT_SHIFT = 8;
+
 struct TileArgs {
     double* X;
     int n_sys, n_row;
@@ -93,8 +102,9 @@ struct TileArgs {
     int n_groups;  // groups of SYS systems
     union {
         struct {  // modes that read A, B, C (GEN == 0)
-            int accumulate;        // 1: X += solution (refinement corrections), 0: X = solution
-            const unsigned* gate;  // non-null: the launch does nothing while *gate == 0
+            int mode;              // TILE_MODE_* bits
+            const unsigned* gate;  // non-null: the launch runs only while *gate != 0
+                                   // (TILE_MODE_GATE_ZERO: while *gate == 0)
         };
         // Generated-coefficient modes (GEN != 0) may store x through a layout
         // map instead of the plain [n_row][n_sys]: with xblk > 0, row j of
@@ -359,8 +369,12 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 
     // a closed gate leaves the CTA without groups (it still runs its setup and
     // exit barriers, so every CTA of a cluster takes the same path)
-    const bool gated_off = !CONSTC && args.gate != nullptr &&
-                           *static_cast<const volatile unsigned*>(args.gate) == 0u;
+    const bool gated_off =
+        !CONSTC && args.gate != nullptr &&
+        ((*static_cast<const volatile unsigned*>(args.gate) == 0u) !=
+         ((args.mode & TILE_MODE_GATE_ZERO) != 0));
+    // Filtered: lanes per segment of the reduced system (0: exact)
+    const int filt_r = CONSTC ? 0 : (args.mode >> TILE_MODE_FILT_SHIFT) & 255;
     const int n_my = (!gated_off && args.n_groups > cluster_id)
                          ? (args.n_groups - cluster_id + n_clusters - 1) / n_clusters
                          : 0;
@@ -721,6 +735,9 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                 double xf, xl;
                 if constexpr (SH)
                     reduced_solve_rhs<CYCLIC>(r0, r1, p, nseg, W, lanes + p, 32, xf, xl);
+                else if (filt_r > 0)
+                    reduced_solve_filtered<CYCLIC>(l0, u0, r0, l1, u1, r1, p, nseg, W, filt_r,
+                                                   act, xf, xl);
                 else
                     reduced_solve_shfl<CYCLIC>(l0, u0, r0, l1, u1, r1, p, nseg, W, act, xf, xl);
                 if (act) {
@@ -827,7 +844,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                 double xo[M] = {};
                 bool acc = false;
                 if constexpr (sizeof(TC) == 4) {
-                    acc = args.accumulate != 0;
+                    acc = (args.mode & TILE_MODE_ACCUMULATE) != 0;
                     if (acc) {
 #pragma unroll
                         for (int k = 0; k < M; ++k) xo[k] = xp[-(ptrdiff_t)(M - 1 - k) * (ptrdiff_t)ns];

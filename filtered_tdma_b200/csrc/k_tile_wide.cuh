@@ -152,9 +152,12 @@ tile_wide_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
     }
     __syncthreads();
 
-    // a closed gate (*gate == 0) leaves the CTA without groups
-    const bool gated_off =
-        args.gate != nullptr && *static_cast<const volatile unsigned*>(args.gate) == 0u;
+    // a closed gate leaves the CTA without groups (TILE_MODE_GATE_ZERO: the
+    // gate is open while *gate == 0)
+    const bool gated_off = args.gate != nullptr &&
+                           ((*static_cast<const volatile unsigned*>(args.gate) == 0u) !=
+                            ((args.mode & TILE_MODE_GATE_ZERO) != 0));
+    const int filt_r = (args.mode >> TILE_MODE_FILT_SHIFT) & 255;  // Filtered: lanes a segment
     const int n_my = (!gated_off && args.n_groups > (int)blockIdx.x)
                          ? (args.n_groups - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x
                          : 0;
@@ -272,7 +275,11 @@ tile_wide_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
                     r1 = src[5 * fstride];
                 }
                 double xf, xl;
-                reduced_solve_shfl<CYCLIC>(l0, u0, r0, l1, u1, r1, p, nseg, W, act, xf, xl);
+                if (filt_r > 0)
+                    reduced_solve_filtered<CYCLIC>(l0, u0, r0, l1, u1, r1, p, nseg, W, filt_r,
+                                                   act, xf, xl);
+                else
+                    reduced_solve_shfl<CYCLIC>(l0, u0, r0, l1, u1, r1, p, nseg, W, act, xf, xl);
                 if (act) {  // over the fields this thread has read
                     src[0] = xf;
                     src[fstride] = xl;

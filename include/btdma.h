@@ -16,7 +16,16 @@
  *                      interface solves, J-truncated correction with J taken after
  *                      the interface solve (FilteredTDMACUDA::solve_filtered_v1)
  *   BTDMA_FILTERED_V2  "filtered_v2"  J taken before the sweeps
- *                      (FilteredTDMACUDA::solve_filtered_v2)
+ *                      (FilteredTDMACUDA::solve_filtered_v2).  Where the P
+ *                      segments are whole power-of-two groups of 16-row
+ *                      sub-segments (n_row / (16 P) = 1, 2, 4 ... and n_row <=
+ *                      512) it runs on the register-tiled kernels: each segment
+ *                      solved exactly, the 2x2 interface solves between
+ *                      segments, the correction applied in full (no J row
+ *                      cut-off: every row is back-substituted anyway); within
+ *                      Filtered's eps of PaScaL and of the reference's Filtered,
+ *                      at the speed of the tiled PaScaL.  Other shapes, and
+ *                      BTDMA_FLAG_REFERENCE_ORDER, run the reference's scheme.
  *   Filtered full-solve fallback: where the reference's truncation gives no
  *   saving or no bound — J >= m - 2 in some segment of m rows (J = m - 1 is
  *   also what the reference sets for rho = 0 or rho >= 0.5,
@@ -80,9 +89,11 @@ enum btdma_flags {
      * bit-identical to PaScaLTDMA::solve with nprocs = P
      * (libs/pascal_tdma/cpu/pascal_tdma.cpp:113-227).  Without the flag PaScaL
      * uses the register-tiled kernel, exact to rounding (<= 1e-12 relative to
-     * the serial Thomas) and faster.  For Filtered handles the flag keeps the
-     * reference's 2x2 interface where J >= m - 2 (no exact fallback), so every
-     * Filtered result is bit-identical to the reference's. */
+     * the serial Thomas) and faster.  For Filtered handles the flag runs the
+     * reference's scheme in its operation order (segment kernels, J-row
+     * cut-off) and keeps its 2x2 interface where J >= m - 2 (no exact
+     * fallback), so every Filtered result is bit-identical to the
+     * reference's. */
     BTDMA_FLAG_REFERENCE_ORDER = 1 << 1
 };
 
@@ -208,7 +219,7 @@ typedef struct btdma_stats {
     int n_fallback;
     /* Filtered solves (P > 1): 1 when the batch was solved with the exact
      * reduced system instead of the Filtered interface (see BTDMA_FILTERED_V1),
-     * 0 when the J-truncated Filtered scheme ran; -1 for other solves. */
+     * 0 when the Filtered scheme ran; -1 for other solves. */
     int filtered_exact;
 } btdma_stats;
 int btdma_last_stats(btdma_t h, btdma_stats* stats);

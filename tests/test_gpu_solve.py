@@ -183,13 +183,28 @@ def test_filtered_bit_exact(cuda, orc, version, cyclic, n_sys, n_row, P):
         assert np.max(np.abs(x - xp)) <= eps
 
 
+def filtered_tiled(version, n_sys, n_row, P, cyclic):
+    # the default Filtered v2 solve runs on the tiled kernels when the segments
+    # are whole power-of-two groups of 16-row sub-segments (at most 32) and
+    # the arrays suit TMA (n_sys even here)
+    if version != 2 or n_row % 16 or n_sys % 2:
+        return False
+    nseg = n_row // 16
+    if nseg > 32 or nseg % P:
+        return False
+    R = nseg // P
+    return R & (R - 1) == 0 and (not cyclic or nseg & (nseg - 1) == 0)
+
+
 @pytest.mark.parametrize("version", [1, 2])
 @pytest.mark.parametrize("cyclic", [False, True])
 @pytest.mark.parametrize("n_sys,n_row,P", FILTERED_SHAPES)
 def test_filtered_default_exact_fallback(cuda, orc, version, cyclic, n_sys, n_row, P):
-    # default Filtered: the reference's scheme bit for bit while every segment
-    # truncates (J < m - 2); the exact reduced solve (within 1e-12 of the serial
-    # Thomas) as soon as one segment does not, reported by last_stats
+    # default Filtered: while every segment truncates (J < m - 2), the
+    # reference's scheme -- bit for bit on the segment kernels, within eps of
+    # it (and of PaScaL) on the tiled kernels; the exact reduced solve (within
+    # 1e-12 of the serial Thomas) as soon as one segment does not, reported by
+    # last_stats
     A, B, C, D = W.diag_dominant(n_sys, n_row, 0.1, 1.0, seed=version + n_row)
     rho = orc.rho_rows_all(A, B, C)
     x, s = run(cuda, f"filtered_v{version}", A, B, C, D, P, cyclic=cyclic, rho=rho)
@@ -201,8 +216,39 @@ def test_filtered_default_exact_fallback(cuda, orc, version, cyclic, n_sys, n_ro
     if exact:
         xt = orc.thomas_cyclic(A, B, C, D) if cyclic else orc.thomas(A, B, C, D)
         assert rel_err(x, xt) <= 1e-12
+    elif filtered_tiled(version, n_sys, n_row, P, cyclic):
+        eps = 1e-3 / float(n_row) ** 2
+        xp = orc.pascal(A, B, C, D, P, cyclic)
+        assert np.max(np.abs(x - xp)) <= eps
+        assert np.max(np.abs(x - xo)) <= 2 * eps
     else:
         assert np.array_equal(x, xo)
+
+
+@pytest.mark.parametrize("cyclic", [False, True])
+@pytest.mark.parametrize("n_sys,n_row,P", [(4096, 512, 8), (2048, 256, 4), (1024, 128, 2),
+                                           (2048, 512, 4), (2050, 384, 6), (512, 512, 16)])
+def test_filtered_v2_tiled_within_eps(cuda, orc, cyclic, n_sys, n_row, P):
+    # Filtered v2 on the tiled kernels (the default where the shape allows):
+    # each segment solved exactly, Filtered's 2 x 2 interfaces between them,
+    # the full correction; J and the fallback decision from the reference's
+    # device estimator.  Bar: within the reference's eps = eps_c / n_row^2 of
+    # PaScaL, and of the reference's own Filtered result.
+    if cyclic and (n_row // 16) & (n_row // 16 - 1):
+        pytest.skip("periodic tiled solves need 2^k sub-segments")
+    A, B, C, D = W.diag_dominant(n_sys, n_row, 0.1, 1.0, seed=40 + P + n_row)
+    rho = orc.rho_rows_all(A, B, C)
+    x, s = run(cuda, "filtered_v2", A, B, C, D, P, cyclic=cyclic, rho=rho)
+    xo, Jo = orc.filtered(A, B, C, D, P, 2, cyclic, 1e-3, rho, orc.J_DEVICE)
+    assert s.last_J() == list(Jo)
+    m = n_row // P
+    assert max(Jo) < m - 2  # the truncation regime: no fallback
+    assert s.last_stats()["filtered_exact"] == 0
+    eps = 1e-3 / float(n_row) ** 2
+    xp = orc.pascal(A, B, C, D, P, cyclic)
+    assert np.max(np.abs(x - xp)) <= eps
+    assert np.max(np.abs(x - xo)) <= 2 * eps
+    assert not np.array_equal(x, xo) or P == 1  # not the segment kernels' result
 
 
 @pytest.mark.parametrize("version", [1, 2])
