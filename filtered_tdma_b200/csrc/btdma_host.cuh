@@ -12,6 +12,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "btdma_common.cuh"
@@ -305,9 +306,9 @@ inline TilePlan tile_plan(int n_row, bool cyclic, int elem = 8, int na = 4, bool
 }
 
 template <int SYS, bool CYCLIC, typename TIN = double, typename TC = double, int GEN = 0,
-          int PR = 1>
+          int PR = 1, bool FILT = false>
 int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st) {
-    auto kern = tile_f64_kernel<SYS, CYCLIC, TIN, TC, GEN, PR>;
+    auto kern = tile_f64_kernel<SYS, CYCLIC, TIN, TC, GEN, PR, FILT>;
     static bool attr_done = false;
     if (!attr_done) {
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -356,18 +357,18 @@ int launch_tile_sys(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st)
     return BTDMA_OK;
 }
 
-template <typename TIN, typename TC>
+template <typename TIN, typename TC, bool FILT = false>
 int launch_tile_plan(const TilePlan& pl, const CUtensorMap* maps, const TileArgs& a, bool cyclic,
                      cudaStream_t st) {
     switch (pl.sys * 2 + (cyclic ? 1 : 0)) {
-        case 256: return launch_tile_sys<128, false, TIN, TC>(maps, a, st);
-        case 257: return launch_tile_sys<128, true, TIN, TC>(maps, a, st);
-        case 128: return launch_tile_sys<64, false, TIN, TC>(maps, a, st);
-        case 129: return launch_tile_sys<64, true, TIN, TC>(maps, a, st);
-        case 64: return launch_tile_sys<32, false, TIN, TC>(maps, a, st);
-        case 65: return launch_tile_sys<32, true, TIN, TC>(maps, a, st);
-        case 33: return launch_tile_sys<16, true, TIN, TC>(maps, a, st);
-        default: return launch_tile_sys<16, false, TIN, TC>(maps, a, st);
+        case 256: return launch_tile_sys<128, false, TIN, TC, 0, 1, FILT>(maps, a, st);
+        case 257: return launch_tile_sys<128, true, TIN, TC, 0, 1, FILT>(maps, a, st);
+        case 128: return launch_tile_sys<64, false, TIN, TC, 0, 1, FILT>(maps, a, st);
+        case 129: return launch_tile_sys<64, true, TIN, TC, 0, 1, FILT>(maps, a, st);
+        case 64: return launch_tile_sys<32, false, TIN, TC, 0, 1, FILT>(maps, a, st);
+        case 65: return launch_tile_sys<32, true, TIN, TC, 0, 1, FILT>(maps, a, st);
+        case 33: return launch_tile_sys<16, true, TIN, TC, 0, 1, FILT>(maps, a, st);
+        default: return launch_tile_sys<16, false, TIN, TC, 0, 1, FILT>(maps, a, st);
     }
 }
 
@@ -403,9 +404,9 @@ inline TilePlan tile_wide_plan(int n_row, bool cyclic, int elem) {
     return pl;
 }
 
-template <int SYS, bool CYCLIC, typename TIN>
+template <int SYS, bool CYCLIC, typename TIN, bool FILT = false>
 int launch_tile_wide(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st) {
-    auto kern = tile_wide_kernel<SYS, CYCLIC, TIN>;
+    auto kern = tile_wide_kernel<SYS, CYCLIC, TIN, FILT>;
     static bool attr_done = false;
     if (!attr_done) {
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -420,16 +421,16 @@ int launch_tile_wide(const CUtensorMap* maps, const TileArgs& a, cudaStream_t st
     return BTDMA_OK;
 }
 
-template <typename TIN>
+template <typename TIN, bool FILT = false>
 int launch_tile_wide_plan(const TilePlan& pl, const CUtensorMap* maps, const TileArgs& a,
                           bool cyclic, cudaStream_t st) {
     switch (pl.sys * 2 + (cyclic ? 1 : 0)) {
-        case 256: return launch_tile_wide<128, false, TIN>(maps, a, st);
-        case 257: return launch_tile_wide<128, true, TIN>(maps, a, st);
-        case 128: return launch_tile_wide<64, false, TIN>(maps, a, st);
-        case 129: return launch_tile_wide<64, true, TIN>(maps, a, st);
-        case 65: return launch_tile_wide<32, true, TIN>(maps, a, st);
-        default: return launch_tile_wide<32, false, TIN>(maps, a, st);
+        case 256: return launch_tile_wide<128, false, TIN, FILT>(maps, a, st);
+        case 257: return launch_tile_wide<128, true, TIN, FILT>(maps, a, st);
+        case 128: return launch_tile_wide<64, false, TIN, FILT>(maps, a, st);
+        case 129: return launch_tile_wide<64, true, TIN, FILT>(maps, a, st);
+        case 65: return launch_tile_wide<32, true, TIN, FILT>(maps, a, st);
+        default: return launch_tile_wide<32, false, TIN, FILT>(maps, a, st);
     }
 }
 
@@ -481,8 +482,18 @@ int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, 
              (filt_r << TILE_MODE_FILT_SHIFT);
     a.gate = gate;
     a.status = status;
-    const int rc = wide ? launch_tile_wide_plan<TIN>(pl, maps, a, cyclic, st)
-                        : launch_tile_plan<TIN, TC>(pl, maps, a, cyclic, st);
+    int rc;
+    if constexpr (std::is_same<TIN, double>::value && std::is_same<TC, double>::value) {
+        if (filt_r > 0) {  // Filtered's instantiations (FP64 only)
+            rc = wide ? launch_tile_wide_plan<TIN, true>(pl, maps, a, cyclic, st)
+                      : launch_tile_plan<TIN, TC, true>(pl, maps, a, cyclic, st);
+            return rc == BTDMA_OK ? 1 : rc;
+        }
+    } else {
+        if (filt_r > 0) return fail(BTDMA_ERR_UNSUPPORTED, "Filtered tiles are FP64 only");
+    }
+    rc = wide ? launch_tile_wide_plan<TIN>(pl, maps, a, cyclic, st)
+              : launch_tile_plan<TIN, TC>(pl, maps, a, cyclic, st);
     return rc == BTDMA_OK ? 1 : rc;
 }
 

@@ -200,8 +200,10 @@ __host__ __device__ __forceinline__ int tile_stage_box_elems(int sys, int nsc, i
 }
 __host__ __device__ __forceinline__ int tile_stage_elems(int sys, int nsc, int elem, int na,
                                                          int gen = 0) {
+    const int b = tile_stage_box_elems(sys, nsc, elem, na, gen);
+    if (gen != 4 && gen != 5) return b;  // rows of SYS systems: whole 128-byte multiples
     const int q = 128 / elem;
-    return (tile_stage_box_elems(sys, nsc, elem, na, gen) + q - 1) / q * q;
+    return (b + q - 1) / q * q;
 }
 // na: arrays per ring stage (4: A, B, C, D; 1: D only).
 __host__ __device__ __forceinline__ size_t tile_ring_bytes(int sys, int nsc, int nst, int elem,
@@ -277,8 +279,11 @@ __device__ __forceinline__ void tile_cluster_sync(int cl) {
 // threads per system, two independent recurrences per thread, and CTAs small
 // enough that two share an SM and one's reduced solve overlaps the other's
 // streaming.
+// FILT: the reduced system takes Filtered's 2 x 2 interfaces between segments
+// of R = (mode >> TILE_MODE_FILT_SHIFT) sub-segments (a separate
+// instantiation: the extra paths would cost the exact kernels registers).
 template <int SYS, bool CYCLIC, typename TIN = double, typename TC = double, int GEN = 0,
-          int PR = 1>
+          int PR = 1, bool FILT = false>
 __global__ void __launch_bounds__(TILE_MAX_THREADS, 1)
 tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 const __grid_constant__ CUtensorMap tmC, const __grid_constant__ CUtensorMap tmD,
@@ -291,6 +296,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     static_assert(GEN != 4 || (SYS == TILE_HEAT_SYS && !CYCLIC), "heat Z sweep: 16 systems");
     static_assert(GEN != 5 || (SYS == TILE_HEAT_SYS && !CYCLIC), "field-box sweep: 16 systems");
     static_assert(PR == 1 || (PR == 2 && SH), "two sub-segments per thread: shared matrix only");
+    static_assert(!FILT || GEN == 0, "Filtered interfaces: matrices read from A, B, C");
     constexpr int NA = CONSTC ? 1 : 4;                // arrays per ring stage
     constexpr int RPS = tile_rps((int)sizeof(TIN), NA);  // rows per ring stage
     constexpr int SPG = M / RPS;                         // stages per group
@@ -373,15 +379,17 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         !CONSTC && args.gate != nullptr &&
         ((*static_cast<const volatile unsigned*>(args.gate) == 0u) !=
          ((args.mode & TILE_MODE_GATE_ZERO) != 0));
-    // Filtered: lanes per segment of the reduced system (0: exact)
-    const int filt_r = CONSTC ? 0 : (args.mode >> TILE_MODE_FILT_SHIFT) & 255;
+    // Filtered: lanes per segment of the reduced system
+    const int filt_r = FILT ? (args.mode >> TILE_MODE_FILT_SHIFT) & 255 : 0;
     const int n_my = (!gated_off && args.n_groups > cluster_id)
                          ? (args.n_groups - cluster_id + n_clusters - 1) / n_clusters
                          : 0;
     const int total = n_my * SPG;  // ring stages this CTA consumes
-    // bytes the TMA boxes of a stage deliver (the stage stride may be padded)
+    // bytes the TMA boxes of a stage deliver (the 18-cell boxes' stride is padded)
     const uint32_t stage_bytes =
-        (uint32_t)tile_stage_box_elems(SYS, nsc, (int)sizeof(TIN), NA, GEN) * sizeof(TIN);
+        (GEN == 4 || GEN == 5)
+            ? (uint32_t)tile_stage_box_elems(SYS, nsc, (int)sizeof(TIN), NA, GEN) * sizeof(TIN)
+            : (uint32_t)sstride * sizeof(TIN);
 
     auto issue = [&](int t) {  // one thread
         const int slot = t % nst;
@@ -735,7 +743,7 @@ tile_f64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                 double xf, xl;
                 if constexpr (SH)
                     reduced_solve_rhs<CYCLIC>(r0, r1, p, nseg, W, lanes + p, 32, xf, xl);
-                else if (filt_r > 0)
+                else if constexpr (FILT)
                     reduced_solve_filtered<CYCLIC>(l0, u0, r0, l1, u1, r1, p, nseg, W, filt_r,
                                                    act, xf, xl);
                 else

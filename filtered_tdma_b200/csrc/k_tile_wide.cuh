@@ -111,7 +111,8 @@ __device__ __forceinline__ void wide_reduced(const WideFwd& f, double* w, int fs
     w[5 * fstride] = f.dep;
 }
 
-template <int SYS, bool CYCLIC, typename TIN>
+// FILT: Filtered's reduced system (as tile_f64_kernel's FILT).
+template <int SYS, bool CYCLIC, typename TIN, bool FILT = false>
 __global__ void __launch_bounds__(TILE_MAX_THREADS, 1)
 tile_wide_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                  const __grid_constant__ CUtensorMap tmC, const __grid_constant__ CUtensorMap tmD,
@@ -157,7 +158,7 @@ tile_wide_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
     const bool gated_off = args.gate != nullptr &&
                            ((*static_cast<const volatile unsigned*>(args.gate) == 0u) !=
                             ((args.mode & TILE_MODE_GATE_ZERO) != 0));
-    const int filt_r = (args.mode >> TILE_MODE_FILT_SHIFT) & 255;  // Filtered: lanes a segment
+    const int filt_r = FILT ? (args.mode >> TILE_MODE_FILT_SHIFT) & 255 : 0;  // lanes a segment
     const int n_my = (!gated_off && args.n_groups > (int)blockIdx.x)
                          ? (args.n_groups - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x
                          : 0;
@@ -275,7 +276,7 @@ tile_wide_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
                     r1 = src[5 * fstride];
                 }
                 double xf, xl;
-                if (filt_r > 0)
+                if constexpr (FILT)
                     reduced_solve_filtered<CYCLIC>(l0, u0, r0, l1, u1, r1, p, nseg, W, filt_r,
                                                    act, xf, xl);
                 else

@@ -163,8 +163,10 @@ def test_filtered_backend_one_segment_is_serial_thomas(cuda, orc, direction):
 def test_filtered_backend_segments(cuda, orc, direction):
     # Filtered v2 over 4 segments: with the reference-order flag bit-identical
     # to the oracle's Filtered v2 on the same A, B, C, D (rho from system 0's
-    # column, the device J estimator, eps_constant as given); by default the
-    # same where every segment truncates, the exact solve where one does not
+    # column, the device J estimator, eps_constant as given); by default, where
+    # every segment truncates, the tiled kernels' Filtered (exact segments, 2x2
+    # interfaces: within eps of the serial Thomas solution), the exact solve
+    # where one does not
     import torch
     from filtered_tdma_b200 import _lib as L
     from filtered_tdma_b200.momentum import ChannelMomentum
@@ -190,9 +192,14 @@ def test_filtered_backend_segments(cuda, orc, direction):
 
             ref = MO.sweep(q, m.metrics, direction, 1, c, direction < 2, solver=filt)
             exact = flags == 0 and max(Js[0]) >= 64 // 4 - 2
-            if exact:
-                ref = MO.sweep(q, m.metrics, direction, 1, c, direction < 2)
-                assert _rel(got[1:-1, 1:-1, 1:-1], ref[1:-1, 1:-1, 1:-1]) <= 1e-12
+            if flags == 0:
+                xt = MO.sweep(q, m.metrics, direction, 1, c, direction < 2)
+                if exact:
+                    assert _rel(got[1:-1, 1:-1, 1:-1], xt[1:-1, 1:-1, 1:-1]) <= 1e-12
+                else:
+                    eps = eps_c / 64.0 ** 2
+                    assert np.max(np.abs(got - xt)) <= eps
+                    assert np.max(np.abs(got - ref)) <= 2 * eps
             else:
                 assert np.array_equal(got, ref)
             m.close()
