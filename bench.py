@@ -380,7 +380,8 @@ def run_case(args):
         return out
 
     if args.case == "batch":
-        A, B, C, D = W.diag_dominant(args.n_sys, args.n_row, seed=2, device=dev)
+        r_lo, r_hi = (float(v) for v in args.r_range.split(","))
+        A, B, C, D = W.diag_dominant(args.n_sys, args.n_row, r_lo, r_hi, seed=2, device=dev)
         X = torch.empty_like(D)
         f32 = args.storage == "f32"
         if f32:
@@ -462,6 +463,8 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="ragged: keep the default plan")
     ap.add_argument("--tile-shape", choices=["auto", "narrow", "wide"], default="auto",
                     help="batch: kernel shape of the tiled PaScaL solve")
+    ap.add_argument("--r-range", default="0.1,10",
+                    help="batch: per-system r log-uniform in [lo, hi] (A = C = -r, B = 1 + 2r)")
     args = ap.parse_args()
     if args.case:
         return run_case(args)
