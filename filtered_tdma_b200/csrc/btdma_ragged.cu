@@ -239,7 +239,18 @@ int rag_launch(btdma_t h, int cta, int P, int mcap, int staged, const int4* task
                                     max_smem_optin()));
             attr_done[staged] = true;
         }
-        kern<<<n_tasks, P, rag_cta_smem_bytes(P, staged, mcap), st>>>(a);
+        const size_t smem = rag_cta_smem_bytes(P, staged, mcap);
+        // co-resident CTAs of this shape (cached per shape): the prefetch distance
+        static int resident[2][4][RAG_MT + 1] = {};
+        const int pi = P == 64 ? 0 : P == 128 ? 1 : P == 256 ? 2 : 3;
+        int& res = resident[staged][pi][std::min(std::max(mcap, 0), RAG_MT)];
+        if (res == 0) {
+            int per_sm = 0;
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P, smem));
+            res = std::max(1, per_sm) * num_sms();
+        }
+        a.pf_ahead = res;
+        kern<<<n_tasks, P, smem, st>>>(a);
     } else {
         auto kern = ragged_kernel<TIN>;
         static bool attr_done = false;

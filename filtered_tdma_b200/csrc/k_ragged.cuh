@@ -44,7 +44,36 @@ struct RagArgs {
     // class's first task and task count in the table
     int* next;
     int cls_first[3], cls_count[3];
+    // ragged_cta_kernel: CTA b prefetches the system of task b + pf_ahead (the
+    // launch's co-resident CTAs: the task that takes over its slot) into L2;
+    // 0: no prefetch
+    int pf_ahead;
 };
+
+// Bulk prefetch into L2 of the 16-byte-aligned interior of elements
+// [o, o + n) of one array (a hint: nothing waits for it and it cannot fault;
+// the at most 15 bytes at either end outside the aligned interior are left out).
+template <typename TIN>
+__device__ __forceinline__ void rag_prefetch_l2(const void* arr, long long o, int n) {
+    const size_t b = __cvta_generic_to_global(static_cast<const TIN*>(arr) + o);
+    const size_t e = b + (size_t)n * sizeof(TIN);
+    const size_t b16 = (b + 15) & ~(size_t)15, e16 = e & ~(size_t)15;
+    if (e16 > b16)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(b16),
+                     "r"((unsigned)(e16 - b16))
+                     : "memory");
+}
+
+// The four input arrays of system sys (one thread issues it).
+template <typename TIN>
+__device__ __forceinline__ void rag_prefetch_system(const RagArgs& a, int sys) {
+    const long long o = a.off[sys];
+    const int n = (int)(a.off[sys + 1] - o);
+    rag_prefetch_l2<TIN>(a.A, o, n);
+    rag_prefetch_l2<TIN>(a.B, o, n);
+    rag_prefetch_l2<TIN>(a.C, o, n);
+    rag_prefetch_l2<TIN>(a.D, o, n);
+}
 
 constexpr int RAG_LOOKAHEAD = 4;  // rows loaded ahead of the elimination
 
@@ -197,8 +226,9 @@ __global__ void __launch_bounds__(256) ragged_kernel(const RagArgs a) {
 constexpr int RAG_MT = 16;
 
 // STAGED: A, C and D of the whole system are first copied into shared memory
-// with coalesced loads (B, read by the forward sweep only, comes straight from
-// global memory a few rows ahead), laid out [array][thread][row of segment]
+// with coalesced loads (B, read by the forward sweep only, goes to registers:
+// each thread requests its rows before the fill, so one memory latency covers
+// both), laid out [array][thread][row of segment]
 // with RAG_MT slots per thread and the row index XOR-swizzled by the thread's
 // low four bits (slot k ^ (p & 15)): consecutive rows of a segment land in
 // distinct banks for the coalesced fill, and the threads reading row k of
@@ -211,8 +241,11 @@ constexpr int RAG_MT = 16;
 // lines per thread.
 // mcap: rows per thread of the launch (<= RAG_MT).
 __host__ __device__ __forceinline__ int rag_slot(int p, int k) { return k ^ (p & 15); }
-__host__ __device__ __forceinline__ size_t rag_cta_smem_bytes(int P, bool staged, int mcap) {
-    return (2ull * 3 * (P + 2) +
+// Shared memory of one system: the sub-segments' first rows (3 fields of P + 2
+// with zero guards), the interface system in the group layout (3 fields of 33
+// slots per row of a group, see rag_cta_body) and the state / staging area.
+__host__ __device__ constexpr size_t rag_cta_smem_bytes(int P, bool staged, int mcap) {
+    return (3ull * (P + 2) + 3ull * 33 * (size_t)(P / 32) +
             (staged ? 3ull * RAG_MT * P : 3ull * (size_t)mcap * P)) *
            sizeof(double);
 }
@@ -260,8 +293,9 @@ __device__ __forceinline__ void rag_cta_body(const RagArgs& a, const int4 task, 
     const bool act = p < P;
     auto gsync = [&]() { asm volatile("bar.sync %0, %1;" ::"r"(bid), "r"(P) : "memory"); };
     const int gs = P + 2;  // guard rows at 0 and P + 1 stay zero (non-periodic ends)
-    auto F = [&](int b, int f, int row) -> double& { return rsm[(b * 3 + f) * gs + row + 1]; };
-    if (p < 6) {
+    // first rows of the sub-segments: field f of sub-segment row at F(f, row)
+    auto F = [&](int f, int row) -> double& { return rsm[f * gs + row + 1]; };
+    if (p < 3) {
         rsm[p * gs] = 0.0;
         rsm[p * gs + P + 1] = 0.0;
     }
@@ -278,7 +312,11 @@ __device__ __forceinline__ void rag_cta_body(const RagArgs& a, const int4 task, 
     const TIN* __restrict__ pC = static_cast<const TIN*>(a.C) + row0;
     const TIN* __restrict__ pD = static_cast<const TIN*>(a.D) + row0;
 
-    double* const stg = rsm + 2 * 3 * gs;  // state / staging area
+    // interface system, group layout (below): row q, field f at T[f * TS + TI(q)]
+    const int G = P >> 5, lg = __ffs(G) - 1, TS = 33 * G;
+    double* const T = rsm + 3 * gs;
+    auto TI = [&](int q) { return (q & (G - 1)) * 33 + (q >> lg); };
+    double* const stg = T + 3 * TS;  // state / staging area
     // this thread's slots (mcap = the launch's rows per thread, <= M):
     // unstaged [field][row][thread] -> stt[(f * mcap + k) * P];
     // staged [field][thread][slot] -> stt[f * P * M + rag_slot(p, k)]
@@ -286,6 +324,14 @@ __device__ __forceinline__ void rag_cta_body(const RagArgs& a, const int4 task, 
     const int fs = STAGED ? P * M : a.mcap * P;  // field stride
     const int ks = STAGED ? 1 : P;               // row stride (unstaged)
     const float inv0 = 1.0f / (float)(base > 0 ? base : 1), inv1 = 1.0f / (float)(base + 1);
+    // staged: the thread's B rows go to registers, requested before the fill so
+    // that both arrive together and the forward sweep waits on shared memory only
+    // (rows past m repeat row m - 1 and are never used)
+    double bq[M];
+    if constexpr (STAGED) {
+#pragma unroll
+        for (int k = 0; k < M; ++k) bq[k] = (double)__ldg(pB + (k < m ? k : m - 1));
+    }
     if constexpr (STAGED) {
         // fields 0..2 = A, C, D; coalesced over the system's rows
         const TIN* __restrict__ gA = static_cast<const TIN*>(a.A) + o;
@@ -332,7 +378,7 @@ __device__ __forceinline__ void rag_cta_body(const RagArgs& a, const int4 task, 
             if constexpr (STAGED) {
                 const int sl = rag_slot(p, kk);
                 fa[j] = stt[0 * fs + sl];
-                fb[j] = (double)__ldg(pB + kk);
+                fb[j] = bq[k0 + j];  // k0 + j < M: a register
                 fc[j] = stt[1 * fs + sl];
                 fd[j] = stt[2 * fs + sl];
             } else {
@@ -402,65 +448,92 @@ __device__ __forceinline__ void rag_cta_body(const RagArgs& a, const int4 task, 
     const double l0 = rr * ab0, u0 = rr * cb0 * pi_last, r0 = rr * (db0 - cb0 * sd);
 
     // ---------------------------------------------- reduced system (shared memory)
+    // One cyclic-reduction level leaves the interface system in the last-row
+    // unknowns (unit diagonal, as in reduced_solve_shfl):
+    //   a_q xL(q-1) + xL(q) + c_q xL(q+1) = d_q,  q = 0 .. P-1.
+    // Warp 0 of the group solves it in two levels: lane t takes the G = P / 32
+    // consecutive rows t G .. t G + G - 1 and runs the modified Thomas steps of
+    // the sweep above on them (unit diagonal), the 32 groups' own interface
+    // rows go through reduced_solve_shfl, and each lane back-substitutes its
+    // group.  Group layout: row q at slot (q % G) * 33 + q / G of each field,
+    // so lane t's k-th row sits at k * 33 + t (the warp reads consecutive
+    // slots) and the other threads' writes and reads of row p land in distinct
+    // banks up to 2-way.  Three barriers per system.
     if (act) {
-        F(1, 0, p) = l0;
-        F(1, 1, p) = u0;
-        F(1, 2, p) = r0;
+        F(0, p) = l0;
+        F(1, p) = u0;
+        F(2, p) = r0;
     }
     gsync();
     if (act) {
         const int pn = (cyclic && p == P - 1) ? 0 : p + 1;  // p + 1 == P: the zero guard
-        const double l0n = F(1, 0, pn), u0n = F(1, 1, pn), r0n = F(1, 2, pn);
+        const double l0n = F(0, pn), u0n = F(1, pn), r0n = F(2, pn);
         const double ib = rcp_nr(1.0 - l1 * u0 - u1 * l0n);
-        F(0, 0, p) = -l1 * l0 * ib;
-        F(0, 1, p) = -u1 * u0n * ib;
-        F(0, 2, p) = (r1 - l1 * r0 - u1 * r0n) * ib;
+        const int ti = TI(p);
+        T[ti] = -l1 * l0 * ib;
+        T[TS + ti] = -u1 * u0n * ib;
+        T[2 * TS + ti] = (r1 - l1 * r0 - u1 * r0n) * ib;
     }
     gsync();
-    int cur = 0;
-    double xl = 0.0;
-    bool solved = false;
-    for (int dl = 1; dl < P; dl <<= 1) {
-        if (act) {
-            int im = p - dl, ip = p + dl;
-            if (cyclic) {
-                im = im < 0 ? im + P : im;
-                ip = ip >= P ? ip - P : ip;
-            } else {
-                im = im < -1 ? -1 : im;
-                ip = ip > P ? P : ip;
+    if (p < 32) {  // warp 0 of the group (P >= 64: whole warps)
+        double* const ta = T + p;
+        double* const tc = T + TS + p;
+        double* const td = T + 2 * TS + p;
+        double gl0, gu0, gr0, gl1, gu1, gr1;  // the group's interface rows
+        if (G == 2) {  // no interior: the two rows are the interface rows
+            gl0 = ta[0], gu0 = tc[0], gr0 = td[0];
+            gl1 = ta[33], gu1 = tc[33], gr1 = td[33];
+        } else {
+            const double ab0 = ta[0], cb0 = tc[0], db0 = td[0];
+            // row 1 with unit diagonal: alpha, gamma, delta are its a, c, d
+            double alp = ta[33], gap = tc[33], dep = td[33];
+            double gpi = 1.0, gsa = alp, gsd = dep, gpi_last = 0.0;
+            for (int k = 2; k < G; ++k) {
+                const double av = ta[k * 33], cv = tc[k * 33], dv = td[k * 33];
+                const double inv = rcp_nr(1.0 - av * gap);
+                const double ga = cv * inv, de = (dv - av * dep) * inv, al = -av * alp * inv;
+                if (k <= G - 2) {
+                    gpi = -gap * gpi;
+                    gsa += gpi * al;
+                    gsd += gpi * de;
+                } else {
+                    gpi_last = -gap * gpi;
+                }
+                ta[k * 33] = al;
+                tc[k * 33] = ga;
+                td[k * 33] = de;
+                alp = al;
+                gap = ga;
+                dep = de;
             }
-            double li = F(cur, 0, p), ui = F(cur, 1, p), ri = F(cur, 2, p);
-            const double lm = F(cur, 0, im), um = F(cur, 1, im), rm = F(cur, 2, im);
-            const double lp = F(cur, 0, ip), up = F(cur, 1, ip), rp = F(cur, 2, ip);
-            if (cyclic && 2 * dl == P) {
-                const double si = li + ui, sj = lm + um;
-                xl = (ri - si * rm) * rcp_nr(1.0 - si * sj);
-                solved = true;
-            } else {
-                pcr_step(li, ui, ri, lm, um, rm, lp, up, rp);
-                F(cur ^ 1, 0, p) = li;
-                F(cur ^ 1, 1, p) = ui;
-                F(cur ^ 1, 2, p) = ri;
-            }
+            const double rr = rcp_nr(1.0 - cb0 * gsa);
+            gl0 = rr * ab0, gu0 = rr * cb0 * gpi_last, gr0 = rr * (db0 - cb0 * gsd);
+            gl1 = alp, gu1 = gap, gr1 = dep;
         }
-        gsync();
-        cur ^= 1;
-    }
-    if (act) {
-        if (!solved) xl = F(cur, 2, p);
-        F(cur ^ 1, 2, p) = xl;
+        double gxf, gxl;
+        if (cyclic)
+            reduced_solve_shfl<true>(gl0, gu0, gr0, gl1, gu1, gr1, p, 32, 32, true, gxf, gxl);
+        else
+            reduced_solve_shfl<false>(gl0, gu0, gr0, gl1, gu1, gr1, p, 32, 32, true, gxf, gxl);
+        // x of the group's rows overwrite their delta
+        td[(G - 1) * 33] = gxl;
+        double gxn = gxl;
+        for (int k = G - 2; k >= 1; --k) {
+            gxn = td[k * 33] - ta[k * 33] * gxf - tc[k * 33] * gxn;
+            td[k * 33] = gxn;
+        }
+        td[0] = gxf;
     }
     gsync();
-    double xlm = 0.0;
+    double xl = 0.0, xlm = 0.0;
     if (act) {
+        xl = T[2 * TS + TI(p)];
         if (cyclic)
-            xlm = F(cur ^ 1, 2, p == 0 ? P - 1 : p - 1);
+            xlm = T[2 * TS + TI(p == 0 ? P - 1 : p - 1)];
         else
-            xlm = p == 0 ? 0.0 : F(cur ^ 1, 2, p - 1);
+            xlm = p == 0 ? 0.0 : T[2 * TS + TI(p - 1)];
     }
     const double xf = act ? r0 - l0 * xlm - u0 * xl : 0.0;
-    if (!act) xl = 0.0;
 
     // ------------------------------------------------ back substitution
     double* xp = a.X + row0;
@@ -503,6 +576,8 @@ __device__ __forceinline__ void rag_cta_body(const RagArgs& a, const int4 task, 
 template <typename TIN, bool STAGED>
 __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
     extern __shared__ double rsm[];
+    if (threadIdx.x == 0 && a.pf_ahead > 0 && (int)blockIdx.x + a.pf_ahead < a.n_tasks)
+        rag_prefetch_system<TIN>(a, a.list[a.tasks[blockIdx.x + a.pf_ahead].x]);
     rag_cta_body<TIN, STAGED>(a, a.tasks[blockIdx.x], (int)blockDim.x, rsm, (int)threadIdx.x, 0);
 }
 
@@ -514,36 +589,53 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
 // c the CTA splits into 2^c groups of P threads, each with its own named
 // barrier and shared-memory slice, taking tasks independently; a group moves
 // on to the next class when its class is drained (the next class's groups lie
-// inside it, with barriers of their own).  a.mcap must be RAG_MT.
+// inside it, with barriers of their own).  A group claims its next task before
+// solving the current one and prefetches that system into L2, so its fill
+// reads L2 instead of waiting on DRAM.  a.mcap must be RAG_MT.
 constexpr int RAG_PERSIST_THREADS = 256;
 constexpr int RAG_PERSIST_CLASSES = 3;
 // shared-memory slice of a group of P threads (nested: two slices of P / 2
 // fit in one of P)
-__host__ __device__ __forceinline__ size_t rag_persist_slice(int P) {
+__host__ __device__ constexpr size_t rag_persist_slice(int P) {
     return rag_cta_smem_bytes(64, true, RAG_MT) * (size_t)(P / 64);
 }
+static_assert(rag_cta_smem_bytes(128, true, RAG_MT) <= rag_persist_slice(128) &&
+                  rag_cta_smem_bytes(256, true, RAG_MT) <= rag_persist_slice(256),
+              "a group's shared memory fits its slice");
 template <typename TIN>
 __global__ void __launch_bounds__(RAG_PERSIST_THREADS, 2) ragged_persist_kernel(const RagArgs a) {
     extern __shared__ double rsm[];
-    __shared__ int next_task[1 << RAG_PERSIST_CLASSES];  // by barrier id (unique per group)
+    // claimed tasks by barrier id (unique per group), two slots: the one written
+    // in an iteration is read after its barriers, and rewritten two iterations on
+    __shared__ int next_task[2][1 << RAG_PERSIST_CLASSES];
     const int tid = threadIdx.x;
+    static_assert(RAG_PERSIST_CLASSES == 3, "class selects below");
     for (int c = 0; c < RAG_PERSIST_CLASSES; ++c) {
         const int P = RAG_PERSIST_THREADS >> c;
         const int g = tid / P, p = tid % P;
         const int bid = (1 << c) + g;  // 1; 2, 3; 4 .. 7
         double* sm = rsm + rag_persist_slice(P) / sizeof(double) * g;
-        for (;;) {
-            if (p == 0) next_task[bid] = atomicAdd(&a.next[c], 1);
-            asm volatile("bar.sync %0, %1;" ::"r"(bid), "r"(P) : "memory");
-            const int t = next_task[bid];
-            if (t >= a.cls_count[c]) break;
-            const int4 task = a.tasks[a.cls_first[c] + t];
+        // constant indices: an index computed at run time would copy the whole
+        // parameter block to local memory
+        const int ccount = c == 0 ? a.cls_count[0] : c == 1 ? a.cls_count[1] : a.cls_count[2];
+        const int cfirst = c == 0 ? a.cls_first[0] : c == 1 ? a.cls_first[1] : a.cls_first[2];
+        if (p == 0) next_task[0][bid] = atomicAdd(&a.next[c], 1);
+        asm volatile("bar.sync %0, %1;" ::"r"(bid), "r"(P) : "memory");
+        int t = next_task[0][bid];
+        for (int it = 1; t < ccount; ++it) {
+            const int4 task = a.tasks[cfirst + t];
+            if (p == 0) {
+                const int tn = atomicAdd(&a.next[c], 1);
+                next_task[it & 1][bid] = tn;
+                if (tn < ccount) rag_prefetch_system<TIN>(a, a.list[a.tasks[cfirst + tn].x]);
+            }
             if (task.w)
                 rag_cta_body<TIN, true>(a, task, P, sm, p, bid);
             else
                 rag_cta_body<TIN, false>(a, task, P, sm, p, bid);
-            // the group's shared memory and next_task are rewritten by its next task
+            // the group's shared memory is rewritten by its next task
             asm volatile("bar.sync %0, %1;" ::"r"(bid), "r"(P) : "memory");
+            t = next_task[it & 1][bid];
         }
     }
 }
