@@ -262,24 +262,23 @@ __device__ __forceinline__ void cp_async_elem(double* dst, const float* src) {
                  : "memory");
 }
 
+// r / d = __umulhi(r, rag_magic(d)) exactly for d >= 2 and r * d < 2^32:
+// rag_magic(d) = ceil(2^32 / d) = 2^32 / d + e / d with 0 <= e < d, so the
+// product's high word is floor(r / d + r e / (d 2^32)), and r e / 2^32 < 1
+// cannot carry the fraction (r mod d) / d <= (d - 1) / d past the next integer.
+__device__ __forceinline__ unsigned rag_magic(int d) { return 0xFFFFFFFFu / (unsigned)d + 1u; }
+
 // (segment, row in segment) of row r of a system split by para_range into P
-// parts of base or base + 1 rows (the first rem parts longer).
-__device__ __forceinline__ void rag_locate(int r, int base, int rem, float inv0, float inv1,
-                                           int& q, int& k) {
-    const int split = rem * (base + 1);
-    if (r < split) {
-        q = (int)((float)r * inv1);
-        if (q * (base + 1) > r) --q;
-        else if ((q + 1) * (base + 1) <= r) ++q;
-        k = r - q * (base + 1);
-    } else {
-        const int r2 = r - split;
-        q = (int)((float)r2 * inv0);
-        if (q * base > r2) --q;
-        else if ((q + 1) * base <= r2) ++q;
-        k = r2 - q * base;
-        q += rem;
-    }
+// parts of base or base + 1 rows (the first rem parts longer, split = rem *
+// (base + 1) rows in all); mag0 / mag1 = rag_magic(base) / rag_magic(base + 1).
+// Rows per system stay below 2^13 and base + 1 below 2^5.
+__device__ __forceinline__ void rag_locate(int r, int base, int rem, int split, unsigned mag0,
+                                           unsigned mag1, int& q, int& k) {
+    const bool lo = r < split;
+    const int rr = lo ? r : r - split;
+    const int qq = (int)__umulhi((unsigned)rr, lo ? mag1 : mag0);
+    k = rr - qq * (lo ? base + 1 : base);
+    q = lo ? qq : qq + rem;
 }
 
 // One system (task {list index, cyclic, ...}) solved by a group of P threads
@@ -323,14 +322,22 @@ __device__ __forceinline__ void rag_cta_body(const RagArgs& a, const int4 task, 
     double* stt = STAGED ? stg + p * M : stg + p;
     const int fs = STAGED ? P * M : a.mcap * P;  // field stride
     const int ks = STAGED ? 1 : P;               // row stride (unstaged)
-    const float inv0 = 1.0f / (float)(base > 0 ? base : 1), inv1 = 1.0f / (float)(base + 1);
+    // rows per thread: base or base + 1; mx, the most, is the same for the
+    // whole group (the B loads stop there)
+    const int mx = base + (rem > 0 ? 1 : 0);
+    const int split = rem * (base + 1);
+    const unsigned mag0 = rag_magic(base > 1 ? base : 2), mag1 = rag_magic(base + 1);
     // staged: the thread's B rows go to registers, requested before the fill so
     // that both arrive together and the forward sweep waits on shared memory only
     // (rows past m repeat row m - 1 and are never used)
     double bq[M];
     if constexpr (STAGED) {
 #pragma unroll
-        for (int k = 0; k < M; ++k) bq[k] = (double)__ldg(pB + (k < m ? k : m - 1));
+        for (int k = 0; k < M; ++k) {
+            double v = 0.0;
+            if (k < mx) v = (double)__ldg(pB + (k < m ? k : m - 1));
+            bq[k] = v;
+        }
     }
     if constexpr (STAGED) {
         // fields 0..2 = A, C, D; coalesced over the system's rows
@@ -342,7 +349,7 @@ __device__ __forceinline__ void rag_cta_body(const RagArgs& a, const int4 task, 
         // 8-byte slot and each thread widens its own rows once they are in
         for (int r = p; r < n; r += NT) {
             int q, k;
-            rag_locate(r, base, rem, inv0, inv1, q, k);
+            rag_locate(r, base, rem, split, mag0, mag1, q, k);
             double* dst = stg + q * M + rag_slot(q, k);
             cp_async_elem(dst + 0 * fs, gA + r);
             cp_async_elem(dst + 1 * fs, gC + r);
@@ -542,9 +549,9 @@ __device__ __forceinline__ void rag_cta_body(const RagArgs& a, const int4 task, 
     // staged: x overwrites delta in the D field (each row's delta is read just
     // before) and leaves coalesced
     auto XO = [&](int k) -> double& { return stt[2 * fs + SL(k)]; };
-#pragma unroll
-    for (int k = M - 2; k >= 1; --k) {
-        if (k <= m - 2) {
+#pragma unroll 4
+    for (int k = m - 2; k >= 1; --k) {
+        {
             xn = DE(k) - AL(k) * xf - GA(k) * xn;
             nonfinite = fma(xn, 0.0, nonfinite);
             if constexpr (STAGED)
@@ -562,7 +569,7 @@ __device__ __forceinline__ void rag_cta_body(const RagArgs& a, const int4 task, 
         double* gX = a.X + o;
         for (int r = p; r < n; r += NT) {
             int q, k;
-            rag_locate(r, base, rem, inv0, inv1, q, k);
+            rag_locate(r, base, rem, split, mag0, mag1, q, k);
             gX[r] = stg[2 * fs + q * M + rag_slot(q, k)];
         }
     } else if (act) {
