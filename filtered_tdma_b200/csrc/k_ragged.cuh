@@ -220,9 +220,10 @@ __global__ void __launch_bounds__(256) ragged_kernel(const RagArgs a) {
 // Long systems: one CTA of P threads (P a power of two, 64..512) per system,
 // at most RAG_MT rows per thread, the elimination state in shared memory laid
 // out [field][row][thread] (consecutive threads, consecutive doubles).  The
-// reduced system of the P sub-segments runs through shared memory: one
-// cyclic-reduction level, then parallel cyclic reduction with a block barrier
-// per level (the same steps as reduced_solve_shfl).
+// reduced system of the P sub-segments goes through shared memory: one
+// cyclic-reduction level leaves P unknowns, which warp 0 solves in two levels
+// (groups of P / 32 rows, then the 32 groups' interfaces with
+// reduced_solve_shfl; see rag_cta_body).
 constexpr int RAG_MT = 16;
 
 // STAGED: A, C and D of the whole system are first copied into shared memory
