@@ -44,23 +44,27 @@ void rag_bucket_tasks(const btdma_handle::RagBucket& b, int cta, int P, std::vec
         out.push_back(make_int4(b.first + i, std::min(G, b.count - i), P, b.cyc));
 }
 
-// Task tables of the whole plan: one warp-kind launch (buckets longest first),
-// one persistent launch for every CTA-kind bucket of at most
-// RAG_PERSIST_THREADS threads (tasks {list index, cyclic, P, staged}, the
-// longest systems first, so the tail of the launch is short work), and one
-// CTA-kind launch per longer P.
+// Task tables of the whole plan: warp-kind launches (buckets longest first;
+// one for the buckets of at most RAG_MT rows per lane and one for the longer
+// ones, since a launch's shared memory is sized by its longest bucket and
+// would otherwise halve the short buckets' occupancy), one persistent launch
+// for every CTA-kind bucket of at most RAG_PERSIST_THREADS threads (tasks
+// {list index, cyclic, P, staged}, the longest systems first, so the tail of
+// the launch is short work), and one CTA-kind launch per longer P.
 int rag_build_launches(btdma_t h) {
     std::vector<int4> tasks;
     h->rag_launches.clear();
-    btdma_handle::RagLaunch wl{0, 0, 0, 0, 1, 0};
-    for (int i = (int)h->rag_buckets.size() - 1; i >= 0; --i) {
-        const auto& b = h->rag_buckets[i];
-        if (b.cta) continue;
-        rag_bucket_tasks(b, 0, b.P, tasks);
-        wl.mcap = std::max(wl.mcap, rag_mcap(b.nmax, b.P));
+    for (int longer = 0; longer < 2; ++longer) {
+        btdma_handle::RagLaunch wl{0, 0, (int)tasks.size(), 0, 1, 0};
+        for (int i = (int)h->rag_buckets.size() - 1; i >= 0; --i) {
+            const auto& b = h->rag_buckets[i];
+            if (b.cta || (rag_mcap(b.nmax, b.P) > RAG_MT) != (longer != 0)) continue;
+            rag_bucket_tasks(b, 0, b.P, tasks);
+            wl.mcap = std::max(wl.mcap, rag_mcap(b.nmax, b.P));
+        }
+        wl.count = (int)tasks.size() - wl.first;
+        if (wl.count) h->rag_launches.push_back(wl);
     }
-    wl.count = (int)tasks.size();
-    if (wl.count) h->rag_launches.push_back(wl);
     if (h->rag_persist) {
         // one class per P (256, 128, 64), each longest first
         btdma_handle::RagLaunch pl{2, RAG_PERSIST_THREADS, (int)tasks.size(), 0, RAG_MT, 0};
