@@ -30,6 +30,18 @@ int fail(int code, const char* fmt, ...) {
 
 }  // namespace btdma_host
 
+int tile_solve_batch(const void* A, const void* B, const void* C, const void* D, int elem,
+                     double* X, int n_sys, int n_row, unsigned* status, cudaStream_t st) {
+    if (elem == 8)
+        return try_tile<double>(static_cast<const double*>(A), static_cast<const double*>(B),
+                                static_cast<const double*>(C), static_cast<const double*>(D), X,
+                                n_sys, n_row, false, status, st, false, nullptr,
+                                BTDMA_TILE_AUTO);
+    return try_tile<float>(static_cast<const float*>(A), static_cast<const float*>(B),
+                           static_cast<const float*>(C), static_cast<const float*>(D), X, n_sys,
+                           n_row, false, status, st, false, nullptr, BTDMA_TILE_AUTO);
+}
+
 namespace {
 
 int jmax_launch(btdma_t h, const double* D, int n_sys, int n_row, cudaStream_t st) {
@@ -303,6 +315,7 @@ int btdma_create(int method, int n_sys, int n_row, int P, int precision, int fla
 
 int btdma_destroy(btdma_t h) {
     if (!h) return BTDMA_OK;
+    for (auto& b : h->rag_buckets) cudaFree(b.ibuf);
     cudaFree(h->rho_row);
     cudaFree(h->J);
     cudaFree(h->work);

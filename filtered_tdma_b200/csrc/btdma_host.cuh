@@ -22,6 +22,13 @@
 
 using namespace btdma;
 
+// The tiled PaScaL solve of one uniform non-periodic batch [n_row][n_sys] with
+// A, B, C, D of elem bytes (8: FP64, 4: FP32 storage), the kernel shape chosen
+// as for a uniform batch (btdma_api.cu).  1: launched; 0: the shape is not
+// tiled; < 0: error.
+int tile_solve_batch(const void* A, const void* B, const void* C, const void* D, int elem,
+                     double* X, int n_sys, int n_row, unsigned* status, cudaStream_t st);
+
 struct btdma_handle {
     int method, P, precision, flags;
     int tile_shape = 0;  // BTDMA_TILE_AUTO / NARROW / WIDE (uniform PaScaL batches)
@@ -53,6 +60,11 @@ struct btdma_handle {
         int staged; // CTA kind: system staged through shared memory (autotuner's choice)
         int P, warps, mcap;
         float best_ms;
+        // interleaved (non-periodic buckets): gathered into a row-interleaved
+        // batch of npad x nbp systems, solved by the tiled kernel, scattered back;
+        // ibuf holds the gathered A, B, C, D and the batch's x
+        int inter = 0, npad = 0, nbp = 0;
+        void* ibuf = nullptr;
     };
     std::vector<long long> rag_off;        // host copy of the offsets of the plan
     std::vector<unsigned char> rag_per;    // host copy of the periodic flags

@@ -23,6 +23,51 @@ int rag_default_P(int nmin, int nmax) {
 
 int rag_mcap(int nmax, int P) { return (nmax + P - 1) / P; }
 
+// Interleaved buckets (cta_per_system 3): the padded batch's rows and systems,
+// and its scratch (gathered A, B, C, D of elem bytes, then x in FP64).
+int rag_il_rows(const btdma_handle::RagBucket& b) { return (b.nmax + TILE_MT - 1) / TILE_MT * TILE_MT; }
+int rag_il_cols(const btdma_handle::RagBucket& b) { return (b.count + 3) / 4 * 4; }
+size_t rag_il_bytes(const btdma_handle::RagBucket& b, int elem) {
+    const size_t plane = (size_t)rag_il_rows(b) * rag_il_cols(b);
+    return plane * (4 * (size_t)elem + sizeof(double));
+}
+// Gives bucket b its scratch for the interleaved kind (kept with the plan).
+int rag_il_alloc(btdma_handle::RagBucket& b, int elem) {
+    cudaFree(b.ibuf);
+    b.ibuf = nullptr;
+    b.npad = rag_il_rows(b);
+    b.nbp = rag_il_cols(b);
+    CK(cudaMalloc(&b.ibuf, rag_il_bytes(b, elem)));
+    return BTDMA_OK;
+}
+void rag_il_free(btdma_handle::RagBucket& b) {
+    cudaFree(b.ibuf);
+    b.ibuf = nullptr;
+}
+
+// One interleaved bucket: gather, tiled solve, scatter (stream order).  1 when
+// solved, 0 when the tiled kernel does not take the padded shape, < 0 on error.
+template <typename TIN>
+int rag_il_run(btdma_t h, const btdma_handle::RagBucket& b, const TIN* A, const TIN* B,
+               const TIN* C, const TIN* D, double* X, cudaStream_t st) {
+    const int npad = b.npad, nbp = b.nbp;
+    const size_t plane = (size_t)npad * nbp;
+    TIN* g = static_cast<TIN*>(b.ibuf);
+    double* xi = reinterpret_cast<double*>(g + 4 * plane);
+    const dim3 blk(32, 8), grd((nbp + RAG_IL_TILE - 1) / RAG_IL_TILE,
+                               (npad + RAG_IL_TILE - 1) / RAG_IL_TILE);
+    rag_gather_kernel<TIN><<<grd, blk, 0, st>>>(A, B, C, D, h->rag_d_off, h->rag_d_list, b.first,
+                                                b.count, npad, nbp, g);
+    CK(cudaGetLastError());
+    const int rc = tile_solve_batch(g, g + plane, g + 2 * plane, g + 3 * plane, (int)sizeof(TIN),
+                                    xi, nbp, npad, h->status, st);
+    if (rc <= 0) return rc;
+    rag_scatter_kernel<<<grd, blk, 0, st>>>(xi, h->rag_d_off, h->rag_d_list, b.first, b.count,
+                                            npad, nbp, X);
+    CK(cudaGetLastError());
+    return 1;
+}
+
 // CTA-per-system shape for long systems: the smallest power of two >= 64 that
 // keeps <= RAG_MT rows per thread (0 when none <= 512 does, or when the
 // shortest system would get fewer than 3 rows per thread).
@@ -58,7 +103,7 @@ int rag_build_launches(btdma_t h) {
         btdma_handle::RagLaunch wl{0, 0, (int)tasks.size(), 0, 1, 0};
         for (int i = (int)h->rag_buckets.size() - 1; i >= 0; --i) {
             const auto& b = h->rag_buckets[i];
-            if (b.cta || (rag_mcap(b.nmax, b.P) > RAG_MT) != (longer != 0)) continue;
+            if (b.inter || b.cta || (rag_mcap(b.nmax, b.P) > RAG_MT) != (longer != 0)) continue;
             rag_bucket_tasks(b, 0, b.P, tasks);
             wl.mcap = std::max(wl.mcap, rag_mcap(b.nmax, b.P));
         }
@@ -72,7 +117,9 @@ int rag_build_launches(btdma_t h) {
             const int Pc = RAG_PERSIST_THREADS >> c;
             std::vector<int> ids;
             for (int i = 0; i < (int)h->rag_buckets.size(); ++i)
-                if (h->rag_buckets[i].cta && h->rag_buckets[i].P == Pc) ids.push_back(i);
+                if (!h->rag_buckets[i].inter && h->rag_buckets[i].cta &&
+                    h->rag_buckets[i].P == Pc)
+                    ids.push_back(i);
             std::stable_sort(ids.begin(), ids.end(), [&](int x, int y) {
                 return h->rag_buckets[x].nmax > h->rag_buckets[y].nmax;
             });
@@ -92,7 +139,7 @@ int rag_build_launches(btdma_t h) {
         for (int stg = 0; stg < 2; ++stg) {
             btdma_handle::RagLaunch cl{1, P, (int)tasks.size(), 0, 1, stg};
             for (const auto& b : h->rag_buckets)
-                if (b.cta && b.P == P && b.staged == stg) {
+                if (!b.inter && b.cta && b.P == P && b.staged == stg) {
                     rag_bucket_tasks(b, 1, P, tasks);
                     cl.mcap = std::max(cl.mcap, rag_mcap(b.nmax, P));
                 }
@@ -100,6 +147,10 @@ int rag_build_launches(btdma_t h) {
             if (cl.count) h->rag_launches.push_back(cl);
         }
     }
+    // interleaved buckets: a launch sequence each (cta 3, P = the bucket's index)
+    for (int i = 0; i < (int)h->rag_buckets.size(); ++i)
+        if (h->rag_buckets[i].inter)
+            h->rag_launches.push_back(btdma_handle::RagLaunch{3, i, 0, 0, 0, 0});
     CK(cudaMemcpy(h->rag_d_tasks, tasks.data(), sizeof(int4) * tasks.size(),
                   cudaMemcpyHostToDevice));
     return BTDMA_OK;
@@ -163,6 +214,7 @@ int rag_plan(btdma_t h, const long long* off, const unsigned char* per, int n_sy
         bk.push_back(b);
         i = j;
     }
+    for (auto& b : h->rag_buckets) rag_il_free(b);
     cudaFree(h->rag_d_off);
     cudaFree(h->rag_d_list);
     cudaFree(h->rag_d_tasks);
@@ -284,6 +336,12 @@ int rag_run(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, d
     }
     for (int i = 0; i < n; ++i) {
         const cudaStream_t s = i == 0 ? st : h->rag_side[(i - 1) % btdma_handle::RAG_STREAMS];
+        if (L[i].cta == 3) {
+            const int rc = rag_il_run<TIN>(h, h->rag_buckets[L[i].P], A, B, C, D, X, s);
+            if (rc < 0) return rc;
+            if (rc == 0) return fail(BTDMA_ERR_UNSUPPORTED, "interleaved bucket not tileable");
+            continue;
+        }
         const int rc = rag_launch<TIN>(h, L[i].cta, L[i].P, L[i].mcap, L[i].staged,
                                        h->rag_d_tasks + L[i].first, L[i].count, A, B, C, D, X,
                                        s);
@@ -328,9 +386,10 @@ int rag_tune(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, 
     std::vector<int4> tasks;
     for (auto& b : h->rag_buckets) {
         struct Cand {
-            int cta, P, staged;
+            int cta, P, staged;  // cta 3: interleaved
         };
         std::vector<Cand> cands;
+        if (!b.cyc) cands.push_back({3, 1, 0});
         for (int P = 1; P <= 32 && b.nmin / P >= 3; P <<= 1)
             if (rag_mcap(b.nmax, P) <= RAG_WARP_MCAP) cands.push_back({0, P, 0});
         for (int P = 64; P <= 512 && b.nmin / P >= 3; P <<= 1)
@@ -341,8 +400,30 @@ int rag_tune(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, 
                     cands.push_back({1, P, 1});
             }
         float best = 1e30f;
-        Cand pick{b.cta, b.P, b.staged};
+        Cand pick{b.inter ? 3 : b.cta, b.P, b.staged};
         for (const Cand& cd : cands) {
+            if (cd.cta == 3) {  // gather + tiled solve + scatter, on its own scratch
+                if ((rc = rag_il_alloc(b, (int)sizeof(TIN)))) break;
+                float ms = 0.f;
+                int ran = 1;
+                for (int rep = 0; rep < 3 && !rc && ran == 1; ++rep) {
+                    CK(cudaEventRecord(e0, st));
+                    ran = rag_il_run<TIN>(h, b, A, B, C, D, X, st);
+                    if (ran < 0) rc = ran;
+                    if (ran != 1) break;
+                    CK(cudaEventRecord(e1, st));
+                    CK(cudaEventSynchronize(e1));
+                    float t = 0.f;
+                    CK(cudaEventElapsedTime(&t, e0, e1));
+                    ms = rep == 0 ? t : std::min(ms, t);
+                }
+                if (rc) break;
+                if (ran == 1 && ms < best) {
+                    best = ms;
+                    pick = cd;
+                }
+                continue;
+            }
             tasks.clear();
             rag_bucket_tasks(b, cd.cta, cd.P, tasks);
             if (cudaMemcpyAsync(h->rag_d_probe, tasks.data(), sizeof(int4) * tasks.size(),
@@ -370,7 +451,9 @@ int rag_tune(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, 
             }
         }
         if (rc) break;
-        b.cta = pick.cta;
+        b.inter = pick.cta == 3;
+        if (!b.inter) rag_il_free(b);
+        b.cta = pick.cta == 3 ? 0 : pick.cta;
         b.staged = pick.staged;
         b.P = pick.P;
         b.warps = pick.cta ? pick.P / 32 : RAG_WPC;
@@ -446,6 +529,13 @@ int btdma_ragged_set_plan(btdma_t h, const btdma_ragged_bucket* in, int n) {
             if (P > 32 || rag_mcap(b.nmax, P) > RAG_WARP_MCAP)
                 return fail(BTDMA_ERR_ARG, "bucket %d: warp kind needs P <= 32 and <= %d rows "
                             "per lane", i, RAG_WARP_MCAP);
+        } else if (kind == 3) {
+            if (b.cyc)
+                return fail(BTDMA_ERR_ARG, "bucket %d: periodic systems cannot be padded into an "
+                            "interleaved batch", i);
+            if (tile_plan(rag_il_rows(b), false, h->precision == BTDMA_FP64 ? 8 : 4).sys == 0)
+                return fail(BTDMA_ERR_ARG, "bucket %d: the tiled kernel does not take %d rows", i,
+                            rag_il_rows(b));
         } else if (kind == 1 || kind == 2) {
             if (P < 64 || P > 512 || rag_mcap(b.nmax, P) > RAG_MT)
                 return fail(BTDMA_ERR_ARG, "bucket %d: CTA kind needs 64 <= P <= 512 and <= %d "
@@ -461,8 +551,15 @@ int btdma_ragged_set_plan(btdma_t h, const btdma_ragged_bucket* in, int n) {
     for (int i = 0; i < n; ++i) {
         auto& b = h->rag_buckets[i];
         b.P = in[i].lanes_per_system;
-        b.cta = in[i].cta_per_system > 0 ? 1 : 0;
+        b.inter = in[i].cta_per_system == 3 ? 1 : 0;
+        b.cta = in[i].cta_per_system == 1 || in[i].cta_per_system == 2 ? 1 : 0;
         b.staged = in[i].cta_per_system == 2 ? 1 : 0;
+        if (b.inter) {
+            const int rc = rag_il_alloc(b, h->precision == BTDMA_FP64 ? 8 : 4);
+            if (rc) return rc;
+        } else {
+            rag_il_free(b);
+        }
         b.warps = b.cta ? b.P / 32 : RAG_WPC;
         b.mcap = rag_mcap(b.nmax, b.P);
         b.best_ms = in[i].tuned_ms;
@@ -484,9 +581,10 @@ int btdma_ragged_plan_info(btdma_t h, btdma_ragged_bucket* out, int cap, int* n_
         out[i].n_row_max = b.nmax;
         out[i].lanes_per_system = b.P;
         out[i].warps_per_cta = b.warps;
-        out[i].cta_per_system = b.cta + b.staged;
+        out[i].cta_per_system = b.inter ? 3 : b.cta + b.staged;
         out[i].tuned_ms = b.best_ms;
-        out[i].persistent = h->rag_persist && b.cta && b.P <= RAG_PERSIST_THREADS ? 1 : 0;
+        out[i].persistent =
+            h->rag_persist && !b.inter && b.cta && b.P <= RAG_PERSIST_THREADS ? 1 : 0;
     }
     return BTDMA_OK;
 }

@@ -648,4 +648,83 @@ __global__ void __launch_bounds__(RAG_PERSIST_THREADS, 2) ragged_persist_kernel(
     }
 }
 
+// Interleaved layout of one bucket (the autotuner's alternative to solving it
+// in place): its `count` non-periodic systems, list[first .. first + count),
+// copied into a row-interleaved batch of npad rows x nbp systems (row r of
+// system j at r * nbp + j; npad a multiple of 16, nbp of 4), which the tiled
+// kernel then solves like any uniform batch.  A system shorter than npad is
+// continued by identity rows (a = c = d = 0, b = 1) and its own A[first] and
+// C[last], which a non-periodic system does not use, are stored as zero, so the
+// padding neither couples to it nor changes its solution; columns past count
+// are identity systems.  32 x 32 tiles through shared memory: read along each
+// system's contiguous rows, write along the interleaved rows.
+constexpr int RAG_IL_TILE = 32;
+
+template <typename TIN>
+__global__ void __launch_bounds__(256) rag_gather_kernel(const TIN* __restrict__ A,
+                                                          const TIN* __restrict__ B,
+                                                          const TIN* __restrict__ C,
+                                                          const TIN* __restrict__ D,
+                                                          const long long* __restrict__ off,
+                                                          const int* __restrict__ list, int first,
+                                                          int count, int npad, int nbp,
+                                                          TIN* __restrict__ out) {
+    __shared__ TIN t[4][RAG_IL_TILE][RAG_IL_TILE + 1];
+    const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+    const int j0 = blockIdx.x * RAG_IL_TILE, r0 = blockIdx.y * RAG_IL_TILE;
+    const size_t plane = (size_t)npad * nbp;
+    for (int jj = ty; jj < RAG_IL_TILE; jj += 8) {
+        const int j = j0 + jj, r = r0 + tx;
+        TIN a = 0, b = 1, c = 0, d = 0;
+        if (j < count) {
+            const int sys = list[first + j];
+            const long long o = off[sys];
+            const int n = (int)(off[sys + 1] - o);
+            if (r < n) {
+                a = r == 0 ? TIN(0) : A[o + r];
+                b = B[o + r];
+                c = r == n - 1 ? TIN(0) : C[o + r];
+                d = D[o + r];
+            }
+        }
+        t[0][jj][tx] = a;
+        t[1][jj][tx] = b;
+        t[2][jj][tx] = c;
+        t[3][jj][tx] = d;
+    }
+    __syncthreads();
+    for (int rr = ty; rr < RAG_IL_TILE; rr += 8) {
+        const int r = r0 + rr, j = j0 + tx;
+        if (r < npad && j < nbp) {
+            const size_t e = (size_t)r * nbp + j;
+#pragma unroll
+            for (int f = 0; f < 4; ++f) out[f * plane + e] = t[f][tx][rr];
+        }
+    }
+}
+
+// The solution back from the interleaved batch to the systems' rows.
+__global__ void __launch_bounds__(256) rag_scatter_kernel(const double* __restrict__ xi,
+                                                           const long long* __restrict__ off,
+                                                           const int* __restrict__ list,
+                                                           int first, int count, int npad,
+                                                           int nbp, double* __restrict__ X) {
+    __shared__ double t[RAG_IL_TILE][RAG_IL_TILE + 1];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int j0 = blockIdx.x * RAG_IL_TILE, r0 = blockIdx.y * RAG_IL_TILE;
+    for (int rr = ty; rr < RAG_IL_TILE; rr += 8) {
+        const int r = r0 + rr, j = j0 + tx;
+        t[rr][tx] = (r < npad && j < nbp) ? xi[(size_t)r * nbp + j] : 0.0;
+    }
+    __syncthreads();
+    for (int jj = ty; jj < RAG_IL_TILE; jj += 8) {
+        const int j = j0 + jj, r = r0 + tx;
+        if (j < count) {
+            const int sys = list[first + j];
+            const long long o = off[sys];
+            if (r < (int)(off[sys + 1] - o)) X[o + r] = t[tx][jj];
+        }
+    }
+}
+
 }  // namespace btdma

@@ -247,8 +247,9 @@ int btdma_solve_ragged_f32(btdma_t h, const float* A, const float* B, const floa
 /* Autotuner of ragged solves: times, for every bucket of the plan, each launch
  * shape — P lanes of a warp per system (P = 1..32) with 1..8 warps per CTA, or
  * one CTA of P = 64..512 threads per system (<= 16 rows per thread) — with at
- * least 3 rows per thread, on this batch, and keeps the fastest for later
- * solves of the same layout.  Then it times the whole solve two ways — every
+ * least 3 rows per thread, and for non-periodic buckets the interleaved layout
+ * (gather into a padded row-interleaved batch, tiled solve, scatter back), on
+ * this batch, and keeps the fastest for later solves of the same layout.  Then it times the whole solve two ways — every
  * CTA-kind shape as a launch of its own, or the CTA-kind buckets of at most
  * 256 threads in one persistent launch (CTAs split into groups of their
  * buckets' thread counts, taking systems longest first from a counter) — and
@@ -268,7 +269,11 @@ typedef struct btdma_ragged_bucket {
     int warps_per_cta;
     int cta_per_system;   /* 0: lanes of a warp per system; 1: one CTA per system
                              (long systems); 2: one CTA per system staged through
-                             shared memory */
+                             shared memory; 3: interleaved layout -- the bucket's
+                             systems copied into a row-interleaved batch padded to
+                             its longest system (identity rows), solved by the
+                             tiled kernel and copied back (non-periodic buckets,
+                             lanes_per_system 1) */
     float tuned_ms;       /* fastest time measured by the autotuner (0 before tuning) */
     int persistent;       /* 1: the bucket's systems run in the plan's one persistent
                              launch (CTA-kind buckets of at most 256 threads, when the

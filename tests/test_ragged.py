@@ -182,6 +182,8 @@ def _shapes(b):
             out.append((P, 1))
             if 4 * P * (mcap | 1) * 8 + 6 * (P + 2) * 8 <= 227 * 1024:  # staged tile fits
                 out.append((P, 2))
+    if not b["periodic"]:
+        out.append((1, 3))  # interleaved: padded row-interleaved batch, tiled kernel
     return out
 
 
@@ -189,7 +191,8 @@ def _shapes(b):
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_ragged_every_launch_shape(cuda, orc, precision):
     """Every shape of every bucket (warp lanes, CTA, CTA staged through shared
-    memory), applied with btdma_ragged_set_plan, against the oracle."""
+    memory, interleaved copy for the tiled kernel), applied with
+    btdma_ragged_set_plan, against the oracle."""
     import torch
     dtype = np.float64 if precision == "fp64" else np.float32
     A, B, C, D, off, per = W.ragged_batch(600, seed=58, dtype=dtype)
@@ -205,6 +208,11 @@ def test_ragged_every_launch_shape(cuda, orc, precision):
         with pytest.raises(L.BtdmaError):
             s.ragged_set_plan([bad] + plan[1:] if bad["n_row_min"] == plan[0]["n_row_min"]
                               else plan[:-1] + [bad])
+    cyc = [i for i, b in enumerate(plan) if b["periodic"]]
+    assert cyc
+    with pytest.raises(L.BtdmaError):  # padding would break the wrap-around coupling
+        s.ragged_set_plan([dict(b, cta_per_system=3, lanes_per_system=1) if i == cyc[0] else b
+                           for i, b in enumerate(plan)])
     assert s.ragged_plan() == plan  # a rejected plan leaves the current one
     opts = [_shapes(b) for b in plan]
     assert all(opts)
@@ -220,7 +228,7 @@ def test_ragged_every_launch_shape(cuda, orc, precision):
             got = s.ragged_plan()
             assert [(b["lanes_per_system"], b["cta_per_system"]) for b in got] == want
             assert [b["persistent"] for b in got] == [
-                int(pers and k > 0 and P <= 256) for P, k in want]
+                int(pers and k in (1, 2) and P <= 256) for P, k in want]
             X.zero_()
             s.solve_ragged(dA, dB, dC, dD, X, off, per)
             torch.cuda.synchronize()
