@@ -74,8 +74,9 @@ struct btdma_handle {
     int* rag_d_list = nullptr;             // device copy of rag_order
     int4* rag_d_tasks = nullptr;           // task tables [2 * n_sys]
     int4* rag_d_probe = nullptr;           // task table of one bucket being tuned [n_sys]
-    int* rag_d_next = nullptr;             // task counters of the persistent launch [3]
+    int* rag_d_next = nullptr;             // task counters of the persistent launch [4]
     int rag_cls_first[3] = {}, rag_cls_count[3] = {};  // its classes (P = 256, 128, 64)
+    int rag_warp_first = 0, rag_warp_count = 0;        // and its warp class
     bool rag_persist = false;              // CTA-kind buckets in the persistent launch
     // launches of a solve: warp-kind tasks (one launch), the long systems of
     // at most RAG_PERSIST_THREADS threads in one persistent launch (cta == 2),

@@ -94,13 +94,16 @@ void rag_bucket_tasks(const btdma_handle::RagBucket& b, int cta, int P, std::vec
 // ones, since a launch's shared memory is sized by its longest bucket and
 // would otherwise halve the short buckets' occupancy), one persistent launch
 // for every CTA-kind bucket of at most RAG_PERSIST_THREADS threads (tasks
-// {list index, cyclic, P, staged}, the longest systems first, so the tail of
-// the launch is short work), and one CTA-kind launch per longer P.
+// {list index, cyclic, P, staged}, the longest systems first) followed by the
+// warp-kind buckets of at most RAG_MT rows per lane as its warp class (so the
+// launch's tail is short work; those buckets then get no launch of their own),
+// and one CTA-kind launch per longer P.
 int rag_build_launches(btdma_t h) {
     std::vector<int4> tasks;
     h->rag_launches.clear();
     for (int longer = 0; longer < 2; ++longer) {
         btdma_handle::RagLaunch wl{0, 0, (int)tasks.size(), 0, 1, 0};
+        if (!longer && h->rag_persist) continue;  // the persistent launch's warp class
         for (int i = (int)h->rag_buckets.size() - 1; i >= 0; --i) {
             const auto& b = h->rag_buckets[i];
             if (b.inter || b.cta || (rag_mcap(b.nmax, b.P) > RAG_MT) != (longer != 0)) continue;
@@ -131,6 +134,14 @@ int rag_build_launches(btdma_t h) {
             }
             h->rag_cls_count[c] = (int)tasks.size() - pl.first - h->rag_cls_first[c];
         }
+        // warp class: warp-kind buckets of at most RAG_MT rows a lane, longest first
+        h->rag_warp_first = (int)tasks.size() - pl.first;
+        for (int i = (int)h->rag_buckets.size() - 1; i >= 0; --i) {
+            const auto& b = h->rag_buckets[i];
+            if (b.inter || b.cta || rag_mcap(b.nmax, b.P) > RAG_MT) continue;
+            rag_bucket_tasks(b, 0, b.P, tasks);
+        }
+        h->rag_warp_count = (int)tasks.size() - pl.first - h->rag_warp_first;
         pl.count = (int)tasks.size() - pl.first;
         if (pl.count) h->rag_launches.push_back(pl);
     }
@@ -227,7 +238,7 @@ int rag_plan(btdma_t h, const long long* off, const unsigned char* per, int n_sy
     CK(cudaMalloc(&h->rag_d_list, sizeof(int) * n_sys));
     CK(cudaMalloc(&h->rag_d_tasks, sizeof(int4) * 2 * n_sys));
     CK(cudaMalloc(&h->rag_d_probe, sizeof(int4) * n_sys));
-    if (!h->rag_d_next) CK(cudaMalloc(&h->rag_d_next, sizeof(int) * RAG_PERSIST_CLASSES));
+    if (!h->rag_d_next) CK(cudaMalloc(&h->rag_d_next, sizeof(int) * (RAG_PERSIST_CLASSES + 1)));
     CK(cudaMemcpy(h->rag_d_off, off, sizeof(long long) * (n_sys + 1), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->rag_d_list, order.data(), sizeof(int) * n_sys, cudaMemcpyHostToDevice));
     if (!h->rag_fork) {
@@ -273,6 +284,8 @@ int rag_launch(btdma_t h, int cta, int P, int mcap, int staged, const int4* task
             a.cls_first[c] = h->rag_cls_first[c];
             a.cls_count[c] = h->rag_cls_count[c];
         }
+        a.warp_first = h->rag_warp_first;
+        a.warp_count = h->rag_warp_count;
         static bool attr_done = false;
         static int per_sm = 1;
         if (!attr_done) {
@@ -284,7 +297,7 @@ int rag_launch(btdma_t h, int cta, int P, int mcap, int staged, const int4* task
             attr_done = true;
         }
         a.mcap = RAG_MT;
-        CK(cudaMemsetAsync(h->rag_d_next, 0, sizeof(int) * RAG_PERSIST_CLASSES, st));
+        CK(cudaMemsetAsync(h->rag_d_next, 0, sizeof(int) * (RAG_PERSIST_CLASSES + 1), st));
         kern<<<std::min(n_tasks, per_sm * num_sms()), RAG_PERSIST_THREADS, smem, st>>>(a);
     } else if (cta) {
         if (staged && rag_cta_smem_bytes(P, true, mcap) > (size_t)max_smem_optin()) staged = 0;
@@ -583,8 +596,11 @@ int btdma_ragged_plan_info(btdma_t h, btdma_ragged_bucket* out, int cap, int* n_
         out[i].warps_per_cta = b.warps;
         out[i].cta_per_system = b.inter ? 3 : b.cta + b.staged;
         out[i].tuned_ms = b.best_ms;
-        out[i].persistent =
-            h->rag_persist && !b.inter && b.cta && b.P <= RAG_PERSIST_THREADS ? 1 : 0;
+        out[i].persistent = h->rag_persist && !b.inter &&
+                                    (b.cta ? b.P <= RAG_PERSIST_THREADS
+                                           : rag_mcap(b.nmax, b.P) <= RAG_MT)
+                                ? 1
+                                : 0;
     }
     return BTDMA_OK;
 }

@@ -44,6 +44,9 @@ struct RagArgs {
     // class's first task and task count in the table
     int* next;
     int cls_first[3], cls_count[3];
+    // ... and its warp class (counter next[3]): warp tasks of at most RAG_MT
+    // rows a lane, table entries warp_first .. warp_first + warp_count - 1
+    int warp_first, warp_count;
     // ragged_cta_kernel: CTA b prefetches the system of task b + pf_ahead (the
     // launch's co-resident CTAs: the task that takes over its slot) into L2;
     // 0: no prefetch
@@ -78,24 +81,21 @@ __device__ __forceinline__ void rag_prefetch_system(const RagArgs& a, int sys) {
 constexpr int RAG_LOOKAHEAD = 4;  // rows loaded ahead of the elimination
 
 // Shared memory per warp: 3 fields x mcap rows x 32 lanes doubles.
-__host__ __device__ __forceinline__ size_t rag_smem_bytes(int warps, int mcap) {
+__host__ __device__ constexpr size_t rag_smem_bytes(int warps, int mcap) {
     return (size_t)warps * 3 * mcap * 32 * sizeof(double);
 }
 
+// One warp task {first list index, systems (<= 32 / P), P, cyclic}, solved by
+// the calling warp (this thread: lane); its state area of 3 x mcap x 32
+// doubles starts at wsm.
 template <typename TIN>
-__global__ void __launch_bounds__(256) ragged_kernel(const RagArgs a) {
-    extern __shared__ double rsm[];
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    const int gw = blockIdx.x * (blockDim.x >> 5) + warp;
-    if (gw >= a.n_tasks) return;  // the whole warp
-    const int4 task = a.tasks[gw];
+__device__ __forceinline__ void rag_warp_body(const RagArgs& a, const int4 task, double* wsm,
+                                              const int lane, const int mcap) {
     const int P = task.z;
     const int g = lane / P;
     const int p = lane % P;
     const bool cyclic = task.w != 0;  // uniform over the warp
-    const int mcap = a.mcap;
-    double* st = rsm + (size_t)warp * 3 * mcap * 32 + lane;  // field f, row k: st[(f*mcap+k)*32]
+    double* st = wsm + lane;  // field f, row k: st[(f*mcap+k)*32]
 
     const bool have = g < task.y;
     int m = 0;
@@ -215,6 +215,16 @@ __global__ void __launch_bounds__(256) ragged_kernel(const RagArgs a) {
         xp[0] = xf;
         if (nonfinite != 0.0) raise_status(a.status, ST_NONFINITE);  // NaN != 0
     }
+}
+
+template <typename TIN>
+__global__ void __launch_bounds__(256) ragged_kernel(const RagArgs a) {
+    extern __shared__ double rsm[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int gw = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (gw >= a.n_tasks) return;  // the whole warp
+    rag_warp_body<TIN>(a, a.tasks[gw], rsm + (size_t)warp * 3 * a.mcap * 32, lane, a.mcap);
 }
 
 // Long systems: one CTA of P threads (P a power of two, 64..512) per system,
@@ -599,7 +609,11 @@ __global__ void __launch_bounds__(512) ragged_cta_kernel(const RagArgs a) {
 // on to the next class when its class is drained (the next class's groups lie
 // inside it, with barriers of their own).  A group claims its next task before
 // solving the current one and prefetches that system into L2, so its fill
-// reads L2 instead of waiting on DRAM.  a.mcap must be RAG_MT.
+// reads L2 instead of waiting on DRAM.  Last, every warp takes warp tasks
+// (short systems, P lanes each) from counter a.next[3] on its own, in half of
+// its 64-thread group's slice, which that group has left (both its warps leave
+// the last CTA class together), so the short work fills the launch's tail.
+// a.mcap must be RAG_MT.
 constexpr int RAG_PERSIST_THREADS = 256;
 constexpr int RAG_PERSIST_CLASSES = 3;
 // shared-memory slice of a group of P threads (nested: two slices of P / 2
@@ -610,6 +624,8 @@ __host__ __device__ constexpr size_t rag_persist_slice(int P) {
 static_assert(rag_cta_smem_bytes(128, true, RAG_MT) <= rag_persist_slice(128) &&
                   rag_cta_smem_bytes(256, true, RAG_MT) <= rag_persist_slice(256),
               "a group's shared memory fits its slice");
+static_assert(2 * rag_smem_bytes(1, RAG_MT) <= rag_persist_slice(64),
+              "a 64-thread group's two warps' warp-task state fits its slice");
 template <typename TIN>
 __global__ void __launch_bounds__(RAG_PERSIST_THREADS, 2) ragged_persist_kernel(const RagArgs a) {
     extern __shared__ double rsm[];
@@ -645,6 +661,17 @@ __global__ void __launch_bounds__(RAG_PERSIST_THREADS, 2) ragged_persist_kernel(
             asm volatile("bar.sync %0, %1;" ::"r"(bid), "r"(P) : "memory");
             t = next_task[it & 1][bid];
         }
+    }
+    const int lane = tid & 31, warp = tid >> 5;
+    double* wsm = rsm + rag_persist_slice(64) / sizeof(double) * (warp >> 1) +
+                  (size_t)(warp & 1) * (rag_smem_bytes(1, RAG_MT) / sizeof(double));
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(&a.next[3], 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= a.warp_count) break;
+        rag_warp_body<TIN>(a, a.tasks[a.warp_first + t], wsm, lane, RAG_MT);
+        __syncwarp();  // the warp's state area is rewritten by its next task
     }
 }
 

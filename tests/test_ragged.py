@@ -219,7 +219,8 @@ def test_ragged_every_launch_shape(cuda, orc, precision):
     assert any((P, 2) in o for o in opts for P in (64, 128, 256))
     assert any((512, 2) in o for o in opts)  # staged 512-thread CTAs (<= 8 rows a thread)
     # each shape as a launch of its own, then in the persistent launch (CTA
-    # kinds of at most 256 threads, split into groups of their thread counts)
+    # kinds of at most 256 threads, split into groups of their thread counts;
+    # warp kinds of at most 16 rows a lane, one warp per task)
     for pers in (0, 1):
         for j in range(max(len(o) for o in opts)):
             want = [o[j % len(o)] for o in opts]
@@ -227,8 +228,12 @@ def test_ragged_every_launch_shape(cuda, orc, precision):
                                for b, (P, k) in zip(plan, want)])
             got = s.ragged_plan()
             assert [(b["lanes_per_system"], b["cta_per_system"]) for b in got] == want
+            # in the persistent launch: CTA kinds of at most 256 threads, and the
+            # warp kind of at most 16 rows a lane as its warp class
             assert [b["persistent"] for b in got] == [
-                int(pers and k in (1, 2) and P <= 256) for P, k in want]
+                int(pers and ((k in (1, 2) and P <= 256) or
+                              (k == 0 and -(-b["n_row_max"] // P) <= 16)))
+                for b, (P, k) in zip(plan, want)]
             X.zero_()
             s.solve_ragged(dA, dB, dC, dD, X, off, per)
             torch.cuda.synchronize()
