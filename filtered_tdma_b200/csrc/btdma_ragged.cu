@@ -473,27 +473,54 @@ int rag_tune(btdma_t h, const TIN* A, const TIN* B, const TIN* C, const TIN* D, 
         b.mcap = rag_mcap(b.nmax, pick.P);
         b.best_ms = best;
     }
-    // the launch structure: a launch per CTA-kind shape, or the persistent
-    // launch; the whole solve timed both ways (best of 3)
-    float whole[2] = {1e30f, 1e30f};
-    for (int pers = 0; pers < 2 && !rc; ++pers) {
-        h->rag_persist = pers != 0;
-        if ((rc = rag_build_launches(h))) break;
-        for (int rep = 0; rep < 4 && !rc; ++rep) {
-            CK(cudaEventRecord(e0, st));
-            rc = rag_run<TIN>(h, A, B, C, D, X, st);
-            if (rc) break;
-            CK(cudaEventRecord(e1, st));
-            CK(cudaEventSynchronize(e1));
-            float t = 0.f;
-            CK(cudaEventElapsedTime(&t, e0, e1));
-            if (rep > 0) whole[pers] = std::min(whole[pers], t);  // rep 0 warms up
+    // the whole plan: the launch structure (a launch per CTA-kind shape, or the
+    // persistent launch) crossed with the CTA-kind buckets' staging as tuned
+    // bucket by bucket, all staged (where the staged tile fits) or all
+    // unstaged -- buckets timed alone do not see how they share the GPU in the
+    // solve; each plan timed as a whole (best of 3 after a warm-up), the
+    // fastest kept
+    std::vector<int> tuned_staged;
+    for (const auto& b : h->rag_buckets) tuned_staged.push_back(b.staged);
+    auto apply = [&](int mode) {  // 0: as tuned, 1: all staged, 2: all unstaged
+        for (size_t i = 0; i < h->rag_buckets.size(); ++i) {
+            auto& b = h->rag_buckets[i];
+            if (!b.cta || b.inter) continue;
+            b.staged = mode == 0 ? tuned_staged[i]
+                       : mode == 2 ? 0
+                                   : (rag_cta_smem_bytes(b.P, true, b.mcap) <=
+                                      (size_t)max_smem_optin());
+        }
+    };
+    float best_whole = 1e30f;
+    int best_mode = 0, best_pers = 0;
+    for (int mode = 0; mode < 3 && !rc; ++mode) {
+        apply(mode);
+        for (int pers = 0; pers < 2 && !rc; ++pers) {
+            h->rag_persist = pers != 0;
+            if ((rc = rag_build_launches(h))) break;
+            float whole = 1e30f;
+            for (int rep = 0; rep < 4 && !rc; ++rep) {
+                CK(cudaEventRecord(e0, st));
+                rc = rag_run<TIN>(h, A, B, C, D, X, st);
+                if (rc) break;
+                CK(cudaEventRecord(e1, st));
+                CK(cudaEventSynchronize(e1));
+                float t = 0.f;
+                CK(cudaEventElapsedTime(&t, e0, e1));
+                if (rep > 0) whole = std::min(whole, t);  // rep 0 warms up
+            }
+            if (whole < best_whole) {
+                best_whole = whole;
+                best_mode = mode;
+                best_pers = pers;
+            }
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc) return rc;
-    h->rag_persist = whole[1] < whole[0];
+    apply(best_mode);
+    h->rag_persist = best_pers != 0;
     return rag_build_launches(h);
 }
 

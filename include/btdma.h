@@ -249,11 +249,13 @@ int btdma_solve_ragged_f32(btdma_t h, const float* A, const float* B, const floa
  * one CTA of P = 64..512 threads per system (<= 16 rows per thread) — with at
  * least 3 rows per thread, and for non-periodic buckets the interleaved layout
  * (gather into a padded row-interleaved batch, tiled solve, scatter back), on
- * this batch, and keeps the fastest for later solves of the same layout.  Then it times the whole solve two ways — every
- * CTA-kind shape as a launch of its own, or the CTA-kind buckets of at most
- * 256 threads in one persistent launch (CTAs split into groups of their
- * buckets' thread counts, taking systems longest first from a counter) — and
- * keeps the faster.
+ * this batch, and keeps the fastest for later solves of the same layout.  Then it times whole
+ * solves — every CTA-kind shape as a launch of its own, or the CTA-kind
+ * buckets of at most 256 threads in one persistent launch (CTAs split into
+ * groups of their buckets' thread counts, taking systems longest first from a
+ * counter, then warp-kind tasks of at most 16 rows a lane) — each with the
+ * CTA-kind buckets staged as tuned, all staged or all unstaged, and keeps the
+ * fastest plan.
  * A..D are double or float as the handle's precision says; X is overwritten.
  * Blocking (it synchronises the stream). */
 int btdma_ragged_autotune(btdma_t h, const void* A, const void* B, const void* C, const void* D,
