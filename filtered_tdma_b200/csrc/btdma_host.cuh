@@ -470,7 +470,13 @@ int try_tile(const TIN* A, const TIN* B, const TIN* C, const TIN* D, double* X, 
         pl = tile_wide_plan(n_row, cyclic, elem);
         wide = pl.sys != 0 && (shape == BTDMA_TILE_WIDE || wide_by_default(n_row, elem));
     }
-    if (!wide) pl = tile_plan(n_row, cyclic, elem);
+    if (!wide) {
+        pl = tile_plan(n_row, cyclic, elem);
+        // small batches: fewer systems per CTA until every SM has a group (the
+        // ring's stages only get smaller, so its depth stays valid)
+        while (pl.sys > 16 && pl.cl == 1 && (n_sys + pl.sys - 1) / pl.sys < num_sms())
+            pl.sys >>= 1;
+    }
     if (pl.sys == 0) return 0;
     if (!(tma_ok_elem(A, n_sys, elem) && tma_ok_elem(B, n_sys, elem) &&
           tma_ok_elem(C, n_sys, elem) && tma_ok_elem(D, n_sys, elem)))
