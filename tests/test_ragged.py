@@ -44,6 +44,8 @@ def solve_on_device(cuda, arrays, off, per, precision=L.FP64, tune=False, inplac
         dD = torch.from_numpy(np.ascontiguousarray(arrays[3])).to(cuda)
         if inplace:
             X = dD
+        else:
+            X.zero_()  # the tuner's solves wrote X: the tuned plan's solve alone counts
     s.solve_ragged(dA, dB, dC, dD, X, off, per)
     torch.cuda.synchronize()
     assert s.status() == 0
