@@ -129,3 +129,27 @@ def test_timing_csv_from_profiled_steps(cuda, tmp_path):
     for t in (1, 2, 3):
         assert vals[(0, t, "solve_z")] >= vals[(0, t, "tdma_z_gpu")] > 0
         assert vals[(0, t, "comm")] == 0.0
+
+
+@pytest.mark.gpu
+def test_step_bit_identical_over_repeats_and_handles(cuda):
+    # the step's sweeps share shared memory between groups and warps run ahead
+    # of one another: a race between them would show as runs that differ.  One
+    # step on the benched sweep lengths (Z 512, Y 384 two sub-segments a
+    # thread, X 256), repeated on one handle's graph and on fresh handles, must
+    # come out bit for bit the same.
+    import torch
+    from filtered_tdma_b200.heat import HeatADI, dt_from_rho
+    ix, iy, iz = 256, 384, 512
+    dt = dt_from_rho(1.0 / 3.0, iz, option="strong")
+    outs = []
+    for handle in range(3):
+        h = HeatADI(ix, iy, iz, dt=dt)
+        for _ in range(2 if handle == 0 else 1):
+            th = h.field(cuda)
+            h.step(th, 1)
+            torch.cuda.synchronize()
+            outs.append(th.clone())
+            del th
+        h.close()
+    assert all(torch.equal(o, outs[0]) for o in outs[1:])

@@ -217,3 +217,30 @@ def test_momentum_argument_checks():
                                          ctypes.byref(h)) == L.ERR_UNSUPPORTED  # 48/16 not 2^k
     assert L.lib().btdma_momentum_sweep(None, 0, 0, None, None, 0.1, None) == L.ERR_ARG
     assert L.lib().btdma_momentum_set_backend(None, 2, 4, 0, 1e-3) == L.ERR_ARG
+
+
+@pytest.mark.gpu
+def test_adi_bit_identical_over_repeats_and_handles(cuda):
+    # z -> y -> x at 256^3 (the benched grid): the sweeps' groups share shared
+    # memory and warps run ahead of one another, so a race between them would
+    # show as runs that differ.  Repeats on one handle and fresh handles must
+    # agree bit for bit, for the staged-store sweeps (x, y) and the field-box
+    # z sweep.
+    import torch
+    from filtered_tdma_b200.momentum import ChannelMomentum
+    c = 0.5 * (1.0 / 180.0) * 1e-3 * 50
+    g = torch.Generator(device=cuda)
+    g.manual_seed(11)
+    first = ChannelMomentum(256, 256, 256, gamma3=1.5)
+    rhs = torch.rand(first.shape, dtype=torch.float64, device=cuda, generator=g)
+    outs = []
+    for handle in range(3):
+        m = first if handle == 0 else ChannelMomentum(256, 256, 256, gamma3=1.5)
+        for _ in range(3 if handle == 0 else 1):
+            q = torch.zeros_like(rhs)
+            m.adi(0, rhs, q, c)
+            torch.cuda.synchronize()
+            assert m.status() == 0
+            outs.append(q)
+        m.close()
+    assert all(torch.equal(o, outs[0]) for o in outs[1:])
