@@ -534,3 +534,31 @@ def test_row_varying_fp32(cuda, orc, precision):
         x, wid = run_f32(cuda, A, B, C, D, prec, cyclic=cyc)
         ref = orc.thomas_cyclic(*wid) if cyc else orc.thomas(*wid)
         assert rel_err(x, ref) <= 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage", ["f64", "f32"])
+def test_tiled_solve_bit_identical_over_repeats(cuda, storage):
+    # the headline kernels (the wide tiled kernel re-reads half of each group
+    # through its TMA ring while warps run ahead of one another): repeated
+    # solves and a fresh handle must agree bit for bit
+    import torch
+    from filtered_tdma_b200 import _lib as L
+    n_sys, n_row = 65536, 512
+    A, B, C, D = W.diag_dominant(n_sys, n_row, 0.1, 10.0, seed=2, device=cuda)
+    if storage == "f32":
+        A, B, C, D = [t.float() for t in (A, B, C, D)]
+    outs = []
+    for handle in range(2):
+        s = Solver("pascal", n_sys, n_row, 8,
+                   precision=L.FP32_STORE if storage == "f32" else L.FP64)
+        for _ in range(3 if handle == 0 else 1):
+            X = torch.empty((n_row, n_sys), dtype=torch.float64, device=cuda)
+            if storage == "f32":
+                s.solve_f32(A, B, C, D, X)
+            else:
+                s.solve_out(A, B, C, D, X)
+            torch.cuda.synchronize()
+            assert s.status() == 0
+            outs.append(X)
+    assert all(torch.equal(o, outs[0]) for o in outs[1:])

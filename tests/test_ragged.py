@@ -241,3 +241,29 @@ def test_ragged_every_launch_shape(cuda, orc, precision):
             torch.cuda.synchronize()
             assert s.status() == 0
             assert per_system_err(X.cpu().numpy(), ref, off) <= 1e-12, (pers, want)
+
+
+@pytest.mark.gpu
+def test_ragged_persistent_plan_bit_identical_over_repeats(cuda, orc):
+    # the persistent launch (groups pulling systems from counters, then warps
+    # pulling short systems) with the in-place shapes of the plan: which CTA
+    # takes which system changes from run to run, the results must not
+    import torch
+    A, B, C, D, off, per = W.ragged_batch(2000, seed=59)
+    dA, dB, dC, dD = [torch.from_numpy(v).to(cuda) for v in (A, B, C, D)]
+    s = Solver("pascal", 2000, 64, 2)
+    X = torch.zeros(int(off[-1]), dtype=torch.float64, device=cuda)
+    s.solve_ragged(dA, dB, dC, dD, X, off, per)
+    plan = [dict(b, persistent=1) for b in s.ragged_plan()]
+    s.ragged_set_plan(plan)
+    assert any(b["persistent"] for b in s.ragged_plan())
+    outs = []
+    for _ in range(4):
+        X = torch.zeros(int(off[-1]), dtype=torch.float64, device=cuda)
+        s.solve_ragged(dA, dB, dC, dD, X, off, per)
+        torch.cuda.synchronize()
+        assert s.status() == 0
+        outs.append(X)
+    assert all(torch.equal(o, outs[0]) for o in outs[1:])
+    ref = ragged_oracle(orc, A, B, C, D, off, per)
+    assert per_system_err(outs[0].cpu().numpy(), ref, off) <= 1e-12
